@@ -1,0 +1,296 @@
+"""ctypes binding of ``libgpum_b200.so`` (the C ABI in ``include/gpum_b200.h``).
+
+The library is built in-tree (``gpumetropolis_b200/build.py``).  There is no
+fallback: if the library is missing or cannot load, every call raises
+:class:`BackendUnavailable`, and a GPU-side failure raises :class:`GpumError`
+with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpum_b200.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE, ERR_DEVICE = range(7)
+MODE_RWM, MODE_DE, MODE_CHOL, MODE_MALA = 0, 1, 2, 3
+RNG_TRIPLE32, RNG_PHILOX = 0, 1
+_ERRLEN = 1024
+
+
+class BackendUnavailable(RuntimeError):
+    """The b200 library is not built or cannot be loaded."""
+
+
+class GpumError(RuntimeError):
+    """A status code other than GPUM_OK from the C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gpum_b200 error {code}: {msg}")
+        self.code = code
+
+
+_u32p = C.POINTER(C.c_uint32)
+_f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
+_sz = C.c_size_t
+_errp = C.c_char_p
+
+# name -> (restype, argtypes); the declarations of include/gpum_b200.h.
+SIGNATURES = {
+    "gpum_b200_available": (C.c_int, []),
+    "gpum_b200_version": (C.c_char_p, []),
+    "gpum_b200_validate_program": (C.c_int, [_u32p, _sz, _sz, C.c_uint32, C.c_uint32, C.c_int,
+                                             C.POINTER(C.c_int), _errp, _sz]),
+    "gpum_b200_run": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz, C.c_uint32,
+                                _f64p, C.c_uint32, C.c_uint64, _f64p, _f64p, _f64p, C.c_uint32,
+                                C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                _f64p, _sz, _f32p, _f32p, _f64p, _errp, _sz]),
+    "gpum_b200_loglik_batch": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p,
+                                         C.c_uint32, C.c_uint64, _f64p, _sz, _f64p, _errp,
+                                         _sz]),
+    "gpum_b200_loglik_pointwise": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p,
+                                             C.c_uint32, C.c_uint64, _f64p, _sz, _f64p, _errp,
+                                             _sz]),
+    "gpum_b200_session_create": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz,
+                                           C.c_uint32, _f64p, C.c_uint32, C.c_uint64,
+                                           C.POINTER(C.c_void_p), _errp, _sz]),
+    "gpum_b200_session_run": (C.c_int, [C.c_void_p, _f64p, _f64p, _f64p, C.c_uint32,
+                                        C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                        C.c_double, _f64p, _sz, C.c_int, _f32p, _f32p, _f64p,
+                                        _errp, _sz]),
+    "gpum_b200_session_loglik_batch": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
+    "gpum_b200_session_loglik_pointwise": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp,
+                                                     _sz]),
+    "gpum_b200_session_prepare": (C.c_int, [C.c_void_p, _f64p, _f64p, _f64p, C.c_uint32,
+                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                            C.c_double, _f64p, _sz, C.c_int, _errp, _sz]),
+    "gpum_b200_session_advance": (C.c_int, [C.c_void_p, C.c_uint32, _errp, _sz]),
+    "gpum_b200_session_sync": (C.c_int, [C.c_void_p, _errp, _sz]),
+    "gpum_b200_session_fetch": (C.c_int, [C.c_void_p, _f32p, _f32p, _f64p,
+                                          C.POINTER(C.c_uint32), _errp, _sz]),
+    "gpum_b200_session_launches": (C.c_uint64, [C.c_void_p]),
+    "gpum_b200_session_destroy": (None, [C.c_void_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (once) and bind every declared symbol."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(path):
+                raise BackendUnavailable(
+                    f"{path} is not built; run `python -m gpumetropolis_b200.build`")
+            try:
+                lib = C.CDLL(path)
+            except OSError as e:
+                raise BackendUnavailable(f"cannot load {path}: {e}") from e
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(lib, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def available() -> bool:
+    try:
+        return bool(load().gpum_b200_available())
+    except BackendUnavailable:
+        return False
+
+
+def _p(a, ctype):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _u32(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.int64).astype(np.uint32)).reshape(-1)
+    return a
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+
+
+def _check(rc: int, err) -> None:
+    if rc != OK:
+        raise GpumError(rc, err.value.decode(errors="replace"))
+
+
+def validate_program(code, n_consts, n_params, n_cols, allow_data=True) -> int:
+    code = _u32(code)
+    err = C.create_string_buffer(_ERRLEN)
+    depth = C.c_int(0)
+    _check(load().gpum_b200_validate_program(_p(code, C.c_uint32), code.size, n_consts,
+                                             n_params, n_cols, int(allow_data),
+                                             C.byref(depth), err, _ERRLEN), err)
+    return depth.value
+
+
+def run(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
+        proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0, de_noise=0.0,
+        proposal_l=None):
+    """One-shot sampler (``gpum_b200_run``); host arrays in, host arrays out."""
+    code, pcode = _u32(code), _u32(prior_code)
+    consts, pconsts = _f64(consts), _f64(prior_consts)
+    data, init = _f64(data), _f64(init)
+    sd, temps = _f64(proposal_sd), _f64(temperatures)
+    n_chains = init.size // n_params
+    L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
+    draws = np.empty(n_iter * n_chains * n_params, np.float32)
+    acc = np.empty(n_chains, np.float32)
+    last = np.empty(n_chains, np.float64)
+    err = C.create_string_buffer(_ERRLEN)
+    rc = load().gpum_b200_run(
+        _p(code, C.c_uint32), code.size, _p(consts, C.c_double), consts.size,
+        _p(pcode, C.c_uint32), pcode.size, _p(pconsts, C.c_double), pconsts.size, n_params,
+        _p(data, C.c_double), n_cols, n_obs, _p(init, C.c_double), _p(sd, C.c_double),
+        _p(temps, C.c_double), n_chains, n_iter, seed & 0xFFFFFFFF, proposal_mode, gamma,
+        de_noise, _p(L, C.c_double), 0 if L is None else L.size, _p(draws, C.c_float),
+        _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
+    _check(rc, err)
+    return draws, acc, last
+
+
+def _batch(fname, code, consts, n_params, data, n_cols, n_obs, points, width):
+    code, consts, data, pts = _u32(code), _f64(consts), _f64(data), _f64(points)
+    n_points = pts.size // n_params
+    out = np.empty(max(n_points * width, 1), np.float64)
+    err = C.create_string_buffer(_ERRLEN)
+    rc = getattr(load(), fname)(_p(code, C.c_uint32), code.size, _p(consts, C.c_double),
+                                consts.size, n_params, _p(data, C.c_double), n_cols, n_obs,
+                                _p(pts, C.c_double), n_points, _p(out, C.c_double), err,
+                                _ERRLEN)
+    _check(rc, err)
+    return out[: n_points * width]
+
+
+def loglik_batch(code, consts, n_params, data, n_cols, n_obs, points):
+    return _batch("gpum_b200_loglik_batch", code, consts, n_params, data, n_cols, n_obs,
+                  points, 1)
+
+
+def loglik_pointwise(code, consts, n_params, data, n_cols, n_obs, points):
+    return _batch("gpum_b200_loglik_pointwise", code, consts, n_params, data, n_cols, n_obs,
+                  points, n_obs)
+
+
+class Session:
+    """A model + data resident on the GPU (``gpum_b200_session_*``)."""
+
+    def __init__(self, code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs):
+        self._lib = load()
+        code, pcode = _u32(code), _u32(prior_code)
+        consts, pconsts = _f64(consts), _f64(prior_consts)
+        data = _f64(data)
+        self.n_params, self.n_cols, self.n_obs = n_params, n_cols, n_obs
+        h = C.c_void_p()
+        err = C.create_string_buffer(_ERRLEN)
+        rc = self._lib.gpum_b200_session_create(
+            _p(code, C.c_uint32), code.size, _p(consts, C.c_double), consts.size,
+            _p(pcode, C.c_uint32), pcode.size, _p(pconsts, C.c_double), pconsts.size,
+            n_params, _p(data, C.c_double), n_cols, n_obs, C.byref(h), err, _ERRLEN)
+        _check(rc, err)
+        self._h = h
+        self.n_chains = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gpum_b200_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def launches(self) -> int:
+        return int(self._lib.gpum_b200_session_launches(self._h))
+
+    def run(self, init, proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0,
+            de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
+        init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
+        n_chains = init.size // self.n_params
+        L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
+        draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
+        acc = np.empty(n_chains, np.float32)
+        last = np.empty(n_chains, np.float64)
+        err = C.create_string_buffer(_ERRLEN)
+        rc = self._lib.gpum_b200_session_run(
+            self._h, _p(init, C.c_double), _p(sd, C.c_double), _p(temps, C.c_double), n_chains,
+            n_iter, seed & 0xFFFFFFFF, proposal_mode, gamma, de_noise, _p(L, C.c_double),
+            0 if L is None else L.size, rng, _p(draws, C.c_float), _p(acc, C.c_float),
+            _p(last, C.c_double), err, _ERRLEN)
+        _check(rc, err)
+        return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def prepare(self, init, proposal_sd, temperatures, max_iter, seed, proposal_mode,
+                gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
+        init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
+        self.n_chains = init.size // self.n_params
+        L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
+        err = C.create_string_buffer(_ERRLEN)
+        rc = self._lib.gpum_b200_session_prepare(
+            self._h, _p(init, C.c_double), _p(sd, C.c_double), _p(temps, C.c_double),
+            self.n_chains, max_iter, seed & 0xFFFFFFFF, proposal_mode, gamma, de_noise,
+            _p(L, C.c_double), 0 if L is None else L.size, rng, err, _ERRLEN)
+        _check(rc, err)
+
+    def advance(self, n_iter):
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_advance(self._h, n_iter, err, _ERRLEN), err)
+
+    def sync(self):
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_sync(self._h, err, _ERRLEN), err)
+
+    def fetch(self, want_draws=True):
+        n = C.c_uint32(0)
+        err = C.create_string_buffer(_ERRLEN)
+        # First call learns n_done without copying draws.
+        _check(self._lib.gpum_b200_session_fetch(self._h, None, None, None, C.byref(n), err,
+                                                 _ERRLEN), err)
+        nd = n.value
+        draws = np.empty(max(nd * self.n_chains * self.n_params, 1), np.float32)
+        acc = np.empty(self.n_chains, np.float32)
+        last = np.empty(self.n_chains, np.float64)
+        _check(self._lib.gpum_b200_session_fetch(
+            self._h, _p(draws, C.c_float) if want_draws else None, _p(acc, C.c_float),
+            _p(last, C.c_double), C.byref(n), err, _ERRLEN), err)
+        return draws[: nd * self.n_chains * self.n_params], acc, last, nd
+
+    def loglik_batch(self, points):
+        pts = _f64(points)
+        n = pts.size // self.n_params
+        out = np.empty(max(n, 1))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_loglik_batch(self._h, _p(pts, C.c_double), n,
+                                                        _p(out, C.c_double), err, _ERRLEN), err)
+        return out[:n]
+
+    def loglik_pointwise(self, points):
+        pts = _f64(points)
+        n = pts.size // self.n_params
+        out = np.empty(max(n * self.n_obs, 1))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_loglik_pointwise(self._h, _p(pts, C.c_double), n,
+                                                            _p(out, C.c_double), err, _ERRLEN),
+               err)
+        return out[: n * self.n_obs]

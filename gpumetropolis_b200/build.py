@@ -1,0 +1,60 @@
+"""Build the B200 backend's shared library in-tree with nvcc (sm_100a).
+
+``python -m gpumetropolis_b200.build`` writes ``gpumetropolis_b200/libgpum_b200.so``.
+The library is the C ABI declared in ``include/gpum_b200.h``; Python loads it
+with ctypes (``gpumetropolis_b200._native``).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libgpum_b200.so")
+SOURCES = ["capi.cu", "program.cpp"]
+HEADERS = ["device.cuh", "interp.cuh", "kernels.cuh", "program.hpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else "nvcc"
+
+
+def host_compiler() -> list:
+    # nvcc picks `gcc` from PATH; pin the system one when present.
+    return ["-ccbin", "/usr/bin/g++"] if os.path.exists("/usr/bin/g++") else []
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "gpum_b200.h"))
+    deps.append(os.path.abspath(__file__))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    tmp = LIB + f".{os.getpid()}.tmp"
+    cmd = [nvcc(), *host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
+           "--shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+           "-I", os.path.join(ROOT, "include"), "-o", tmp]
+    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    cmd += ["-lcudart"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

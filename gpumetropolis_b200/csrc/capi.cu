@@ -1,0 +1,718 @@
+// capi.cu -- host side of the B200 backend: sessions (model + data resident
+// in HBM), launch geometry, CUDA-graph replay of the iteration loop, and the
+// extern "C" entry points declared in include/gpum_b200.h.
+//
+// Replaces the reference's per-call CubeCL client + upload + launch +
+// readback (src/rust/src/chain_kernel.rs:372-463) and its backend dispatch
+// (chain_kernel.rs:469-532).  No entry point throws across the ABI: every
+// failure becomes a status code and a message.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gpum_b200.h"
+#include "kernels.cuh"
+#include "program.hpp"
+
+using namespace gpum;
+
+namespace {
+
+struct Failure {
+  int code;
+  std::string msg;
+};
+
+void set_err(char* err, size_t len, const std::string& m) {
+  if (err && len) {
+    const size_t n = std::min(len - 1, m.size());
+    std::memcpy(err, m.data(), n);
+    err[n] = '\0';
+  }
+}
+
+#define GPUM_CK(call)                                                                 \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      throw Failure{e_ == cudaErrorMemoryAllocation ? GPUM_ERR_NOMEM : GPUM_ERR_CUDA, \
+                    std::string(#call) + ": " + cudaGetErrorString(e_)};             \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void ensure(size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) count = 1;
+    GPUM_CK(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+};
+
+using EncodeTiledFn = PFN_cuTensorMapEncodeTiled_v12000;
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      throw Failure{GPUM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable"};
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// Interpreter variants by peak stack depth: registers are spent on depth or
+// on chains per thread.
+enum Variant { V8x8 = 0, V4x16 = 1, V2x32 = 2 };
+int variant_G(int v) { return v == V8x8 ? 8 : (v == V4x16 ? 4 : 2); }
+
+const void* kernel_ptr(int v) {
+  switch (v) {
+    case V8x8: return (const void*)iter_kernel<8, 8>;
+    case V4x16: return (const void*)iter_kernel<4, 16>;
+    default: return (const void*)iter_kernel<2, 32>;
+  }
+}
+
+void launch_iter(int v, dim3 grid, size_t smem, cudaStream_t st, const EvalProg& prog,
+                 const CUtensorMap& tmap, const EvalArgs& E, const ChainArgs& A, int phase) {
+  switch (v) {
+    case V8x8: iter_kernel<8, 8><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    case V4x16: iter_kernel<4, 16><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    default: iter_kernel<2, 32><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+  }
+  GPUM_CK(cudaGetLastError());
+}
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+struct Geometry {
+  int G, WC, CG, NCB, C_pad, NOB, tiles_per_cta, ntiles;
+  size_t smem;
+};
+
+}  // namespace
+
+struct gpum_b200_session {
+  cudaStream_t stream = nullptr;
+  UProg ll;
+  std::unique_ptr<EvalProg> prog;
+  std::vector<uint32_t> prior_code;
+  std::vector<double> prior_consts;
+  uint32_t np = 0, ncols = 0;
+  uint64_t n_obs = 0;
+  int variant = V8x8;
+  int T = 256;
+  int64_t ld = 0;
+  DBuf<float> data;
+  CUtensorMap tmap;
+  DBuf<uint32_t> d_prior_code;
+  DBuf<double> d_prior_consts;
+  DBuf<uint32_t> d_err;
+  // run state
+  Geometry geo{};
+  int n_chains = 0;
+  uint32_t max_iter = 0, n_done = 0;
+  bool prepared = false;
+  DBuf<double> state, prop, cur, last_eval, sd, temp, L, snap, zbuf, partials, pointwise,
+      points, out64;
+  DBuf<float> params, draws, draws_out;
+  DBuf<uint32_t> ctr, accepts, iter, tickets;
+  EvalArgs E{};
+  ChainArgs A{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_len = 0;
+  uint64_t launches = 0;
+
+  ~gpum_b200_session() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  Geometry geometry(int n) const {
+    Geometry g{};
+    g.G = variant_G(variant);
+    const int groups = (n + g.G - 1) / g.G;
+    g.WC = 1;
+    while (g.WC < kWarps && g.WC < groups) g.WC *= 2;
+    g.CG = g.WC * g.G;
+    g.NCB = (n + g.CG - 1) / g.CG;
+    g.C_pad = g.NCB * g.CG;
+    g.ntiles = (int)((n_obs + T - 1) / T);
+    const size_t stage = (size_t)T * ncols * sizeof(float);
+    const size_t pbytes = (((size_t)np * g.CG + 3) & ~(size_t)3) * sizeof(float);
+    g.smem = 2 * stage + pbytes + (size_t)kWarps * g.G * sizeof(double) + 2 * 8 + 16;
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_ptr(variant), kThreads, g.smem);
+    if (occ < 1) occ = 1;
+    const int slots = num_sms() * occ;
+    int nob = std::max(1, (4 * slots) / g.NCB);
+    nob = std::min(nob, std::max(1, g.ntiles));
+    g.tiles_per_cta = g.ntiles > 0 ? (g.ntiles + nob - 1) / nob : 0;
+    g.NOB = g.ntiles > 0 ? (g.ntiles + g.tiles_per_cta - 1) / g.tiles_per_cta : 1;
+    return g;
+  }
+
+  void check_device_error() {
+    uint32_t e = 0;
+    GPUM_CK(cudaMemcpyAsync(&e, d_err.p, sizeof e, cudaMemcpyDeviceToHost, stream));
+    GPUM_CK(cudaStreamSynchronize(stream));
+    if (e) {
+      GPUM_CK(cudaMemsetAsync(d_err.p, 0, sizeof(uint32_t), stream));
+      throw Failure{GPUM_ERR_DEVICE, "a kernel reported a device-side failure (code " +
+                                         std::to_string(e) + ")"};
+    }
+  }
+
+  // Evaluation-argument block for `n` points whose f32 params live in `params`.
+  void setup_eval(int n) {
+    geo = geometry(n);
+    const size_t smax = geo.smem;
+    if (smax > 48 * 1024)
+      GPUM_CK(cudaFuncSetAttribute(kernel_ptr(variant),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+    params.ensure((size_t)np * geo.C_pad);
+    partials.ensure((size_t)geo.NOB * geo.C_pad);
+    tickets.ensure(geo.NCB);
+    GPUM_CK(cudaMemsetAsync(tickets.p, 0, sizeof(uint32_t) * geo.NCB, stream));
+    E = EvalArgs{};
+    E.n_obs = (int)n_obs;
+    E.ncols = (int)ncols;
+    E.T = T;
+    E.ntiles = geo.ntiles;
+    E.tiles_per_cta = geo.tiles_per_cta;
+    E.CG = geo.CG;
+    E.WC = geo.WC;
+    E.C_pad = geo.C_pad;
+    E.np = (int)np;
+    E.params = params.p;
+    E.partials = partials.p;
+    E.n_points = n;
+    E.tickets = tickets.p;
+    E.err = d_err.p;
+  }
+
+  void upload_points(const double* pts, int n) {
+    points.ensure((size_t)n * np);
+    GPUM_CK(cudaMemcpyAsync(points.p, pts, sizeof(double) * n * np, cudaMemcpyHostToDevice,
+                            stream));
+    const int total = (int)(np * geo.C_pad);
+    points_to_params_kernel<<<(total + 255) / 256, 256, 0, stream>>>(points.p, params.p, n,
+                                                                     (int)np, geo.C_pad);
+    GPUM_CK(cudaGetLastError());
+    ++launches;
+  }
+
+  void launch(int phase) {
+    launch_iter(variant, dim3(geo.NOB, geo.NCB), geo.smem, stream, *prog, tmap, E, A, phase);
+    ++launches;
+  }
+};
+
+namespace {
+
+// Runs `body`, converting every failure into a status code and message.
+int guard(char* err, size_t len, const std::function<void()>& body) {
+  try {
+    body();
+    set_err(err, len, "");
+    return GPUM_OK;
+  } catch (const Failure& f) {
+    set_err(err, len, f.msg);
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    set_err(err, len, "host allocation failed");
+    return GPUM_ERR_NOMEM;
+  } catch (...) {
+    set_err(err, len, "unexpected internal error");
+    return GPUM_ERR_CUDA;
+  }
+}
+
+void require(bool ok, const std::string& m, int code = GPUM_ERR_INVALID) {
+  if (!ok) throw Failure{code, m};
+}
+
+void require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
+    throw Failure{GPUM_ERR_NODEVICE, "no CUDA device is visible"};
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10)
+    throw Failure{GPUM_ERR_NODEVICE,
+                  "the b200 backend needs an sm_100 (B200) GPU; found compute capability " +
+                      std::to_string(major) + ".x"};
+}
+
+gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const double* consts,
+                                  size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                                  const double* prior_consts, size_t n_prior_consts,
+                                  uint32_t n_params, const double* data, uint32_t n_cols,
+                                  uint64_t n_obs) {
+  require(n_params >= 1, "n_params must be at least 1");
+  require(n_params <= 256, "more than 256 parameters", GPUM_ERR_UNSUPPORTED);
+  require(n_cols <= 256, "more than 256 data columns", GPUM_ERR_UNSUPPORTED);
+  require(n_obs < (1ull << 31) - 1024, "more than 2^31 observations", GPUM_ERR_UNSUPPORTED);
+  require(n_obs == 0 || n_cols == 0 || data != nullptr, "data pointer is NULL");
+  std::unique_ptr<gpum_b200_session> s(new gpum_b200_session());
+  std::string msg;
+  if (compile_program(code, n_code, consts, n_consts, n_params, n_cols, true, &s->ll, &msg))
+    throw Failure{GPUM_ERR_INVALID, "log-likelihood bytecode: " + msg};
+  int pdepth = 0;
+  if (validate_program(prior_code, n_prior, n_prior_consts, n_params, 0, false, &pdepth, &msg))
+    throw Failure{GPUM_ERR_INVALID, "prior bytecode: " + msg};
+  require(n_prior_consts == 0 || prior_consts != nullptr, "prior constant pointer is NULL");
+  require_device();
+
+  s->np = n_params;
+  s->ncols = n_cols;
+  s->n_obs = n_obs;
+  s->variant = s->ll.depth <= 8 ? V8x8 : (s->ll.depth <= 16 ? V4x16 : V2x32);
+  s->prog.reset(new EvalProg());
+  std::memset(s->prog.get(), 0, sizeof(EvalProg));
+  s->prog->n_uops = (uint32_t)s->ll.uops.size();
+  std::copy(s->ll.uops.begin(), s->ll.uops.end(), s->prog->uop);
+  std::copy(s->ll.consts.begin(), s->ll.consts.end(), s->prog->cst);
+  s->prior_code.assign(prior_code, prior_code + n_prior);
+  s->prior_consts.assign(prior_consts, prior_consts + n_prior_consts);
+
+  GPUM_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  s->d_err.ensure(1);
+  GPUM_CK(cudaMemsetAsync(s->d_err.p, 0, sizeof(uint32_t), s->stream));
+  s->d_prior_code.ensure(std::max<size_t>(n_prior, 2));
+  s->d_prior_consts.ensure(std::max<size_t>(n_prior_consts, 1));
+  if (n_prior)
+    GPUM_CK(cudaMemcpyAsync(s->d_prior_code.p, prior_code, n_prior * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s->stream));
+  if (n_prior_consts)
+    GPUM_CK(cudaMemcpyAsync(s->d_prior_consts.p, prior_consts, n_prior_consts * sizeof(double),
+                            cudaMemcpyHostToDevice, s->stream));
+
+  // Observations per tile: a multiple of 32 (one per lane), <= 256 (TMA box
+  // limit), with a stage of at most 32 KB.
+  if (n_cols > 0) {
+    int T = (int)((8192 / n_cols) / 32 * 32);
+    s->T = std::max(32, std::min(256, T));
+  } else {
+    s->T = 256;
+  }
+  std::memset(&s->tmap, 0, sizeof s->tmap);
+  if (n_cols > 0 && n_obs > 0) {
+    // Column-major f32 in HBM: each column contiguous, leading dimension
+    // padded to 4 floats so every TMA row stride is a multiple of 16 bytes.
+    s->ld = (int64_t)((n_obs + 3) & ~3ull);
+    s->data.ensure((size_t)s->ld * n_cols);
+    const int64_t rows_per_chunk = std::max<int64_t>(1, (int64_t)(32u << 20) / n_cols);
+    DBuf<double> stage;
+    stage.ensure((size_t)std::min<int64_t>(rows_per_chunk, (int64_t)n_obs) * n_cols);
+    for (int64_t r0 = 0; r0 < (int64_t)n_obs; r0 += rows_per_chunk) {
+      const int64_t nr = std::min<int64_t>(rows_per_chunk, (int64_t)n_obs - r0);
+      GPUM_CK(cudaMemcpyAsync(stage.p, data + r0 * n_cols, sizeof(double) * nr * n_cols,
+                              cudaMemcpyHostToDevice, s->stream));
+      const int64_t tot = nr * n_cols;
+      convert_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s->stream>>>(
+          stage.p, s->data.p, (int)n_cols, s->ld, r0, nr);
+      GPUM_CK(cudaGetLastError());
+    }
+    GPUM_CK(cudaStreamSynchronize(s->stream));
+    cuuint64_t gdim[2] = {(cuuint64_t)n_obs, (cuuint64_t)n_cols};
+    cuuint64_t gstride[1] = {(cuuint64_t)s->ld * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)s->T, (cuuint32_t)n_cols};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&s->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->data.p, gdim,
+                             gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      throw Failure{GPUM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")"};
+  }
+  return s.release();
+}
+
+void prepare(gpum_b200_session* s, const double* init, const double* sd, const double* temps,
+             uint32_t C, uint32_t max_iter, uint32_t seed, uint32_t mode, double gamma,
+             double de_noise, const double* L, size_t n_l, int rng) {
+  require(s != nullptr, "session is NULL");
+  require(C >= 1, "n_chains must be at least 1");
+  require(init && sd && temps, "init, proposal_sd and temperatures must be non-NULL");
+  require(mode <= 3, "proposal_mode must be 0 (rwm), 1 (de), 2 (cholesky) or 3 (mala)");
+  require(mode != 3, "proposal_mode 3 (MALA) is not implemented by this backend build",
+          GPUM_ERR_UNSUPPORTED);
+  require(rng == GPUM_RNG_TRIPLE32 || rng == GPUM_RNG_PHILOX, "rng must be 0 or 1");
+  const size_t np = s->np;
+  if (mode == 2)
+    require(L != nullptr && n_l == (size_t)C * np * np,
+            "proposal_mode 2 needs proposal_l of n_chains*n_params^2 values");
+  require(C <= (1u << 24), "more than 2^24 chains", GPUM_ERR_UNSUPPORTED);
+  require((uint64_t)max_iter * np * C <= (1ull << 33), "draw storage above 32 GiB",
+          GPUM_ERR_UNSUPPORTED);
+
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+  if (s->graph) {
+    cudaGraphDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  s->n_chains = (int)C;
+  s->setup_eval((int)C);
+  const Geometry& g = s->geo;
+  s->state.ensure(C * np);
+  s->prop.ensure(C * np);
+  s->snap.ensure(C * np);
+  s->sd.ensure(C * np);
+  s->zbuf.ensure(C * np);
+  s->temp.ensure(C);
+  s->cur.ensure(C);
+  s->last_eval.ensure(C);
+  s->ctr.ensure(C);
+  s->accepts.ensure(C);
+  s->iter.ensure(g.NCB);
+  s->draws.ensure(std::max<size_t>(1, (size_t)max_iter * np * g.C_pad));
+  if (mode == 2) s->L.ensure((size_t)C * np * np);
+  cudaStream_t st = s->stream;
+  GPUM_CK(cudaMemcpyAsync(s->state.p, init, sizeof(double) * C * np, cudaMemcpyHostToDevice, st));
+  GPUM_CK(cudaMemcpyAsync(s->snap.p, s->state.p, sizeof(double) * C * np,
+                          cudaMemcpyDeviceToDevice, st));
+  GPUM_CK(cudaMemcpyAsync(s->sd.p, sd, sizeof(double) * C * np, cudaMemcpyHostToDevice, st));
+  GPUM_CK(cudaMemcpyAsync(s->temp.p, temps, sizeof(double) * C, cudaMemcpyHostToDevice, st));
+  if (mode == 2)
+    GPUM_CK(cudaMemcpyAsync(s->L.p, L, sizeof(double) * C * np * np, cudaMemcpyHostToDevice, st));
+  GPUM_CK(cudaMemsetAsync(s->ctr.p, 0, sizeof(uint32_t) * C, st));
+  GPUM_CK(cudaMemsetAsync(s->accepts.p, 0, sizeof(uint32_t) * C, st));
+  GPUM_CK(cudaMemsetAsync(s->iter.p, 0, sizeof(uint32_t) * g.NCB, st));
+  const int total = (int)(np * g.C_pad);
+  points_to_params_kernel<<<(total + 255) / 256, 256, 0, st>>>(s->state.p, s->params.p, (int)C,
+                                                               (int)np, g.C_pad);
+  GPUM_CK(cudaGetLastError());
+  ++s->launches;
+
+  ChainArgs& A = s->A;
+  A = ChainArgs{};
+  A.n_chains = (int)C;
+  A.np = (int)np;
+  A.state = s->state.p;
+  A.prop = s->prop.p;
+  A.cur = s->cur.p;
+  A.last_eval = s->last_eval.p;
+  A.ctr = s->ctr.p;
+  A.accepts = s->accepts.p;
+  A.iter = s->iter.p;
+  A.sd = s->sd.p;
+  A.temp = s->temp.p;
+  A.L = mode == 2 ? s->L.p : nullptr;
+  A.snap = s->snap.p;
+  A.draws = s->draws.p;
+  A.n_iter = max_iter;
+  A.seed = seed;
+  A.mode = (int)(mode == 0 || mode == 2 ? mode : 1);
+  A.rng = rng;
+  A.gamma = gamma;
+  A.de_noise = de_noise;
+  A.prior_code = s->d_prior_code.p;
+  A.prior_consts = s->d_prior_consts.p;
+  A.n_prior = (int)(s->prior_code.size() / 2);
+  A.zbuf = s->zbuf.p;
+  s->launch(PH_INIT);
+  s->max_iter = max_iter;
+  s->n_done = 0;
+  s->prepared = true;
+}
+
+void advance(gpum_b200_session* s, uint32_t n) {
+  require(s && s->prepared, "session has no prepared run");
+  require((uint64_t)s->n_done + n <= s->max_iter, "advance beyond the prepared max_iter");
+  if (n == 0) return;
+  constexpr int kGraphLen = 32;
+  if (n >= (uint32_t)kGraphLen && !s->gexec) {
+    GPUM_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      for (int i = 0; i < kGraphLen; ++i)
+        launch_iter(s->variant, dim3(s->geo.NOB, s->geo.NCB), s->geo.smem, s->stream, *s->prog,
+                    s->tmap, s->E, s->A, PH_STEP);
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(s->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    GPUM_CK(cudaStreamEndCapture(s->stream, &s->graph));
+    GPUM_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
+    s->graph_len = kGraphLen;
+  }
+  uint32_t left = n;
+  while (s->gexec && left >= (uint32_t)s->graph_len) {
+    GPUM_CK(cudaGraphLaunch(s->gexec, s->stream));
+    s->launches += s->graph_len;
+    left -= s->graph_len;
+  }
+  for (; left > 0; --left) s->launch(PH_STEP);
+  s->n_done += n;
+}
+
+void fetch(gpum_b200_session* s, float* out_draws, float* out_accept, double* out_last,
+           uint32_t* n_done) {
+  require(s && s->prepared, "session has no prepared run");
+  s->check_device_error();
+  const uint32_t n = s->n_done;
+  const int C = s->n_chains;
+  const size_t np = s->np;
+  if (n_done) *n_done = n;
+  cudaStream_t st = s->stream;
+  if (out_draws && n > 0) {
+    s->draws_out.ensure((size_t)n * C * np);
+    dim3 grid((C + 31) / 32, (n + 31) / 32, (unsigned)np);
+    draws_layout_kernel<<<grid, dim3(32, 8), 0, st>>>(s->draws.p, s->draws_out.p, (int)n,
+                                                      (int)np, C, s->geo.C_pad);
+    GPUM_CK(cudaGetLastError());
+    ++s->launches;
+    GPUM_CK(cudaMemcpyAsync(out_draws, s->draws_out.p, sizeof(float) * n * C * np,
+                            cudaMemcpyDeviceToHost, st));
+  }
+  std::vector<uint32_t> acc(C);
+  GPUM_CK(cudaMemcpyAsync(acc.data(), s->accepts.p, sizeof(uint32_t) * C,
+                          cudaMemcpyDeviceToHost, st));
+  if (out_last)
+    GPUM_CK(cudaMemcpyAsync(out_last, s->cur.p, sizeof(double) * C, cudaMemcpyDeviceToHost, st));
+  GPUM_CK(cudaStreamSynchronize(st));
+  if (out_accept)
+    for (int c = 0; c < C; ++c) out_accept[c] = n == 0 ? 0.0f : (float)acc[c] / (float)n;
+}
+
+void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out, bool pointwise) {
+  require(s != nullptr, "session is NULL");
+  require(out != nullptr || n_points == 0, "output pointer is NULL");
+  require(pts != nullptr || n_points == 0, "points pointer is NULL");
+  if (n_points == 0) return;
+  require(n_points <= (1u << 24), "more than 2^24 points", GPUM_ERR_UNSUPPORTED);
+  s->prepared = false;  // the eval buffers are reused
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+  if (s->graph) {
+    cudaGraphDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  size_t chunk = n_points;
+  if (pointwise && s->n_obs > 0)
+    chunk = std::max<size_t>(1, std::min<size_t>(n_points, (size_t)(1ull << 27) / s->n_obs));
+  for (size_t p0 = 0; p0 < n_points; p0 += chunk) {
+    const int n = (int)std::min(chunk, n_points - p0);
+    s->setup_eval(n);
+    s->upload_points(pts + p0 * s->np, n);
+    s->A = ChainArgs{};
+    if (pointwise) {
+      if (s->n_obs == 0) continue;
+      s->pointwise.ensure((size_t)n * s->n_obs);
+      s->E.pointwise = s->pointwise.p;
+      if (s->ll.empty()) {
+        GPUM_CK(cudaMemsetAsync(s->pointwise.p, 0, sizeof(double) * n * s->n_obs, s->stream));
+      } else {
+        s->launch(PH_POINTWISE);
+      }
+      GPUM_CK(cudaMemcpyAsync(out + p0 * s->n_obs, s->pointwise.p,
+                              sizeof(double) * n * s->n_obs, cudaMemcpyDeviceToHost, s->stream));
+    } else {
+      s->out64.ensure(n);
+      if (s->ll.empty()) {
+        GPUM_CK(cudaMemsetAsync(s->out64.p, 0, sizeof(double) * n, s->stream));
+      } else {
+        s->launch(PH_EVAL);
+        reduce_partials_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->partials.p,
+                                                                        s->out64.p, s->geo.NOB,
+                                                                        s->geo.C_pad, n);
+        GPUM_CK(cudaGetLastError());
+        ++s->launches;
+      }
+      GPUM_CK(cudaMemcpyAsync(out + p0, s->out64.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                              s->stream));
+    }
+    s->check_device_error();
+  }
+  if (pointwise && s->n_obs == 0) return;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+int gpum_b200_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) return 0;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kernel_ptr(V8x8)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return 1;
+}
+
+const char* gpum_b200_version(void) { return "gpum_b200 0.1.0 sm_100a"; }
+
+int gpum_b200_validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
+                               uint32_t n_params, uint32_t n_cols, int allow_data, int* depth,
+                               char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    int d = 0;
+    std::string m;
+    if (validate_program(code, n_code, n_consts, n_params, n_cols, allow_data != 0, &d, &m))
+      throw Failure{GPUM_ERR_INVALID, m};
+    if (depth) *depth = d;
+  });
+}
+
+int gpum_b200_session_create(const uint32_t* code, size_t n_code, const double* consts,
+                             size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                             const double* prior_consts, size_t n_prior_consts,
+                             uint32_t n_params, const double* data, uint32_t n_cols,
+                             uint64_t n_obs, gpum_b200_session** out, char* err,
+                             size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(out != nullptr, "output session pointer is NULL");
+    *out = nullptr;
+    *out = create_session(code, n_code, consts, n_consts, prior_code, n_prior, prior_consts,
+                          n_prior_consts, n_params, data, n_cols, n_obs);
+  });
+}
+
+void gpum_b200_session_destroy(gpum_b200_session* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  delete s;
+}
+
+uint64_t gpum_b200_session_launches(const gpum_b200_session* s) { return s ? s->launches : 0; }
+
+int gpum_b200_session_prepare(gpum_b200_session* s, const double* init, const double* sd,
+                              const double* temps, uint32_t n_chains, uint32_t max_iter,
+                              uint32_t seed, uint32_t mode, double gamma, double de_noise,
+                              const double* L, size_t n_l, int rng, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    prepare(s, init, sd, temps, n_chains, max_iter, seed, mode, gamma, de_noise, L, n_l, rng);
+  });
+}
+
+int gpum_b200_session_advance(gpum_b200_session* s, uint32_t n, char* err, size_t err_len) {
+  return guard(err, err_len, [&] { advance(s, n); });
+}
+
+int gpum_b200_session_sync(gpum_b200_session* s, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    GPUM_CK(cudaStreamSynchronize(s->stream));
+  });
+}
+
+int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, float* out_accept,
+                            double* out_last, uint32_t* n_done, char* err, size_t err_len) {
+  return guard(err, err_len, [&] { fetch(s, out_draws, out_accept, out_last, n_done); });
+}
+
+int gpum_b200_session_run(gpum_b200_session* s, const double* init, const double* sd,
+                          const double* temps, uint32_t n_chains, uint32_t n_iter, uint32_t seed,
+                          uint32_t mode, double gamma, double de_noise, const double* L,
+                          size_t n_l, int rng, float* out_draws, float* out_accept,
+                          double* out_last, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    prepare(s, init, sd, temps, n_chains, n_iter, seed, mode, gamma, de_noise, L, n_l, rng);
+    advance(s, n_iter);
+    fetch(s, out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_session_loglik_batch(gpum_b200_session* s, const double* points, size_t n_points,
+                                   double* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] { batch(s, points, n_points, out, false); });
+}
+
+int gpum_b200_session_loglik_pointwise(gpum_b200_session* s, const double* points,
+                                       size_t n_points, double* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] { batch(s, points, n_points, out, true); });
+}
+
+int gpum_b200_run(const uint32_t* code, size_t n_code, const double* consts, size_t n_consts,
+                  const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
+                  size_t n_prior_consts, uint32_t n_params, const double* data, uint32_t n_cols,
+                  uint64_t n_obs, const double* init, const double* sd, const double* temps,
+                  uint32_t n_chains, uint32_t n_iter, uint32_t seed, uint32_t mode, double gamma,
+                  double de_noise, const double* L, size_t n_l, float* out_draws,
+                  float* out_accept, double* out_last, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    std::unique_ptr<gpum_b200_session> s(create_session(code, n_code, consts, n_consts,
+                                                        prior_code, n_prior, prior_consts,
+                                                        n_prior_consts, n_params, data, n_cols,
+                                                        n_obs));
+    prepare(s.get(), init, sd, temps, n_chains, n_iter, seed, mode, gamma, de_noise, L, n_l,
+            GPUM_RNG_TRIPLE32);
+    advance(s.get(), n_iter);
+    fetch(s.get(), out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_loglik_batch(const uint32_t* code, size_t n_code, const double* consts,
+                           size_t n_consts, uint32_t n_params, const double* data, uint32_t n_cols,
+                           uint64_t n_obs, const double* points, size_t n_points, double* out,
+                           char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    std::unique_ptr<gpum_b200_session> s(create_session(
+        code, n_code, consts, n_consts, nullptr, 0, nullptr, 0, n_params, data, n_cols, n_obs));
+    batch(s.get(), points, n_points, out, false);
+  });
+}
+
+int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, const double* consts,
+                               size_t n_consts, uint32_t n_params, const double* data,
+                               uint32_t n_cols, uint64_t n_obs, const double* points,
+                               size_t n_points, double* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    std::unique_ptr<gpum_b200_session> s(create_session(
+        code, n_code, consts, n_consts, nullptr, 0, nullptr, 0, n_params, data, n_cols, n_obs));
+    batch(s.get(), points, n_points, out, true);
+  });
+}
+
+}  // extern "C"

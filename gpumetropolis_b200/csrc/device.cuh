@@ -1,0 +1,133 @@
+// device.cuh -- sm_100a device helpers: TMA bulk-tensor loads with mbarrier
+// completion (bounded waits), counter-based RNGs, compensated accumulation.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gpum {
+
+// ---------------------------------------------------------------- errors
+// Bits of the device error word a kernel sets instead of trapping; the host
+// reads it after every run and turns it into a status code.
+enum DevErr : uint32_t {
+  DEV_ERR_TMA_TIMEOUT = 1u << 0,   // a tile never arrived within the wait limit
+};
+
+// ------------------------------------------------------------- mbarrier/TMA
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Every wait is bounded: after the limit the caller records an error and
+// carries on, so a lost transfer can never hang the GPU.
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// 2-D tiled TMA load (no multicast): box at (x, y) of `map` into smem `dst`,
+// completion counted on `bar`.  x * elemsize must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// ------------------------------------------------------------------ RNGs
+// triple32 integer hash (Wellons), the reference's stream
+// (src/rust/src/cpu_native.rs:14-28, chain_kernel.rs:23-41).
+__host__ __device__ __forceinline__ uint32_t triple32(uint32_t h) {
+  h ^= h >> 17;
+  h *= 2129725213u;
+  h ^= h >> 11;
+  h *= 2890025505u;
+  h ^= h >> 15;
+  h *= 831628273u;
+  h ^= h >> 14;
+  return h;
+}
+
+__device__ __forceinline__ double t32_uniform(uint32_t seedmix, uint32_t ctr) {
+  return ((double)triple32(seedmix + ctr) + 0.5) / 4294967296.0;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw; SC'11): counter-based, so a
+// chain's stream is a pure function of (seed, chain, iteration, draw).
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// 53-bit uniform in (0, 1) from two 32-bit words.
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+  const uint64_t m = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);
+  return ((double)(m & ((1ull << 53) - 1)) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// ------------------------------------------------- compensated accumulation
+// Fast2Sum-compensated FP32 sum.  `s` follows plain summation exactly (so an
+// infinite or NaN term propagates as in the reference's naive sum, which
+// decides acceptance of non-finite proposals), and `c` collects the finite
+// rounding errors; the total is s + c.
+struct Comp {
+  float s, c;
+  __device__ __forceinline__ void init() { s = 0.f; c = 0.f; }
+  __device__ __forceinline__ void add(float x) {
+    const float t = s + x;
+    const float e = x - (t - s);
+    c += (fabsf(e) <= 3.402823466e38f) ? e : 0.f;
+    s = t;
+  }
+  __device__ __forceinline__ double total() const {
+    return isfinite(s) ? (double)s + (double)c : (double)s;
+  }
+};
+
+}  // namespace gpum

@@ -1,0 +1,266 @@
+// interp.cuh -- the warp-uniform register-stack bytecode interpreter.
+//
+// Replaces the reference's per-thread `vm_eval` (src/rust/src/chain_kernel.rs
+// :63-120), whose `stack[32]` lives in local memory and whose opcode dispatch
+// is an if-chain executed once per (chain, observation).  Here:
+//   * the micro-op stream sits in the constant bank (a __grid_constant__
+//     kernel parameter), read at a warp-uniform pc, so the dispatch is a
+//     uniform indirect branch with no divergence;
+//   * every case names its stack slot at compile time, so the operand stack
+//     `s[D][G]` is an array of registers (never local memory);
+//   * each thread carries G chains through the same instruction, amortising
+//     one dispatch over G chain-observations; the 32 lanes of a warp take 32
+//     consecutive observations of the shared-memory tile;
+//   * expensive ops (divide, pow, lgamma) share one code block per kind
+//     instead of being inlined per slot.
+#pragma once
+#include "device.cuh"
+#include "program.hpp"
+
+namespace gpum {
+
+struct __align__(16) EvalProg {
+  uint32_t n_uops;
+  uint32_t pad_[3];
+  uint32_t uop[kMaxUops];
+  float cst[kMaxConsts];
+};
+
+enum HeavyKind : int { H_NONE = -1, H_DIV = 0, H_POW = 1, H_LGAMMA = 2 };
+
+// Interpret the program once for G chains at one observation.
+//   xo : this lane's observation inside the tile; column j is at xo[j*T]
+//   pc0: this thread's first chain in the param tile; param p, chain g at
+//        pc0[p*CG + g]  (16-byte aligned; G is a multiple of 2)
+template <int G, int D>
+__device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
+                                           const float* __restrict__ xo, int T,
+                                           const float* __restrict__ pc0, int CG) {
+  const uint32_t n = pg.n_uops;
+  for (uint32_t pc = 0; pc < n; ++pc) {
+    const uint32_t w = pg.uop[pc];
+    const uint32_t a0 = (w >> 10) & 0x7FFu;
+    const uint32_t a1 = w >> 21;
+    int hk = H_NONE, hs = 0;
+    float ta[G], tb[G];
+
+#define GPUM_PL(g) pc0[(size_t)a0 * CG + (g)]
+#define GPUM_XD(a) xo[(size_t)(a) * T]
+#define GPUM_SLOT(S)                                                                   \
+  case S * NKIND + K_PUSH_C:                                                           \
+    if constexpr (S < D) {                                                             \
+      const float v = pg.cst[a0];                                                      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = v;                       \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_PUSH_P:                                                           \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = GPUM_PL(g);              \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_PUSH_D:                                                           \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a0);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = v;                       \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_ADD:                                                              \
+    if constexpr (S + 1 < D) {                                                         \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + s[S + 1][g];   \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SUB:                                                              \
+    if constexpr (S + 1 < D) {                                                         \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - s[S + 1][g];   \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_MUL:                                                              \
+    if constexpr (S + 1 < D) {                                                         \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * s[S + 1][g];   \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_DIV:                                                              \
+  case S * NKIND + K_POW:                                                              \
+    if constexpr (S + 1 < D) {                                                         \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
+        ta[g] = s[S][g];                                                               \
+        tb[g] = s[S + 1][g];                                                           \
+      }                                                                                \
+      hk = ((w & 1023u) == S * NKIND + K_DIV) ? H_DIV : H_POW;                         \
+      hs = S;                                                                          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_ADD_C:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = pg.cst[a0];                                                      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SUB_C:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = pg.cst[a0];                                                      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_MUL_C:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = pg.cst[a0];                                                      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_DIV_C:                                                            \
+  case S * NKIND + K_POW_C:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = pg.cst[a0];                                                      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
+        ta[g] = s[S][g];                                                               \
+        tb[g] = v;                                                                     \
+      }                                                                                \
+      hk = ((w & 1023u) == S * NKIND + K_DIV_C) ? H_DIV : H_POW;                       \
+      hs = S;                                                                          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_ADD_P:                                                            \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + GPUM_PL(g);    \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SUB_P:                                                            \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - GPUM_PL(g);    \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_MUL_P:                                                            \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * GPUM_PL(g);    \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_DIV_P:                                                            \
+  case S * NKIND + K_POW_P:                                                            \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
+        ta[g] = s[S][g];                                                               \
+        tb[g] = GPUM_PL(g);                                                            \
+      }                                                                                \
+      hk = ((w & 1023u) == S * NKIND + K_DIV_P) ? H_DIV : H_POW;                       \
+      hs = S;                                                                          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_ADD_D:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a0);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SUB_D:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a0);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_MUL_D:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a0);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * v;             \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_DIV_D:                                                            \
+  case S * NKIND + K_POW_D:                                                            \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a0);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
+        ta[g] = s[S][g];                                                               \
+        tb[g] = v;                                                                     \
+      }                                                                                \
+      hk = ((w & 1023u) == S * NKIND + K_DIV_D) ? H_DIV : H_POW;                       \
+      hs = S;                                                                          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_NEG:                                                              \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = -s[S][g];                \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_EXP:                                                              \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = expf(s[S][g]);           \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_LOG:                                                              \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = logf(s[S][g]);           \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SQRT:                                                             \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sqrtf(s[S][g]);          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_LGAMMA:                                                           \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) ta[g] = s[S][g];                   \
+      hk = H_LGAMMA;                                                                   \
+      hs = S;                                                                          \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SQR:                                                              \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * s[S][g];       \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_FMA_PD:                                                           \
+    if constexpr (S < D) {                                                             \
+      const float v = GPUM_XD(a1);                                                     \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
+    }                                                                                  \
+    break;
+
+    switch (w & 1023u) {
+      GPUM_SLOT(0) GPUM_SLOT(1) GPUM_SLOT(2) GPUM_SLOT(3)
+      GPUM_SLOT(4) GPUM_SLOT(5) GPUM_SLOT(6) GPUM_SLOT(7)
+#if 1
+      GPUM_SLOT(8) GPUM_SLOT(9) GPUM_SLOT(10) GPUM_SLOT(11)
+      GPUM_SLOT(12) GPUM_SLOT(13) GPUM_SLOT(14) GPUM_SLOT(15)
+      GPUM_SLOT(16) GPUM_SLOT(17) GPUM_SLOT(18) GPUM_SLOT(19)
+      GPUM_SLOT(20) GPUM_SLOT(21) GPUM_SLOT(22) GPUM_SLOT(23)
+      GPUM_SLOT(24) GPUM_SLOT(25) GPUM_SLOT(26) GPUM_SLOT(27)
+      GPUM_SLOT(28) GPUM_SLOT(29) GPUM_SLOT(30) GPUM_SLOT(31)
+#endif
+      default: break;
+    }
+#undef GPUM_SLOT
+#undef GPUM_PL
+#undef GPUM_XD
+
+    if (hk != H_NONE) {  // warp-uniform
+      if (hk == H_DIV) {
+#pragma unroll
+        for (int g = 0; g < G; ++g) ta[g] = ta[g] / tb[g];
+      } else if (hk == H_POW) {
+#pragma unroll
+        for (int g = 0; g < G; ++g) ta[g] = powf(ta[g], tb[g]);
+      } else {
+#pragma unroll
+        for (int g = 0; g < G; ++g) ta[g] = lgammaf(ta[g]);
+      }
+      // Write back to the slot named by the case (a second uniform switch).
+#define GPUM_WB(S)                                                        \
+  case S:                                                                 \
+    if constexpr (S < D) {                                                \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = ta[g];      \
+    }                                                                     \
+    break;
+      switch (hs) {
+        GPUM_WB(0) GPUM_WB(1) GPUM_WB(2) GPUM_WB(3) GPUM_WB(4) GPUM_WB(5) GPUM_WB(6)
+        GPUM_WB(7) GPUM_WB(8) GPUM_WB(9) GPUM_WB(10) GPUM_WB(11) GPUM_WB(12) GPUM_WB(13)
+        GPUM_WB(14) GPUM_WB(15) GPUM_WB(16) GPUM_WB(17) GPUM_WB(18) GPUM_WB(19)
+        GPUM_WB(20) GPUM_WB(21) GPUM_WB(22) GPUM_WB(23) GPUM_WB(24) GPUM_WB(25)
+        GPUM_WB(26) GPUM_WB(27) GPUM_WB(28) GPUM_WB(29) GPUM_WB(30) GPUM_WB(31)
+        default: break;
+      }
+#undef GPUM_WB
+    }
+  }
+}
+
+}  // namespace gpum

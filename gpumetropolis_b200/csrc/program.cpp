@@ -1,0 +1,200 @@
+// program.cpp -- bytecode validation and micro-op compilation (see program.hpp).
+#include "program.hpp"
+
+#include <cmath>
+#include <cstdio>
+
+namespace gpum {
+
+namespace {
+
+enum SrcOp : uint32_t {
+  OP_CONST = 0, OP_PARAM = 1, OP_DATA = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5,
+  OP_DIV = 6, OP_NEG = 7, OP_EXP = 8, OP_LOG = 9, OP_SQRT = 10, OP_POW = 11,
+  OP_LGAMMA = 12
+};
+
+// The reference dispatches every unknown opcode to POW
+// (cpu_native.rs:103, chain_kernel.rs:109-111); normalise it here.
+inline uint32_t norm_op(uint32_t op) {
+  return (op <= OP_SQRT || op == OP_LGAMMA) ? op : OP_POW;
+}
+inline bool is_push(uint32_t op) { return op <= OP_DATA; }
+inline bool is_unary(uint32_t op) {
+  return (op >= OP_NEG && op <= OP_SQRT) || op == OP_LGAMMA;
+}
+inline bool is_binary(uint32_t op) { return !is_push(op) && !is_unary(op); }
+
+std::string fmt(const char* f, long a, long b = 0) {
+  char buf[256];
+  std::snprintf(buf, sizeof buf, f, a, b);
+  return buf;
+}
+
+}  // namespace
+
+int validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
+                     uint32_t n_params, uint32_t n_cols, bool allow_data, int* depth,
+                     std::string* err) {
+  *depth = 0;
+  if (n_code % 2 != 0) {
+    *err = "bytecode length must be even (opcode/argument pairs)";
+    return 1;
+  }
+  if (n_code > 0 && code == nullptr) {
+    *err = "bytecode pointer is NULL";
+    return 1;
+  }
+  const size_t n = n_code / 2;
+  int sp = 0, maxd = 0;
+  for (size_t pc = 0; pc < n; ++pc) {
+    const uint32_t op = norm_op(code[2 * pc]);
+    const uint32_t arg = code[2 * pc + 1];
+    if (is_push(op)) {
+      if (op == OP_CONST && arg >= n_consts) {
+        *err = fmt("instruction %ld: constant index %ld out of range", (long)pc, arg);
+        return 1;
+      }
+      if (op == OP_PARAM && arg >= n_params) {
+        *err = fmt("instruction %ld: parameter index %ld out of range", (long)pc, arg);
+        return 1;
+      }
+      if (op == OP_DATA && (!allow_data || arg >= n_cols)) {
+        *err = allow_data
+                   ? fmt("instruction %ld: data column %ld out of range", (long)pc, arg)
+                   : fmt("instruction %ld: the prior may not read data (column %ld)",
+                         (long)pc, arg);
+        return 1;
+      }
+      ++sp;
+    } else if (is_unary(op)) {
+      if (sp < 1) {
+        *err = fmt("instruction %ld: stack underflow", (long)pc);
+        return 1;
+      }
+    } else {
+      if (sp < 2) {
+        *err = fmt("instruction %ld: stack underflow", (long)pc);
+        return 1;
+      }
+      --sp;
+    }
+    if (sp > maxd) maxd = sp;
+    if (maxd > kMaxStack) {
+      *err = fmt("stack depth %ld exceeds the interpreter limit %ld", maxd, kMaxStack);
+      return 1;
+    }
+  }
+  if (n > 0 && sp < 1) {
+    *err = "program leaves an empty stack";
+    return 1;
+  }
+  *depth = maxd;
+  return 0;
+}
+
+int compile_program(const uint32_t* code, size_t n_code, const double* consts,
+                    size_t n_consts, uint32_t n_params, uint32_t n_cols,
+                    bool allow_data, UProg* out, std::string* err) {
+  *out = UProg();
+  int depth = 0;
+  if (validate_program(code, n_code, n_consts, n_params, n_cols, allow_data, &depth,
+                       err))
+    return 1;
+  if (n_params > (uint32_t)kMaxIndex || n_cols > (uint32_t)kMaxIndex) {
+    *err = "more than 2047 parameters or data columns";
+    return 1;
+  }
+  if (n_consts > 0 && consts == nullptr) {
+    *err = "constant pool pointer is NULL";
+    return 1;
+  }
+  const size_t n = n_code / 2;
+  out->depth = depth;
+  out->n_src = (int)n;
+  for (size_t i = 0; i < n_consts; ++i) out->consts.push_back((float)consts[i]);
+
+  // Stack depth before each source instruction.
+  std::vector<int> before(n + 1, 0);
+  std::vector<uint32_t> op(n), arg(n);
+  int sp = 0;
+  for (size_t pc = 0; pc < n; ++pc) {
+    op[pc] = norm_op(code[2 * pc]);
+    arg[pc] = code[2 * pc + 1];
+    before[pc] = sp;
+    if (is_push(op[pc])) ++sp;
+    else if (is_binary(op[pc])) --sp;
+    if (op[pc] == OP_DATA) out->uses_data = true;
+  }
+
+  auto add_const = [&](float v) -> int {
+    out->consts.push_back(v);
+    return (int)out->consts.size() - 1;
+  };
+  auto emit = [&](uint32_t kind, int slot, uint32_t a0, uint32_t a1) {
+    out->uops.push_back(uop_word(kind, (uint32_t)slot, a0, a1));
+  };
+  static const uint32_t kBin[5] = {K_ADD, K_SUB, K_MUL, K_DIV, K_POW};
+  auto bin_index = [](uint32_t o) -> int {
+    return o == OP_POW ? 4 : (int)(o - OP_ADD);
+  };
+
+  size_t pc = 0;
+  while (pc < n) {
+    const uint32_t o = op[pc];
+    // acc + p*x  or  acc + x*p  -> one multiply-add into the accumulator slot.
+    if (pc + 3 < n && before[pc] >= 1 && op[pc + 2] == OP_MUL && op[pc + 3] == OP_ADD &&
+        ((o == OP_PARAM && op[pc + 1] == OP_DATA) ||
+         (o == OP_DATA && op[pc + 1] == OP_PARAM))) {
+      const uint32_t p = o == OP_PARAM ? arg[pc] : arg[pc + 1];
+      const uint32_t x = o == OP_PARAM ? arg[pc + 1] : arg[pc];
+      emit(K_FMA_PD, before[pc] - 1, p, x);
+      pc += 4;
+      continue;
+    }
+    // push followed by the binary op that consumes it: fold the operand.
+    if (is_push(o) && pc + 1 < n && is_binary(op[pc + 1])) {
+      const uint32_t b = op[pc + 1];
+      const int slot = before[pc] - 1;
+      if (o == OP_CONST && b == OP_POW && consts[arg[pc]] == 2.0) {
+        emit(K_SQR, slot, 0, 0);
+      } else if (o == OP_CONST && b == OP_DIV && consts[arg[pc]] != 0.0 &&
+                 std::isfinite(consts[arg[pc]]) &&
+                 std::ldexp(1.0, std::ilogb(consts[arg[pc]])) ==
+                     std::fabs(consts[arg[pc]])) {
+        // Division by a power of two is exactly a multiply by its reciprocal.
+        emit(K_MUL_C, slot, (uint32_t)add_const((float)(1.0 / consts[arg[pc]])), 0);
+      } else {
+        const uint32_t base = o == OP_CONST ? K_ADD_C : (o == OP_PARAM ? K_ADD_P : K_ADD_D);
+        emit(base + (uint32_t)bin_index(b), slot, arg[pc], 0);
+      }
+      pc += 2;
+      continue;
+    }
+    switch (o) {
+      case OP_CONST: emit(K_PUSH_C, before[pc], arg[pc], 0); break;
+      case OP_PARAM: emit(K_PUSH_P, before[pc], arg[pc], 0); break;
+      case OP_DATA: emit(K_PUSH_D, before[pc], arg[pc], 0); break;
+      case OP_NEG: emit(K_NEG, before[pc] - 1, 0, 0); break;
+      case OP_EXP: emit(K_EXP, before[pc] - 1, 0, 0); break;
+      case OP_LOG: emit(K_LOG, before[pc] - 1, 0, 0); break;
+      case OP_SQRT: emit(K_SQRT, before[pc] - 1, 0, 0); break;
+      case OP_LGAMMA: emit(K_LGAMMA, before[pc] - 1, 0, 0); break;
+      default: emit(kBin[bin_index(o)], before[pc] - 2, 0, 0); break;
+    }
+    ++pc;
+  }
+  if ((int)out->uops.size() > kMaxUops) {
+    *err = fmt("program compiles to %ld micro-ops, limit %ld", (long)out->uops.size(),
+               kMaxUops);
+    return 1;
+  }
+  if ((int)out->consts.size() > kMaxConsts) {
+    *err = fmt("constant pool of %ld entries exceeds %ld", (long)out->consts.size(),
+               kMaxConsts);
+    return 1;
+  }
+  return 0;
+}
+
+}  // namespace gpum

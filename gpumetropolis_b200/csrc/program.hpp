@@ -1,0 +1,70 @@
+// program.hpp -- host-side compiler from gpumetropolis bytecode to the
+// register-slot micro-op stream the B200 interpreter executes.
+//
+// Input format (R/dsl.R:13-17, emitted as (opcode, arg) u32 pairs):
+//   0 PUSH_CONST, 1 PUSH_PARAM, 2 PUSH_DATA, 3 ADD, 4 SUB, 5 MUL, 6 DIV,
+//   7 NEG, 8 EXP, 9 LOG, 10 SQRT, 11 POW, 12 LGAMMA.
+// Semantics follow the reference interpreter (src/rust/src/cpu_native.rs:80-107
+// and chain_kernel.rs:63-120): an empty program evaluates to 0, the result is
+// stack slot 0, and every opcode outside {0..10,12} acts as POW.  Unlike the
+// reference (which validates only in R, dsl.R:115-119, and otherwise panics on
+// an out-of-range index), this compiler rejects malformed programs with an
+// error before anything reaches the GPU.
+//
+// Output: one 32-bit word per micro-op,
+//   bits  0..9   case id = slot * NKIND + kind   (slot = stack index of the
+//                 result, a compile-time register index in the kernel)
+//   bits 10..20  a0 (const / param / column index)
+//   bits 21..31  a1 (second index for two-operand fused forms)
+// plus an f32 constant pool.  Peephole fusion folds a push into the binary op
+// that consumes it, and `p*x + acc` patterns into one multiply-add.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace gpum {
+
+enum Kind : uint32_t {
+  K_PUSH_C = 0, K_PUSH_P, K_PUSH_D,
+  K_ADD, K_SUB, K_MUL, K_DIV, K_POW,            // s[t] = s[t] op s[t+1]
+  K_ADD_C, K_SUB_C, K_MUL_C, K_DIV_C, K_POW_C,  // s[t] = s[t] op const
+  K_ADD_P, K_SUB_P, K_MUL_P, K_DIV_P, K_POW_P,  // s[t] = s[t] op param
+  K_ADD_D, K_SUB_D, K_MUL_D, K_DIV_D, K_POW_D,  // s[t] = s[t] op data
+  K_NEG, K_EXP, K_LOG, K_SQRT, K_LGAMMA,        // s[t] = f(s[t])
+  K_SQR,                                        // s[t] = s[t]*s[t]  (x^2)
+  K_FMA_PD,                                     // s[t] += param[a0]*data[a1]
+  NKIND
+};
+
+constexpr int kMaxStack = 32;      // reference limit (R/dsl.R:20)
+constexpr int kMaxUops = 1024;     // micro-ops per program (constant bank)
+constexpr int kMaxConsts = 512;    // f32 constants per program
+constexpr int kMaxIndex = 2047;    // 11-bit operand fields
+constexpr int kMaxSlots = 32;      // deepest interpreter variant
+
+struct UProg {
+  std::vector<uint32_t> uops;
+  std::vector<float> consts;
+  int depth = 0;          // peak stack depth of the source program
+  int n_src = 0;          // source instructions
+  bool uses_data = false;
+  bool empty() const { return n_src == 0; }
+};
+
+inline uint32_t uop_word(uint32_t kind, uint32_t slot, uint32_t a0, uint32_t a1) {
+  return (slot * NKIND + kind) | (a0 << 10) | (a1 << 21);
+}
+
+// Validates and compiles.  Returns 0 or an error message in *err.
+int compile_program(const uint32_t* code, size_t n_code, const double* consts,
+                    size_t n_consts, uint32_t n_params, uint32_t n_cols,
+                    bool allow_data, UProg* out, std::string* err);
+
+// Validation only (stack discipline, operand ranges, depth), for programs
+// that are interpreted in f64 directly from the source bytecode (the prior).
+int validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
+                     uint32_t n_params, uint32_t n_cols, bool allow_data,
+                     int* depth, std::string* err);
+
+}  // namespace gpum

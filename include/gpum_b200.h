@@ -1,0 +1,156 @@
+/*
+ * gpum_b200.h -- C ABI of the B200 (sm_100a) backend for gpumetropolis.
+ *
+ * Plain pointers and sizes only; no function throws, aborts or exits.  Every
+ * compute entry point returns GPUM_OK (0) or a GPUM_ERR_* code and, when `err`
+ * is non-NULL, writes a NUL-terminated message of at most err_len bytes.
+ *
+ * Layouts follow the reference's FFI (src/rust/src/lib.rs):
+ *   code        u32 (opcode, arg) pairs, length n_code (even)   R/dsl.R:13-17
+ *   consts      f64 constant pool
+ *   data        f64 row-major n_obs x n_cols                     R/api.R:281-294
+ *   init, proposal_sd   f64 chain-major n_chains x n_params      R/api.R:297-346
+ *   proposal_l  f64 n_chains x n_params x n_params, row-major lower factors,
+ *               or NULL / n_l == 0                               chain_kernel.rs:224-249
+ *   out_draws   f32 n_iter*n_chains*n_params, column-major (n_iter, n_chains,
+ *               n_params): draws[t + n_iter*(c + n_chains*j)]     chain_kernel.rs:345
+ *   points      f64 point-major n_points x n_params              lib.rs:131-207
+ *
+ * Arithmetic: the per-observation bytecode runs in FP32 on the GPU with
+ * compensated FP32 partial sums; totals, the prior, proposals and the
+ * acceptance ratio are FP64.
+ */
+#ifndef GPUM_B200_H
+#define GPUM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GPUM_API __attribute__((visibility("default")))
+#else
+#define GPUM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUM_OK 0
+#define GPUM_ERR_INVALID 1      /* bad argument or malformed bytecode          */
+#define GPUM_ERR_CUDA 2         /* CUDA runtime / driver failure               */
+#define GPUM_ERR_NOMEM 3        /* device or host allocation failed            */
+#define GPUM_ERR_UNSUPPORTED 4  /* valid input beyond this backend's limits    */
+#define GPUM_ERR_NODEVICE 5     /* no sm_100 GPU visible                       */
+#define GPUM_ERR_DEVICE 6       /* a kernel reported a device-side failure     */
+
+/* proposal_mode values (lib.rs:85; chain_kernel.rs:212-295; cpu_native.rs:573-784) */
+#define GPUM_MODE_RWM 0         /* diagonal Gaussian random walk               */
+#define GPUM_MODE_DE 1          /* differential evolution on the init snapshot */
+#define GPUM_MODE_CHOL 2        /* random walk with per-chain Cholesky factor  */
+#define GPUM_MODE_MALA 3        /* Metropolis-adjusted Langevin                */
+
+/* rng values for the session API */
+#define GPUM_RNG_TRIPLE32 0     /* the reference's counter hash stream         */
+#define GPUM_RNG_PHILOX 1       /* Philox4x32-10 counter-based stream          */
+
+/* 1 if an sm_100 device is visible and the kernels load, else 0.
+ * Replaces rust_available_backends()'s feature probe (lib.rs:51-61). */
+GPUM_API int gpum_b200_available(void);
+
+/* Library version string, e.g. "gpum_b200 0.1.0 sm_100a". */
+GPUM_API const char* gpum_b200_version(void);
+
+/* Check a program without touching the GPU: opcode/argument ranges, stack
+ * discipline, depth <= 32 (R/dsl.R:115-119).  allow_data = 0 for a prior.
+ * Writes the peak stack depth to *depth (may be NULL). */
+GPUM_API int gpum_b200_validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
+                               uint32_t n_params, uint32_t n_cols, int allow_data,
+                               int* depth, char* err, size_t err_len);
+
+/* Whole sampler, one call per batch, inputs and outputs in host memory.
+ * Replaces rust_gpu_metropolis -> gpu_metropolis_chain (lib.rs:69-123,
+ * chain_kernel.rs:469-532).  Uses the reference's triple32 stream, so with
+ * the same seed the b200 chains follow the CPU backend's chains up to FP32
+ * evaluation differences in the data sum. */
+GPUM_API int gpum_b200_run(const uint32_t* code, size_t n_code, const double* consts, size_t n_consts,
+                  const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
+                  size_t n_prior_consts, uint32_t n_params, const double* data, uint32_t n_cols,
+                  uint64_t n_obs, const double* init, const double* proposal_sd,
+                  const double* temperatures, uint32_t n_chains, uint32_t n_iter, uint32_t seed,
+                  uint32_t proposal_mode, double gamma, double de_noise,
+                  const double* proposal_l, size_t n_l, float* out_draws, float* out_accept,
+                  double* out_last_logpost, char* err, size_t err_len);
+
+/* Summed log-likelihood at each point, out[n_points] f64
+ * (rust_loglik_batch, lib.rs:131-151). */
+GPUM_API int gpum_b200_loglik_batch(const uint32_t* code, size_t n_code, const double* consts,
+                           size_t n_consts, uint32_t n_params, const double* data,
+                           uint32_t n_cols, uint64_t n_obs, const double* points,
+                           size_t n_points, double* out, char* err, size_t err_len);
+
+/* Per-observation log-likelihood, out[p*n_obs + i] f64
+ * (rust_loglik_pointwise, lib.rs:187-207). */
+GPUM_API int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, const double* consts,
+                               size_t n_consts, uint32_t n_params, const double* data,
+                               uint32_t n_cols, uint64_t n_obs, const double* points,
+                               size_t n_points, double* out, char* err, size_t err_len);
+
+/* ------------------------------------------------------------- sessions --
+ * A session keeps the model and the data resident on the GPU, so batches of a
+ * host-orchestrated run (adaptive warmup, PT, DE snapshots) do not re-upload
+ * the data each call as the reference does (chain_kernel.rs:391-413). */
+typedef struct gpum_b200_session gpum_b200_session;
+
+GPUM_API int gpum_b200_session_create(const uint32_t* code, size_t n_code, const double* consts,
+                             size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                             const double* prior_consts, size_t n_prior_consts,
+                             uint32_t n_params, const double* data, uint32_t n_cols,
+                             uint64_t n_obs, gpum_b200_session** out, char* err,
+                             size_t err_len);
+
+/* Same contract as gpum_b200_run on a session; rng selects the stream. */
+GPUM_API int gpum_b200_session_run(gpum_b200_session* s, const double* init, const double* proposal_sd,
+                          const double* temperatures, uint32_t n_chains, uint32_t n_iter,
+                          uint32_t seed, uint32_t proposal_mode, double gamma, double de_noise,
+                          const double* proposal_l, size_t n_l, int rng, float* out_draws,
+                          float* out_accept, double* out_last_logpost, char* err,
+                          size_t err_len);
+
+/* loglik_batch / loglik_pointwise on a session. */
+GPUM_API int gpum_b200_session_loglik_batch(gpum_b200_session* s, const double* points, size_t n_points,
+                                   double* out, char* err, size_t err_len);
+GPUM_API int gpum_b200_session_loglik_pointwise(gpum_b200_session* s, const double* points,
+                                       size_t n_points, double* out, char* err,
+                                       size_t err_len);
+
+/* Device-resident stepping, for callers that keep chain state on the GPU
+ * between calls: prepare() uploads the batch-start state and evaluates it,
+ * advance() runs n more iterations entirely on the device (CUDA graph),
+ * fetch() copies results out.  Draw storage is reserved for max_iter
+ * iterations at prepare(). */
+GPUM_API int gpum_b200_session_prepare(gpum_b200_session* s, const double* init,
+                              const double* proposal_sd, const double* temperatures,
+                              uint32_t n_chains, uint32_t max_iter, uint32_t seed,
+                              uint32_t proposal_mode, double gamma, double de_noise,
+                              const double* proposal_l, size_t n_l, int rng, char* err,
+                              size_t err_len);
+GPUM_API int gpum_b200_session_advance(gpum_b200_session* s, uint32_t n_iter, char* err, size_t err_len);
+GPUM_API int gpum_b200_session_sync(gpum_b200_session* s, char* err, size_t err_len);
+/* Copies draws of the iterations advanced so far (n_done <= max_iter) in the
+ * reference layout with n_iter = n_done, accept rates over n_done, last
+ * log posteriors.  Any output pointer may be NULL. */
+GPUM_API int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, float* out_accept,
+                            double* out_last_logpost, uint32_t* n_done, char* err,
+                            size_t err_len);
+
+/* Kernel launches issued by this session so far (every node of a replayed
+ * graph counts once per replay). */
+GPUM_API uint64_t gpum_b200_session_launches(const gpum_b200_session* s);
+
+GPUM_API void gpum_b200_session_destroy(gpum_b200_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUM_B200_H */
