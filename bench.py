@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Throughput of the B200 sampler hot path on the logistic-regression workload.
+
+Workload (the config the headline metric is quoted on that fits one GPU):
+logistic regression, N = 2^20 observations, 16 N(0,1) covariates plus an
+intercept (17 parameters, 17 data columns), N(0, 10^2) priors, 1,024 chains,
+plain exact random-walk Metropolis with FP32 per-observation bytecode and
+compensated sums.  One *step* is one Metropolis iteration of all 1,024 chains
+over all N observations (1.07e9 chain-observation evaluations plus the
+accept/propose step).
+
+* ``value``: chain-obs/s with the data and chain state resident in HBM,
+  device-timed with CUDA events around each step on the session's stream;
+  L2 is flushed (256 MiB write) before every timed step because the data
+  (71 MB in f32) fits in the 126 MB L2.
+* ``e2e``: the same metric through the reference-facing C ABI
+  (``gpum_b200_run``) with host buffers: data upload + layout conversion,
+  K iterations, draws copied back, wall-clock.
+* ``roofline``: the iteration kernel against the FP32 pipe (the kernel is
+  FP32/issue-bound), plus the HBM view of the same launch.
+* ``cpu_baseline``: the oracle port of the reference CPU backend (bytecode ->
+  C -> gcc JIT, OpenMP over chains) on this host, a bounded sample.
+
+``--impl reference`` times that CPU implementation alone as the reference arm.
+Multi-GPU (torchrun): one independent replica per GPU (the chains shard with
+no collective), weak scaling, max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("ESS/s on 1 B200, surrogate-DA vs plain exact MH at <=1e-6 rel logp err; "
+          "chain-obs/s")
+UNIT = "chain-obs/s"
+FLOP_PER_CHAIN_OBS = 34.0   # essential FP32 flops of the logistic term (FMA = 2)
+MUFU_PER_CHAIN_OBS = 2.0    # exp, log
+ROW_BYTES = 17 * 4          # one f32 observation row
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--n-obs", type=int, default=1 << 20)
+    p.add_argument("--chains", type=int, default=1024)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def _workload(n_obs):
+    from gpumetropolis_b200 import workloads as W
+    return W.make("logistic", n_obs=n_obs)
+
+
+def _init(w, C, seed=0):
+    rng = np.random.default_rng(seed)
+    m = w.model
+    init = w.truth["beta"] + rng.normal(0, 0.01, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.0015)
+    return init, sd, np.ones(C)
+
+
+def _cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(w, seconds, chains_cap):
+    """Time the oracle port (JIT'd data term, OpenMP over chains) on a bounded
+    sample of the workload: all N observations, one iteration of a number of
+    chains sized to about `seconds` of work.  Every (chain, observation)
+    evaluation counts, the start-state evaluation included."""
+    from oracle import cjit
+    from oracle import oracle as O
+    m = w.model
+    cores = _cpu_cores()
+    fn = cjit.compile_loglik(m.loglik.code, m.loglik.consts)
+
+    def once(C, n_iter):
+        init, sd, temps = _init(w, C, seed=1)
+        t = time.perf_counter()
+        O.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+              w.data, m.n_cols, w.n_obs, init, sd, temps, n_iter, 1, 0, jit=fn,
+              n_threads=cores)
+        return time.perf_counter() - t, C * (n_iter + 1) * w.n_obs
+
+    dt, work = once(cores, 0)
+    rate = work / dt
+    C = int(max(cores, min(chains_cap, round(rate * seconds / (2 * w.n_obs)))))
+    C = max(cores, (C // cores) * cores)
+    dt, work = once(C, 1)
+    return {"value": work / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{C} chains x 1 iteration (+ start evaluation) x {w.n_obs} obs, "
+                      f"{work:.3g} chain-obs in {dt:.1f} s; oracle port of cpu_native::run "
+                      "with the bytecode->C gcc JIT, OpenMP over chains"}
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _traffic_per_launch():
+    """dram read+write bytes of one iteration launch from the committed ncu
+    summary (profiles/iter_kernel_logistic.md, line `dram_bytes_per_launch: X`)."""
+    path = os.path.join(ROOT, "profiles", "iter_kernel_logistic.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def run_b200(a):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+
+    w = _workload(a.n_obs)
+    m = w.model
+    C, N = a.chains, w.n_obs
+    init, sd, temps = _init(w, C, seed=rank)
+    K, Wm = a.steps, max(3, a.warmup)
+
+    sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                           m.n_params, w.data, m.n_cols, w.n_obs)
+    sess.prepare(init, sd, temps, Wm + K, 1 + rank, 0, rng=_native.RNG_PHILOX)
+    sess.advance(Wm)
+    sess.sync()
+    stream = torch.cuda.ExternalStream(sess.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = sess.launches
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for k in range(K):
+                flush.zero_()
+                starts[k].record(stream)
+                sess.advance(1)
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches = sess.launches - l0
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    dev_ms = float(step_ms.sum())
+    if world > 1:
+        t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        dist.barrier()
+    _, acc, _, _ = sess.fetch(want_draws=False)
+    sess.close()
+    value = world * K * C * N / (dev_ms / 1e3)
+    ms_step = dev_ms / K
+
+    clocks = clk.summary()
+    mhz = clocks["sm_mhz"] or 1965.0
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    fp32_peak = n_sm * 128 * 2 * mhz * 1e6 / 1e12
+    achieved = C * N * FLOP_PER_CHAIN_OBS / (ms_step / 1e3) / 1e12
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = _traffic_per_launch()
+    roofline = {
+        "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak, 3),
+        "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4), "traffic": traffic,
+        "peak_source": f"nominal {n_sm} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz "
+                       "(median SM clock sampled in the timed region; "
+                       "MEASURED_PEAKS.json has no FP32 figure)",
+        "work_per_launch": f"{C} chains x {N} obs x {FLOP_PER_CHAIN_OBS:.0f} flop "
+                           f"(+{MUFU_PER_CHAIN_OBS:.0f} MUFU)",
+        "hbm": {"achieved_gbs": round(N * ROW_BYTES / (ms_step / 1e3) / 1e9, 2),
+                "peak_gbs": hbm_peak, "peak_source": hbm_src,
+                "frac": round(N * ROW_BYTES / (ms_step / 1e3) / 1e9 / hbm_peak, 5),
+                "bytes_per_launch": N * ROW_BYTES},
+    }
+
+    e2e = None
+    if rank == 0 and not a.no_e2e:
+        init2, sd2, temps2 = _init(w, C, seed=7)
+        t = time.perf_counter()
+        _native.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                    w.data, m.n_cols, w.n_obs, init2, sd2, temps2, K, 3, 0)
+        dt = time.perf_counter() - t
+        h2d = (w.data.nbytes + init2.nbytes + sd2.nbytes + temps2.nbytes
+               + m.loglik.code.nbytes + m.loglik.consts.nbytes + m.prior.code.nbytes
+               + m.prior.consts.nbytes)
+        d2h = K * C * m.n_params * 4 + C * 4 + C * 8
+        e2e = {"value": K * C * N / dt, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+               "d2h_bytes_per_step": d2h / K,
+               "note": "gpum_b200_run: one call of K iterations from host buffers (data "
+                       "upload + f64->f32 column layout + K iterations + draws back), wall"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_sample(w, a.cpu_seconds, C)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": Wm, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "logistic regression (BASELINE config 2): N=2^20 obs, 16 "
+                               "N(0,1) covariates + intercept, 17 params, 1024 chains, exact "
+                               "RWM, FP32 bytecode + compensated sums, f64 totals/accept",
+                   "n_obs": N, "n_chains": C, "n_params": m.n_params,
+                   "bytecode_instructions": m.loglik.n_instr,
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "rng": "philox", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clocks, "wall_s_timed_region": wall,
+        "accept_rate_mean": float(np.mean(acc)),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = _workload(a.n_obs)
+    m = w.model
+    from oracle import cjit
+    from oracle import oracle as O
+    cores = _cpu_cores()
+    fn = cjit.compile_loglik(m.loglik.code, m.loglik.consts)
+    K, Wm = a.steps, max(3, a.warmup)
+    # size each step to about min(2 s, 150 s / (K + W)) of work
+    budget = min(2.0, 150.0 / (K + Wm))
+    init, sd, temps = _init(w, cores, seed=1)
+    t = time.perf_counter()
+    O.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params, w.data,
+          m.n_cols, w.n_obs, init, sd, temps, 0, 1, 0, jit=fn, n_threads=cores)
+    rate = cores * w.n_obs / (time.perf_counter() - t)
+    C = max(cores, int(rate * budget / (2 * w.n_obs)) // cores * cores)
+    init, sd, temps = _init(w, C, seed=1)
+    times = []
+    for k in range(Wm + K):
+        t = time.perf_counter()
+        O.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+              w.data, m.n_cols, w.n_obs, init, sd, temps, 1, 1 + k, 0, jit=fn,
+              n_threads=cores)
+        if k >= Wm:
+            times.append(time.perf_counter() - t)
+    work = 2 * C * w.n_obs
+    value = K * work / sum(times)
+    sample = (f"{C} chains x 1 iteration (+ start evaluation) x {w.n_obs} obs per step; "
+              "oracle port of cpu_native::run (reference Rust/R unbuildable here) with the "
+              "bytecode->C gcc JIT, OpenMP over chains")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": K, "warmup": Wm, "ms_per_step": 1e3 * sum(times) / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "logistic regression (BASELINE config 2): N=2^20 obs, 17 "
+                               "params; bounded chain sample per step", "n_obs": w.n_obs,
+                   "n_chains_per_step": C},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)
+
+
+if __name__ == "__main__":
+    main()

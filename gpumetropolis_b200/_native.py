@@ -74,6 +74,7 @@ SIGNATURES = {
     "gpum_b200_session_fetch": (C.c_int, [C.c_void_p, _f32p, _f32p, _f64p,
                                           C.POINTER(C.c_uint32), _errp, _sz]),
     "gpum_b200_session_launches": (C.c_uint64, [C.c_void_p]),
+    "gpum_b200_session_stream": (C.c_void_p, [C.c_void_p]),
     "gpum_b200_session_destroy": (None, [C.c_void_p]),
 }
 
@@ -223,6 +224,11 @@ class Session:
     @property
     def launches(self) -> int:
         return int(self._lib.gpum_b200_session_launches(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The session's cudaStream_t as an integer handle."""
+        return int(self._lib.gpum_b200_session_stream(self._h) or 0)
 
     def run(self, init, proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0,
             de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):

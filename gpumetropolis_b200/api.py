@@ -1,0 +1,230 @@
+"""User-facing sampler: ``gpu_metropolis(model, data, ..., backend="b200")``.
+
+Restates the reference's ``gpu_metropolis`` (``R/api.R:247-599``) over the B200
+session: input validation and flattening (``R/api.R:281-346``), method routing
+(rwm with adaptive warmup, pt, de, mala) and the fit object.  The compute
+backend is always the B200 library; ``backend`` accepts ``"b200"`` (and
+``"auto"``, which resolves to it) -- the reference's ``"cpu"``/``"cuda"``/
+``"vulkan"`` backends live in the reference package, not here.
+
+Differences forced by leaving R: when ``init`` is omitted the starting values
+are standard normals from a PCG64 stream seeded with ``seed`` (the reference
+draws them with R's ``rnorm`` after ``set.seed(seed)``, ``R/api.R:302-307``),
+and PT swap uniforms use PCG64 seeded with the reference's mix
+(``R/adaptive.R:537-539``).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _native
+from . import adaptive as AD
+from .dsl import GpumModel
+
+
+class GpumInputError(ValueError):
+    """Invalid argument to gpu_metropolis (the reference raises an R error)."""
+
+
+@dataclass
+class GpumFit:
+    draws: np.ndarray              # (n_iter_kept, n_chains, n_params)
+    accept_rate: np.ndarray
+    model: GpumModel
+    n_iter: int
+    n_iter_total: int
+    warmup: int
+    n_chains: int
+    n_params: int
+    backend: str
+    seed: int
+    method: str
+    adaptation: Optional[dict] = None
+    extra: dict = field(default_factory=dict)
+
+    def __getitem__(self, name):
+        return self.draws[:, :, self.model.params.index(name)]
+
+    def __repr__(self):
+        lines = ["<gpum_fit>",
+                 f"  parameters  : {', '.join(self.model.params)}",
+                 f"  method      : {self.method}",
+                 f"  backend     : {self.backend}",
+                 f"  chains      : {self.n_chains}",
+                 f"  iterations  : {self.n_iter} per chain ({self.n_iter_total} raw, "
+                 f"{self.warmup} {'adaptive' if self.adaptation else 'trim'} warmup discarded)",
+                 f"  accept_rate : {self.accept_rate.min():.3f} to {self.accept_rate.max():.3f}"]
+        for j, p in enumerate(self.model.params):
+            post = self.draws[:, 0, j] if self.method == "pt" else self.draws[:, :, j]
+            lines.append(f"  {p:<11} : posterior mean {post.mean():.4f} (sd {post.std(ddof=1):.4f})")
+        return "\n".join(lines)
+
+
+def _data_matrix(model: GpumModel, data):
+    if model.n_cols == 0:
+        return np.zeros((0, 0)), 0
+    if data is None:
+        raise GpumInputError("missing data columns: " + ", ".join(model.data))
+    if isinstance(data, np.ndarray):
+        mat = np.asarray(data, dtype=np.float64)
+        if mat.ndim == 1:
+            mat = mat[:, None]
+        if mat.shape[1] != model.n_cols:
+            raise GpumInputError(f"data must have {model.n_cols} columns")
+        return np.ascontiguousarray(mat), mat.shape[0]
+    missing = [c for c in model.data if c not in data]
+    if missing:
+        raise GpumInputError("missing data columns: " + ", ".join(missing))
+    cols = [np.asarray(data[c], dtype=np.float64).ravel() for c in model.data]
+    n = cols[0].size
+    if any(c.size != n for c in cols):
+        raise GpumInputError("data columns must have equal length")
+    return np.ascontiguousarray(np.stack(cols, axis=1)), n
+
+
+class _Backend:
+    """One data-resident session serving every batch of a run (the
+    ``rust_call`` closure of ``R/api.R:379-393``)."""
+
+    def __init__(self, model: GpumModel, data_mat, n_obs, rng_kind):
+        m = model
+        self.np = m.n_params
+        self.rng = rng_kind
+        self.session = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code,
+                                       m.prior.consts, m.n_params, data_mat, m.n_cols, n_obs)
+
+    def __call__(self, init, sd, n_iter, seed, temperatures=None, proposal_mode=0, gamma=0.0,
+                 de_noise=0.0, proposal_l=None):
+        init = np.asarray(init, dtype=np.float64)
+        C = init.shape[0]
+        temps = np.ones(C) if temperatures is None else np.asarray(temperatures, np.float64)
+        d, acc, last = self.session.run(init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF,
+                                        proposal_mode, gamma, de_noise, proposal_l, rng=self.rng)
+        return d.reshape((int(n_iter), C, self.np), order="F"), acc.astype(np.float64), last
+
+    def close(self):
+        self.session.close()
+
+
+def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_iter=2000,
+                   n_chains=4, warmup=None, adapt=True, method="rwm", temperatures=None,
+                   swap_every=None, gamma=None, de_noise=1e-3, de_every=None, de_sync=False,
+                   seed=1, backend="b200", rng="triple32") -> GpumFit:
+    """Run the batched Metropolis sampler on the B200 backend (``R/api.R:247-599``)."""
+    if not isinstance(model, GpumModel):
+        raise GpumInputError("`model` must be a gpum_model from gpum_model().")
+    if backend not in ("b200", "auto"):
+        raise GpumInputError(f"backend '{backend}' is not available in this build. "
+                             "Available: b200")
+    if method not in ("rwm", "pt", "de", "mala"):
+        raise GpumInputError("`method` must be one of rwm, pt, de, mala")
+    rng_kind = {"triple32": _native.RNG_TRIPLE32, "philox": _native.RNG_PHILOX}[rng]
+    data_mat, n_obs = _data_matrix(model, data)
+    npar = model.n_params
+    if init is None:
+        n_chains = int(n_chains)
+        g = np.random.Generator(np.random.PCG64(int(seed)))
+        init_mat = g.standard_normal((n_chains, npar))
+    else:
+        init_mat = np.asarray(init, dtype=np.float64)
+        if init_mat.ndim == 1:
+            init_mat = init_mat.reshape(-1, 1) if npar == 1 else init_mat.reshape(1, -1)
+        if init_mat.shape[1] != npar:
+            raise GpumInputError(f"`init` must have one column per parameter ({npar}).")
+        n_chains = init_mat.shape[0]
+    n_iter = int(n_iter)
+    warmup_auto = isinstance(warmup, str) and warmup == "auto"
+    if warmup is None or warmup_auto:
+        warmup = n_iter // 2
+    warmup = int(warmup)
+    if warmup < 0 or warmup >= n_iter:
+        raise GpumInputError("`warmup` must be a non-negative integer strictly less than "
+                             "`n_iter`.")
+    psd = np.asarray(proposal_sd, dtype=np.float64)
+    if psd.ndim == 2:
+        if psd.shape != (n_chains, npar):
+            raise GpumInputError(f"`proposal_sd` matrix must be `n_chains` by `n_params` "
+                                 f"({n_chains} by {npar}).")
+        sd_mat = psd.copy()
+    else:
+        sd_mat = np.tile(np.resize(psd.ravel(), npar), (n_chains, 1))
+    if not np.all(np.isfinite(sd_mat)) or np.any(sd_mat <= 0):
+        raise GpumInputError("`proposal_sd` must be positive and finite.")
+
+    call = _Backend(model, data_mat, n_obs, rng_kind)
+    try:
+        return _route(model, call, method, npar, n_chains, init_mat, sd_mat, n_iter, warmup,
+                      warmup_auto, adapt, temperatures, swap_every, gamma, de_noise, de_every,
+                      de_sync, int(seed), backend)
+    finally:
+        call.close()
+
+
+def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmup_auto, adapt,
+           temperatures, swap_every, gamma, de_noise, de_every, de_sync, seed, backend):
+    if method == "pt":
+        if temperatures is None:
+            temps = AD.pt_default_ladder(C)
+        else:
+            temps = np.asarray(temperatures, dtype=np.float64).ravel()
+            if temps.size != C:
+                raise GpumInputError("`temperatures` must have one value per chain.")
+            if not np.all(np.isfinite(temps)) or np.any(temps <= 0):
+                raise GpumInputError("`temperatures` must be positive and finite.")
+        if swap_every is None:
+            swap_every = max(C, 10)
+        r = AD.pt_orchestrate(call, npar, C, init_mat, sd_mat, temps, n_iter, warmup,
+                              int(swap_every), bool(adapt), seed)
+        return GpumFit(r.draws, r.accept_rate, model, r.draws.shape[0],
+                       r.warmup_used + r.draws.shape[0], r.warmup_used, C, npar, backend, seed,
+                       "pt", {"final_proposal_sd": r.final_proposal_sd,
+                              "final_scales": r.final_scales, "n_batches": r.n_batches,
+                              "batch_sizes": r.batch_sizes, "accept_history": r.accept_history,
+                              "swap_history": r.swap_history},
+                       {"temperatures": temps, "swap_every": int(swap_every)})
+    if method == "de":
+        if C < 4:
+            raise GpumInputError('`method = "de"` needs at least 4 chains; the proposal draws '
+                                 "a distinct pair of other chains for each difference vector. "
+                                 "Increase `n_chains`.")
+        g = 2.38 / np.sqrt(2 * npar) if gamma is None else float(gamma)
+        if not np.isfinite(g) or g <= 0:
+            raise GpumInputError("`gamma` must be positive and finite.")
+        dn = float(de_noise)
+        if not np.isfinite(dn) or dn < 0:
+            raise GpumInputError("`de_noise` must be non-negative and finite.")
+        if de_every is None:
+            de_every = max(C, 10)
+        if de_sync:
+            raise GpumInputError("`de_sync = TRUE` (synchronous per-generation DE) is not "
+                                 "available on the b200 backend in this build.")
+        r = AD.de_orchestrate(call, npar, C, init_mat, sd_mat, g, dn, n_iter, warmup,
+                              int(de_every), bool(adapt), seed)
+        return GpumFit(r.draws, r.accept_rate, model, r.draws.shape[0],
+                       r.warmup_used + r.draws.shape[0], r.warmup_used, C, npar, backend, seed,
+                       "de", {"final_proposal_sd": r.final_proposal_sd,
+                              "n_batches": r.n_batches, "batch_sizes": r.batch_sizes,
+                              "accept_history": r.accept_history,
+                              "disp_history": r.disp_history},
+                       {"gamma": g, "de_noise": dn, "de_every": int(de_every)})
+    langevin = method == "mala"
+    if adapt and warmup > 0:
+        am = AD.am_orchestrate_warmup(call, npar, C, init_mat, sd_mat, warmup, seed,
+                                      auto_stop=warmup_auto, langevin=langevin)
+        samp = max(1, n_iter - am.warmup_used)
+        use_L = npar > 1 and am.final_L is not None
+        draws, acc, _ = call(am.final_init, am.final_proposal_sd, samp, am.seed_next, None,
+                             3 if langevin else (2 if use_L else 0), 0.0, 0.0,
+                             am.final_L if use_L else None)
+        return GpumFit(draws, acc, model, samp, am.warmup_used + samp, am.warmup_used, C, npar,
+                       backend, seed, method,
+                       {"final_proposal_sd": am.final_proposal_sd,
+                        "final_scales": am.final_scales, "n_batches": am.n_batches,
+                        "batch_sizes": am.batch_sizes, "accept_history": am.accept_history})
+    draws, acc, _ = call(init_mat, sd_mat, n_iter, seed, None, 3 if langevin else 0)
+    kept = draws[warmup:] if warmup > 0 else draws
+    return GpumFit(kept, acc, model, n_iter - warmup, n_iter, warmup, C, npar, backend, seed,
+                   method)

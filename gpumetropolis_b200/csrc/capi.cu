@@ -627,6 +627,10 @@ void gpum_b200_session_destroy(gpum_b200_session* s) {
 
 uint64_t gpum_b200_session_launches(const gpum_b200_session* s) { return s ? s->launches : 0; }
 
+void* gpum_b200_session_stream(const gpum_b200_session* s) {
+  return s ? (void*)s->stream : nullptr;
+}
+
 int gpum_b200_session_prepare(gpum_b200_session* s, const double* init, const double* sd,
                               const double* temps, uint32_t n_chains, uint32_t max_iter,
                               uint32_t seed, uint32_t mode, double gamma, double de_noise,

@@ -144,6 +144,10 @@ GPUM_API int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, flo
                             double* out_last_logpost, uint32_t* n_done, char* err,
                             size_t err_len);
 
+/* The session's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events with the session's launches. */
+GPUM_API void* gpum_b200_session_stream(const gpum_b200_session* s);
+
 /* Kernel launches issued by this session so far (every node of a replayed
  * graph counts once per replay). */
 GPUM_API uint64_t gpum_b200_session_launches(const gpum_b200_session* s);

@@ -83,7 +83,11 @@ def test_interpreter_variants_by_depth(gpu, depth):
     pts = np.array([[0.5, 1.5], [-0.25, 2.0], [1.0, -1.0]])
     ref = O.loglik_batch(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
     got = gpu.loglik_batch(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
-    np.testing.assert_allclose(got, ref, rtol=1e-6)
+    # these sums cancel (terms of both signs): bound the error by the sum of
+    # |per-observation values|, the condition of an FP32-per-observation sum
+    pw = O.loglik_pointwise(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
+    scale = np.abs(pw.reshape(3, -1)).sum(axis=1)
+    assert np.all(np.abs(got - ref) <= 1e-6 * scale)
 
 
 def test_every_opcode_and_edge_sizes(gpu, golden):
@@ -132,4 +136,5 @@ def test_session_reuse_and_determinism(gpu):
         b = s.loglik_batch(pts)
         c = s.loglik_batch(pts[:3])
     assert np.array_equal(a, b)        # fixed-order reductions: bitwise repeatable
-    np.testing.assert_allclose(a[:3], c, rtol=1e-12)  # another launch geometry
+    # another launch geometry partitions the observations differently
+    np.testing.assert_allclose(a[:3], c, rtol=1e-9)
