@@ -59,6 +59,8 @@ def _args():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-interp", action="store_true")
+    p.add_argument("--engine", type=int, default=2, help="0 interpreter, 1 compiled, 2 auto")
     return p.parse_args()
 
 
@@ -200,7 +202,8 @@ def run_b200(a):
     K, Wm = a.steps, max(3, a.warmup)
 
     sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
-                           m.n_params, w.data, m.n_cols, w.n_obs)
+                           m.n_params, w.data, m.n_cols, w.n_obs, engine=a.engine)
+    engine = {0: "interpreter", 1: "compiled"}[sess.engine]
     sess.prepare(init, sd, temps, Wm + K, 1 + rank, 0, rng=_native.RNG_PHILOX)
     sess.advance(Wm)
     sess.sync()
@@ -262,6 +265,32 @@ def run_b200(a):
                 "bytes_per_launch": N * ROW_BYTES},
     }
 
+    # The interpreter engine on the same workload (a few steps, same timing).
+    interp = None
+    if rank == 0 and not a.no_interp:
+        si = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                             m.n_params, w.data, m.n_cols, w.n_obs, engine=_native.ENGINE_INTERP)
+        Ki = max(3, min(K, 10))
+        si.prepare(init, sd, temps, 3 + Ki, 1 + rank, 0, rng=_native.RNG_PHILOX)
+        si.advance(3)
+        si.sync()
+        st_i = torch.cuda.ExternalStream(si.stream, device=dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(Ki)]
+        with torch.cuda.stream(st_i):
+            for s0, s1 in ev:
+                flush.zero_()
+                s0.record(st_i)
+                si.advance(1)
+                s1.record(st_i)
+        torch.cuda.synchronize()
+        ms_i = float(np.mean([s0.elapsed_time(s1) for s0, s1 in ev]))
+        si.close()
+        interp = {"value": C * N / (ms_i / 1e3), "unit": UNIT, "ms_per_step": ms_i,
+                  "steps": Ki,
+                  "fp32_frac": round(C * N * FLOP_PER_CHAIN_OBS / (ms_i / 1e3) / 1e12
+                                     / fp32_peak, 4)}
+
     e2e = None
     if rank == 0 and not a.no_e2e:
         init2, sd2, temps2 = _init(w, C, seed=7)
@@ -297,6 +326,7 @@ def run_b200(a):
                    "bytecode_instructions": m.loglik.n_instr,
                    "l2": "flushed (256 MiB write) before every timed step",
                    "rng": "philox", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "engine": engine, "interpreter_engine": interp,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clocks, "wall_s_timed_region": wall,
         "accept_rate_mean": float(np.mean(acc)),

@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgpum_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE, ERR_DEVICE = range(7)
+ENGINE_INTERP, ENGINE_COMPILED, ENGINE_AUTO = 0, 1, 2
 MODE_RWM, MODE_DE, MODE_CHOL, MODE_MALA = 0, 1, 2, 3
 RNG_TRIPLE32, RNG_PHILOX = 0, 1
 _ERRLEN = 1024
@@ -56,6 +57,14 @@ SIGNATURES = {
     "gpum_b200_loglik_pointwise": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p,
                                              C.c_uint32, C.c_uint64, _f64p, _sz, _f64p, _errp,
                                              _sz]),
+    "gpum_b200_grad_batch": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p,
+                                       C.c_uint32, C.c_uint64, _f64p, _sz, _f64p, _errp, _sz]),
+    "gpum_b200_compile_check": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz,
+                                          C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t), _errp,
+                                          _sz]),
+    "gpum_b200_session_set_engine": (C.c_int, [C.c_void_p, C.c_int, _errp, _sz]),
+    "gpum_b200_session_engine": (C.c_int, [C.c_void_p]),
+    "gpum_b200_session_grad_batch": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
     "gpum_b200_session_create": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz,
                                            C.c_uint32, _f64p, C.c_uint32, C.c_uint64,
                                            C.POINTER(C.c_void_p), _errp, _sz]),
@@ -185,10 +194,31 @@ def loglik_pointwise(code, consts, n_params, data, n_cols, n_obs, points):
                   points, n_obs)
 
 
+def grad_batch(code, consts, n_params, data, n_cols, n_obs, points):
+    """Point-major gradient of the data term (``gpum_b200_grad_batch``)."""
+    return _batch("gpum_b200_grad_batch", code, consts, n_params, data, n_cols, n_obs,
+                  points, n_params)
+
+
+def compile_check(code, consts, prior_code, prior_consts, n_params, n_cols) -> int:
+    """NVRTC-build the compiled engine for a model (no GPU needed); returns
+    the module size in bytes."""
+    code, pcode = _u32(code), _u32(prior_code)
+    consts, pconsts = _f64(consts), _f64(prior_consts)
+    nbytes = C.c_size_t(0)
+    err = C.create_string_buffer(8192)
+    _check(load().gpum_b200_compile_check(
+        _p(code, C.c_uint32), code.size, _p(consts, C.c_double), consts.size,
+        _p(pcode, C.c_uint32), pcode.size, _p(pconsts, C.c_double), pconsts.size, n_params,
+        n_cols, C.byref(nbytes), err, 8192), err)
+    return nbytes.value
+
+
 class Session:
     """A model + data resident on the GPU (``gpum_b200_session_*``)."""
 
-    def __init__(self, code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs):
+    def __init__(self, code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs,
+                 engine=ENGINE_AUTO):
         self._lib = load()
         code, pcode = _u32(code), _u32(prior_code)
         consts, pconsts = _f64(consts), _f64(prior_consts)
@@ -203,6 +233,8 @@ class Session:
         _check(rc, err)
         self._h = h
         self.n_chains = 0
+        if engine != ENGINE_AUTO:
+            self.set_engine(engine)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -290,6 +322,23 @@ class Session:
         _check(self._lib.gpum_b200_session_loglik_batch(self._h, _p(pts, C.c_double), n,
                                                         _p(out, C.c_double), err, _ERRLEN), err)
         return out[:n]
+
+    def set_engine(self, engine: int):
+        err = C.create_string_buffer(8192)
+        _check(self._lib.gpum_b200_session_set_engine(self._h, engine, err, 8192), err)
+
+    @property
+    def engine(self) -> int:
+        return int(self._lib.gpum_b200_session_engine(self._h))
+
+    def grad_batch(self, points):
+        pts = _f64(points)
+        n = pts.size // self.n_params
+        out = np.empty(max(n * self.n_params, 1))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_grad_batch(self._h, _p(pts, C.c_double), n,
+                                                      _p(out, C.c_double), err, _ERRLEN), err)
+        return out[: n * self.n_params]
 
     def loglik_pointwise(self, points):
         pts = _f64(points)

@@ -14,8 +14,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpum_b200.so")
-SOURCES = ["capi.cu", "program.cpp"]
-HEADERS = ["device.cuh", "interp.cuh", "kernels.cuh", "program.hpp"]
+SOURCES = ["capi.cu", "program.cpp", "codegen.cpp", "jit.cpp"]
+HEADERS = ["device.cuh", "interp.cuh", "kernels.cuh", "common.cuh", "compiled.cuh",
+           "program.hpp", "codegen.hpp", "jit.hpp"]
+# Headers the compiled engine hands to NVRTC at run time, embedded as strings.
+EMBED = [("kEmbeddedDevice", "device.cuh"), ("kEmbeddedCommon", "common.cuh"),
+         ("kEmbeddedCompiled", "compiled.cuh")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -39,15 +43,31 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def write_embedded() -> str:
+    """Write csrc/_embedded.inc: the NVRTC headers as raw string literals."""
+    out = os.path.join(CSRC, "_embedded.inc")
+    parts = ["// generated by build.py from the kernel headers; do not edit\n"]
+    for name, fn in EMBED:
+        src = open(os.path.join(CSRC, fn)).read()
+        assert ")GPUMSRC\"" not in src
+        parts.append(f'static const char* {name} = R"GPUMSRC({src})GPUMSRC";\n')
+    text = "".join(parts)
+    if not os.path.exists(out) or open(out).read() != text:
+        with open(out, "w") as f:
+            f.write(text)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
+    write_embedded()
     tmp = LIB + f".{os.getpid()}.tmp"
     cmd = [nvcc(), *host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
            "--shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
            "-I", os.path.join(ROOT, "include"), "-o", tmp]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-lcudart"]
+    cmd += ["-lcudart", "-ldl"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

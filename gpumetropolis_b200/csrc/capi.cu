@@ -1,11 +1,20 @@
 // capi.cu -- host side of the B200 backend: sessions (model + data resident
-// in HBM), launch geometry, CUDA-graph replay of the iteration loop, and the
-// extern "C" entry points declared in include/gpum_b200.h.
+// in HBM), the two evaluation engines, launch geometry, CUDA-graph replay of
+// the iteration loop, and the extern "C" entry points of include/gpum_b200.h.
 //
 // Replaces the reference's per-call CubeCL client + upload + launch +
 // readback (src/rust/src/chain_kernel.rs:372-463) and its backend dispatch
 // (chain_kernel.rs:469-532).  No entry point throws across the ABI: every
 // failure becomes a status code and a message.
+//
+// Engines:
+//   interpreter -- the register-stack bytecode interpreter (interp.cuh), the
+//                  micro-op stream in the constant bank; compiled ahead of
+//                  time, works for every valid program;
+//   compiled    -- the program translated to straight-line CUDA C
+//                  (codegen.cpp) and built by NVRTC for sm_100a at session
+//                  creation (jit.cpp); required for gradients (MALA,
+//                  grad_batch).
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -19,10 +28,14 @@
 #include <vector>
 
 #include "../../include/gpum_b200.h"
+#include "codegen.hpp"
+#include "jit.hpp"
 #include "kernels.cuh"
 #include "program.hpp"
 
 using namespace gpum;
+
+static_assert(sizeof(CUtensorMap) == sizeof(TmapDesc), "tensor map size");
 
 namespace {
 
@@ -82,12 +95,12 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// Interpreter variants by peak stack depth: registers are spent on depth or
-// on chains per thread.
+// Interpreter variants by peak stack depth: registers go to depth or to
+// chains per thread.
 enum Variant { V8x8 = 0, V4x16 = 1, V2x32 = 2 };
 int variant_G(int v) { return v == V8x8 ? 8 : (v == V4x16 ? 4 : 2); }
 
-const void* kernel_ptr(int v) {
+const void* interp_kernel(int v) {
   switch (v) {
     case V8x8: return (const void*)iter_kernel<8, 8>;
     case V4x16: return (const void*)iter_kernel<4, 16>;
@@ -95,8 +108,8 @@ const void* kernel_ptr(int v) {
   }
 }
 
-void launch_iter(int v, dim3 grid, size_t smem, cudaStream_t st, const EvalProg& prog,
-                 const CUtensorMap& tmap, const EvalArgs& E, const ChainArgs& A, int phase) {
+void launch_interp(int v, dim3 grid, size_t smem, cudaStream_t st, const EvalProg& prog,
+                   const TmapDesc& tmap, const EvalArgs& E, const ChainArgs& A, int phase) {
   switch (v) {
     case V8x8: iter_kernel<8, 8><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
     case V4x16: iter_kernel<4, 16><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
@@ -116,6 +129,14 @@ int num_sms() {
   return n;
 }
 
+// Which kernel evaluates the current run or batch.
+struct KernelChoice {
+  bool compiled = false;
+  const void* fn = nullptr;  // __global__ pointer or cudaKernel_t
+  int G = 8;                 // chains per thread
+  int W = 1;                 // values per chain (1, or 1 + np with the gradient)
+};
+
 struct Geometry {
   int G, WC, CG, NCB, C_pad, NOB, tiles_per_cta, ntiles;
   size_t smem;
@@ -127,6 +148,11 @@ struct gpum_b200_session {
   cudaStream_t stream = nullptr;
   UProg ll;
   std::unique_ptr<EvalProg> prog;
+  GenModel gm;
+  CompiledModel cm;
+  bool cm_ready = false;
+  std::string cm_error;
+  int engine = GPUM_ENGINE_AUTO;
   std::vector<uint32_t> prior_code;
   std::vector<double> prior_consts;
   uint32_t np = 0, ncols = 0;
@@ -135,17 +161,18 @@ struct gpum_b200_session {
   int T = 256;
   int64_t ld = 0;
   DBuf<float> data;
-  CUtensorMap tmap;
+  TmapDesc tmap;
   DBuf<uint32_t> d_prior_code;
   DBuf<double> d_prior_consts;
   DBuf<uint32_t> d_err;
   // run state
+  KernelChoice kc;
   Geometry geo{};
   int n_chains = 0;
   uint32_t max_iter = 0, n_done = 0;
   bool prepared = false;
   DBuf<double> state, prop, cur, last_eval, sd, temp, L, snap, zbuf, partials, pointwise,
-      points, out64;
+      points, out64, gx, gy, mx, my, vbuf;
   DBuf<float> params, draws, draws_out;
   DBuf<uint32_t> ctr, accepts, iter, tickets;
   EvalArgs E{};
@@ -156,14 +183,57 @@ struct gpum_b200_session {
   uint64_t launches = 0;
 
   ~gpum_b200_session() {
-    if (gexec) cudaGraphExecDestroy(gexec);
-    if (graph) cudaGraphDestroy(graph);
+    drop_graph();
     if (stream) cudaStreamDestroy(stream);
   }
 
-  Geometry geometry(int n) const {
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+  }
+
+  // Builds the compiled engine once; false (with cm_error) when NVRTC is
+  // unavailable or the build fails.
+  bool compiled_available() {
+    if (cm_ready) return true;
+    if (!cm_error.empty()) return false;
+    std::string e;
+    if (jit_compile(gm, &cm, &e)) {
+      cm_error = e.empty() ? "compiled engine unavailable" : e;
+      return false;
+    }
+    cm_ready = true;
+    return true;
+  }
+
+  KernelChoice choose(bool need_grad) {
+    KernelChoice k;
+    const bool want_compiled =
+        need_grad || engine == GPUM_ENGINE_COMPILED ||
+        (engine == GPUM_ENGINE_AUTO && compiled_available());
+    if (want_compiled) {
+      if (!compiled_available())
+        throw Failure{GPUM_ERR_UNSUPPORTED,
+                      std::string(need_grad ? "gradients need" : "engine=compiled needs") +
+                          " the compiled engine: " + cm_error};
+      k.compiled = true;
+      k.fn = need_grad ? (const void*)cm.k_grad : (const void*)cm.k_value;
+      k.G = need_grad ? cm.GG : cm.G;
+      k.W = need_grad ? 1 + (int)np : 1;
+    } else {
+      k.compiled = false;
+      k.fn = interp_kernel(variant);
+      k.G = variant_G(variant);
+      k.W = 1;
+    }
+    return k;
+  }
+
+  Geometry geometry(int n, const KernelChoice& k) const {
     Geometry g{};
-    g.G = variant_G(variant);
+    g.G = k.G;
     const int groups = (n + g.G - 1) / g.G;
     g.WC = 1;
     while (g.WC < kWarps && g.WC < groups) g.WC *= 2;
@@ -171,11 +241,9 @@ struct gpum_b200_session {
     g.NCB = (n + g.CG - 1) / g.CG;
     g.C_pad = g.NCB * g.CG;
     g.ntiles = (int)((n_obs + T - 1) / T);
-    const size_t stage = (size_t)T * ncols * sizeof(float);
-    const size_t pbytes = (((size_t)np * g.CG + 3) & ~(size_t)3) * sizeof(float);
-    g.smem = 2 * stage + pbytes + (size_t)kWarps * g.G * sizeof(double) + 2 * 8 + 16;
+    g.smem = skel_smem_bytes(T, (int)ncols, (int)np, g.CG, g.G, k.W);
     int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_ptr(variant), kThreads, g.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
     if (occ < 1) occ = 1;
     const int slots = num_sms() * occ;
     int nob = std::max(1, (4 * slots) / g.NCB);
@@ -196,15 +264,15 @@ struct gpum_b200_session {
     }
   }
 
-  // Evaluation-argument block for `n` points whose f32 params live in `params`.
-  void setup_eval(int n) {
-    geo = geometry(n);
-    const size_t smax = geo.smem;
-    if (smax > 48 * 1024)
-      GPUM_CK(cudaFuncSetAttribute(kernel_ptr(variant),
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  // Evaluation-argument block for `n` points (params in `params`).
+  void setup_eval(int n, bool need_grad) {
+    kc = choose(need_grad);
+    geo = geometry(n, kc);
+    if (geo.smem > 48 * 1024)
+      GPUM_CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)geo.smem));
     params.ensure((size_t)np * geo.C_pad);
-    partials.ensure((size_t)geo.NOB * geo.C_pad);
+    partials.ensure((size_t)geo.NOB * geo.C_pad * kc.W);
     tickets.ensure(geo.NCB);
     GPUM_CK(cudaMemsetAsync(tickets.p, 0, sizeof(uint32_t) * geo.NCB, stream));
     E = EvalArgs{};
@@ -217,6 +285,7 @@ struct gpum_b200_session {
     E.WC = geo.WC;
     E.C_pad = geo.C_pad;
     E.np = (int)np;
+    E.width = kc.W;
     E.params = params.p;
     E.partials = partials.p;
     E.n_points = n;
@@ -236,7 +305,13 @@ struct gpum_b200_session {
   }
 
   void launch(int phase) {
-    launch_iter(variant, dim3(geo.NOB, geo.NCB), geo.smem, stream, *prog, tmap, E, A, phase);
+    const dim3 grid(geo.NOB, geo.NCB);
+    if (kc.compiled) {
+      void* args[] = {(void*)&tmap, (void*)&E, (void*)&A, (void*)&phase};
+      GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, geo.smem, stream));
+    } else {
+      launch_interp(variant, grid, geo.smem, stream, *prog, tmap, E, A, phase);
+    }
     ++launches;
   }
 };
@@ -267,8 +342,10 @@ void require(bool ok, const std::string& m, int code = GPUM_ERR_INVALID) {
 
 void require_device() {
   int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+    cudaGetLastError();
     throw Failure{GPUM_ERR_NODEVICE, "no CUDA device is visible"};
+  }
   int dev = 0, major = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
@@ -278,24 +355,36 @@ void require_device() {
                       std::to_string(major) + ".x"};
 }
 
-gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const double* consts,
-                                  size_t n_consts, const uint32_t* prior_code, size_t n_prior,
-                                  const double* prior_consts, size_t n_prior_consts,
-                                  uint32_t n_params, const double* data, uint32_t n_cols,
-                                  uint64_t n_obs) {
+// Validation and code generation shared by sessions and the compile check.
+void check_model(const uint32_t* code, size_t n_code, const double* consts, size_t n_consts,
+                 const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
+                 size_t n_prior_consts, uint32_t n_params, uint32_t n_cols, UProg* ll,
+                 GenModel* gm) {
   require(n_params >= 1, "n_params must be at least 1");
   require(n_params <= 256, "more than 256 parameters", GPUM_ERR_UNSUPPORTED);
   require(n_cols <= 256, "more than 256 data columns", GPUM_ERR_UNSUPPORTED);
-  require(n_obs < (1ull << 31) - 1024, "more than 2^31 observations", GPUM_ERR_UNSUPPORTED);
-  require(n_obs == 0 || n_cols == 0 || data != nullptr, "data pointer is NULL");
-  std::unique_ptr<gpum_b200_session> s(new gpum_b200_session());
   std::string msg;
-  if (compile_program(code, n_code, consts, n_consts, n_params, n_cols, true, &s->ll, &msg))
+  if (compile_program(code, n_code, consts, n_consts, n_params, n_cols, true, ll, &msg))
     throw Failure{GPUM_ERR_INVALID, "log-likelihood bytecode: " + msg};
   int pdepth = 0;
   if (validate_program(prior_code, n_prior, n_prior_consts, n_params, 0, false, &pdepth, &msg))
     throw Failure{GPUM_ERR_INVALID, "prior bytecode: " + msg};
   require(n_prior_consts == 0 || prior_consts != nullptr, "prior constant pointer is NULL");
+  if (generate_model(code, n_code, consts, prior_code, n_prior, prior_consts, n_params, n_cols,
+                     gm, &msg))
+    throw Failure{GPUM_ERR_INVALID, "code generation: " + msg};
+}
+
+gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const double* consts,
+                                  size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                                  const double* prior_consts, size_t n_prior_consts,
+                                  uint32_t n_params, const double* data, uint32_t n_cols,
+                                  uint64_t n_obs) {
+  require(n_obs < (1ull << 31) - 1024, "more than 2^31 observations", GPUM_ERR_UNSUPPORTED);
+  require(n_obs == 0 || n_cols == 0 || data != nullptr, "data pointer is NULL");
+  std::unique_ptr<gpum_b200_session> s(new gpum_b200_session());
+  check_model(code, n_code, consts, n_consts, prior_code, n_prior, prior_consts, n_prior_consts,
+              n_params, n_cols, &s->ll, &s->gm);
   require_device();
 
   s->np = n_params;
@@ -325,7 +414,7 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
   // Observations per tile: a multiple of 32 (one per lane), <= 256 (TMA box
   // limit), with a stage of at most 32 KB.
   if (n_cols > 0) {
-    int T = (int)((8192 / n_cols) / 32 * 32);
+    const int T = (int)((8192 / n_cols) / 32 * 32);
     s->T = std::max(32, std::min(256, T));
   } else {
     s->T = 256;
@@ -349,16 +438,18 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
       GPUM_CK(cudaGetLastError());
     }
     GPUM_CK(cudaStreamSynchronize(s->stream));
+    CUtensorMap tm;
     cuuint64_t gdim[2] = {(cuuint64_t)n_obs, (cuuint64_t)n_cols};
     cuuint64_t gstride[1] = {(cuuint64_t)s->ld * sizeof(float)};
     cuuint32_t box[2] = {(cuuint32_t)s->T, (cuuint32_t)n_cols};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&s->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->data.p, gdim,
-                             gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->data.p, gdim, gstride,
+                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
       throw Failure{GPUM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")"};
+    std::memcpy(&s->tmap, &tm, sizeof tm);
   }
   return s.release();
 }
@@ -370,27 +461,23 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   require(C >= 1, "n_chains must be at least 1");
   require(init && sd && temps, "init, proposal_sd and temperatures must be non-NULL");
   require(mode <= 3, "proposal_mode must be 0 (rwm), 1 (de), 2 (cholesky) or 3 (mala)");
-  require(mode != 3, "proposal_mode 3 (MALA) is not implemented by this backend build",
-          GPUM_ERR_UNSUPPORTED);
   require(rng == GPUM_RNG_TRIPLE32 || rng == GPUM_RNG_PHILOX, "rng must be 0 or 1");
   const size_t np = s->np;
+  const bool mala = mode == 3;
+  const bool use_L = mode == 2 || (mala && L != nullptr && n_l > 0);
   if (mode == 2)
     require(L != nullptr && n_l == (size_t)C * np * np,
             "proposal_mode 2 needs proposal_l of n_chains*n_params^2 values");
+  if (mala && use_L)
+    require(n_l == (size_t)C * np * np, "proposal_l must hold n_chains*n_params^2 values");
   require(C <= (1u << 24), "more than 2^24 chains", GPUM_ERR_UNSUPPORTED);
   require((uint64_t)max_iter * np * C <= (1ull << 33), "draw storage above 32 GiB",
           GPUM_ERR_UNSUPPORTED);
 
-  if (s->gexec) {
-    cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
-  }
-  if (s->graph) {
-    cudaGraphDestroy(s->graph);
-    s->graph = nullptr;
-  }
+  s->drop_graph();
+  s->prepared = false;
   s->n_chains = (int)C;
-  s->setup_eval((int)C);
+  s->setup_eval((int)C, mala);
   const Geometry& g = s->geo;
   s->state.ensure(C * np);
   s->prop.ensure(C * np);
@@ -404,14 +491,21 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   s->accepts.ensure(C);
   s->iter.ensure(g.NCB);
   s->draws.ensure(std::max<size_t>(1, (size_t)max_iter * np * g.C_pad));
-  if (mode == 2) s->L.ensure((size_t)C * np * np);
+  if (use_L) s->L.ensure((size_t)C * np * np);
+  if (mala) {
+    s->gx.ensure(C * np);
+    s->gy.ensure(C * np);
+    s->mx.ensure(C * np);
+    s->my.ensure(C * np);
+    s->vbuf.ensure(C * np);
+  }
   cudaStream_t st = s->stream;
   GPUM_CK(cudaMemcpyAsync(s->state.p, init, sizeof(double) * C * np, cudaMemcpyHostToDevice, st));
   GPUM_CK(cudaMemcpyAsync(s->snap.p, s->state.p, sizeof(double) * C * np,
                           cudaMemcpyDeviceToDevice, st));
   GPUM_CK(cudaMemcpyAsync(s->sd.p, sd, sizeof(double) * C * np, cudaMemcpyHostToDevice, st));
   GPUM_CK(cudaMemcpyAsync(s->temp.p, temps, sizeof(double) * C, cudaMemcpyHostToDevice, st));
-  if (mode == 2)
+  if (use_L)
     GPUM_CK(cudaMemcpyAsync(s->L.p, L, sizeof(double) * C * np * np, cudaMemcpyHostToDevice, st));
   GPUM_CK(cudaMemsetAsync(s->ctr.p, 0, sizeof(uint32_t) * C, st));
   GPUM_CK(cudaMemsetAsync(s->accepts.p, 0, sizeof(uint32_t) * C, st));
@@ -435,12 +529,12 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   A.iter = s->iter.p;
   A.sd = s->sd.p;
   A.temp = s->temp.p;
-  A.L = mode == 2 ? s->L.p : nullptr;
+  A.L = use_L ? s->L.p : nullptr;
   A.snap = s->snap.p;
   A.draws = s->draws.p;
   A.n_iter = max_iter;
   A.seed = seed;
-  A.mode = (int)(mode == 0 || mode == 2 ? mode : 1);
+  A.mode = mode == 0 ? MODE_RWM : (mode == 2 ? MODE_CHOL : (mala ? MODE_MALA : MODE_DE));
   A.rng = rng;
   A.gamma = gamma;
   A.de_noise = de_noise;
@@ -448,6 +542,13 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   A.prior_consts = s->d_prior_consts.p;
   A.n_prior = (int)(s->prior_code.size() / 2);
   A.zbuf = s->zbuf.p;
+  if (mala) {
+    A.gx = s->gx.p;
+    A.gy = s->gy.p;
+    A.mx = s->mx.p;
+    A.my = s->my.p;
+    A.vbuf = s->vbuf.p;
+  }
   s->launch(PH_INIT);
   s->max_iter = max_iter;
   s->n_done = 0;
@@ -462,15 +563,14 @@ void advance(gpum_b200_session* s, uint32_t n) {
   if (n >= (uint32_t)kGraphLen && !s->gexec) {
     GPUM_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     try {
-      for (int i = 0; i < kGraphLen; ++i)
-        launch_iter(s->variant, dim3(s->geo.NOB, s->geo.NCB), s->geo.smem, s->stream, *s->prog,
-                    s->tmap, s->E, s->A, PH_STEP);
+      for (int i = 0; i < kGraphLen; ++i) s->launch(PH_STEP);
     } catch (...) {
-      cudaGraph_t g;
+      cudaGraph_t g = nullptr;
       cudaStreamEndCapture(s->stream, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
+    s->launches -= kGraphLen;  // counted per replay below
     GPUM_CK(cudaStreamEndCapture(s->stream, &s->graph));
     GPUM_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
     s->graph_len = kGraphLen;
@@ -514,30 +614,26 @@ void fetch(gpum_b200_session* s, float* out_draws, float* out_accept, double* ou
     for (int c = 0; c < C; ++c) out_accept[c] = n == 0 ? 0.0f : (float)acc[c] / (float)n;
 }
 
-void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out, bool pointwise) {
+enum BatchKind { B_SUM = 0, B_POINTWISE = 1, B_GRAD = 2 };
+
+void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out, int kind) {
   require(s != nullptr, "session is NULL");
   require(out != nullptr || n_points == 0, "output pointer is NULL");
   require(pts != nullptr || n_points == 0, "points pointer is NULL");
   if (n_points == 0) return;
   require(n_points <= (1u << 24), "more than 2^24 points", GPUM_ERR_UNSUPPORTED);
-  s->prepared = false;  // the eval buffers are reused
-  if (s->gexec) {
-    cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
-  }
-  if (s->graph) {
-    cudaGraphDestroy(s->graph);
-    s->graph = nullptr;
-  }
+  s->prepared = false;  // the evaluation buffers are reused
+  s->drop_graph();
+  const size_t np = s->np;
   size_t chunk = n_points;
-  if (pointwise && s->n_obs > 0)
+  if (kind == B_POINTWISE && s->n_obs > 0)
     chunk = std::max<size_t>(1, std::min<size_t>(n_points, (size_t)(1ull << 27) / s->n_obs));
   for (size_t p0 = 0; p0 < n_points; p0 += chunk) {
     const int n = (int)std::min(chunk, n_points - p0);
-    s->setup_eval(n);
-    s->upload_points(pts + p0 * s->np, n);
+    s->setup_eval(n, kind == B_GRAD);
+    s->upload_points(pts + p0 * np, n);
     s->A = ChainArgs{};
-    if (pointwise) {
+    if (kind == B_POINTWISE) {
       if (s->n_obs == 0) continue;
       s->pointwise.ensure((size_t)n * s->n_obs);
       s->E.pointwise = s->pointwise.p;
@@ -549,23 +645,31 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
       GPUM_CK(cudaMemcpyAsync(out + p0 * s->n_obs, s->pointwise.p,
                               sizeof(double) * n * s->n_obs, cudaMemcpyDeviceToHost, s->stream));
     } else {
-      s->out64.ensure(n);
+      const int W = s->kc.W;
+      s->out64.ensure((size_t)n * W);
       if (s->ll.empty()) {
-        GPUM_CK(cudaMemsetAsync(s->out64.p, 0, sizeof(double) * n, s->stream));
+        GPUM_CK(cudaMemsetAsync(s->out64.p, 0, sizeof(double) * n * W, s->stream));
       } else {
         s->launch(PH_EVAL);
-        reduce_partials_kernel<<<(n + 255) / 256, 256, 0, s->stream>>>(s->partials.p,
-                                                                        s->out64.p, s->geo.NOB,
-                                                                        s->geo.C_pad, n);
+        reduce_partials_kernel<<<(n * W + 255) / 256, 256, 0, s->stream>>>(
+            s->partials.p, s->out64.p, s->geo.NOB, s->geo.C_pad, n, W);
         GPUM_CK(cudaGetLastError());
         ++s->launches;
       }
-      GPUM_CK(cudaMemcpyAsync(out + p0, s->out64.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                              s->stream));
+      if (kind == B_GRAD) {
+        std::vector<double> tmp((size_t)n * W);
+        GPUM_CK(cudaMemcpyAsync(tmp.data(), s->out64.p, sizeof(double) * n * W,
+                                cudaMemcpyDeviceToHost, s->stream));
+        GPUM_CK(cudaStreamSynchronize(s->stream));
+        for (int p = 0; p < n; ++p)
+          for (size_t j = 0; j < np; ++j) out[(p0 + p) * np + j] = tmp[(size_t)p * W + 1 + j];
+      } else {
+        GPUM_CK(cudaMemcpyAsync(out + p0, s->out64.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                s->stream));
+      }
     }
     s->check_device_error();
   }
-  if (pointwise && s->n_obs == 0) return;
 }
 
 }  // namespace
@@ -584,14 +688,14 @@ int gpum_b200_available(void) {
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   if (major != 10) return 0;
   cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, kernel_ptr(V8x8)) != cudaSuccess) {
+  if (cudaFuncGetAttributes(&fa, interp_kernel(V8x8)) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   return 1;
 }
 
-const char* gpum_b200_version(void) { return "gpum_b200 0.1.0 sm_100a"; }
+const char* gpum_b200_version(void) { return "gpum_b200 0.2.0 sm_100a"; }
 
 int gpum_b200_validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
                                uint32_t n_params, uint32_t n_cols, int allow_data, int* depth,
@@ -602,6 +706,21 @@ int gpum_b200_validate_program(const uint32_t* code, size_t n_code, size_t n_con
     if (validate_program(code, n_code, n_consts, n_params, n_cols, allow_data != 0, &d, &m))
       throw Failure{GPUM_ERR_INVALID, m};
     if (depth) *depth = d;
+  });
+}
+
+int gpum_b200_compile_check(const uint32_t* code, size_t n_code, const double* consts,
+                            size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                            const double* prior_consts, size_t n_prior_consts,
+                            uint32_t n_params, uint32_t n_cols, size_t* cubin_bytes, char* err,
+                            size_t err_len) {
+  return guard(err, err_len, [&] {
+    UProg ll;
+    GenModel gm;
+    check_model(code, n_code, consts, n_consts, prior_code, n_prior, prior_consts,
+                n_prior_consts, n_params, n_cols, &ll, &gm);
+    std::string m;
+    if (jit_compile_check(gm, cubin_bytes, &m)) throw Failure{GPUM_ERR_UNSUPPORTED, m};
   });
 }
 
@@ -617,6 +736,27 @@ int gpum_b200_session_create(const uint32_t* code, size_t n_code, const double* 
     *out = create_session(code, n_code, consts, n_consts, prior_code, n_prior, prior_consts,
                           n_prior_consts, n_params, data, n_cols, n_obs);
   });
+}
+
+int gpum_b200_session_set_engine(gpum_b200_session* s, int engine, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    require(engine == GPUM_ENGINE_INTERP || engine == GPUM_ENGINE_COMPILED ||
+                engine == GPUM_ENGINE_AUTO,
+            "engine must be 0 (interpreter), 1 (compiled) or 2 (auto)");
+    if (engine == GPUM_ENGINE_COMPILED && !s->compiled_available())
+      throw Failure{GPUM_ERR_UNSUPPORTED, "compiled engine unavailable: " + s->cm_error};
+    s->engine = engine;
+    s->drop_graph();
+    s->prepared = false;
+  });
+}
+
+int gpum_b200_session_engine(gpum_b200_session* s) {
+  if (!s) return -1;
+  if (s->engine == GPUM_ENGINE_AUTO)
+    return s->compiled_available() ? GPUM_ENGINE_COMPILED : GPUM_ENGINE_INTERP;
+  return s->engine;
 }
 
 void gpum_b200_session_destroy(gpum_b200_session* s) {
@@ -670,12 +810,17 @@ int gpum_b200_session_run(gpum_b200_session* s, const double* init, const double
 
 int gpum_b200_session_loglik_batch(gpum_b200_session* s, const double* points, size_t n_points,
                                    double* out, char* err, size_t err_len) {
-  return guard(err, err_len, [&] { batch(s, points, n_points, out, false); });
+  return guard(err, err_len, [&] { batch(s, points, n_points, out, B_SUM); });
 }
 
 int gpum_b200_session_loglik_pointwise(gpum_b200_session* s, const double* points,
                                        size_t n_points, double* out, char* err, size_t err_len) {
-  return guard(err, err_len, [&] { batch(s, points, n_points, out, true); });
+  return guard(err, err_len, [&] { batch(s, points, n_points, out, B_POINTWISE); });
+}
+
+int gpum_b200_session_grad_batch(gpum_b200_session* s, const double* points, size_t n_points,
+                                 double* out, char* err, size_t err_len) {
+  return guard(err, err_len, [&] { batch(s, points, n_points, out, B_GRAD); });
 }
 
 int gpum_b200_run(const uint32_t* code, size_t n_code, const double* consts, size_t n_consts,
@@ -697,26 +842,39 @@ int gpum_b200_run(const uint32_t* code, size_t n_code, const double* consts, siz
   });
 }
 
+static int one_shot_batch(const uint32_t* code, size_t n_code, const double* consts,
+                          size_t n_consts, uint32_t n_params, const double* data, uint32_t n_cols,
+                          uint64_t n_obs, const double* points, size_t n_points, double* out,
+                          char* err, size_t err_len, int kind) {
+  return guard(err, err_len, [&] {
+    std::unique_ptr<gpum_b200_session> s(create_session(
+        code, n_code, consts, n_consts, nullptr, 0, nullptr, 0, n_params, data, n_cols, n_obs));
+    batch(s.get(), points, n_points, out, kind);
+  });
+}
+
 int gpum_b200_loglik_batch(const uint32_t* code, size_t n_code, const double* consts,
                            size_t n_consts, uint32_t n_params, const double* data, uint32_t n_cols,
                            uint64_t n_obs, const double* points, size_t n_points, double* out,
                            char* err, size_t err_len) {
-  return guard(err, err_len, [&] {
-    std::unique_ptr<gpum_b200_session> s(create_session(
-        code, n_code, consts, n_consts, nullptr, 0, nullptr, 0, n_params, data, n_cols, n_obs));
-    batch(s.get(), points, n_points, out, false);
-  });
+  return one_shot_batch(code, n_code, consts, n_consts, n_params, data, n_cols, n_obs, points,
+                        n_points, out, err, err_len, B_SUM);
 }
 
 int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, const double* consts,
                                size_t n_consts, uint32_t n_params, const double* data,
                                uint32_t n_cols, uint64_t n_obs, const double* points,
                                size_t n_points, double* out, char* err, size_t err_len) {
-  return guard(err, err_len, [&] {
-    std::unique_ptr<gpum_b200_session> s(create_session(
-        code, n_code, consts, n_consts, nullptr, 0, nullptr, 0, n_params, data, n_cols, n_obs));
-    batch(s.get(), points, n_points, out, true);
-  });
+  return one_shot_batch(code, n_code, consts, n_consts, n_params, data, n_cols, n_obs, points,
+                        n_points, out, err, err_len, B_POINTWISE);
+}
+
+int gpum_b200_grad_batch(const uint32_t* code, size_t n_code, const double* consts,
+                         size_t n_consts, uint32_t n_params, const double* data, uint32_t n_cols,
+                         uint64_t n_obs, const double* points, size_t n_points, double* out,
+                         char* err, size_t err_len) {
+  return one_shot_batch(code, n_code, consts, n_consts, n_params, data, n_cols, n_obs, points,
+                        n_points, out, err, err_len, B_GRAD);
 }
 
 }  // extern "C"

@@ -1,0 +1,411 @@
+// codegen.cpp -- bytecode -> CUDA C model functions (see codegen.hpp).
+//
+// Generated interface (all __device__ __forceinline__):
+//   void   gm_data(const float* xo, int T, float* d)     per observation
+//   void   gm_hoist(const float* p, float* h)            per chain
+//   float  gm_value(const float* d, const float* p, const float* h)
+//   float  gm_value_grad(d, p, h, float* gp, float* gh)  gp/gh accumulated
+//   void   gm_hoist_grad(const float* p, const float* gh, float* gp)
+//   double gm_prior(const double* p)
+//   double gm_prior_grad(const double* p, double* g)     g accumulated
+// `xo` points at this lane's observation in the shared-memory tile; column j
+// is xo[j*T].
+#include "codegen.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <set>
+#include <sstream>
+#include <tuple>
+
+namespace gpum {
+
+namespace {
+
+enum : uint32_t { O_C = 0, O_P = 1, O_D = 2, O_ADD = 3, O_SUB = 4, O_MUL = 5, O_DIV = 6,
+                  O_NEG = 7, O_EXP = 8, O_LOG = 9, O_SQRT = 10, O_POW = 11, O_LGAMMA = 12 };
+enum : uint8_t { DEP_P = 1, DEP_D = 2 };
+
+struct Node {
+  uint32_t op;
+  int a = -1, b = -1;
+  uint32_t arg = 0;
+  double c = 0.0;
+  uint8_t dep = 0;
+};
+
+inline uint32_t norm(uint32_t op) { return (op <= O_SQRT || op == O_LGAMMA) ? op : O_POW; }
+inline bool unary(uint32_t op) { return (op >= O_NEG && op <= O_SQRT) || op == O_LGAMMA; }
+
+double fold(uint32_t op, double a, double b) {
+  switch (op) {
+    case O_ADD: return a + b;
+    case O_SUB: return a - b;
+    case O_MUL: return a * b;
+    case O_DIV: return a / b;
+    case O_NEG: return -a;
+    case O_EXP: return std::exp(a);
+    case O_LOG: return std::log(a);
+    case O_SQRT: return std::sqrt(a);
+    case O_LGAMMA: return std::lgamma(a);
+    default: return std::pow(a, b);
+  }
+}
+
+struct Graph {
+  std::vector<Node> n;
+  std::map<std::tuple<uint32_t, int, int, uint32_t, uint64_t>, int> memo;
+  int add(Node x) {
+    uint64_t bits = 0;
+    if (x.op == O_C) std::memcpy(&bits, &x.c, sizeof bits);
+    auto key = std::make_tuple(x.op, x.a, x.b, x.arg, bits);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+    n.push_back(x);
+    memo[key] = (int)n.size() - 1;
+    return (int)n.size() - 1;
+  }
+  // Build from a validated program; returns the root (or -1 if empty).
+  int build(const uint32_t* code, size_t n_code, const double* consts) {
+    std::vector<int> st;
+    for (size_t pc = 0; pc < n_code / 2; ++pc) {
+      const uint32_t op = norm(code[2 * pc]), arg = code[2 * pc + 1];
+      Node x;
+      x.op = op;
+      if (op == O_C) {
+        x.c = consts[arg];
+        st.push_back(add(x));
+      } else if (op == O_P || op == O_D) {
+        x.arg = arg;
+        x.dep = op == O_P ? DEP_P : DEP_D;
+        st.push_back(add(x));
+      } else if (unary(op)) {
+        const int a = st.back();
+        st.pop_back();
+        if (n[a].op == O_C && n[a].dep == 0) {
+          Node k;
+          k.op = O_C;
+          k.c = fold(op, n[a].c, 0.0);
+          st.push_back(add(k));
+        } else {
+          x.a = a;
+          x.dep = n[a].dep;
+          st.push_back(add(x));
+        }
+      } else {
+        const int b = st.back();
+        st.pop_back();
+        const int a = st.back();
+        st.pop_back();
+        if (n[a].op == O_C && n[b].op == O_C) {
+          Node k;
+          k.op = O_C;
+          k.c = fold(op, n[a].c, n[b].c);
+          st.push_back(add(k));
+        } else {
+          x.a = a;
+          x.b = b;
+          x.dep = n[a].dep | n[b].dep;
+          st.push_back(add(x));
+        }
+      }
+    }
+    return st.empty() ? -1 : st.front();  // the result is slot 0
+  }
+  std::vector<char> reachable(int root) const {
+    std::vector<char> r(n.size(), 0);
+    if (root < 0) return r;
+    r[root] = 1;
+    for (int i = root; i >= 0; --i) {
+      if (!r[i]) continue;
+      if (n[i].a >= 0) r[n[i].a] = 1;
+      if (n[i].b >= 0) r[n[i].b] = 1;
+    }
+    return r;
+  }
+};
+
+std::string flit(double v) {
+  const float f = (float)v;
+  if (std::isnan(f)) return "__int_as_float(0x7fffffff)";
+  if (std::isinf(f)) return f > 0 ? "__int_as_float(0x7f800000)" : "__int_as_float(0xff800000)";
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%af", (double)f);
+  return buf;
+}
+
+std::string dlit(double v) {
+  if (std::isnan(v)) return "__longlong_as_double(0x7fffffffffffffffll)";
+  if (std::isinf(v))
+    return v > 0 ? "__longlong_as_double(0x7ff0000000000000ll)"
+                 : "__longlong_as_double(0xfff0000000000000ll)";
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%a", v);
+  return buf;
+}
+
+bool is_const2(const Graph& g, int i) { return g.n[i].op == O_C && g.n[i].c == 2.0; }
+
+// Emits the value of `i` from child names.
+std::string op_expr(const Graph& g, int i, const std::string& a, const std::string& b,
+                    bool f32) {
+  const char* sfx = f32 ? "f" : "";
+  switch (g.n[i].op) {
+    case O_ADD: return "(" + a + " + " + b + ")";
+    case O_SUB: return "(" + a + " - " + b + ")";
+    case O_MUL: return "(" + a + " * " + b + ")";
+    case O_DIV: return "(" + a + " / " + b + ")";
+    case O_NEG: return "(-" + a + ")";
+    case O_EXP: return std::string("exp") + sfx + "(" + a + ")";
+    case O_LOG: return std::string("log") + sfx + "(" + a + ")";
+    case O_SQRT: return std::string("sqrt") + sfx + "(" + a + ")";
+    case O_LGAMMA: return std::string("lgamma") + sfx + "(" + a + ")";
+    default:
+      if (is_const2(g, g.n[i].b)) return "(" + a + " * " + a + ")";
+      return std::string("pow") + sfx + "(" + a + ", " + b + ")";
+  }
+}
+
+// Local-derivative contributions of node i with adjoint `G` to its children,
+// as (child, expression) pairs (cpu_native.rs:217-277).
+std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const std::string& G,
+                                                  const std::string& v, const std::string& a,
+                                                  const std::string& b, bool f32) {
+  const Node& x = g.n[i];
+  const std::string one = f32 ? "1.0f" : "1.0";
+  const std::string half = f32 ? "0.5f" : "0.5";
+  const std::string zero = f32 ? "0.0f" : "0.0";
+  const char* sfx = f32 ? "f" : "";
+  std::vector<std::pair<int, std::string>> out;
+  switch (x.op) {
+    case O_ADD: out = {{x.a, G}, {x.b, G}}; break;
+    case O_SUB: out = {{x.a, G}, {x.b, "(-" + G + ")"}}; break;
+    case O_MUL: out = {{x.a, G + " * " + b}, {x.b, G + " * " + a}}; break;
+    case O_DIV: out = {{x.a, G + " / " + b}, {x.b, "(-" + G + " * " + v + " / " + b + ")"}}; break;
+    case O_NEG: out = {{x.a, "(-" + G + ")"}}; break;
+    case O_EXP: out = {{x.a, G + " * " + v}}; break;
+    case O_LOG: out = {{x.a, G + " / " + a}}; break;
+    case O_SQRT: out = {{x.a, G + " * " + half + " / " + v}}; break;
+    case O_LGAMMA:
+      out = {{x.a, G + " * " + std::string(f32 ? "gm_digammaf(" : "gm_digamma(") + a + ")"}};
+      break;
+    default:
+      if (is_const2(g, x.b)) {
+        out = {{x.a, G + " * " + (f32 ? std::string("2.0f") : std::string("2.0")) + " * " + a}};
+      } else {
+        out = {{x.a, G + " * " + b + " * pow" + sfx + "(" + a + ", " + b + " - " + one + ")"},
+               {x.b, "((" + a + " > " + zero + ") ? " + G + " * " + v + " * log" + sfx + "(" +
+                         a + ") : " + zero + ")"}};
+      }
+      break;
+  }
+  return out;
+}
+
+}  // namespace
+
+int generate_model(const uint32_t* code, size_t n_code, const double* consts,
+                   const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
+                   uint32_t n_params, uint32_t n_cols, GenModel* out, std::string* err) {
+  (void)n_cols;
+  *out = GenModel();
+  Graph g;
+  const int root = g.build(code, n_code, consts);
+  const std::vector<char> live = g.reachable(root);
+  const int N = (int)g.n.size();
+
+  // Names and storage classes.
+  std::vector<std::string> name(N);
+  std::vector<int> hslot(N, -1), dslot(N, -1);
+  std::set<int> need_h, need_d;  // referenced from per-observation code
+  auto is_pd = [&](int i) { return g.n[i].dep == (DEP_P | DEP_D); };
+  auto is_h = [&](int i) { return g.n[i].dep == DEP_P && g.n[i].op != O_P; };
+  auto is_d = [&](int i) { return g.n[i].dep == DEP_D; };
+  for (int i = 0; i < N; ++i) {
+    if (!live[i]) continue;
+    if (is_pd(i)) {
+      for (int c : {g.n[i].a, g.n[i].b}) {
+        if (c < 0) continue;
+        if (is_h(c)) need_h.insert(c);
+        if (is_d(c)) need_d.insert(c);
+      }
+    }
+  }
+  if (root >= 0 && is_h(root)) need_h.insert(root);
+  if (root >= 0 && is_d(root)) need_d.insert(root);
+  for (int i : need_h) hslot[i] = out->n_hoist++;
+  for (int i : need_d) dslot[i] = out->n_data++;
+  for (int i = 0; i < N; ++i) {
+    const Node& x = g.n[i];
+    if (x.op == O_C) name[i] = flit(x.c);
+    else if (x.op == O_P) name[i] = "p[" + std::to_string(x.arg) + "]";
+    else name[i] = "v" + std::to_string(i);
+  }
+  auto ref_obs = [&](int i) -> std::string {  // name inside per-observation code
+    if (hslot[i] >= 0) return "h[" + std::to_string(hslot[i]) + "]";
+    if (dslot[i] >= 0) return "d[" + std::to_string(dslot[i]) + "]";
+    return name[i];
+  };
+
+  std::ostringstream s;
+  s << "#define GM_NP " << n_params << "\n";
+  s << "#define GM_NH " << std::max(1, out->n_hoist) << "\n";
+  s << "#define GM_ND " << std::max(1, out->n_data) << "\n";
+
+  // gm_data: data leaves and data-only subexpressions, per observation.
+  s << "__device__ __forceinline__ void gm_data(const float* __restrict__ xo, int T, "
+       "float* __restrict__ d) {\n";
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || !is_d(i)) continue;
+    const Node& x = g.n[i];
+    std::string e = x.op == O_D ? "xo[" + std::to_string(x.arg) + " * T]"
+                                : op_expr(g, i, name[x.a], x.b >= 0 ? name[x.b] : "", true);
+    s << "  const float " << name[i] << " = " << e << ";\n";
+    if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
+  }
+  s << "  (void)xo; (void)T; (void)d;\n}\n";
+
+  // gm_hoist: parameter-only subexpressions, once per chain.
+  auto emit_hoist_body = [&](std::ostringstream& o) {
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_h(i)) continue;
+      const Node& x = g.n[i];
+      o << "  const float " << name[i] << " = "
+        << op_expr(g, i, name[x.a], x.b >= 0 ? name[x.b] : "", true) << ";\n";
+    }
+  };
+  s << "__device__ __forceinline__ void gm_hoist(const float* __restrict__ p, "
+       "float* __restrict__ h) {\n";
+  emit_hoist_body(s);
+  for (int i : need_h) s << "  h[" << hslot[i] << "] = " << name[i] << ";\n";
+  s << "  (void)p; (void)h;\n}\n";
+
+  // Per-observation forward code.
+  auto emit_fwd = [&](std::ostringstream& o) {
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i)) continue;
+      const Node& x = g.n[i];
+      o << "  const float " << name[i] << " = "
+        << op_expr(g, i, ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "", true) << ";\n";
+      ++out->n_fwd;
+    }
+  };
+  const std::string rootv = root < 0 ? std::string("0.0f") : ref_obs(root);
+  s << "__device__ __forceinline__ float gm_value(const float* __restrict__ d, "
+       "const float* __restrict__ p, const float* __restrict__ h) {\n";
+  emit_fwd(s);
+  s << "  (void)d; (void)p; (void)h;\n  return " << rootv << ";\n}\n";
+
+  // Value + gradient: forward, then adjoints in reverse order.
+  s << "__device__ __forceinline__ float gm_value_grad(const float* __restrict__ d, "
+       "const float* __restrict__ p, const float* __restrict__ h, float* __restrict__ gp, "
+       "float* __restrict__ gh) {\n";
+  {
+    std::ostringstream f;
+    const int nf = out->n_fwd;
+    emit_fwd(f);
+    out->n_fwd = nf;
+    s << f.str();
+    // adjoint accumulators of per-observation nodes
+    for (int i = 0; i < N; ++i)
+      if (live[i] && is_pd(i)) s << "  float g" << i << " = 0.0f;\n";
+    auto sink = [&](int c, const std::string& e) {
+      if (c < 0 || !(g.n[c].dep & DEP_P)) return;
+      if (g.n[c].op == O_P) s << "  gp[" << g.n[c].arg << "] += " << e << ";\n";
+      else if (hslot[c] >= 0) s << "  gh[" << hslot[c] << "] += " << e << ";\n";
+      else s << "  g" << c << " += " << e << ";\n";
+    };
+    if (root >= 0 && (g.n[root].dep & DEP_P)) {
+      if (is_pd(root)) s << "  g" << root << " = 1.0f;\n";
+      else sink(root, "1.0f");
+    }
+    for (int i = N - 1; i >= 0; --i) {
+      if (!live[i] || !is_pd(i)) continue;
+      const Node& x = g.n[i];
+      const std::string G = "g" + std::to_string(i);
+      for (auto& ce : adjoints(g, i, G, name[i], ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "",
+                               true))
+        sink(ce.first, ce.second);
+    }
+    s << "  (void)d; (void)p; (void)h; (void)gp; (void)gh;\n  return " << rootv << ";\n}\n";
+  }
+
+  // Chain rule through the hoisted parameter-only nodes, once per chain.
+  s << "__device__ __forceinline__ void gm_hoist_grad(const float* __restrict__ p, "
+       "const float* __restrict__ gh, float* __restrict__ gp) {\n";
+  emit_hoist_body(s);
+  for (int i = 0; i < N; ++i)
+    if (live[i] && is_h(i))
+      s << "  float a" << i << " = " << (hslot[i] >= 0 ? "gh[" + std::to_string(hslot[i]) + "]"
+                                                       : std::string("0.0f"))
+        << ";\n";
+  for (int i = N - 1; i >= 0; --i) {
+    if (!live[i] || !is_h(i)) continue;
+    const Node& x = g.n[i];
+    for (auto& ce : adjoints(g, i, "a" + std::to_string(i), name[i], name[x.a],
+                             x.b >= 0 ? name[x.b] : "", true)) {
+      const int c = ce.first;
+      if (c < 0 || !(g.n[c].dep & DEP_P)) continue;
+      if (g.n[c].op == O_P) s << "  gp[" << g.n[c].arg << "] += " << ce.second << ";\n";
+      else s << "  a" << c << " += " << ce.second << ";\n";
+    }
+  }
+  s << "  (void)p; (void)gh; (void)gp;\n}\n";
+
+  // Prior in f64 (parameters only).
+  Graph pg;
+  const int proot = pg.build(prior_code, n_prior, prior_consts);
+  const std::vector<char> plive = pg.reachable(proot);
+  std::vector<std::string> pn(pg.n.size());
+  for (size_t i = 0; i < pg.n.size(); ++i) {
+    const Node& x = pg.n[i];
+    if (x.op == O_C) pn[i] = dlit(x.c);
+    else if (x.op == O_P) pn[i] = "p[" + std::to_string(x.arg) + "]";
+    else if (x.op == O_D) {
+      *err = "the prior may not read data";
+      return 1;
+    } else pn[i] = "w" + std::to_string(i);
+  }
+  auto emit_prior_fwd = [&](std::ostringstream& o) {
+    for (size_t i = 0; i < pg.n.size(); ++i) {
+      if (!plive[i] || pg.n[i].op <= O_D) continue;
+      const Node& x = pg.n[i];
+      o << "  const double " << pn[i] << " = "
+        << op_expr(pg, (int)i, pn[x.a], x.b >= 0 ? pn[x.b] : "", false) << ";\n";
+    }
+  };
+  const std::string proot_v = proot < 0 ? std::string("0.0") : pn[proot];
+  s << "__device__ __forceinline__ double gm_prior(const double* __restrict__ p) {\n";
+  emit_prior_fwd(s);
+  s << "  (void)p;\n  return " << proot_v << ";\n}\n";
+  s << "__device__ __forceinline__ double gm_prior_grad(const double* __restrict__ p, "
+       "double* __restrict__ g) {\n";
+  emit_prior_fwd(s);
+  for (size_t i = 0; i < pg.n.size(); ++i)
+    if (plive[i] && pg.n[i].op > O_D) s << "  double a" << i << " = 0.0;\n";
+  if (proot >= 0 && (pg.n[proot].dep & DEP_P)) {
+    if (pg.n[proot].op == O_P) s << "  g[" << pg.n[proot].arg << "] += 1.0;\n";
+    else s << "  a" << proot << " = 1.0;\n";
+  }
+  for (int i = (int)pg.n.size() - 1; i >= 0; --i) {
+    if (!plive[i] || pg.n[i].op <= O_D || !(pg.n[i].dep & DEP_P)) continue;
+    const Node& x = pg.n[i];
+    for (auto& ce : adjoints(pg, i, "a" + std::to_string(i), pn[i], pn[x.a],
+                             x.b >= 0 ? pn[x.b] : "", false)) {
+      const int c = ce.first;
+      if (c < 0 || !(pg.n[c].dep & DEP_P)) continue;
+      if (pg.n[c].op == O_P) s << "  g[" << pg.n[c].arg << "] += " << ce.second << ";\n";
+      else s << "  a" << c << " += " << ce.second << ";\n";
+    }
+  }
+  s << "  (void)p; (void)g;\n  return " << proot_v << ";\n}\n";
+
+  out->source = s.str();
+  out->np = (int)n_params;
+  out->has_grad = true;
+  return 0;
+}
+
+}  // namespace gpum

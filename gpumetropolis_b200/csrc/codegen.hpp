@@ -1,0 +1,39 @@
+// codegen.hpp -- translate gpumetropolis bytecode into straight-line CUDA C
+// for the compiled tier (NVRTC, sm_100a).
+//
+// The GPU analogue of the reference's Cranelift JIT (src/rust/src/jit.rs:
+// compile_loglik :441-631, compile_grad :97-436): the stack program becomes
+// SSA values; here additionally
+//   * identical subexpressions are computed once (hash-consing), so e.g. the
+//     linear predictor that a logistic log-likelihood spells twice is one sum;
+//   * constant subexpressions are folded in f64;
+//   * parameter-only subexpressions (exp(log_sigma), 1/(1+exp(-lw)), ...) are
+//     hoisted out of the observation loop and computed once per chain;
+//   * the reverse-mode gradient is unrolled (local derivatives of
+//     cpu_native.rs:217-277, including the POW exponent guard a > 0 and the
+//     digamma derivative of lgamma), with parameter-only nodes receiving
+//     accumulated adjoints that are pushed to the parameters once per chain.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace gpum {
+
+struct GenModel {
+  std::string source;     // device functions gm_* (see codegen.cpp)
+  int np = 0;             // parameters
+  int n_hoist = 0;        // per-chain hoisted values
+  int n_data = 0;         // per-observation data registers
+  int n_fwd = 0;          // per-observation forward nodes
+  bool has_grad = false;
+};
+
+// Builds the model functions for the log-likelihood program (f32 per
+// observation) and the prior program (f64, parameters only).  Returns 0, or
+// 1 with a message.  The programs must already be validated.
+int generate_model(const uint32_t* code, size_t n_code, const double* consts,
+                   const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
+                   uint32_t n_params, uint32_t n_cols, GenModel* out, std::string* err);
+
+}  // namespace gpum

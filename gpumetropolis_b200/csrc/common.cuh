@@ -1,0 +1,468 @@
+// common.cuh -- the per-iteration kernel skeleton shared by the interpreter
+// and the compiled (NVRTC) evaluation bodies, plus the accept/propose logic.
+//
+// One launch = one Metropolis iteration for every chain (the reference runs
+// a whole chain inside one CTA, src/rust/src/chain_kernel.rs:123-357; here
+// the data sum of every chain is spread over the whole GPU):
+//   grid.x = observation blocks, grid.y = chain blocks of CG chains;
+//   each CTA streams its observation tiles through shared memory with TMA
+//   (double-buffered, mbarrier completion, bounded waits) and evaluates its
+//   CG chains on every observation, so one tile read serves CG chains;
+//   per-thread compensated FP32 sums -> FP64 warp-shuffle tree -> FP64 sum
+//   over warps in fixed order -> FP64 partial per (obs block, chain, value);
+//   the last CTA of a chain block (atomic ticket, no spinning) sums the
+//   partials in obs-block order, adds the f64 prior, makes the tempered f64
+//   accept decision, records the draw and draws the next proposal.
+// Results are deterministic for a given launch geometry.
+#pragma once
+#include "device.cuh"
+
+namespace gpum {
+
+constexpr int kWarps = 8;  // warps per CTA
+constexpr int kThreads = kWarps * 32;
+constexpr int kMaxStackF64 = 32;
+
+enum Phase : int { PH_EVAL = 0, PH_INIT = 1, PH_STEP = 2, PH_POINTWISE = 3 };
+enum RngKind : int { RNG_TRIPLE32 = 0, RNG_PHILOX = 1 };
+enum ModeKind : int { MODE_RWM = 0, MODE_DE = 1, MODE_CHOL = 2, MODE_MALA = 3 };
+
+// Chain state of a run, all device pointers.
+struct ChainArgs {
+  int n_chains, np;
+  double* state;        // [C][np]
+  double* prop;         // [C][np]
+  double* cur;          // [C]   current log posterior (untempered)
+  double* last_eval;    // [C]   log posterior of the latest evaluated point
+  uint32_t* ctr;        // [C]   triple32 counters
+  uint32_t* accepts;    // [C]
+  uint32_t* iter;       // [NCB] iterations done, per chain block
+  const double* sd;     // [C][np]
+  const double* temp;   // [C]
+  const double* L;      // [C][np][np] row-major lower factors, or nullptr
+  const double* snap;   // [C][np] DE pool snapshot (batch start states)
+  float* draws;         // [n_iter][np][C_pad] internal layout
+  uint32_t n_iter;
+  uint32_t seed;
+  int mode;             // ModeKind
+  int rng;              // RngKind
+  double gamma, de_noise;
+  const uint32_t* prior_code;   // f64-interpreted prior (validated)
+  const double* prior_consts;
+  int n_prior;
+  double* zbuf;         // [C][np] scratch: normals
+  // MALA (mode 3)
+  double* gx;           // [C][np] gradient of the log posterior at `state`
+  double* gy;           // [C][np] gradient at `prop`
+  double* mx;           // [C][np] proposal mean from `state`
+  double* my;           // [C][np] proposal mean from `prop`
+  double* vbuf;         // [C][np] scratch
+};
+
+struct EvalArgs {
+  int n_obs, ncols, T, ntiles, tiles_per_cta, CG, WC, C_pad, np;
+  int width;            // values per (chain, obs block): 1, or 1 + np with the gradient
+  const float* params;  // [np][C_pad] evaluation points (f32)
+  double* partials;     // [NOB][C_pad][width]
+  double* pointwise;    // [C][n_obs] (PH_POINTWISE)
+  int n_points;         // chains/points that are real (rest padding)
+  uint32_t* tickets;    // [NCB]
+  uint32_t* err;        // device error word
+};
+
+// ------------------------------------------------------ f64 prior, interpreted
+// The prior is a handful of ops once per chain per iteration; it is
+// interpreted in f64 from the source bytecode (semantics of
+// src/rust/src/cpu_native.rs:80-107) so the prior term carries no f32 error.
+__device__ inline double prior_interp(const uint32_t* __restrict__ code, int n,
+                                      const double* __restrict__ cst,
+                                      const double* __restrict__ p) {
+  if (n == 0) return 0.0;
+  double st[kMaxStackF64];
+  int sp = 0;
+  for (int pc = 0; pc < n; ++pc) {
+    const uint32_t op = code[2 * pc], a = code[2 * pc + 1];
+    switch (op) {
+      case 0: st[sp++] = cst[a]; break;
+      case 1: st[sp++] = p[a]; break;
+      case 2: st[sp++] = 0.0; break;  // rejected by validation
+      case 3: st[sp - 2] += st[sp - 1]; --sp; break;
+      case 4: st[sp - 2] -= st[sp - 1]; --sp; break;
+      case 5: st[sp - 2] *= st[sp - 1]; --sp; break;
+      case 6: st[sp - 2] /= st[sp - 1]; --sp; break;
+      case 7: st[sp - 1] = -st[sp - 1]; break;
+      case 8: st[sp - 1] = exp(st[sp - 1]); break;
+      case 9: st[sp - 1] = log(st[sp - 1]); break;
+      case 10: st[sp - 1] = sqrt(st[sp - 1]); break;
+      case 12: st[sp - 1] = lgamma(st[sp - 1]); break;
+      default: st[sp - 2] = pow(st[sp - 2], st[sp - 1]); --sp; break;
+    }
+  }
+  return st[0];
+}
+
+// ------------------------------------------------------- uniform streams
+struct Stream {
+  int kind;
+  uint32_t seedmix;             // triple32: hash(seed) + chain * 2654435761
+  uint32_t ctr;                 // triple32 counter
+  uint32_t seed, chain, it, k;  // philox counter fields
+  __device__ __forceinline__ double next() {
+    if (kind == RNG_TRIPLE32) {
+      ctr += 1;
+      return t32_uniform(seedmix, ctr);
+    }
+    const U4 r = philox4x32_10(U4{k++, it, chain, 0xB2000001u}, seed, 0x6A09E667u);
+    return u53(r.x, r.y);
+  }
+  __device__ __forceinline__ double normal() {
+    const double u1 = next();
+    const double u2 = next();
+    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+  }
+};
+
+__device__ __forceinline__ Stream make_stream(const ChainArgs& A, int c) {
+  Stream rs;
+  rs.kind = A.rng;
+  rs.seedmix = triple32(A.seed) + (uint32_t)c * 2654435761u;
+  rs.ctr = A.ctr[c];
+  rs.seed = A.seed;
+  rs.chain = (uint32_t)c;
+  rs.it = 0;
+  rs.k = 0;
+  return rs;
+}
+
+// -------------------------------------------------------------- MALA helpers
+// out = f * (1/2) M g, M = Ls Ls' (or diag sd^2), the whitened drift capped at
+// 2 sqrt(d) (MALTA; cpu_native.rs:617-651).
+__device__ inline void half_m_times(int np, const double* sd, const double* L, const double* g,
+                                    double* out, double* tmp) {
+  const double dmax = 2.0 * sqrt((double)np);
+  if (!L) {
+    for (int j = 0; j < np; ++j) tmp[j] = 0.5 * sd[j] * g[j];
+  } else {
+    for (int j = 0; j < np; ++j) {
+      double acc = 0.0;
+      for (int k = j; k < np; ++k) acc += L[(size_t)k * np + j] * g[k];
+      tmp[j] = 0.5 * acc;
+    }
+  }
+  double ss = 0.0;
+  for (int j = 0; j < np; ++j) ss += tmp[j] * tmp[j];
+  const double norm = sqrt(ss);
+  const double f = norm > dmax ? dmax / norm : 1.0;
+  if (!L) {
+    for (int j = 0; j < np; ++j) out[j] = f * sd[j] * tmp[j];
+  } else {
+    for (int k = 0; k < np; ++k) {
+      double acc = 0.0;
+      for (int j = 0; j <= k; ++j) acc += L[(size_t)k * np + j] * tmp[j];
+      out[k] = f * acc;
+    }
+  }
+}
+
+// -1/2 |Ls^{-1}(v - m)|^2 by forward substitution (cpu_native.rs:655-673).
+__device__ inline double log_q(int np, const double* sd, const double* L, const double* v,
+                               const double* m, double* tmp) {
+  double q = 0.0;
+  if (!L) {
+    for (int j = 0; j < np; ++j) {
+      const double r = (v[j] - m[j]) / sd[j];
+      q -= 0.5 * r * r;
+    }
+  } else {
+    for (int k = 0; k < np; ++k) {
+      double acc = v[k] - m[k];
+      for (int j = 0; j < k; ++j) acc -= L[(size_t)k * np + j] * tmp[j];
+      tmp[k] = acc / L[(size_t)k * np + k];
+      q -= 0.5 * tmp[k] * tmp[k];
+    }
+  }
+  return q;
+}
+
+// ------------------------------------------------------------- proposals
+// Next proposal of chain c into prop (f64) and params (f32).
+// Diagonal RWM chain_kernel.rs:212-223 / cpu_native.rs:726-735; Cholesky
+// RWM :224-249 / :736-753; DE on the frozen snapshot :250-295 / :754-784;
+// MALA :681-703 (mean from the cached gradient, then L z or sd * z).
+__device__ inline void propose(const ChainArgs& A, int c, Stream& rs, float* params, int C_pad) {
+  const int np = A.np;
+  const double* x = A.state + (size_t)c * np;
+  double* y = A.prop + (size_t)c * np;
+  const double* sd = A.sd + (size_t)c * np;
+  const double* L = A.L ? A.L + (size_t)c * np * np : nullptr;
+  if (A.mode == MODE_RWM) {
+    for (int j = 0; j < np; ++j) y[j] = x[j] + sd[j] * rs.normal();
+  } else if (A.mode == MODE_CHOL || A.mode == MODE_MALA) {
+    double* z = A.zbuf + (size_t)c * np;
+    const double* base = x;
+    if (A.mode == MODE_MALA) {
+      double* mx = A.mx + (size_t)c * np;
+      half_m_times(np, sd, L, A.gx + (size_t)c * np, mx, A.vbuf + (size_t)c * np);
+      for (int j = 0; j < np; ++j) mx[j] += x[j];
+      base = mx;
+    }
+    for (int j = 0; j < np; ++j) z[j] = rs.normal();
+    if (L) {
+      for (int k = 0; k < np; ++k) {
+        double acc = base[k];
+        for (int j = 0; j <= k; ++j) acc += L[(size_t)k * np + j] * z[j];
+        y[k] = acc;
+      }
+    } else {
+      for (int j = 0; j < np; ++j) y[j] = base[j] + sd[j] * z[j];
+    }
+  } else {
+    const int n = A.n_chains;
+    int a = (int)(rs.next() * (double)n);
+    if (a >= n) a = n - 1;
+    int b = (int)(rs.next() * (double)n);
+    if (b >= n) b = n - 1;
+    if (b == a) b = (b + 1) % n;
+    const double g = rs.next() < 0.1 ? 1.0 : A.gamma;
+    const double* pa = A.snap + (size_t)a * np;
+    const double* pb = A.snap + (size_t)b * np;
+    for (int j = 0; j < np; ++j) {
+      const double z = rs.normal();
+      const double diff = pa[j] - pb[j];
+      y[j] = x[j] + g * diff + A.de_noise * sd[j] * z;
+    }
+  }
+  for (int j = 0; j < np; ++j) params[(size_t)j * C_pad + c] = (float)y[j];
+}
+
+// Accept/reject + record + propose for chain c.  `ll` is the data-term sum;
+// with MALA the data-term gradient has been summed into A.gy (STEP) or A.gx
+// (INIT).  Prior::value(A, p) and Prior::value_grad(A, p, g) give the f64
+// prior (value_grad accumulates into g).
+template <class Prior>
+__device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double ll, int phase,
+                                      float* params, int C_pad) {
+  const int np = A.np;
+  const uint32_t t = A.iter[cb];
+  Stream rs = make_stream(A, c);
+  const bool mala = A.mode == MODE_MALA;
+  double* x = A.state + (size_t)c * np;
+  if (phase == PH_INIT) {
+    const double lp = ll + (mala ? Prior::value_grad(A, x, A.gx + (size_t)c * np)
+                                 : Prior::value(A, x));
+    A.cur[c] = lp;
+    A.last_eval[c] = lp;
+    if (A.n_iter > 0) {
+      rs.it = 0;
+      propose(A, c, rs, params, C_pad);
+    }
+  } else {
+    const double* y = A.prop + (size_t)c * np;
+    const double plp = ll + (mala ? Prior::value_grad(A, y, A.gy + (size_t)c * np)
+                                  : Prior::value(A, y));
+    A.last_eval[c] = plp;
+    double lqd = 0.0;
+    if (mala) {
+      // q(x | y) - q(y | x) with the truncated drift at y (cpu_native.rs:704-710)
+      const double* sd = A.sd + (size_t)c * np;
+      const double* L = A.L ? A.L + (size_t)c * np * np : nullptr;
+      double* my = A.my + (size_t)c * np;
+      double* tmp = A.vbuf + (size_t)c * np;
+      half_m_times(np, sd, L, A.gy + (size_t)c * np, my, tmp);
+      for (int j = 0; j < np; ++j) my[j] += y[j];
+      lqd = log_q(np, sd, L, x, my, tmp) - log_q(np, sd, L, y, A.mx + (size_t)c * np, tmp);
+    }
+    double u;
+    if (A.rng == RNG_TRIPLE32) {
+      u = rs.next();
+    } else {
+      rs.it = t;
+      rs.k = 0xFFFF0000u;
+      u = rs.next();
+    }
+    // Tempered acceptance on the f64 totals (chain_kernel.rs:334,
+    // cpu_native.rs:792); MALA adds the proposal ratio and requires a
+    // finite proposal log density (cpu_native.rs:713-714).
+    const bool take = mala ? (isfinite(plp) && log(u) < (plp - A.cur[c]) / A.temp[c] + lqd)
+                           : (log(u) < (plp - A.cur[c]) / A.temp[c]);
+    if (take) {
+      for (int j = 0; j < np; ++j) x[j] = y[j];
+      if (mala) {
+        double* gx = A.gx + (size_t)c * np;
+        const double* gy = A.gy + (size_t)c * np;
+        for (int j = 0; j < np; ++j) gx[j] = gy[j];
+      }
+      A.cur[c] = plp;
+      A.accepts[c] += 1;
+    }
+    if (t < A.n_iter)
+      for (int j = 0; j < np; ++j) A.draws[((size_t)t * np + j) * C_pad + c] = (float)x[j];
+    if (t + 1 < A.n_iter) {
+      rs.it = t + 1;
+      rs.k = 0;
+      propose(A, c, rs, params, C_pad);
+    }
+  }
+  A.ctr[c] = rs.ctr;
+}
+
+// --------------------------------------------------------- kernel skeleton
+// Shared-memory carve-up (the host's smem_bytes() must agree):
+//   2 data stages [ncols][T] f32 | params [np][CG] f32 (rounded to 4) |
+//   reduction [kWarps][G][width] f64 | 2 mbarriers | ticket.
+__host__ __device__ inline size_t skel_smem_bytes(int T, int ncols, int np, int CG, int G,
+                                                  int width) {
+  return 2 * (size_t)T * ncols * 4 + (((size_t)np * CG + 3) & ~(size_t)3) * 4 +
+         (size_t)kWarps * G * width * 8 + 2 * 8 + 16;
+}
+
+// Body contract (G chains per thread):
+//   void begin(const float* pc0, int CG)   pc0 = this thread's first chain in
+//                                          the [np][CG] parameter tile
+//   void eval(const float* xo, int T, bool valid)  one observation
+//   float last(int g)                      value of the last eval (pointwise)
+//   void end()                             after the last observation
+//   double total(int g, int w)             w = 0 value, 1.. gradient entries
+//   W (compile time) = E.width values reduced per chain
+template <int G, int W, class Body, class Prior>
+__device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalArgs& E,
+                                              const ChainArgs& A, int phase, Body& body) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int CG = E.CG, T = E.T, ncols = E.ncols, np = E.np;
+  const int cb = blockIdx.y, ob = blockIdx.x;
+  const int WO = kWarps / E.WC;
+  const int wc = warp % E.WC, wo = warp / E.WC;
+
+  const size_t stage_floats = (size_t)T * ncols;
+  float* xs = reinterpret_cast<float*>(smem_raw);
+  float* psm = xs + 2 * stage_floats;
+  double* red = reinterpret_cast<double*>(psm + (((size_t)np * CG + 3) & ~(size_t)3));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + (size_t)kWarps * G * W);
+  uint32_t* s_ticket = reinterpret_cast<uint32_t*>(bars + 2);
+
+  for (int i = tid; i < np * CG; i += kThreads) {
+    const int p = i / CG, cl = i % CG;
+    psm[i] = E.params[(size_t)p * E.C_pad + (size_t)cb * CG + cl];
+  }
+
+  const int t0 = ob * E.tiles_per_cta;
+  const int t1 = min(t0 + E.tiles_per_cta, E.ntiles);
+  const int nt = max(t1 - t0, 0);
+  const uint32_t tile_bytes = (uint32_t)(stage_floats * sizeof(float));
+  // No tiles (or no data columns): the tensor map is never touched.
+  const bool staged = ncols > 0 && nt > 0;
+  if (tid == 0 && staged) {
+    tma_prefetch_desc(tmap);
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0 && staged) {
+    for (int s = 0; s < 2 && s < nt; ++s) {
+      mbar_expect_tx(&bars[s], tile_bytes);
+      tma_load_2d(xs + s * stage_floats, tmap, &bars[s], (t0 + s) * T, 0);
+    }
+  }
+  body.begin(psm + wc * G, CG);
+
+  for (int k = 0; k < nt; ++k) {
+    const int st = k & 1;
+    const float* tile = xs + st * stage_floats;
+    if (staged && !mbar_wait_bounded(&bars[st], (uint32_t)((k >> 1) & 1))) {
+      if (lane == 0) atomicOr(E.err, DEV_ERR_TMA_TIMEOUT);
+    }
+    const int obs0 = (t0 + k) * T;
+    for (int ol = lane + 32 * wo; ol < T; ol += 32 * WO) {
+      const int obs = obs0 + ol;
+      const bool valid = obs < E.n_obs;
+      body.eval(tile + ol, T, valid);
+      if (phase == PH_POINTWISE && valid) {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          const int c = cb * CG + wc * G + g;
+          if (c < E.n_points) E.pointwise[(size_t)c * E.n_obs + obs] = (double)body.last(g);
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with this stage
+    if (tid == 0 && staged && k + 2 < nt) {
+      mbar_expect_tx(&bars[st], tile_bytes);
+      tma_load_2d(xs + st * stage_floats, tmap, &bars[st], (t0 + k + 2) * T, 0);
+    }
+  }
+  if (phase == PH_POINTWISE) return;
+  body.end();
+
+  // FP64 fixed-order reduction of each of the W values: lanes (shuffle
+  // tree), then the WO warps that share a chain group, in warp order.
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    double tot[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) tot[g] = body.total(g, w);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) tot[g] += __shfl_down_sync(0xffffffffu, tot[g], off);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) red[((size_t)warp * G + g) * W + w] = tot[g];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < CG * W; i += kThreads) {
+    const int cl = i / W, w = i % W;
+    const int wcc = cl / G, g = cl % G;
+    double v = 0.0;
+    for (int o = 0; o < WO; ++o) v += red[((size_t)(o * E.WC + wcc) * G + g) * W + w];
+    E.partials[((size_t)ob * E.C_pad + (size_t)cb * CG + cl) * W + w] = v;
+  }
+  if (phase == PH_EVAL) return;
+
+  // Last CTA of this chain block (ticket) finishes the iteration.
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) *s_ticket = atomicAdd(&E.tickets[cb], 1u);
+  __syncthreads();
+  const uint32_t nob = gridDim.x;
+  if (*s_ticket != nob - 1) return;
+  __threadfence();
+  for (int cl = tid; cl < CG; cl += kThreads) {
+    const int c = cb * CG + cl;
+    if (c >= A.n_chains) continue;
+    double ll = 0.0;
+    for (uint32_t o = 0; o < nob; ++o) ll += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W]);
+    if (A.mode == MODE_MALA) {
+      double* gsum = (phase == PH_INIT ? A.gx : A.gy) + (size_t)c * np;
+      for (int j = 0; j < np; ++j) {
+        double v = 0.0;
+        for (uint32_t o = 0; o < nob; ++o)
+          v += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W + 1 + j]);
+        gsum[j] = v;
+      }
+    }
+    finalize_chain<Prior>(A, c, cb, ll, phase, const_cast<float*>(E.params), E.C_pad);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    E.tickets[cb] = 0;
+    if (phase == PH_STEP) A.iter[cb] += 1;
+  }
+}
+
+// Fixed-order sum of the partials of each point: out[p*W + w].
+__global__ void reduce_partials_kernel(const double* __restrict__ partials,
+                                       double* __restrict__ out, int nob, int C_pad, int n,
+                                       int W) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * W) return;
+  const int c = i / W, w = i % W;
+  double v = 0.0;
+  for (int o = 0; o < nob; ++o) v += partials[((size_t)o * C_pad + c) * W + w];
+  out[i] = v;
+}
+
+}  // namespace gpum

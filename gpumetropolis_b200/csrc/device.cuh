@@ -1,11 +1,24 @@
 // device.cuh -- sm_100a device helpers: TMA bulk-tensor loads with mbarrier
 // completion (bounded waits), counter-based RNGs, compensated accumulation.
 #pragma once
-#include <cuda.h>
+#ifdef __CUDACC_RTC__
+// Compiled at run time by NVRTC: no host headers.
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+#else
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 namespace gpum {
+
+// Opaque 128-byte TMA descriptor (same size and alignment as CUtensorMap);
+// the host fills it with cuTensorMapEncodeTiled.
+struct __align__(64) TmapDesc {
+  uint64_t opaque[16];
+};
 
 // ---------------------------------------------------------------- errors
 // Bits of the device error word a kernel sets instead of trapping; the host
@@ -58,7 +71,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // 2-D tiled TMA load (no multicast): box at (x, y) of `map` into smem `dst`,
 // completion counted on `bar`.  x * elemsize must be a multiple of 16 bytes.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+__device__ __forceinline__ void tma_load_2d(void* dst, const TmapDesc* map, uint64_t* bar,
                                             int x, int y) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
@@ -67,7 +80,7 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
+__device__ __forceinline__ void tma_prefetch_desc(const TmapDesc* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
@@ -109,6 +122,32 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
 __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
   const uint64_t m = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);
   return ((double)(m & ((1ull << 53) - 1)) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// ------------------------------------------------------------- digamma
+// Digamma by the reference's method (src/rust/src/cpu_native.rs:66-77):
+// recurrence psi(x) = psi(x+1) - 1/x up past 6, then the asymptotic series
+// ln x - 1/(2x) - 1/(12x^2) + 1/(120x^4) - 1/(252x^6).  It is the local
+// derivative of the lgamma opcode in the adjoint.
+__device__ __forceinline__ double gm_digamma(double x) {
+  double r = 0.0;
+  for (int i = 0; i < 64 && x < 6.0; ++i) {
+    r -= 1.0 / x;
+    x += 1.0;
+  }
+  const double f = 1.0 / (x * x);
+  return r + log(x) - 1.0 / (2.0 * x) - f * (1.0 / 12.0 - f * (1.0 / 120.0 - f * (1.0 / 252.0)));
+}
+
+__device__ __forceinline__ float gm_digammaf(float x) {
+  float r = 0.0f;
+  for (int i = 0; i < 64 && x < 6.0f; ++i) {
+    r -= 1.0f / x;
+    x += 1.0f;
+  }
+  const float f = 1.0f / (x * x);
+  return r + logf(x) - 1.0f / (2.0f * x) -
+         f * (1.0f / 12.0f - f * (1.0f / 120.0f - f * (1.0f / 252.0f)));
 }
 
 // ------------------------------------------------- compensated accumulation

@@ -50,6 +50,11 @@ extern "C" {
 #define GPUM_MODE_CHOL 2        /* random walk with per-chain Cholesky factor  */
 #define GPUM_MODE_MALA 3        /* Metropolis-adjusted Langevin                */
 
+/* evaluation engines (gpum_b200_session_set_engine) */
+#define GPUM_ENGINE_INTERP 0    /* register-stack bytecode interpreter          */
+#define GPUM_ENGINE_COMPILED 1  /* bytecode -> CUDA C -> NVRTC (sm_100a)        */
+#define GPUM_ENGINE_AUTO 2      /* compiled when NVRTC builds it, else interp.  */
+
 /* rng values for the session API */
 #define GPUM_RNG_TRIPLE32 0     /* the reference's counter hash stream         */
 #define GPUM_RNG_PHILOX 1       /* Philox4x32-10 counter-based stream          */
@@ -89,6 +94,23 @@ GPUM_API int gpum_b200_loglik_batch(const uint32_t* code, size_t n_code, const d
                            uint32_t n_cols, uint64_t n_obs, const double* points,
                            size_t n_points, double* out, char* err, size_t err_len);
 
+/* Gradient of the summed log-likelihood (data term) at each point,
+ * point-major out[p*n_params + j] f64, by the compiled engine's reverse-mode
+ * adjoint (rust_grad_batch, lib.rs:158-179; cpu_native.rs:306-329). */
+GPUM_API int gpum_b200_grad_batch(const uint32_t* code, size_t n_code, const double* consts,
+                         size_t n_consts, uint32_t n_params, const double* data,
+                         uint32_t n_cols, uint64_t n_obs, const double* points,
+                         size_t n_points, double* out, char* err, size_t err_len);
+
+/* Build the compiled engine's kernels for a model with NVRTC without touching
+ * a GPU; *cubin_bytes (may be NULL) receives the module size.  No reference
+ * counterpart: the reference's JIT (jit.rs) is CPU-only. */
+GPUM_API int gpum_b200_compile_check(const uint32_t* code, size_t n_code, const double* consts,
+                            size_t n_consts, const uint32_t* prior_code, size_t n_prior,
+                            const double* prior_consts, size_t n_prior_consts,
+                            uint32_t n_params, uint32_t n_cols, size_t* cubin_bytes,
+                            char* err, size_t err_len);
+
 /* Per-observation log-likelihood, out[p*n_obs + i] f64
  * (rust_loglik_pointwise, lib.rs:187-207). */
 GPUM_API int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, const double* consts,
@@ -117,12 +139,22 @@ GPUM_API int gpum_b200_session_run(gpum_b200_session* s, const double* init, con
                           float* out_accept, double* out_last_logpost, char* err,
                           size_t err_len);
 
-/* loglik_batch / loglik_pointwise on a session. */
+/* Select the evaluation engine (GPUM_ENGINE_*); the default is AUTO.
+ * Gradients (MALA, grad_batch) always use the compiled engine. */
+GPUM_API int gpum_b200_session_set_engine(gpum_b200_session* s, int engine, char* err,
+                                          size_t err_len);
+/* The engine plain evaluations use (GPUM_ENGINE_INTERP or _COMPILED). */
+GPUM_API int gpum_b200_session_engine(gpum_b200_session* s);
+
+/* loglik_batch / loglik_pointwise / grad_batch on a session. */
 GPUM_API int gpum_b200_session_loglik_batch(gpum_b200_session* s, const double* points, size_t n_points,
                                    double* out, char* err, size_t err_len);
 GPUM_API int gpum_b200_session_loglik_pointwise(gpum_b200_session* s, const double* points,
                                        size_t n_points, double* out, char* err,
                                        size_t err_len);
+GPUM_API int gpum_b200_session_grad_batch(gpum_b200_session* s, const double* points,
+                                          size_t n_points, double* out, char* err,
+                                          size_t err_len);
 
 /* Device-resident stepping, for callers that keep chain state on the GPU
  * between calls: prepare() uploads the batch-start state and evaluates it,

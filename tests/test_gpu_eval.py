@@ -33,31 +33,36 @@ def _points(w, n, seed=0, scale=0.05):
     return base + rng.normal(0, scale, (n, m.n_params))
 
 
+@pytest.mark.parametrize("engine", [0, 1], ids=["interp", "compiled"])
 @pytest.mark.parametrize("name,n_obs", [("gaussian", 5003), ("logistic", 4099),
                                          ("poisson", 3001), ("mixture", 6007),
                                          ("student_t", 1031)])
-def test_loglik_batch_matches_oracle(gpu, name, n_obs):
+def test_loglik_batch_matches_oracle(gpu, name, n_obs, engine):
     w = W.make(name, n_obs=n_obs)
     m = w.model
     pts = _points(w, 37)
     ref = O.loglik_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
                          w.n_obs, pts)
-    got = gpu.loglik_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
-                           w.n_obs, pts)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                     m.n_params, w.data, m.n_cols, w.n_obs, engine=engine) as s:
+        assert s.engine == engine
+        got = s.loglik_batch(pts)
     rel = np.abs(got - ref) / np.abs(ref)
     assert rel.max() <= REL_SUM, (name, rel.max())
 
 
+@pytest.mark.parametrize("engine", [0, 1], ids=["interp", "compiled"])
 @pytest.mark.parametrize("name,n_obs", [("logistic", 777), ("mixture", 513),
                                          ("student_t", 300)])
-def test_pointwise_matches_oracle(gpu, name, n_obs):
+def test_pointwise_matches_oracle(gpu, name, n_obs, engine):
     w = W.make(name, n_obs=n_obs)
     m = w.model
     pts = _points(w, 5, seed=1)
     ref = O.loglik_pointwise(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
                              w.n_obs, pts)
-    got = gpu.loglik_pointwise(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
-                               w.n_obs, pts)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                     m.n_params, w.data, m.n_cols, w.n_obs, engine=engine) as s:
+        got = s.loglik_pointwise(pts)
     np.testing.assert_allclose(got, ref, rtol=2e-5, atol=2e-5)
 
 
@@ -75,6 +80,7 @@ def test_many_points_and_chain_blocks(gpu):
 
 @pytest.mark.parametrize("depth", [3, 12, 24])
 def test_interpreter_variants_by_depth(gpu, depth):
+    """Through the one-shot ABI call (default engine) and the interpreter."""
     # right-nested sums push `depth` values: exercises the 8x8, 4x16, 2x32 variants
     f = "~ " + "(y * a + " * (depth - 1) + "b" + ")" * (depth - 1)
     m = gpum_model(f, ["a", "b"], "y")
@@ -83,11 +89,14 @@ def test_interpreter_variants_by_depth(gpu, depth):
     pts = np.array([[0.5, 1.5], [-0.25, 2.0], [1.0, -1.0]])
     ref = O.loglik_batch(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
     got = gpu.loglik_batch(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
+    with gpu.Session(m.loglik.code, m.loglik.consts, [], [], 2, y, 1, y.size, engine=0) as s:
+        got_i = s.loglik_batch(pts)
     # these sums cancel (terms of both signs): bound the error by the sum of
     # |per-observation values|, the condition of an FP32-per-observation sum
     pw = O.loglik_pointwise(m.loglik.code, m.loglik.consts, 2, y, 1, y.size, pts)
     scale = np.abs(pw.reshape(3, -1)).sum(axis=1)
     assert np.all(np.abs(got - ref) <= 1e-6 * scale)
+    assert np.all(np.abs(got_i - ref) <= 1e-6 * scale)
 
 
 def test_every_opcode_and_edge_sizes(gpu, golden):

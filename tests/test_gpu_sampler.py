@@ -77,8 +77,9 @@ def test_single_step_decisions_match(gpu):
     np.testing.assert_allclose(l_g[same], l_o[same], rtol=1e-6)
 
 
+@pytest.mark.parametrize("engine", [0, 1], ids=["interp", "compiled"])
 @pytest.mark.parametrize("mode", [0, 1, 2])
-def test_trajectories_follow_the_oracle(gpu, mode):
+def test_trajectories_follow_the_oracle(gpu, mode, engine):
     w = W.make("gaussian", n_obs=2000)
     C, n_iter, seed = 8, 300, 5
     rng = np.random.default_rng(1)
@@ -89,7 +90,8 @@ def test_trajectories_follow_the_oracle(gpu, mode):
     if mode == 2:
         L = np.full((C, 1, 1), 0.05)
     kw = dict(gamma=0.9, de_noise=0.01, proposal_l=L)
-    d_g, a_g, l_g = gpu.run(*_model_args(w), init, sd, temps, n_iter, seed, mode, **kw)
+    with gpu.Session(*_model_args(w), engine=engine) as s:
+        d_g, a_g, l_g = s.run(init, sd, temps, n_iter, seed, mode, **kw)
     d_o, a_o, l_o = O.run(*_model_args(w), init, sd, temps, n_iter, seed, mode, **kw)
     np.testing.assert_array_equal(a_g, a_o)
     np.testing.assert_allclose(d_g, d_o, rtol=1e-6, atol=1e-6)
