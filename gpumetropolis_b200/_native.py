@@ -65,6 +65,10 @@ SIGNATURES = {
     "gpum_b200_session_set_engine": (C.c_int, [C.c_void_p, C.c_int, _errp, _sz]),
     "gpum_b200_session_engine": (C.c_int, [C.c_void_p]),
     "gpum_b200_session_grad_batch": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
+    "gpum_b200_loglik_batch_noalloc": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32,
+                                                 C.c_void_p, C.c_uint64, C.c_uint32,
+                                                 C.c_uint64, C.c_void_p, _sz, C.c_void_p,
+                                                 C.c_void_p, _errp, _sz]),
     "gpum_b200_session_create": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz,
                                            C.c_uint32, _f64p, C.c_uint32, C.c_uint64,
                                            C.POINTER(C.c_void_p), _errp, _sz]),

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpum_b200.so")
-SOURCES = ["capi.cu", "program.cpp", "codegen.cpp", "jit.cpp"]
+SOURCES = ["capi.cu", "program.cpp", "codegen.cpp", "jit.cpp", "noalloc.cu"]
 HEADERS = ["device.cuh", "interp.cuh", "kernels.cuh", "common.cuh", "compiled.cuh",
            "program.hpp", "codegen.hpp", "jit.hpp"]
 # Headers the compiled engine hands to NVRTC at run time, embedded as strings.

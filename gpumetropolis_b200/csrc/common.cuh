@@ -454,7 +454,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
 }
 
 // Fixed-order sum of the partials of each point: out[p*W + w].
-__global__ void reduce_partials_kernel(const double* __restrict__ partials,
+static __global__ void reduce_partials_kernel(const double* __restrict__ partials,
                                        double* __restrict__ out, int nob, int C_pad, int n,
                                        int W) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -56,7 +56,7 @@ iter_kernel(const __grid_constant__ EvalProg prog, const __grid_constant__ TmapD
 
 // ------------------------------------------------------------- helpers
 // Row-major f64 rows [r0, r0+nr) -> column-major f32 [ncols][ld].
-__global__ void convert_rows_kernel(const double* __restrict__ src, float* __restrict__ dst,
+static __global__ void convert_rows_kernel(const double* __restrict__ src, float* __restrict__ dst,
                                     int ncols, int64_t ld, int64_t r0, int64_t nr) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nr * ncols) return;
@@ -65,7 +65,7 @@ __global__ void convert_rows_kernel(const double* __restrict__ src, float* __res
 }
 
 // f64 chain-major points [C][np] -> f32 [np][C_pad]; pad chains copy chain 0.
-__global__ void points_to_params_kernel(const double* __restrict__ pts, float* __restrict__ params,
+static __global__ void points_to_params_kernel(const double* __restrict__ pts, float* __restrict__ params,
                                         int n, int np, int C_pad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= np * C_pad) return;
@@ -76,7 +76,7 @@ __global__ void points_to_params_kernel(const double* __restrict__ pts, float* _
 
 // Internal draws [n_iter][np][C_pad] -> the reference layout, column-major
 // (n_iter, C, np): out[t + n_iter*(c + C*j)] (chain_kernel.rs:345).
-__global__ void draws_layout_kernel(const float* __restrict__ in, float* __restrict__ out,
+static __global__ void draws_layout_kernel(const float* __restrict__ in, float* __restrict__ out,
                                     int n_iter, int np, int C, int C_pad) {
   __shared__ float tile[32][33];
   const int j = blockIdx.z;

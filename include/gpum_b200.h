@@ -118,6 +118,27 @@ GPUM_API int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, con
                                uint32_t n_cols, uint64_t n_obs, const double* points,
                                size_t n_points, double* out, char* err, size_t err_len);
 
+/* Summed log-likelihood at each point for callers that cannot allocate
+ * device memory (their memory is owned by another allocator or budget).  No
+ * counterpart in the reference.  Allocates nothing: inputs and outputs are
+ * the caller's DEVICE buffers -- data column-major f32 d_data[j*ld + i]
+ * (ld >= n_obs, ld % 4 == 0, 16-byte aligned), points f64 n_points x
+ * n_params, out f64 n_points -- and the scratch is a fixed 16 MiB
+ * __device__ array per GPU, held from library load to process exit; inputs
+ * needing more (n_params x points beyond it) are rejected with
+ * GPUM_ERR_UNSUPPORTED.  Work is enqueued on `stream` (a cudaStream_t, NULL
+ * for the legacy stream) and the call waits for it.  Calls share the scratch:
+ * calls that overlap on the GPU race.  The first call on a device sets up
+ * the scratch address; make it before any stream capture.  The program is
+ * interpreted one micro-op per instruction (at most 1024 instructions). */
+GPUM_API int gpum_b200_loglik_batch_noalloc(const uint32_t* code, size_t n_code,
+                                            const double* consts, size_t n_consts,
+                                            uint32_t n_params, const float* d_data, uint64_t ld,
+                                            uint32_t n_cols, uint64_t n_obs,
+                                            const double* d_points, size_t n_points,
+                                            double* d_out, void* stream, char* err,
+                                            size_t err_len);
+
 /* ------------------------------------------------------------- sessions --
  * A session keeps the model and the data resident on the GPU, so batches of a
  * host-orchestrated run (adaptive warmup, PT, DE snapshots) do not re-upload
