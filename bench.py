@@ -165,12 +165,13 @@ class Clocks:
 
 def _traffic_per_launch():
     """dram read+write bytes of one iteration launch from the committed ncu
-    summary (profiles/iter_kernel_logistic.md, line `dram_bytes_per_launch: X`)."""
-    path = os.path.join(ROOT, "profiles", "iter_kernel_logistic.md")
+    summary (profiles/gm_iter_value_logistic_n2e20_c1024.md, line `dram_bytes_per_launch: X`)."""
+    path = os.path.join(ROOT, "profiles", "gm_iter_value_logistic_n2e20_c1024.md")
     try:
         for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+            cell = line.strip().strip("|").strip()
+            if cell.startswith("dram_bytes_per_launch:"):
+                return float(cell.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None

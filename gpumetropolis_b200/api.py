@@ -154,17 +154,8 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
     if not np.all(np.isfinite(sd_mat)) or np.any(sd_mat <= 0):
         raise GpumInputError("`proposal_sd` must be positive and finite.")
 
-    call = _Backend(model, data_mat, n_obs, rng_kind)
-    try:
-        return _route(model, call, method, npar, n_chains, init_mat, sd_mat, n_iter, warmup,
-                      warmup_auto, adapt, temperatures, swap_every, gamma, de_noise, de_every,
-                      de_sync, int(seed), backend)
-    finally:
-        call.close()
-
-
-def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmup_auto, adapt,
-           temperatures, swap_every, gamma, de_noise, de_every, de_sync, seed, backend):
+    C = n_chains
+    temps = None
     if method == "pt":
         if temperatures is None:
             temps = AD.pt_default_ladder(C)
@@ -176,6 +167,35 @@ def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmu
                 raise GpumInputError("`temperatures` must be positive and finite.")
         if swap_every is None:
             swap_every = max(C, 10)
+    if method == "de":
+        if C < 4:
+            raise GpumInputError('`method = "de"` needs at least 4 chains; the proposal draws '
+                                 "a distinct pair of other chains for each difference vector. "
+                                 "Increase `n_chains`.")
+        gamma = 2.38 / np.sqrt(2 * npar) if gamma is None else float(gamma)
+        if not np.isfinite(gamma) or gamma <= 0:
+            raise GpumInputError("`gamma` must be positive and finite.")
+        de_noise = float(de_noise)
+        if not np.isfinite(de_noise) or de_noise < 0:
+            raise GpumInputError("`de_noise` must be non-negative and finite.")
+        if de_every is None:
+            de_every = max(C, 10)
+        if de_sync:
+            raise GpumInputError("`de_sync = TRUE` (synchronous per-generation DE) is not "
+                                 "available on the b200 backend in this build.")
+
+    call = _Backend(model, data_mat, n_obs, rng_kind)
+    try:
+        return _route(model, call, method, npar, n_chains, init_mat, sd_mat, n_iter, warmup,
+                      warmup_auto, adapt, temps, swap_every, gamma, de_noise, de_every,
+                      int(seed), backend)
+    finally:
+        call.close()
+
+
+def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmup_auto, adapt,
+           temps, swap_every, gamma, de_noise, de_every, seed, backend):
+    if method == "pt":
         r = AD.pt_orchestrate(call, npar, C, init_mat, sd_mat, temps, n_iter, warmup,
                               int(swap_every), bool(adapt), seed)
         return GpumFit(r.draws, r.accept_rate, model, r.draws.shape[0],
@@ -186,21 +206,7 @@ def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmu
                               "swap_history": r.swap_history},
                        {"temperatures": temps, "swap_every": int(swap_every)})
     if method == "de":
-        if C < 4:
-            raise GpumInputError('`method = "de"` needs at least 4 chains; the proposal draws '
-                                 "a distinct pair of other chains for each difference vector. "
-                                 "Increase `n_chains`.")
-        g = 2.38 / np.sqrt(2 * npar) if gamma is None else float(gamma)
-        if not np.isfinite(g) or g <= 0:
-            raise GpumInputError("`gamma` must be positive and finite.")
-        dn = float(de_noise)
-        if not np.isfinite(dn) or dn < 0:
-            raise GpumInputError("`de_noise` must be non-negative and finite.")
-        if de_every is None:
-            de_every = max(C, 10)
-        if de_sync:
-            raise GpumInputError("`de_sync = TRUE` (synchronous per-generation DE) is not "
-                                 "available on the b200 backend in this build.")
+        g, dn = gamma, de_noise
         r = AD.de_orchestrate(call, npar, C, init_mat, sd_mat, g, dn, n_iter, warmup,
                               int(de_every), bool(adapt), seed)
         return GpumFit(r.draws, r.accept_rate, model, r.draws.shape[0],

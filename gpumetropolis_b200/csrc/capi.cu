@@ -305,7 +305,7 @@ struct gpum_b200_session {
   }
 
   void launch(int phase) {
-    const dim3 grid(geo.NOB, geo.NCB);
+    const dim3 grid(geo.NCB, geo.NOB);
     if (kc.compiled) {
       void* args[] = {(void*)&tmap, (void*)&E, (void*)&A, (void*)&phase};
       GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, geo.smem, stream));

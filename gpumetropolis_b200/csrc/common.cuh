@@ -4,7 +4,7 @@
 // One launch = one Metropolis iteration for every chain (the reference runs
 // a whole chain inside one CTA, src/rust/src/chain_kernel.rs:123-357; here
 // the data sum of every chain is spread over the whole GPU):
-//   grid.x = observation blocks, grid.y = chain blocks of CG chains;
+//   grid.x = chain blocks of CG chains, grid.y = observation blocks;
 //   each CTA streams its observation tiles through shared memory with TMA
 //   (double-buffered, mbarrier completion, bounded waits) and evaluates its
 //   CG chains on every observation, so one tile read serves CG chains;
@@ -330,7 +330,9 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int CG = E.CG, T = E.T, ncols = E.ncols, np = E.np;
-  const int cb = blockIdx.y, ob = blockIdx.x;
+  // Chain blocks vary fastest, so the CTAs that share an observation tile
+  // run in the same wave and read it through L2 once.
+  const int cb = blockIdx.x, ob = blockIdx.y;
   const int WO = kWarps / E.WC;
   const int wc = warp % E.WC, wo = warp / E.WC;
 
@@ -427,7 +429,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   __syncthreads();
   if (tid == 0) *s_ticket = atomicAdd(&E.tickets[cb], 1u);
   __syncthreads();
-  const uint32_t nob = gridDim.x;
+  const uint32_t nob = gridDim.y;
   if (*s_ticket != nob - 1) return;
   __threadfence();
   for (int cl = tid; cl < CG; cl += kThreads) {

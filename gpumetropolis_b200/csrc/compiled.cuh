@@ -13,11 +13,20 @@
 
 namespace gpum {
 
+// Each observation's FP32 value is accumulated into an FP64 sum (exact per
+// term, two instructions), so per-thread partial sums carry no FP32 error.
+struct Acc64 {
+  double s;
+  __device__ __forceinline__ void init() { s = 0.0; }
+  __device__ __forceinline__ void add(float x) { s += (double)x; }
+  __device__ __forceinline__ double total() const { return s; }
+};
+
 template <int G, bool GRAD>
 struct JitBody {
   float p[G][GM_NP];
   float h[G][GM_NH];
-  Comp acc[G];
+  Acc64 acc[G];
   float lastv[G];
   float gp[GRAD ? G : 1][GRAD ? GM_NP : 1];
   float gh[GRAD ? G : 1][GRAD ? GM_NH : 1];

@@ -28,6 +28,28 @@ struct __align__(16) EvalProg {
 
 enum HeavyKind : int { H_NONE = -1, H_DIV = 0, H_POW = 1, H_LGAMMA = 2 };
 
+// The G parameters of this thread's chains for one parameter index: one
+// broadcast 16- or 8-byte shared load per 4 or 2 chains.
+template <int G>
+__device__ __forceinline__ void load_params(const float* __restrict__ p, float (&v)[G]) {
+  if constexpr (G % 4 == 0) {
+#pragma unroll
+    for (int g = 0; g < G; g += 4) {
+      const float4 q = *reinterpret_cast<const float4*>(p + g);
+      v[g] = q.x; v[g + 1] = q.y; v[g + 2] = q.z; v[g + 3] = q.w;
+    }
+  } else if constexpr (G % 2 == 0) {
+#pragma unroll
+    for (int g = 0; g < G; g += 2) {
+      const float2 q = *reinterpret_cast<const float2*>(p + g);
+      v[g] = q.x; v[g + 1] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int g = 0; g < G; ++g) v[g] = p[g];
+  }
+}
+
 // Interpret the program once for G chains at one observation.
 //   xo : this lane's observation inside the tile; column j is at xo[j*T]
 //   pc0: this thread's first chain in the param tile; param p, chain g at
@@ -44,7 +66,7 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     int hk = H_NONE, hs = 0;
     float ta[G], tb[G];
 
-#define GPUM_PL(g) pc0[(size_t)a0 * CG + (g)]
+#define GPUM_PL(g) pv[g]
 #define GPUM_XD(a) xo[(size_t)(a) * T]
 #define GPUM_SLOT(S)                                                                   \
   case S * NKIND + K_PUSH_C:                                                           \
@@ -55,6 +77,8 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     break;                                                                             \
   case S * NKIND + K_PUSH_P:                                                           \
     if constexpr (S < D) {                                                             \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = GPUM_PL(g);              \
     }                                                                                  \
     break;                                                                             \
@@ -122,22 +146,30 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     break;                                                                             \
   case S * NKIND + K_ADD_P:                                                            \
     if constexpr (S < D) {                                                             \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + GPUM_PL(g);    \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SUB_P:                                                            \
     if constexpr (S < D) {                                                             \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - GPUM_PL(g);    \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_MUL_P:                                                            \
     if constexpr (S < D) {                                                             \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * GPUM_PL(g);    \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_DIV_P:                                                            \
   case S * NKIND + K_POW_P:                                                            \
     if constexpr (S < D) {                                                             \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
         ta[g] = s[S][g];                                                               \
         tb[g] = GPUM_PL(g);                                                            \
@@ -211,23 +243,41 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
   case S * NKIND + K_FMA_PD:                                                           \
     if constexpr (S < D) {                                                             \
       const float v = GPUM_XD(a1);                                                     \
+      float pv[G];                                                                     \
+      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
     }                                                                                  \
     break;
 
-    switch (w & 1023u) {
-      GPUM_SLOT(0) GPUM_SLOT(1) GPUM_SLOT(2) GPUM_SLOT(3)
-      GPUM_SLOT(4) GPUM_SLOT(5) GPUM_SLOT(6) GPUM_SLOT(7)
-#if 1
-      GPUM_SLOT(8) GPUM_SLOT(9) GPUM_SLOT(10) GPUM_SLOT(11)
-      GPUM_SLOT(12) GPUM_SLOT(13) GPUM_SLOT(14) GPUM_SLOT(15)
-      GPUM_SLOT(16) GPUM_SLOT(17) GPUM_SLOT(18) GPUM_SLOT(19)
-      GPUM_SLOT(20) GPUM_SLOT(21) GPUM_SLOT(22) GPUM_SLOT(23)
-      GPUM_SLOT(24) GPUM_SLOT(25) GPUM_SLOT(26) GPUM_SLOT(27)
-      GPUM_SLOT(28) GPUM_SLOT(29) GPUM_SLOT(30) GPUM_SLOT(31)
-#endif
-      default: break;
+    // Only the labels a variant can reach (slot < D) are emitted, so each
+    // variant's switch is dense from 0 and compiles to one indexed branch.
+#define GPUM_SLOTS_8 GPUM_SLOT(0) GPUM_SLOT(1) GPUM_SLOT(2) GPUM_SLOT(3) \
+  GPUM_SLOT(4) GPUM_SLOT(5) GPUM_SLOT(6) GPUM_SLOT(7)
+#define GPUM_SLOTS_16 GPUM_SLOTS_8 GPUM_SLOT(8) GPUM_SLOT(9) GPUM_SLOT(10) GPUM_SLOT(11) \
+  GPUM_SLOT(12) GPUM_SLOT(13) GPUM_SLOT(14) GPUM_SLOT(15)
+#define GPUM_SLOTS_32 GPUM_SLOTS_16 GPUM_SLOT(16) GPUM_SLOT(17) GPUM_SLOT(18) \
+  GPUM_SLOT(19) GPUM_SLOT(20) GPUM_SLOT(21) GPUM_SLOT(22) GPUM_SLOT(23) GPUM_SLOT(24) \
+  GPUM_SLOT(25) GPUM_SLOT(26) GPUM_SLOT(27) GPUM_SLOT(28) GPUM_SLOT(29) GPUM_SLOT(30) \
+  GPUM_SLOT(31)
+    if constexpr (D <= 8) {
+      switch (w & 1023u) {
+        GPUM_SLOTS_8
+        default: break;
+      }
+    } else if constexpr (D <= 16) {
+      switch (w & 1023u) {
+        GPUM_SLOTS_16
+        default: break;
+      }
+    } else {
+      switch (w & 1023u) {
+        GPUM_SLOTS_32
+        default: break;
+      }
     }
+#undef GPUM_SLOTS_8
+#undef GPUM_SLOTS_16
+#undef GPUM_SLOTS_32
 #undef GPUM_SLOT
 #undef GPUM_PL
 #undef GPUM_XD

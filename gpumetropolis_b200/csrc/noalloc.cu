@@ -240,7 +240,7 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
   const int total = (int)(n_params * C_pad);
   points_to_params_kernel<<<(total + 255) / 256, 256, 0, st>>>(d_points, d_params, n,
                                                                (int)n_params, C_pad);
-  const dim3 grid(nob, NCB);
+  const dim3 grid(NCB, nob);
   switch (G) {
     case 8: iter_kernel<8, 8><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, PH_EVAL); break;
     case 4: iter_kernel<4, 16><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, PH_EVAL); break;

@@ -1,0 +1,113 @@
+"""gpu_metropolis end to end on the B200 backend, mirroring the reference's
+integration tests (tests/testthat/test-api.R, test-pt.R, test-de.R,
+test-mala.R, test-adaptive.R) with posterior checks against closed forms."""
+import math
+
+import numpy as np
+import pytest
+
+from gpumetropolis_b200 import workloads as W
+from gpumetropolis_b200.api import gpu_metropolis
+from gpumetropolis_b200.diagnostics import ess, rhat
+from gpumetropolis_b200.dsl import gpum_model
+
+pytestmark = pytest.mark.gpu
+
+
+def _mcse(d):
+    return d.std() / math.sqrt(ess(d, warmup=0))
+
+
+def test_config1_adaptive_rwm_recovers_closed_form(gpu):
+    # y ~ N(3.4, 2^2), N = 20,000; rwm, 8 chains x 3,000
+    # iterations, adaptive warmup, proposal_sd 0.5; posterior N(mean y, 4/N)
+    w = W.make("gaussian")
+    fit = gpu_metropolis(w.model, data={"y": w.data[:, 0]}, proposal_sd=0.5, n_iter=3000,
+                         n_chains=8, seed=1)
+    d = fit["mu"]
+    assert d.shape == (1500, 8)
+    assert fit.warmup == 1500 and fit.n_iter_total == 3000
+    assert abs(d.mean() - w.truth["post_mean"]) < 5 * _mcse(d)
+    assert abs(d.std() - w.truth["post_sd"]) < 0.15 * w.truth["post_sd"]
+    assert rhat(d, warmup=0) < 1.01
+    assert fit.adaptation is not None and fit.adaptation["batch_sizes"].sum() == 1500
+
+
+def test_adaptation_rescues_a_bad_proposal(gpu):
+    # test-adaptive.R:275-294
+    rng = np.random.default_rng(42)
+    y = rng.normal(5.0, 1.0, 500)
+    m = gpum_model("~ -((y - mu)^2) / 2", "mu", "y")
+    on = gpu_metropolis(m, {"y": y}, proposal_sd=1e-4, n_iter=2000, n_chains=4, warmup=1000,
+                        adapt=True, seed=1)
+    off = gpu_metropolis(m, {"y": y}, proposal_sd=1e-4, n_iter=2000, n_chains=4, warmup=1000,
+                         adapt=False, seed=1)
+    assert abs(on["mu"].mean() - y.mean()) < 0.1
+    assert abs(off["mu"].mean() - y.mean()) > abs(on["mu"].mean() - y.mean())
+    assert off.adaptation is None
+
+
+def test_same_seed_same_draws(gpu):
+    rng = np.random.default_rng(2)
+    y = rng.normal(1.0, 2.0, 1000)
+    m = gpum_model("~ -((y - mu)^2) / 8", "mu", "y")
+    a = gpu_metropolis(m, {"y": y}, proposal_sd=0.1, n_iter=500, n_chains=2, seed=7)
+    b = gpu_metropolis(m, {"y": y}, proposal_sd=0.1, n_iter=500, n_chains=2, seed=7)
+    assert np.array_equal(a.draws, b.draws)
+
+
+def test_pt_cold_chain_covers_both_modes(gpu):
+    # test-pt.R:198-217: y ~ N(|mu|, 1); without swaps a chain keeps its mode
+    rng = np.random.default_rng(1)
+    y = rng.normal(3.0, 1.0, 400)
+    m = gpum_model("~ log(exp(-((y - mu)^2) / 2) + exp(-((y + mu)^2) / 2))", "mu", "y")
+    init = np.linspace(-6, 6, 8).reshape(8, 1)
+    fit = gpu_metropolis(m, {"y": y}, init=init, proposal_sd=0.15, n_iter=4000, method="pt",
+                         seed=1)
+    cold = fit.draws[:, 0, 0]
+    assert fit.extra["temperatures"][0] == 1.0
+    assert np.any(cold > 1.5) and np.any(cold < -1.5)
+    assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
+    sh = fit.adaptation["swap_history"]
+    assert sh.shape == (7, fit.adaptation["n_batches"])
+
+
+def test_de_recovers_correlated_bivariate(gpu):
+    # test-de.R:43-72
+    rng = np.random.default_rng(1)
+    rho = 0.9
+    S = np.array([[1, rho], [rho, 1]])
+    y = rng.standard_normal((500, 2)) @ np.linalg.cholesky(S).T + np.array([2.0, -1.0])
+    Si = np.linalg.inv(S)
+    f = (f"~ -0.5 * ({Si[0, 0]:.6f}*(y1-mu1)^2 + 2*{Si[0, 1]:.6f}*(y1-mu1)*(y2-mu2)"
+         f" + {Si[1, 1]:.6f}*(y2-mu2)^2)")
+    m = gpum_model(f, ["mu1", "mu2"], ["y1", "y2"])
+    fit = gpu_metropolis(m, {"y1": y[:, 0], "y2": y[:, 1]}, n_iter=8000, n_chains=16,
+                         method="de", seed=1)
+    d1, d2 = fit["mu1"].ravel(), fit["mu2"].ravel()
+    assert abs(d1.mean() - y[:, 0].mean()) < 0.02
+    assert abs(d2.mean() - y[:, 1].mean()) < 0.02
+    assert abs(np.corrcoef(d1, d2)[0, 1] - rho) < 0.05
+    assert rhat(fit["mu1"], warmup=0) < 1.05
+
+
+def test_mala_recovers_gaussian_at_its_target_rate(gpu):
+    # test-mala.R:35-46 (runs on the GPU here; the reference refuses a GPU)
+    rng = np.random.default_rng(1)
+    y = rng.normal(2.5, 1.0, 400)
+    m = gpum_model("~ -((y - mu)^2) / 2", "mu", "y")
+    fit = gpu_metropolis(m, {"y": y}, n_iter=8000, n_chains=4, method="mala", seed=1)
+    assert fit.method == "mala"
+    assert abs(fit.draws.mean() - y.mean()) < 0.01
+    assert abs(fit.draws.std() - 1 / math.sqrt(400)) < 0.15 / math.sqrt(400)
+    assert np.all((fit.accept_rate > 0.45) & (fit.accept_rate < 0.70))
+
+
+def test_nonfinite_start_and_proposals(gpu):
+    # test-numerical.R:32-67
+    m = gpum_model("~ log(mu) - mu + 0 * y", "mu", "y")
+    fit = gpu_metropolis(m, {"y": [0.0]}, init=[[1.5]], proposal_sd=0.4, n_iter=3000, seed=1)
+    d = fit.draws[:, 0, 0]
+    assert np.all(np.isfinite(d)) and d.min() > 0 and abs(d.mean() - 2) < 0.4
+    fit = gpu_metropolis(m, {"y": [0.0]}, init=[[-1.0]], proposal_sd=0.3, n_iter=500, seed=1)
+    assert fit.draws.shape == (250, 1, 1)
