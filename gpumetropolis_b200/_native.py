@@ -69,6 +69,19 @@ SIGNATURES = {
                                                  C.c_void_p, C.c_uint64, C.c_uint32,
                                                  C.c_uint64, C.c_void_p, _sz, C.c_void_p,
                                                  C.c_void_p, _errp, _sz]),
+    "gpum_b200_mlp_create": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.POINTER(C.c_void_p), _errp, _sz]),
+    "gpum_b200_mlp_destroy": (None, [C.c_void_p]),
+    "gpum_b200_mlp_set_normalizer": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_double,
+                                               C.c_double, _errp, _sz]),
+    "gpum_b200_mlp_train": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, C.c_uint32, C.c_double,
+                                      _f32p, _errp, _sz]),
+    "gpum_b200_mlp_predict": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
+    "gpum_b200_mlp_gradients": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, _f32p, _f32p, _errp,
+                                          _sz]),
+    "gpum_b200_mlp_get_params": (C.c_int, [C.c_void_p, _f32p, _errp, _sz]),
+    "gpum_b200_mlp_gemm_check": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, _f32p, _f32p,
+                                           _f32p, _errp, _sz]),
     "gpum_b200_session_create": (C.c_int, [_u32p, _sz, _f64p, _sz, _u32p, _sz, _f64p, _sz,
                                            C.c_uint32, _f64p, C.c_uint32, C.c_uint64,
                                            C.POINTER(C.c_void_p), _errp, _sz]),
@@ -353,3 +366,91 @@ class Session:
                                                             _p(out, C.c_double), err, _ERRLEN),
                err)
         return out[: n * self.n_obs]
+
+
+def gemm_check(A, B):
+    """C = bf16(A) . bf16(B)^T through the tcgen05 GEMM (test hook)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    M, K = A.shape
+    N = B.shape[0]
+    out = np.empty((M, N), np.float32)
+    err = C.create_string_buffer(_ERRLEN)
+    _check(load().gpum_b200_mlp_gemm_check(M, N, K, _p(A, C.c_float), _p(B, C.c_float),
+                                           _p(out, C.c_float), err, _ERRLEN), err)
+    return out
+
+
+class Surrogate:
+    """The d-H-H-1 SiLU MLP surrogate trained on the GPU (``gpum_b200_mlp_*``)."""
+
+    def __init__(self, d, hidden=256, batch=4096, seed=1):
+        self._lib = load()
+        h = C.c_void_p()
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_create(d, hidden, batch, seed, C.byref(h), err,
+                                              _ERRLEN), err)
+        self._h = h
+        self.d, self.hidden, self.batch = d, hidden, batch
+        self.dp = (d + 63) // 64 * 64
+        self.n_params = hidden * self.dp + hidden + hidden * hidden + hidden + hidden + 1
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gpum_b200_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_normalizer(self, xmean, xsd, ymean, ysd):
+        xm, xs = _f64(xmean), _f64(xsd)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_set_normalizer(self._h, _p(xm, C.c_double),
+                                                      _p(xs, C.c_double), float(ymean),
+                                                      float(ysd), err, _ERRLEN), err)
+
+    def fit_normalizer(self, theta, ll):
+        theta = np.asarray(theta, dtype=np.float64).reshape(-1, self.d)
+        sd = theta.std(axis=0)
+        sd = np.where(sd > 0, sd, 1.0)
+        ysd = float(np.std(ll)) or 1.0
+        self.set_normalizer(theta.mean(axis=0), sd, float(np.mean(ll)), ysd)
+
+    def train(self, theta, ll, steps, lr=1e-3):
+        th, y = _f64(theta), _f64(ll)
+        losses = np.empty(max(steps, 1), np.float32)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_train(self._h, _p(th, C.c_double), _p(y, C.c_double),
+                                             y.size, steps, lr, _p(losses, C.c_float), err,
+                                             _ERRLEN), err)
+        return losses[:steps]
+
+    def predict(self, theta):
+        th = _f64(theta)
+        n = th.size // self.d
+        out = np.empty(max(n, 1))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_predict(self._h, _p(th, C.c_double), n,
+                                               _p(out, C.c_double), err, _ERRLEN), err)
+        return out[:n]
+
+    def gradients(self, theta, ll):
+        th, y = _f64(theta), _f64(ll)
+        g = np.empty(self.n_params, np.float32)
+        loss = np.zeros(1, np.float32)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_gradients(self._h, _p(th, C.c_double),
+                                                 _p(y, C.c_double), y.size, _p(g, C.c_float),
+                                                 _p(loss, C.c_float), err, _ERRLEN), err)
+        return g, float(loss[0])
+
+    def params(self):
+        out = np.empty(self.n_params, np.float32)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_get_params(self._h, _p(out, C.c_float), err, _ERRLEN),
+               err)
+        return out

@@ -14,9 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpum_b200.so")
-SOURCES = ["capi.cu", "program.cpp", "codegen.cpp", "jit.cpp", "noalloc.cu"]
+SOURCES = ["capi.cu", "program.cpp", "codegen.cpp", "jit.cpp", "noalloc.cu", "mlp.cu"]
 HEADERS = ["device.cuh", "interp.cuh", "kernels.cuh", "common.cuh", "compiled.cuh",
-           "program.hpp", "codegen.hpp", "jit.hpp"]
+           "program.hpp", "codegen.hpp", "jit.hpp", "tc_gemm.cuh"]
 # Headers the compiled engine hands to NVRTC at run time, embedded as strings.
 EMBED = [("kEmbeddedDevice", "device.cuh"), ("kEmbeddedCommon", "common.cuh"),
          ("kEmbeddedCompiled", "compiled.cuh")]

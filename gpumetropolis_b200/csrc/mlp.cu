@@ -1,0 +1,608 @@
+// mlp.cu -- the surrogate of the log-likelihood: a d-H-H-1 MLP with SiLU,
+// trained and evaluated on the GPU with the tcgen05 GEMM (tc_gemm.cuh).
+// No reference counterpart: the surrogate and delayed acceptance are new.
+//
+// Inputs are standardised parameters (per-coordinate mean and sd of the
+// training pairs), the target is the standardised exact log-likelihood, the
+// loss is the mean squared error.  Weights live in f32 (master) with Adam
+// moments; BF16 copies feed the tensor cores.  All reductions are fixed-order
+// (no atomics), so training is bitwise repeatable for a given seed.
+//
+// Per training step, for a batch of B rows (B, H multiples of 128; the input
+// width is padded to dp, a multiple of 64):
+//   Z1 = X W1^T + b1, A1 = silu(Z1)          tcgen05 GEMM, fused epilogue
+//   Z2 = A1 W2^T + b2, A2 = silu(Z2)         tcgen05 GEMM, fused epilogue
+//   yhat = A2 w3 + b3; r = yhat - t          row kernel (warp per row)
+//   dZ2 = (2r/B) w3 * silu'(Z2)              row kernel
+//   dW2 = dZ2^T A1                           tcgen05 GEMM (K = B)
+//   dA1 = dZ2 W2                             tcgen05 GEMM (K = H)
+//   dZ1 = dA1 * silu'(Z1); dW1 = dZ1^T X     elementwise + tcgen05 GEMM
+//   biases / w3: fixed-order column sums; Adam on every parameter.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/gpum_b200.h"
+#include "tc_gemm.cuh"
+
+using namespace gpum;
+typedef __nv_bfloat16 bf16;
+
+namespace {
+
+struct MlpFail {
+  int code;
+  std::string msg;
+};
+
+#define MLP_CK(call)                                                                   \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      throw MlpFail{e_ == cudaErrorMemoryAllocation ? GPUM_ERR_NOMEM : GPUM_ERR_CUDA,  \
+                    std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+  } while (0)
+
+template <class T>
+struct Buf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    MLP_CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    n = count;
+  }
+  ~Buf() {
+    if (p) cudaFree(p);
+  }
+};
+
+// ----------------------------------------------------------------- kernels
+__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = sigmoidf_(z);
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// Deterministic uniform index for (seed, step, row): Philox counter.
+__device__ __forceinline__ uint32_t pick(uint32_t seed, uint32_t step, uint32_t row, uint32_t n) {
+  const U4 r = philox4x32_10(U4{row, step, 0x4D4C5031u, 0u}, seed, 0x2545F491u);
+  return (uint32_t)(((uint64_t)r.x * n) >> 32);
+}
+
+// Batch rows: standardised inputs (bf16, padded with zeros) and targets.
+// idx_mode 0: rows 0..n-1 in order (inference / gradient check);
+//          1: Philox-random rows of the training set.
+__global__ void mlp_gather(const float* __restrict__ theta, const double* __restrict__ ll,
+                           size_t n, int d, int dp, int B, int idx_mode, uint32_t seed,
+                           uint32_t step, const float* __restrict__ xmean,
+                           const float* __restrict__ xinv, float ymean, float yinv,
+                           bf16* __restrict__ Xh, float* __restrict__ t) {
+  const int row = blockIdx.x;
+  if (row >= B) return;
+  size_t src = idx_mode ? pick(seed, step, (uint32_t)row, (uint32_t)n) : (size_t)row;
+  const bool live = src < n;
+  if (!live) src = 0;
+  for (int j = threadIdx.x; j < dp; j += blockDim.x) {
+    float v = 0.0f;
+    if (live && j < d) v = (theta[src * d + j] - xmean[j]) * xinv[j];
+    Xh[(size_t)row * dp + j] = __float2bfloat16(v);
+  }
+  if (threadIdx.x == 0 && t) t[row] = live && ll ? (float)((ll[src] - ymean) * yinv) : 0.0f;
+}
+
+// Output layer, loss and dZ2 for one row per warp (fixed lane-order sums).
+//   yhat = silu(Z2) . w3 + b3; r = yhat - t; loss row = r^2
+//   dZ2 = (2 r / B) w3 * silu'(Z2)  (f32 and bf16, and bf16 transposed)
+__global__ void mlp_head(const float* __restrict__ Z2, const float* __restrict__ w3,
+                         const float* __restrict__ b3, const float* __restrict__ t, int B,
+                         int H, int n_live, float* __restrict__ yhat, float* __restrict__ rsq,
+                         float* __restrict__ dyhat, bf16* __restrict__ dZ2h,
+                         bf16* __restrict__ dZ2Th, int backward) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= B) return;
+  const float* z = Z2 + (size_t)warp * H;
+  float acc = 0.0f;
+  for (int j = lane; j < H; j += 32) acc += silu(z[j]) * w3[j];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  const float y = acc + b3[0];
+  if (lane == 0 && yhat) yhat[warp] = y;
+  if (!backward) return;
+  const bool live = warp < n_live;
+  const float r = live ? y - t[warp] : 0.0f;
+  if (lane == 0) {
+    rsq[warp] = r * r;
+    dyhat[warp] = 2.0f * r / (float)n_live;
+  }
+  const float g = 2.0f * r / (float)n_live;
+  for (int j = lane; j < H; j += 32) {
+    const float dz = g * w3[j] * dsilu(z[j]);
+    dZ2h[(size_t)warp * H + j] = __float2bfloat16(dz);
+    dZ2Th[(size_t)j * B + warp] = __float2bfloat16(dz);
+  }
+}
+
+// dZ1 = dA1 * silu'(Z1) -> bf16 transposed [H][B] and f32 [B][H] for db1.
+__global__ void mlp_dz1(const float* __restrict__ dA1, const float* __restrict__ Z1, int B, int H,
+                        float* __restrict__ dZ1, bf16* __restrict__ dZ1Th) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)B * H) return;
+  const size_t b = i / H, j = i % H;
+  const float v = dA1[i] * dsilu(Z1[i]);
+  dZ1[i] = v;
+  dZ1Th[j * B + b] = __float2bfloat16(v);
+}
+
+// bf16 [R][Cc] -> [Cc][R]
+__global__ void mlp_transpose(const bf16* __restrict__ in, bf16* __restrict__ out, int R, int Cc) {
+  __shared__ bf16 tile[32][34];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int r = r0 + y, c = c0 + threadIdx.x;
+    if (r < R && c < Cc) tile[y][threadIdx.x] = in[(size_t)r * Cc + c];
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = c0 + y, r = r0 + threadIdx.x;
+    if (r < R && c < Cc) out[(size_t)c * R + r] = tile[threadIdx.x][y];
+  }
+}
+
+// out[j] = sum_b M[b][j] * (s ? s[b] : 1), fixed order over b.
+__global__ void mlp_colsum(const float* __restrict__ M, const float* __restrict__ s, int B, int H,
+                           float* __restrict__ out, int silu_in) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= H) return;
+  float acc = 0.0f;
+  for (int b = 0; b < B; ++b) {
+    float v = M[(size_t)b * H + j];
+    if (silu_in) v = silu(v);
+    acc += s ? v * s[b] : v;
+  }
+  out[j] = acc;
+}
+
+__global__ void mlp_sum(const float* __restrict__ v, int n, float* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float acc = 0.0f;
+  for (int i = 0; i < n; ++i) acc += v[i];
+  out[0] = acc;
+}
+
+// Adam (Kingma & Ba) with bias correction; also refreshes the bf16 copy and,
+// when `wt` is set, the transposed bf16 copy of an R x Cc weight.
+__global__ void mlp_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                         const float* __restrict__ g, size_t n, float lr, float b1, float b2,
+                         float c1, float c2, float eps, bf16* __restrict__ wh,
+                         bf16* __restrict__ wt, int R, int Cc) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wh) wh[i] = __float2bfloat16(wi);
+  if (wt) wt[(i % Cc) * R + i / Cc] = __float2bfloat16(wi);
+}
+
+__global__ void mlp_init_weights(float* __restrict__ w, size_t n, int fan_in, int cols_live,
+                                 int cols, uint32_t seed, uint32_t tag) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int col = (int)(i % cols);
+  const U4 r = philox4x32_10(U4{(uint32_t)i, tag, 0x57494E49u, 0u}, seed, 0x9E3779B9u);
+  const float u = ((float)(r.x >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  const float bound = sqrtf(6.0f / (float)fan_in);  // He-uniform style for SiLU
+  w[i] = col < cols_live ? (2.0f * u - 1.0f) * bound : 0.0f;
+}
+
+__global__ void mlp_to_bf16(const float* __restrict__ w, bf16* __restrict__ wh,
+                            bf16* __restrict__ wt, size_t n, int R, int Cc) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  wh[i] = __float2bfloat16(w[i]);
+  if (wt) wt[(i % Cc) * R + i / Cc] = __float2bfloat16(w[i]);
+}
+
+unsigned blocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+struct gpum_b200_mlp {
+  int d = 0, dp = 0, H = 0, B = 0;
+  uint32_t seed = 0;
+  uint32_t step = 0;
+  cudaStream_t st = nullptr;
+  // parameters (f32 master), Adam moments, gradients
+  Buf<float> W1, b1, W2, b2, w3, b3;
+  Buf<float> mW1, mb1, mW2, mb2, mw3, mb3, vW1, vb1, vW2, vb2, vw3, vb3;
+  Buf<float> gW1, gb1, gW2, gb2, gw3, gb3;
+  Buf<bf16> W1h, W2h, W2Th;
+  // activations and work buffers (batch rows)
+  Buf<bf16> Xh, XTh, A1h, A1Th, A2h, dZ2h, dZ2Th, dZ1Th;
+  Buf<float> Z1, Z2, t, yhat, rsq, dyhat, dA1, dZ1, loss, scratch;
+  // normaliser
+  Buf<float> xmean, xinv;
+  float ymean = 0.0f, yinv = 1.0f, ysd = 1.0f;
+  Buf<uint32_t> err;
+  int adam_t = 0;
+
+  ~gpum_b200_mlp() {
+    if (st) cudaStreamDestroy(st);
+  }
+
+  template <int BN>
+  void gemm(const bf16* A, const bf16* Bm, float* C, const float* bias, bf16* act, int M, int N,
+            int K) {
+    const size_t smem = tc_gemm_smem<BN>();
+    MLP_CK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+    dim3 grid(N / BN, M / kGemmBM);
+    tc_gemm_kernel<BN><<<grid, kGemmThreads, smem, st>>>(A, Bm, C, bias, act, M, N, K, err.p);
+    MLP_CK(cudaGetLastError());
+  }
+
+  void gemm_any(const bf16* A, const bf16* Bm, float* C, const float* bias, bf16* act, int M,
+                int N, int K) {
+    if (N % 128 == 0) gemm<128>(A, Bm, C, bias, act, M, N, K);
+    else gemm<64>(A, Bm, C, bias, act, M, N, K);
+  }
+
+  // Forward of the first `rows` rows already gathered into Xh.
+  void forward(int rows) {
+    gemm_any(Xh.p, W1h.p, Z1.p, b1.p, A1h.p, rows, H, dp);
+    gemm_any(A1h.p, W2h.p, Z2.p, b2.p, A2h.p, rows, H, H);
+  }
+
+  // Gradients for the gathered batch (n_live real rows of B).
+  void backward(int n_live) {
+    mlp_head<<<blocks((size_t)B * 32), 256, 0, st>>>(Z2.p, w3.p, b3.p, t.p, B, H, n_live, yhat.p,
+                                                     rsq.p, dyhat.p, dZ2h.p, dZ2Th.p, 1);
+    MLP_CK(cudaGetLastError());
+    // w3 and b3: dw3[j] = sum_b dyhat[b] silu(Z2[b][j]); db3 = sum dyhat
+    mlp_colsum<<<blocks(H), 256, 0, st>>>(Z2.p, dyhat.p, B, H, gw3.p, 1);
+    mlp_sum<<<1, 32, 0, st>>>(dyhat.p, B, gb3.p);
+    mlp_sum<<<1, 32, 0, st>>>(rsq.p, B, loss.p);
+    // db2 = column sums of dZ2 (from its bf16 transpose would lose bits: use
+    // the f32 row kernel output through dA1's buffer as scratch)
+    mlp_transpose<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(A1h.p, A1Th.p, B, H);
+    gemm_any(dZ2Th.p, A1Th.p, gW2.p, nullptr, nullptr, H, H, B);  // dW2 = dZ2^T A1
+    gemm_any(dZ2h.p, W2Th.p, dA1.p, nullptr, nullptr, B, H, H);   // dA1 = dZ2 W2
+    // db2 = sum_b dZ2[b][j]: recompute in f32 from Z2 and dyhat
+    db2_from_head();
+    mlp_dz1<<<blocks((size_t)B * H), 256, 0, st>>>(dA1.p, Z1.p, B, H, dZ1.p, dZ1Th.p);
+    mlp_colsum<<<blocks(H), 256, 0, st>>>(dZ1.p, nullptr, B, H, gb1.p, 0);
+    mlp_transpose<<<dim3(dp / 32, B / 32), dim3(32, 8), 0, st>>>(Xh.p, XTh.p, B, dp);
+    gemm_any(dZ1Th.p, XTh.p, gW1.p, nullptr, nullptr, H, dp, B);  // dW1 = dZ1^T X
+    MLP_CK(cudaGetLastError());
+  }
+
+  // db2[j] = sum_b dyhat[b] w3[j] silu'(Z2[b][j]), fixed order over b.
+  void db2_from_head();
+
+  void adam(float lr) {
+    ++adam_t;
+    const float bb1 = 0.9f, bb2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.0f - std::pow(bb1, (float)adam_t), c2 = 1.0f - std::pow(bb2, (float)adam_t);
+    auto go = [&](Buf<float>& w, Buf<float>& m, Buf<float>& v, Buf<float>& g, bf16* wh, bf16* wt,
+                  int R, int Cc) {
+      mlp_adam<<<blocks(w.n), 256, 0, st>>>(w.p, m.p, v.p, g.p, w.n, lr, bb1, bb2, c1, c2, eps,
+                                            wh, wt, R, Cc);
+    };
+    go(W1, mW1, vW1, gW1, W1h.p, nullptr, H, dp);
+    go(b1, mb1, vb1, gb1, nullptr, nullptr, 1, H);
+    go(W2, mW2, vW2, gW2, W2h.p, W2Th.p, H, H);
+    go(b2, mb2, vb2, gb2, nullptr, nullptr, 1, H);
+    go(w3, mw3, vw3, gw3, nullptr, nullptr, 1, H);
+    go(b3, mb3, vb3, gb3, nullptr, nullptr, 1, 1);
+    MLP_CK(cudaGetLastError());
+  }
+
+  void check_err() {
+    uint32_t e = 0;
+    MLP_CK(cudaMemcpyAsync(&e, err.p, sizeof e, cudaMemcpyDeviceToHost, st));
+    MLP_CK(cudaStreamSynchronize(st));
+    if (e) {
+      MLP_CK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
+      throw MlpFail{GPUM_ERR_DEVICE, "a tensor-core kernel reported a device-side failure"};
+    }
+  }
+};
+
+namespace {
+
+__global__ void mlp_db2(const float* __restrict__ Z2, const float* __restrict__ dyhat,
+                        const float* __restrict__ w3, int B, int H, float* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= H) return;
+  float acc = 0.0f;
+  for (int b = 0; b < B; ++b) acc += dyhat[b] * dsilu(Z2[(size_t)b * H + j]);
+  out[j] = acc * w3[j];
+}
+
+int mlp_guard(char* err, size_t len, const std::function<void()>& body) {
+  try {
+    body();
+    if (err && len) err[0] = '\0';
+    return GPUM_OK;
+  } catch (const MlpFail& f) {
+    if (err && len) std::snprintf(err, len, "%s", f.msg.c_str());
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    if (err && len) std::snprintf(err, len, "host allocation failed");
+    return GPUM_ERR_NOMEM;
+  } catch (...) {
+    if (err && len) std::snprintf(err, len, "unexpected internal error");
+    return GPUM_ERR_CUDA;
+  }
+}
+
+void need(bool ok, const char* msg, int code = GPUM_ERR_INVALID) {
+  if (!ok) throw MlpFail{code, msg};
+}
+
+}  // namespace
+
+void gpum_b200_mlp::db2_from_head() {
+  mlp_db2<<<blocks(H), 256, 0, st>>>(Z2.p, dyhat.p, w3.p, B, H, gb2.p);
+  MLP_CK(cudaGetLastError());
+}
+
+namespace {
+
+// Upload host pairs (theta f64 -> f32, ll f64) into device buffers.
+void upload_pairs(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n,
+                  Buf<float>& dth, Buf<double>& dll) {
+  std::vector<float> th((size_t)n * m->d);
+  for (size_t i = 0; i < th.size(); ++i) th[i] = (float)theta[i];
+  dth.alloc(th.size());
+  MLP_CK(cudaMemcpyAsync(dth.p, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice,
+                         m->st));
+  if (ll) {
+    dll.alloc(n);
+    MLP_CK(cudaMemcpyAsync(dll.p, ll, n * sizeof(double), cudaMemcpyHostToDevice, m->st));
+  }
+  MLP_CK(cudaStreamSynchronize(m->st));
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t seed,
+                         gpum_b200_mlp** out, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(out != nullptr, "output pointer is NULL");
+    *out = nullptr;
+    need(d >= 1 && d <= 256, "input width must be in 1..256");
+    need(hidden >= 128 && hidden <= 1024 && hidden % 128 == 0,
+         "hidden width must be a multiple of 128 in 128..1024");
+    need(batch >= 128 && batch <= 65536 && batch % 128 == 0,
+         "batch must be a multiple of 128 in 128..65536");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      throw MlpFail{GPUM_ERR_NODEVICE, "no CUDA device is visible"};
+    }
+    std::unique_ptr<gpum_b200_mlp> m(new gpum_b200_mlp());
+    m->d = (int)d;
+    m->dp = (int)((d + 63) / 64 * 64);
+    m->H = (int)hidden;
+    m->B = (int)batch;
+    m->seed = seed;
+    MLP_CK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
+    const int H = m->H, dp = m->dp, B = m->B;
+    for (auto* b : {&m->W1, &m->mW1, &m->vW1, &m->gW1}) b->alloc((size_t)H * dp);
+    for (auto* b : {&m->W2, &m->mW2, &m->vW2, &m->gW2}) b->alloc((size_t)H * H);
+    for (auto* b : {&m->b1, &m->mb1, &m->vb1, &m->gb1, &m->b2, &m->mb2, &m->vb2, &m->gb2, &m->w3,
+                    &m->mw3, &m->vw3, &m->gw3})
+      b->alloc(H);
+    for (auto* b : {&m->b3, &m->mb3, &m->vb3, &m->gb3}) b->alloc(1);
+    m->W1h.alloc((size_t)H * dp);
+    m->W2h.alloc((size_t)H * H);
+    m->W2Th.alloc((size_t)H * H);
+    m->Xh.alloc((size_t)B * dp);
+    m->XTh.alloc((size_t)dp * B);
+    for (auto* b : {&m->A1h, &m->A2h, &m->dZ2h}) b->alloc((size_t)B * H);
+    for (auto* b : {&m->A1Th, &m->dZ2Th, &m->dZ1Th}) b->alloc((size_t)H * B);
+    for (auto* b : {&m->Z1, &m->Z2, &m->dA1, &m->dZ1}) b->alloc((size_t)B * H);
+    for (auto* b : {&m->t, &m->yhat, &m->rsq, &m->dyhat}) b->alloc(B);
+    m->loss.alloc(1);
+    m->xmean.alloc(d);
+    m->xinv.alloc(d);
+    m->err.alloc(1);
+    MLP_CK(cudaMemsetAsync(m->err.p, 0, sizeof(uint32_t), m->st));
+    // zero moments and padded rows
+    for (auto* b : {&m->mW1, &m->vW1, &m->mW2, &m->vW2, &m->mb1, &m->vb1, &m->mb2, &m->vb2,
+                    &m->mw3, &m->vw3, &m->mb3, &m->vb3, &m->b1, &m->b2, &m->b3})
+      MLP_CK(cudaMemsetAsync(b->p, 0, b->n * sizeof(float), m->st));
+    mlp_init_weights<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1.p, (size_t)H * dp, (int)d,
+                                                                (int)d, dp, seed, 1);
+    mlp_init_weights<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2.p, (size_t)H * H, H, H, H,
+                                                               seed, 2);
+    mlp_init_weights<<<blocks(H), 256, 0, m->st>>>(m->w3.p, H, H, H, H, seed, 3);
+    mlp_to_bf16<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1.p, m->W1h.p, nullptr,
+                                                           (size_t)H * dp, H, dp);
+    mlp_to_bf16<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2.p, m->W2h.p, m->W2Th.p,
+                                                          (size_t)H * H, H, H);
+    MLP_CK(cudaGetLastError());
+    std::vector<float> ones(d, 1.0f);
+    MLP_CK(cudaMemsetAsync(m->xmean.p, 0, d * sizeof(float), m->st));
+    MLP_CK(cudaMemcpyAsync(m->xinv.p, ones.data(), d * sizeof(float), cudaMemcpyHostToDevice,
+                           m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
+    *out = m.release();
+  });
+}
+
+void gpum_b200_mlp_destroy(gpum_b200_mlp* m) {
+  if (!m) return;
+  if (m->st) cudaStreamSynchronize(m->st);
+  delete m;
+}
+
+int gpum_b200_mlp_set_normalizer(gpum_b200_mlp* m, const double* xmean, const double* xsd,
+                                 double ymean, double ysd, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && xmean && xsd, "NULL argument");
+    need(std::isfinite(ymean) && ysd > 0 && std::isfinite(ysd), "ysd must be positive");
+    std::vector<float> mu(m->d), inv(m->d);
+    for (int j = 0; j < m->d; ++j) {
+      need(xsd[j] > 0 && std::isfinite(xsd[j]) && std::isfinite(xmean[j]), "xsd must be positive");
+      mu[j] = (float)xmean[j];
+      inv[j] = (float)(1.0 / xsd[j]);
+    }
+    MLP_CK(cudaMemcpyAsync(m->xmean.p, mu.data(), m->d * sizeof(float), cudaMemcpyHostToDevice,
+                           m->st));
+    MLP_CK(cudaMemcpyAsync(m->xinv.p, inv.data(), m->d * sizeof(float), cudaMemcpyHostToDevice,
+                           m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
+    m->ymean = (float)ymean;
+    m->ysd = (float)ysd;
+    m->yinv = (float)(1.0 / ysd);
+  });
+}
+
+int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n_pairs,
+                        uint32_t steps, double lr, float* out_loss, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && theta && ll, "NULL argument");
+    need(n_pairs >= 1 && n_pairs <= (1u << 28), "n_pairs must be in 1..2^28");
+    Buf<float> dth;
+    Buf<double> dll;
+    upload_pairs(m, theta, ll, n_pairs, dth, dll);
+    std::vector<float> losses(steps);
+    for (uint32_t s = 0; s < steps; ++s) {
+      mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed,
+                                          m->step++, m->xmean.p, m->xinv.p, m->ymean, m->yinv,
+                                          m->Xh.p, m->t.p);
+      m->forward(m->B);
+      m->backward(m->B);
+      m->adam((float)lr);
+      if (out_loss)
+        MLP_CK(cudaMemcpyAsync(&losses[s], m->loss.p, sizeof(float), cudaMemcpyDeviceToHost,
+                               m->st));
+    }
+    m->check_err();
+    if (out_loss)
+      for (uint32_t s = 0; s < steps; ++s) out_loss[s] = losses[s] / (float)m->B;
+  });
+}
+
+int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, double* out, char* err,
+                          size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && theta && out, "NULL argument");
+    Buf<float> dth;
+    Buf<double> none;
+    upload_pairs(m, theta, nullptr, n, dth, none);
+    std::vector<float> y(m->B);
+    for (size_t r0 = 0; r0 < n; r0 += m->B) {
+      const size_t rows = std::min<size_t>(m->B, n - r0);
+      mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p + r0 * m->d, nullptr, rows, m->d, m->dp, m->B, 0,
+                                          0, 0, m->xmean.p, m->xinv.p, 0.0f, 1.0f, m->Xh.p,
+                                          nullptr);
+      m->forward(m->B);
+      mlp_head<<<blocks((size_t)m->B * 32), 256, 0, m->st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr,
+                                                            m->B, m->H, m->B, m->yhat.p, nullptr,
+                                                            nullptr, nullptr, nullptr, 0);
+      MLP_CK(cudaGetLastError());
+      MLP_CK(cudaMemcpyAsync(y.data(), m->yhat.p, rows * sizeof(float), cudaMemcpyDeviceToHost,
+                             m->st));
+      MLP_CK(cudaStreamSynchronize(m->st));
+      for (size_t i = 0; i < rows; ++i) out[r0 + i] = (double)y[i] * m->ysd + m->ymean;
+    }
+    m->check_err();
+  });
+}
+
+int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n,
+                            float* out_grads, float* out_loss, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && theta && ll && out_grads, "NULL argument");
+    need(n >= 1 && n <= (size_t)m->B, "n must be in 1..batch");
+    Buf<float> dth;
+    Buf<double> dll;
+    upload_pairs(m, theta, ll, n, dth, dll);
+    mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n, m->d, m->dp, m->B, 0, 0, 0, m->xmean.p,
+                                        m->xinv.p, m->ymean, m->yinv, m->Xh.p, m->t.p);
+    m->forward(m->B);
+    m->backward((int)n);
+    const int H = m->H, dp = m->dp;
+    size_t off = 0;
+    auto cp = [&](const float* src, size_t cnt) {
+      MLP_CK(cudaMemcpyAsync(out_grads + off, src, cnt * sizeof(float), cudaMemcpyDeviceToHost,
+                             m->st));
+      off += cnt;
+    };
+    cp(m->gW1.p, (size_t)H * dp);
+    cp(m->gb1.p, H);
+    cp(m->gW2.p, (size_t)H * H);
+    cp(m->gb2.p, H);
+    cp(m->gw3.p, H);
+    cp(m->gb3.p, 1);
+    float l = 0.0f;
+    MLP_CK(cudaMemcpyAsync(&l, m->loss.p, sizeof l, cudaMemcpyDeviceToHost, m->st));
+    m->check_err();
+    if (out_loss) *out_loss = l / (float)n;
+  });
+}
+
+int gpum_b200_mlp_get_params(gpum_b200_mlp* m, float* out, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && out, "NULL argument");
+    const int H = m->H, dp = m->dp;
+    size_t off = 0;
+    auto cp = [&](const float* src, size_t cnt) {
+      MLP_CK(cudaMemcpyAsync(out + off, src, cnt * sizeof(float), cudaMemcpyDeviceToHost, m->st));
+      off += cnt;
+    };
+    cp(m->W1.p, (size_t)H * dp);
+    cp(m->b1.p, H);
+    cp(m->W2.p, (size_t)H * H);
+    cp(m->b2.p, H);
+    cp(m->w3.p, H);
+    cp(m->b3.p, 1);
+    MLP_CK(cudaStreamSynchronize(m->st));
+  });
+}
+
+int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A, const float* B,
+                             float* C, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(A && B && C, "NULL argument");
+    need(M % 128 == 0 && K % 64 == 0 && (N % 128 == 0 || N % 64 == 0) && M && N && K,
+         "M, N, K must be multiples of 128, 64 and 64");
+    std::vector<bf16> ah((size_t)M * K), bh((size_t)N * K);
+    for (size_t i = 0; i < ah.size(); ++i) ah[i] = __float2bfloat16(A[i]);
+    for (size_t i = 0; i < bh.size(); ++i) bh[i] = __float2bfloat16(B[i]);
+    gpum_b200_mlp tmp;
+    MLP_CK(cudaStreamCreateWithFlags(&tmp.st, cudaStreamNonBlocking));
+    Buf<bf16> da, db;
+    Buf<float> dc;
+    da.alloc(ah.size());
+    db.alloc(bh.size());
+    dc.alloc((size_t)M * N);
+    tmp.err.alloc(1);
+    MLP_CK(cudaMemsetAsync(tmp.err.p, 0, sizeof(uint32_t), tmp.st));
+    MLP_CK(cudaMemcpyAsync(da.p, ah.data(), ah.size() * 2, cudaMemcpyHostToDevice, tmp.st));
+    MLP_CK(cudaMemcpyAsync(db.p, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice, tmp.st));
+    tmp.gemm_any(da.p, db.p, dc.p, nullptr, nullptr, (int)M, (int)N, (int)K);
+    MLP_CK(cudaMemcpyAsync(C, dc.p, (size_t)M * N * 4, cudaMemcpyDeviceToHost, tmp.st));
+    tmp.check_err();
+  });
+}
+
+}  // extern "C"

@@ -207,6 +207,43 @@ GPUM_API uint64_t gpum_b200_session_launches(const gpum_b200_session* s);
 
 GPUM_API void gpum_b200_session_destroy(gpum_b200_session* s);
 
+/* ------------------------------------------------------- surrogate MLP --
+ * A d-H-H-1 SiLU network approximating the log-likelihood over the
+ * parameters, trained and evaluated on the GPU with BF16 tcgen05 tensor-core
+ * GEMMs (f32 accumulation in tensor memory), f32 master weights and Adam.
+ * No counterpart in the reference: it is the first stage of delayed
+ * acceptance.  hidden and batch are multiples of 128; d <= 256. */
+typedef struct gpum_b200_mlp gpum_b200_mlp;
+
+GPUM_API int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t seed,
+                                  gpum_b200_mlp** out, char* err, size_t err_len);
+GPUM_API void gpum_b200_mlp_destroy(gpum_b200_mlp* m);
+/* Standardisation of inputs (per coordinate) and of the target. */
+GPUM_API int gpum_b200_mlp_set_normalizer(gpum_b200_mlp* m, const double* xmean,
+                                          const double* xsd, double ymean, double ysd, char* err,
+                                          size_t err_len);
+/* `steps` Adam steps on random batches of the pairs (host arrays theta
+ * n_pairs x d, ll n_pairs); out_loss (may be NULL) receives each step's mean
+ * squared error in standardised units. */
+GPUM_API int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll,
+                                 size_t n_pairs, uint32_t steps, double lr, float* out_loss,
+                                 char* err, size_t err_len);
+/* Predicted log-likelihood at n points (host arrays). */
+GPUM_API int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, double* out,
+                                   char* err, size_t err_len);
+/* Gradients of the batch loss at the first n <= batch pairs, without an
+ * update: out = [dW1 (H x dp) | db1 (H) | dW2 (H x H) | db2 (H) | dw3 (H) |
+ * db3 (1)], dp = d rounded up to 64; *out_loss = mean squared error. */
+GPUM_API int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double* ll,
+                                     size_t n, float* out_grads, float* out_loss, char* err,
+                                     size_t err_len);
+/* Master weights in the same order as the gradients. */
+GPUM_API int gpum_b200_mlp_get_params(gpum_b200_mlp* m, float* out, char* err, size_t err_len);
+/* C[M x N] = bf16(A)[M x K] . bf16(B)[N x K]^T through the tcgen05 GEMM
+ * (host f32 arrays; M % 128 == 0, K % 64 == 0, N % 64 == 0). */
+GPUM_API int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
+                                      const float* B, float* C, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
