@@ -102,6 +102,13 @@ SIGNATURES = {
     "gpum_b200_session_launches": (C.c_uint64, [C.c_void_p]),
     "gpum_b200_session_stream": (C.c_void_p, [C.c_void_p]),
     "gpum_b200_session_destroy": (None, [C.c_void_p]),
+    "gpum_b200_session_record": (C.c_int, [C.c_void_p, C.c_uint64, _errp, _sz]),
+    "gpum_b200_session_recorded": (C.c_int, [C.c_void_p, _f32p, _f64p, C.c_uint64,
+                                             C.POINTER(C.c_uint64), _errp, _sz]),
+    "gpum_b200_session_run_da": (C.c_int, [C.c_void_p, C.c_void_p, _f64p, _f64p, _f64p,
+                                           C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                           C.c_double, C.c_double, _f64p, _sz, C.c_int, _f32p,
+                                           _f32p, _f64p, _u32p, _errp, _sz]),
 }
 
 _lib = None
@@ -295,6 +302,45 @@ class Session:
             _p(last, C.c_double), err, _ERRLEN)
         _check(rc, err)
         return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def record(self, capacity):
+        """Store the (theta, log-likelihood) pair of every exactly evaluated
+        proposal of later exact runs, up to `capacity` pairs (0: off)."""
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_record(self._h, int(capacity), err, _ERRLEN), err)
+
+    def recorded(self):
+        """The recorded pairs: (theta float32 n x n_params, ll float64 n)."""
+        n = C.c_uint64(0)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_recorded(self._h, None, None, 0, C.byref(n), err,
+                                                    _ERRLEN), err)
+        theta = np.empty((max(n.value, 1), self.n_params), np.float32)
+        ll = np.empty(max(n.value, 1), np.float64)
+        _check(self._lib.gpum_b200_session_recorded(
+            self._h, _p(theta, C.c_float), _p(ll, C.c_double), n.value, C.byref(n), err,
+            _ERRLEN), err)
+        return theta[: n.value], ll[: n.value]
+
+    def run_da(self, surrogate, init, proposal_sd, temperatures, n_iter, seed, proposal_mode,
+               gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
+        """Delayed-acceptance run with `surrogate` (a Surrogate) as stage 1.
+        Returns (draws, accept, last_logpost, exact_evals per chain)."""
+        init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
+        n_chains = init.size // self.n_params
+        L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
+        draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
+        acc = np.empty(n_chains, np.float32)
+        last = np.empty(n_chains, np.float64)
+        exact = np.empty(n_chains, np.uint32)
+        err = C.create_string_buffer(_ERRLEN)
+        rc = self._lib.gpum_b200_session_run_da(
+            self._h, surrogate._h, _p(init, C.c_double), _p(sd, C.c_double),
+            _p(temps, C.c_double), n_chains, n_iter, seed & 0xFFFFFFFF, proposal_mode, gamma,
+            de_noise, _p(L, C.c_double), 0 if L is None else L.size, rng, _p(draws, C.c_float),
+            _p(acc, C.c_float), _p(last, C.c_double), _p(exact, C.c_uint32), err, _ERRLEN)
+        _check(rc, err)
+        return draws[: n_iter * n_chains * self.n_params], acc, last, exact
 
     def prepare(self, init, proposal_sd, temperatures, max_iter, seed, proposal_mode,
                 gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):

@@ -12,6 +12,14 @@ are standard normals from a PCG64 stream seeded with ``seed`` (the reference
 draws them with R's ``rnorm`` after ``set.seed(seed)``, ``R/api.R:302-307``),
 and PT swap uniforms use PCG64 seeded with the reference's mix
 (``R/adaptive.R:537-539``).
+
+``surrogate=True`` (or a dict of options) adds delayed acceptance, which the
+reference does not have: the exact proposals of the second half of warmup are
+recorded on the device, an MLP surrogate of the log-likelihood is trained on
+them on the tensor cores, and the sampling phase runs two-stage
+Metropolis-Hastings (surrogate screen, exact correction), which leaves the
+target posterior unchanged while evaluating only the screened proposals
+exactly.
 """
 from __future__ import annotations
 
@@ -85,35 +93,113 @@ def _data_matrix(model: GpumModel, data):
     return np.ascontiguousarray(np.stack(cols, axis=1)), n
 
 
+SURROGATE_DEFAULTS = {"hidden": 256, "batch": 4096, "steps": 3000, "lr": 1e-3,
+                      "max_pairs": 1 << 20, "min_pairs": 2048, "seed": 1}
+
+
 class _Backend:
     """One data-resident session serving every batch of a run (the
-    ``rust_call`` closure of ``R/api.R:379-393``)."""
+    ``rust_call`` closure of ``R/api.R:379-393``).
 
-    def __init__(self, model: GpumModel, data_mat, n_obs, rng_kind):
+    With a surrogate configuration it also drives delayed acceptance:
+    recording starts once `record_at` iterations have run, the surrogate is
+    trained when `da_at` iterations have run (or on ``start_da()``), and
+    from then on batches run two-stage steps."""
+
+    def __init__(self, model: GpumModel, data_mat, n_obs, rng_kind, surrogate=None):
         m = model
         self.np = m.n_params
         self.rng = rng_kind
         self.session = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code,
                                        m.prior.consts, m.n_params, data_mat, m.n_cols, n_obs)
+        self.cfg = surrogate
+        self.consumed = 0
+        self.record_at = None
+        self.da_at = None
+        self.recording = False
+        self.net = None
+        self.info = {}
+        self.exact_evals = 0
+        self.da_iters = 0
+
+    def _maybe_record(self, C, n_iter):
+        if self.cfg is None or self.net is not None or self.recording or self.record_at is None:
+            return
+        if self.consumed >= self.record_at:
+            self.session.record(int(self.cfg["max_pairs"]))
+            self.recording = True
+
+    def start_da(self):
+        """Train the surrogate on the recorded pairs; later batches use it."""
+        if self.cfg is None or self.net is not None:
+            return
+        if not self.recording:
+            self.info = {"used": False, "reason": "no exact pairs were recorded"}
+            return
+        theta, ll = self.session.recorded()
+        self.session.record(0)
+        self.recording = False
+        ok = np.isfinite(ll) & np.all(np.isfinite(theta), axis=1)
+        theta, ll = theta[ok].astype(np.float64), ll[ok]
+        if theta.shape[0] < int(self.cfg["min_pairs"]):
+            self.info = {"used": False, "reason": f"only {theta.shape[0]} finite pairs"}
+            return
+        g = np.random.Generator(np.random.PCG64(int(self.cfg["seed"])))
+        idx = g.permutation(theta.shape[0])
+        n_hold = max(1, theta.shape[0] // 10)
+        hold, train = idx[:n_hold], idx[n_hold:]
+        net = _native.Surrogate(self.np, hidden=int(self.cfg["hidden"]),
+                                batch=int(self.cfg["batch"]), seed=int(self.cfg["seed"]))
+        net.fit_normalizer(theta[train], ll[train])
+        loss = net.train(theta[train], ll[train], int(self.cfg["steps"]), lr=float(self.cfg["lr"]))
+        resid = net.predict(theta[hold]) - ll[hold]
+        self.net = net
+        self.info = {"used": True, "pairs": int(theta.shape[0]),
+                     "final_loss": float(np.mean(loss[-50:])),
+                     "holdout_resid_sd": float(np.std(resid))}
 
     def __call__(self, init, sd, n_iter, seed, temperatures=None, proposal_mode=0, gamma=0.0,
                  de_noise=0.0, proposal_l=None):
         init = np.asarray(init, dtype=np.float64)
         C = init.shape[0]
         temps = np.ones(C) if temperatures is None else np.asarray(temperatures, np.float64)
-        d, acc, last = self.session.run(init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF,
-                                        proposal_mode, gamma, de_noise, proposal_l, rng=self.rng)
+        if self.da_at is not None and self.consumed >= self.da_at:
+            self.start_da()
+        self._maybe_record(C, n_iter)
+        if self.net is not None and proposal_mode != _native.MODE_MALA:
+            d, acc, last, exact = self.session.run_da(
+                self.net, init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF, proposal_mode,
+                gamma, de_noise, proposal_l, rng=self.rng)
+            self.exact_evals += int(exact.sum())
+            self.da_iters += int(n_iter) * C
+        else:
+            d, acc, last = self.session.run(init, sd, temps, int(n_iter),
+                                            int(seed) & 0xFFFFFFFF, proposal_mode, gamma,
+                                            de_noise, proposal_l, rng=self.rng)
+        self.consumed += int(n_iter)
         return d.reshape((int(n_iter), C, self.np), order="F"), acc.astype(np.float64), last
 
+    def da_summary(self):
+        out = dict(self.info)
+        if self.da_iters:
+            out["exact_fraction"] = self.exact_evals / self.da_iters
+        return out
+
     def close(self):
+        if self.net is not None:
+            self.net.close()
         self.session.close()
 
 
 def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_iter=2000,
                    n_chains=4, warmup=None, adapt=True, method="rwm", temperatures=None,
                    swap_every=None, gamma=None, de_noise=1e-3, de_every=None, de_sync=False,
-                   seed=1, backend="b200", rng="triple32") -> GpumFit:
-    """Run the batched Metropolis sampler on the B200 backend (``R/api.R:247-599``)."""
+                   seed=1, backend="b200", rng="triple32", surrogate=None) -> GpumFit:
+    """Run the batched Metropolis sampler on the B200 backend (``R/api.R:247-599``).
+
+    ``surrogate``: None/False (exact Metropolis, the reference's behaviour),
+    True, or a dict overriding ``SURROGATE_DEFAULTS`` -- delayed acceptance
+    in the sampling phase (rwm, pt, de; needs warmup > 0)."""
     if not isinstance(model, GpumModel):
         raise GpumInputError("`model` must be a gpum_model from gpum_model().")
     if backend not in ("b200", "auto"):
@@ -184,11 +270,36 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
             raise GpumInputError("`de_sync = TRUE` (synchronous per-generation DE) is not "
                                  "available on the b200 backend in this build.")
 
-    call = _Backend(model, data_mat, n_obs, rng_kind)
+    scfg = None
+    if surrogate is not None and surrogate is not False:
+        if method == "mala":
+            raise GpumInputError("`surrogate` (delayed acceptance) needs a symmetric proposal: "
+                                 'method "rwm", "pt" or "de", not "mala".')
+        if warmup <= 0:
+            raise GpumInputError("`surrogate` needs warmup > 0: its training pairs come from "
+                                 "the warmup's exact evaluations.")
+        scfg = dict(SURROGATE_DEFAULTS)
+        if isinstance(surrogate, dict):
+            unknown = set(surrogate) - set(scfg)
+            if unknown:
+                raise GpumInputError("unknown surrogate option(s): " + ", ".join(sorted(unknown)))
+            scfg.update(surrogate)
+        elif surrogate is not True:
+            raise GpumInputError("`surrogate` must be None, True or a dict of options.")
+
+    call = _Backend(model, data_mat, n_obs, rng_kind, scfg)
+    if scfg is not None:
+        every = {"pt": swap_every, "de": de_every}.get(method)
+        w_eff = warmup if every is None else max(0, min(-(-n_iter // every), warmup // every)) * every
+        call.record_at = w_eff // 2
+        call.da_at = w_eff if method != "rwm" else None
     try:
-        return _route(model, call, method, npar, n_chains, init_mat, sd_mat, n_iter, warmup,
-                      warmup_auto, adapt, temps, swap_every, gamma, de_noise, de_every,
-                      int(seed), backend)
+        fit = _route(model, call, method, npar, n_chains, init_mat, sd_mat, n_iter, warmup,
+                     warmup_auto, adapt, temps, swap_every, gamma, de_noise, de_every,
+                     int(seed), backend)
+        if scfg is not None:
+            fit.extra["surrogate"] = call.da_summary()
+        return fit
     finally:
         call.close()
 
@@ -220,6 +331,7 @@ def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmu
     if adapt and warmup > 0:
         am = AD.am_orchestrate_warmup(call, npar, C, init_mat, sd_mat, warmup, seed,
                                       auto_stop=warmup_auto, langevin=langevin)
+        call.start_da()
         samp = max(1, n_iter - am.warmup_used)
         use_L = npar > 1 and am.final_L is not None
         draws, acc, _ = call(am.final_init, am.final_proposal_sd, samp, am.seed_next, None,
@@ -230,6 +342,19 @@ def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmu
                        {"final_proposal_sd": am.final_proposal_sd,
                         "final_scales": am.final_scales, "n_batches": am.n_batches,
                         "batch_sizes": am.batch_sizes, "accept_history": am.accept_history})
+    if call.cfg is not None:
+        # Delayed acceptance without adaptation: exact warmup in two halves
+        # (the second recorded), then two-stage sampling from its last state.
+        h1 = warmup // 2
+        cur = init_mat
+        if h1 > 0:
+            d1, _, _ = call(cur, sd_mat, h1, seed, None, 0)
+            cur = d1[-1]
+        d2, _, _ = call(cur, sd_mat, warmup - h1, seed + 1, None, 0)
+        call.start_da()
+        draws, acc, _ = call(d2[-1], sd_mat, n_iter - warmup, seed + 2, None, 0)
+        return GpumFit(draws, acc, model, n_iter - warmup, n_iter, warmup, C, npar, backend,
+                       seed, method)
     draws, acc, _ = call(init_mat, sd_mat, n_iter, seed, None, 3 if langevin else 0)
     kept = draws[warmup:] if warmup > 0 else draws
     return GpumFit(kept, acc, model, n_iter - warmup, n_iter, warmup, C, npar, backend, seed,

@@ -35,6 +35,13 @@
 
 using namespace gpum;
 
+namespace gpum {
+// Surrogate inference on device parameters (mlp.cu).
+int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
+              std::string* err);
+int mlp_batch_rows(const gpum_b200_mlp* m);
+}  // namespace gpum
+
 static_assert(sizeof(CUtensorMap) == sizeof(TmapDesc), "tensor map size");
 
 namespace {
@@ -181,6 +188,19 @@ struct gpum_b200_session {
   cudaGraphExec_t gexec = nullptr;
   int graph_len = 0;
   uint64_t launches = 0;
+  // Training pairs for the surrogate (exact runs only).
+  DBuf<float> rec_theta;
+  DBuf<double> rec_ll;
+  uint64_t rec_cap = 0, rec_count = 0;
+  // Delayed acceptance.
+  DBuf<double> sll_x, sll_y, prior_x, prior_y, da_partials;
+  DBuf<uint32_t> da_flag, da_slot, da_active, da_iter, da_stage1;
+  DBuf<float> da_params;
+  Geometry geo_da{};
+  EvalArgs E_da{};
+  DaArgs D{};
+  gpum_b200_mlp* da_mlp = nullptr;
+  int da_chunks = 0;
 
   ~gpum_b200_session() {
     drop_graph();
@@ -231,7 +251,9 @@ struct gpum_b200_session {
     return k;
   }
 
-  Geometry geometry(int n, const KernelChoice& k) const {
+  // `busy_blocks`: chain blocks expected to do work (delayed acceptance
+  // evaluates a compacted subset); 0 means all of them.
+  Geometry geometry(int n, const KernelChoice& k, int busy_blocks = 0) const {
     Geometry g{};
     g.G = k.G;
     const int groups = (n + g.G - 1) / g.G;
@@ -246,7 +268,8 @@ struct gpum_b200_session {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
     if (occ < 1) occ = 1;
     const int slots = num_sms() * occ;
-    int nob = std::max(1, (4 * slots) / g.NCB);
+    const int busy = busy_blocks > 0 ? std::min(busy_blocks, g.NCB) : g.NCB;
+    int nob = std::max(1, (4 * slots) / busy);
     nob = std::min(nob, std::max(1, g.ntiles));
     g.tiles_per_cta = g.ntiles > 0 ? (g.ntiles + nob - 1) / nob : 0;
     g.NOB = g.ntiles > 0 ? (g.ntiles + g.tiles_per_cta - 1) / g.tiles_per_cta : 1;
@@ -304,15 +327,23 @@ struct gpum_b200_session {
     ++launches;
   }
 
-  void launch(int phase) {
-    const dim3 grid(geo.NCB, geo.NOB);
+  void launch(int phase) { launch_with(geo, E, phase); }
+
+  void launch_with(const Geometry& g, EvalArgs& e, int phase) {
+    const dim3 grid(g.NCB, g.NOB);
     if (kc.compiled) {
-      void* args[] = {(void*)&tmap, (void*)&E, (void*)&A, (void*)&phase};
-      GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, geo.smem, stream));
+      void* args[] = {(void*)&tmap, (void*)&e, (void*)&A, (void*)&phase};
+      GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, g.smem, stream));
     } else {
-      launch_interp(variant, grid, geo.smem, stream, *prog, tmap, E, A, phase);
+      launch_interp(variant, grid, g.smem, stream, *prog, tmap, e, A, phase);
     }
     ++launches;
+  }
+
+  // Pairs recorded so far, after `n_done` iterations of the prepared run.
+  void settle_recording() {
+    if (A.rec_ll && prepared)
+      rec_count = std::min<uint64_t>(rec_cap, A.rec_base + (uint64_t)n_done * n_chains);
   }
 };
 
@@ -474,6 +505,7 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   require((uint64_t)max_iter * np * C <= (1ull << 33), "draw storage above 32 GiB",
           GPUM_ERR_UNSUPPORTED);
 
+  s->settle_recording();
   s->drop_graph();
   s->prepared = false;
   s->n_chains = (int)C;
@@ -549,6 +581,12 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
     A.my = s->my.p;
     A.vbuf = s->vbuf.p;
   }
+  if (s->rec_cap > 0) {
+    A.rec_theta = s->rec_theta.p;
+    A.rec_ll = s->rec_ll.p;
+    A.rec_base = s->rec_count;
+    A.rec_cap = s->rec_cap;
+  }
   s->launch(PH_INIT);
   s->max_iter = max_iter;
   s->n_done = 0;
@@ -622,6 +660,7 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
   require(pts != nullptr || n_points == 0, "points pointer is NULL");
   if (n_points == 0) return;
   require(n_points <= (1u << 24), "more than 2^24 points", GPUM_ERR_UNSUPPORTED);
+  s->settle_recording();
   s->prepared = false;  // the evaluation buffers are reused
   s->drop_graph();
   const size_t np = s->np;
@@ -670,6 +709,131 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
     }
     s->check_device_error();
   }
+}
+
+// ------------------------------------------------------ delayed acceptance
+// Exact start as prepare() (PH_INIT), then per iteration: surrogate at the
+// proposals (tcgen05 MLP) -> stage-1 decision -> compaction of the
+// survivors -> exact evaluation of the compacted prefix only (CTAs of dead
+// chain blocks exit at once) -> stage-2 decision, draw, next proposal.
+// The loop is captured in a CUDA graph of kDaGraphLen iterations.
+void da_step(gpum_b200_session* s) {
+  const int C = s->n_chains, np = (int)s->np;
+  std::string e;
+  const int rc = mlp_infer(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->stream, &e);
+  if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
+  cudaStream_t st = s->stream;
+  const unsigned cb = (unsigned)((C + 255) / 256);
+  da_stage1_kernel<<<cb, 256, 0, st>>>(s->A, s->D);
+  da_compact_kernel<<<1, 1024, 0, st>>>(s->A, s->D);
+  da_pack_kernel<<<(unsigned)(((size_t)C * np + 255) / 256), 256, 0, st>>>(s->A, s->D);
+  GPUM_CK(cudaGetLastError());
+  s->launch_with(s->geo_da, s->E_da, PH_EVAL);
+  da_finalize_kernel<<<cb, 256, 0, st>>>(s->A, s->D, s->da_partials.p, s->geo_da.NOB,
+                                         s->geo_da.C_pad);
+  da_tick_kernel<<<1, 32, 0, st>>>(s->D);
+  GPUM_CK(cudaGetLastError());
+  s->launches += 5 + 5 * (uint64_t)s->da_chunks;
+}
+
+void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const double* sd,
+            const double* temps, uint32_t C, uint32_t n_iter, uint32_t seed, uint32_t mode,
+            double gamma, double de_noise, const double* L, size_t n_l, int rng, float* out_draws,
+            float* out_accept, double* out_last, uint32_t* out_exact) {
+  require(s != nullptr, "session is NULL");
+  require(mlp != nullptr, "surrogate is NULL");
+  require(mode <= 2, "delayed acceptance needs a symmetric proposal: mode 0 (rwm), 1 (de) or 2 "
+                     "(cholesky)");
+  const uint64_t keep_cap = s->rec_cap;
+  s->rec_cap = 0;  // stage-1 rejections leave no exact pair to record
+  try {
+    prepare(s, init, sd, temps, C, n_iter, seed, mode, gamma, de_noise, L, n_l, rng);
+  } catch (...) {
+    s->rec_cap = keep_cap;
+    throw;
+  }
+  s->rec_cap = keep_cap;
+  const int np = (int)s->np;
+  cudaStream_t st = s->stream;
+  const Geometry& g = s->geo;
+  s->sll_x.ensure(C);
+  s->sll_y.ensure(C);
+  s->prior_x.ensure(C);
+  s->prior_y.ensure(C);
+  s->da_flag.ensure(C);
+  s->da_slot.ensure(C);
+  s->da_stage1.ensure(C);
+  s->da_active.ensure(1);
+  s->da_iter.ensure(1);
+  s->da_params.ensure((size_t)np * g.C_pad);
+  // The exact evaluation sees about a quarter of the chains (a tuned RWM
+  // accepts ~1/4 at stage 1): more observation blocks keep the GPU full.
+  s->geo_da = s->geometry((int)C, s->kc, std::max(1, g.NCB / 4));
+  s->da_partials.ensure((size_t)s->geo_da.NOB * s->geo_da.C_pad);
+  GPUM_CK(cudaMemsetAsync(s->da_params.p, 0, sizeof(float) * np * g.C_pad, st));
+  s->E_da = s->E;
+  s->E_da.tiles_per_cta = s->geo_da.tiles_per_cta;
+  s->E_da.params = s->da_params.p;
+  s->E_da.partials = s->da_partials.p;
+  s->E_da.active = s->da_active.p;
+  DaArgs& D = s->D;
+  D.sll_x = s->sll_x.p;
+  D.sll_y = s->sll_y.p;
+  D.prior_x = s->prior_x.p;
+  D.prior_y = s->prior_y.p;
+  D.flag = s->da_flag.p;
+  D.slot = s->da_slot.p;
+  D.active = s->da_active.p;
+  D.iter = s->da_iter.p;
+  D.stage1 = s->da_stage1.p;
+  D.params = s->da_params.p;
+  D.full = s->params.p;
+  D.C_pad = g.C_pad;
+  s->da_mlp = mlp;
+  s->da_chunks = 0;
+  std::string e;
+  int rc = mlp_infer(mlp, s->state.p, (int)C, np, s->sll_x.p, st, &e);
+  if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
+  s->da_chunks = (int)((C + mlp_batch_rows(mlp) - 1) / mlp_batch_rows(mlp));
+  s->launches += 5 * (uint64_t)s->da_chunks;
+  da_setup_kernel<<<(C + 255) / 256, 256, 0, st>>>(s->A, D);
+  GPUM_CK(cudaGetLastError());
+  ++s->launches;
+
+  constexpr uint32_t kDaGraphLen = 16;
+  uint32_t left = n_iter;
+  if (n_iter >= kDaGraphLen) {
+    GPUM_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = s->launches;
+    try {
+      for (uint32_t i = 0; i < kDaGraphLen; ++i) da_step(s);
+    } catch (...) {
+      cudaGraph_t gr = nullptr;
+      cudaStreamEndCapture(st, &gr);
+      if (gr) cudaGraphDestroy(gr);
+      throw;
+    }
+    const uint64_t per_graph = s->launches - before;
+    s->launches = before;
+    GPUM_CK(cudaStreamEndCapture(st, &s->graph));
+    GPUM_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
+    while (left >= kDaGraphLen) {
+      GPUM_CK(cudaGraphLaunch(s->gexec, st));
+      s->launches += per_graph;
+      left -= kDaGraphLen;
+    }
+    s->drop_graph();
+  }
+  for (; left > 0; --left) da_step(s);
+  s->n_done = n_iter;
+  s->A.rec_ll = nullptr;
+  fetch(s, out_draws, out_accept, out_last, nullptr);
+  if (out_exact) {
+    GPUM_CK(cudaMemcpyAsync(out_exact, s->da_stage1.p, sizeof(uint32_t) * C,
+                            cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaStreamSynchronize(st));
+  }
+  s->prepared = false;  // the DA state is not resumable through advance()
 }
 
 }  // namespace
@@ -875,6 +1039,56 @@ int gpum_b200_grad_batch(const uint32_t* code, size_t n_code, const double* cons
                          char* err, size_t err_len) {
   return one_shot_batch(code, n_code, consts, n_consts, n_params, data, n_cols, n_obs, points,
                         n_points, out, err, err_len, B_GRAD);
+}
+
+int gpum_b200_session_record(gpum_b200_session* s, uint64_t capacity, char* err,
+                             size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    require(capacity <= (1ull << 28), "more than 2^28 recorded pairs", GPUM_ERR_UNSUPPORTED);
+    s->settle_recording();
+    s->drop_graph();
+    s->prepared = false;
+    s->rec_count = 0;
+    s->rec_cap = capacity;
+    if (capacity == 0) {
+      s->rec_theta.release();
+      s->rec_ll.release();
+      return;
+    }
+    s->rec_theta.ensure((size_t)capacity * s->np);
+    s->rec_ll.ensure((size_t)capacity);
+  });
+}
+
+int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, double* out_ll,
+                               uint64_t max_pairs, uint64_t* n_pairs, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    s->settle_recording();
+    const uint64_t n = std::min<uint64_t>(s->rec_count, max_pairs);
+    if (n_pairs) *n_pairs = s->rec_count;
+    if (n == 0) return;
+    require(out_theta && out_ll, "output pointers are NULL");
+    s->check_device_error();
+    GPUM_CK(cudaMemcpyAsync(out_theta, s->rec_theta.p, sizeof(float) * n * s->np,
+                            cudaMemcpyDeviceToHost, s->stream));
+    GPUM_CK(cudaMemcpyAsync(out_ll, s->rec_ll.p, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                            s->stream));
+    GPUM_CK(cudaStreamSynchronize(s->stream));
+  });
+}
+
+int gpum_b200_session_run_da(gpum_b200_session* s, gpum_b200_mlp* surrogate, const double* init,
+                             const double* sd, const double* temps, uint32_t n_chains,
+                             uint32_t n_iter, uint32_t seed, uint32_t mode, double gamma,
+                             double de_noise, const double* L, size_t n_l, int rng,
+                             float* out_draws, float* out_accept, double* out_last,
+                             uint32_t* out_exact, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    run_da(s, surrogate, init, sd, temps, n_chains, n_iter, seed, mode, gamma, de_noise, L, n_l,
+           rng, out_draws, out_accept, out_last, out_exact);
+  });
 }
 
 }  // extern "C"

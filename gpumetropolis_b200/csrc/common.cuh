@@ -57,6 +57,11 @@ struct ChainArgs {
   double* mx;           // [C][np] proposal mean from `state`
   double* my;           // [C][np] proposal mean from `prop`
   double* vbuf;         // [C][np] scratch
+  // Training pairs for the surrogate: every exactly evaluated proposal's
+  // (theta, data-term log-likelihood), slot rec_base + t*C + c (< rec_cap).
+  float* rec_theta;     // [rec_cap][np] or nullptr
+  double* rec_ll;       // [rec_cap]
+  uint64_t rec_base, rec_cap;
 };
 
 struct EvalArgs {
@@ -68,6 +73,7 @@ struct EvalArgs {
   int n_points;         // chains/points that are real (rest padding)
   uint32_t* tickets;    // [NCB]
   uint32_t* err;        // device error word
+  const uint32_t* active;  // if set: only the first *active points are live
 };
 
 // ------------------------------------------------------ f64 prior, interpreted
@@ -261,6 +267,13 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
     const double plp = ll + (mala ? Prior::value_grad(A, y, A.gy + (size_t)c * np)
                                   : Prior::value(A, y));
     A.last_eval[c] = plp;
+    if (A.rec_ll) {
+      const uint64_t slot = A.rec_base + (uint64_t)t * A.n_chains + c;
+      if (slot < A.rec_cap) {
+        for (int j = 0; j < np; ++j) A.rec_theta[slot * np + j] = (float)y[j];
+        A.rec_ll[slot] = ll;
+      }
+    }
     double lqd = 0.0;
     if (mala) {
       // q(x | y) - q(y | x) with the truncated drift at y (cpu_native.rs:704-710)
@@ -333,6 +346,8 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   // Chain blocks vary fastest, so the CTAs that share an observation tile
   // run in the same wave and read it through L2 once.
   const int cb = blockIdx.x, ob = blockIdx.y;
+  // Delayed acceptance evaluates a compacted prefix of live points only.
+  if (E.active && cb * CG >= (int)*E.active) return;
   const int WO = kWarps / E.WC;
   const int wc = warp % E.WC, wo = warp / E.WC;
 

@@ -94,3 +94,149 @@ static __global__ void draws_layout_kernel(const float* __restrict__ in, float* 
 }
 
 }  // namespace gpum
+
+// ===================================================== delayed acceptance
+// Two-stage Metropolis-Hastings (Christen & Fox 2005) with the surrogate
+// log-likelihood s() as stage 1 and the exact log-likelihood l() as stage 2:
+//   stage 1: accept y with min(1, exp([s(y)+p(y) - s(x)-p(x)] / T))
+//   stage 2: accept with min(1, exp([(l(y)-l(x)) - (s(y)-s(x))] / T))
+// (p = prior, which cancels in stage 2).  The product of the two acceptance
+// probabilities satisfies detailed balance for the exact tempered posterior,
+// so the target is unchanged; only stage-1 survivors are evaluated exactly.
+namespace gpum {
+
+struct DaArgs {
+  double* sll_x;     // [C] surrogate log-likelihood at the state
+  double* sll_y;     // [C] surrogate log-likelihood at the proposal
+  double* prior_x;   // [C] prior at the state
+  double* prior_y;   // [C] prior at the proposal
+  uint32_t* flag;    // [C] stage 1 accepted this iteration
+  uint32_t* slot;    // [C] position in the compacted evaluation
+  uint32_t* active;  // [1] stage-1 acceptances this iteration
+  uint32_t* iter;    // [1] iterations done
+  uint32_t* stage1;  // [C] stage-1 acceptance counts
+  float* params;     // [np][C_pad] compacted evaluation points
+  float* full;       // [np][C_pad] scratch for propose()
+  int C_pad;
+};
+
+__device__ __forceinline__ double da_uniform(Stream& rs, uint32_t t, uint32_t k) {
+  if (rs.kind == RNG_TRIPLE32) return rs.next();
+  rs.it = t;
+  rs.k = k;
+  return rs.next();
+}
+
+// After the exact start (PH_INIT): the prior at each state, zero counters.
+static __global__ void da_setup_kernel(ChainArgs A, DaArgs D) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c == 0) D.iter[0] = 0;
+  if (c >= A.n_chains) return;
+  D.prior_x[c] = InterpPrior::value(A, A.state + (size_t)c * A.np);
+  D.stage1[c] = 0;
+}
+
+static __global__ void da_stage1_kernel(ChainArgs A, DaArgs D) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.n_chains) return;
+  const uint32_t t = D.iter[0];
+  const double* y = A.prop + (size_t)c * A.np;
+  const double py = InterpPrior::value(A, y);
+  D.prior_y[c] = py;
+  Stream rs = make_stream(A, c);
+  const double u = da_uniform(rs, t, 0xFFFF0001u);
+  const double a1 = ((D.sll_y[c] + py) - (D.sll_x[c] + D.prior_x[c])) / A.temp[c];
+  D.flag[c] = log(u) < a1 ? 1u : 0u;
+  A.ctr[c] = rs.ctr;
+}
+
+// Deterministic compaction: one block scans the flags in chain order.
+static __global__ void da_compact_kernel(ChainArgs A, DaArgs D) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < A.n_chains; base += blockDim.x) {
+    const int c = base + tid;
+    const uint32_t f = c < A.n_chains ? D.flag[c] : 0u;
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += v;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const int nw = blockDim.x >> 5;
+      uint32_t ws = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, ws, off);
+        if (lane >= off) ws += v;
+      }
+      if (lane < nw) warp_sums[lane] = ws;  // inclusive warp prefix
+    }
+    __syncthreads();
+    const uint32_t before = carry + (warp > 0 ? warp_sums[warp - 1] : 0u) + incl - f;
+    if (c < A.n_chains) D.slot[c] = before;
+    __syncthreads();
+    if (tid == blockDim.x - 1) carry += warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+  }
+  if (tid == 0) D.active[0] = carry;
+}
+
+// Stage-1 survivors' proposals into the compacted f32 evaluation array.
+static __global__ void da_pack_kernel(ChainArgs A, DaArgs D) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)A.n_chains * A.np) return;
+  const int c = (int)(i / A.np), j = (int)(i % A.np);
+  if (!D.flag[c]) return;
+  D.params[(size_t)j * D.C_pad + D.slot[c]] = (float)A.prop[i];
+}
+
+// Stage 2 for the survivors, the draw for every chain, the next proposal.
+static __global__ void da_finalize_kernel(ChainArgs A, DaArgs D, const double* __restrict__ partials,
+                                          int nob, int C_pad_eval) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.n_chains) return;
+  const int np = A.np;
+  const uint32_t t = D.iter[0];
+  double* x = A.state + (size_t)c * np;
+  const double* y = A.prop + (size_t)c * np;
+  Stream rs = make_stream(A, c);
+  if (D.flag[c]) {
+    const uint32_t k = D.slot[c];
+    double ll = 0.0;
+    for (int o = 0; o < nob; ++o) ll += partials[(size_t)o * C_pad_eval + k];
+    const double plp = ll + D.prior_y[c];
+    A.last_eval[c] = plp;
+    const double u = da_uniform(rs, t, 0xFFFF0002u);
+    const double llx = A.cur[c] - D.prior_x[c];
+    const double a2 = ((ll - llx) - (D.sll_y[c] - D.sll_x[c])) / A.temp[c];
+    if (log(u) < a2) {
+      for (int j = 0; j < np; ++j) x[j] = y[j];
+      A.cur[c] = plp;
+      D.sll_x[c] = D.sll_y[c];
+      D.prior_x[c] = D.prior_y[c];
+      A.accepts[c] += 1;
+    }
+    D.stage1[c] += 1;
+  }
+  if (t < A.n_iter)
+    for (int j = 0; j < np; ++j) A.draws[((size_t)t * np + j) * D.C_pad + c] = (float)x[j];
+  if (t + 1 < A.n_iter) {
+    rs.it = t + 1;
+    rs.k = 0;
+    propose(A, c, rs, D.full, D.C_pad);
+  }
+  A.ctr[c] = rs.ctr;
+}
+
+static __global__ void da_tick_kernel(DaArgs D) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) D.iter[0] += 1;
+}
+
+}  // namespace gpum

@@ -218,6 +218,25 @@ __global__ void mlp_to_bf16(const float* __restrict__ w, bf16* __restrict__ wh,
 
 unsigned blocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
+// Inference gather from f64 chain-major parameters [n][d].
+__global__ void mlp_gather64(const double* __restrict__ theta, int n, int d, int dp, int B,
+                             const float* __restrict__ xmean, const float* __restrict__ xinv,
+                             bf16* __restrict__ Xh) {
+  const int row = blockIdx.x;
+  if (row >= B) return;
+  for (int j = threadIdx.x; j < dp; j += blockDim.x) {
+    float v = 0.0f;
+    if (row < n && j < d) v = ((float)theta[(size_t)row * d + j] - xmean[j]) * xinv[j];
+    Xh[(size_t)row * dp + j] = __float2bfloat16(v);
+  }
+}
+
+__global__ void mlp_unscale(const float* __restrict__ y, int n, float ysd, float ymean,
+                            double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)y[i] * ysd + ymean;
+}
+
 }  // namespace
 
 struct gpum_b200_mlp {
@@ -238,6 +257,7 @@ struct gpum_b200_mlp {
   float ymean = 0.0f, yinv = 1.0f, ysd = 1.0f;
   Buf<uint32_t> err;
   int adam_t = 0;
+  bool smem_set[2] = {false, false};
 
   ~gpum_b200_mlp() {
     if (st) cudaStreamDestroy(st);
@@ -247,8 +267,13 @@ struct gpum_b200_mlp {
   void gemm(const bf16* A, const bf16* Bm, float* C, const float* bias, bf16* act, int M, int N,
             int K) {
     const size_t smem = tc_gemm_smem<BN>();
-    MLP_CK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
+    // Set once, so later launches (possibly under stream capture) make no
+    // non-stream API calls.
+    if (!smem_set[BN == 128]) {
+      MLP_CK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+      smem_set[BN == 128] = true;
+    }
     dim3 grid(N / BN, M / kGemmBM);
     tc_gemm_kernel<BN><<<grid, kGemmThreads, smem, st>>>(A, Bm, C, bias, act, M, N, K, err.p);
     MLP_CK(cudaGetLastError());
@@ -378,6 +403,43 @@ void upload_pairs(gpum_b200_mlp* m, const double* theta, const double* ll, size_
 }
 
 }  // namespace
+
+namespace gpum {
+
+int mlp_batch_rows(const gpum_b200_mlp* m) { return m->B; }
+
+// Surrogate log-likelihood of n f64 parameter vectors (device, chain-major)
+// into out (device), enqueued on `st`.  Used by the delayed-acceptance loop.
+int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
+              std::string* err) {
+  if (!m || d != m->d) {
+    *err = "surrogate input width does not match the model's parameter count";
+    return GPUM_ERR_INVALID;
+  }
+  cudaStream_t keep = m->st;
+  m->st = st;
+  int rc = GPUM_OK;
+  try {
+    for (int r0 = 0; r0 < n; r0 += m->B) {
+      const int rows = std::min(m->B, n - r0);
+      mlp_gather64<<<m->B, 128, 0, st>>>(theta + (size_t)r0 * d, rows, d, m->dp, m->B,
+                                         m->xmean.p, m->xinv.p, m->Xh.p);
+      m->forward(m->B);
+      mlp_head<<<blocks((size_t)m->B * 32), 256, 0, st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr,
+                                                         m->B, m->H, m->B, m->yhat.p, nullptr,
+                                                         nullptr, nullptr, nullptr, 0);
+      mlp_unscale<<<blocks(rows), 256, 0, st>>>(m->yhat.p, rows, m->ysd, m->ymean, out + r0);
+      MLP_CK(cudaGetLastError());
+    }
+  } catch (const MlpFail& f) {
+    *err = f.msg;
+    rc = f.code;
+  }
+  m->st = keep;
+  return rc;
+}
+
+}  // namespace gpum
 
 extern "C" {
 

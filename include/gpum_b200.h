@@ -244,6 +244,34 @@ GPUM_API int gpum_b200_mlp_get_params(gpum_b200_mlp* m, float* out, char* err, s
 GPUM_API int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
                                       const float* B, float* C, char* err, size_t err_len);
 
+/* ------------------------------------------------- delayed acceptance --
+ * No counterpart in the reference.  Training pairs come from exact runs:
+ * with recording on, every proposal an exact step (session_run / advance)
+ * evaluates is stored as (theta as f32, data-term log-likelihood), up to
+ * `capacity` pairs; capacity 0 turns recording off and frees the store.
+ * Calling record() again restarts the store. */
+GPUM_API int gpum_b200_session_record(gpum_b200_session* s, uint64_t capacity, char* err,
+                                      size_t err_len);
+/* Copies the first min(recorded, max_pairs) pairs (theta row-major
+ * n x n_params, ll n); *n_pairs = pairs recorded so far. */
+GPUM_API int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, double* out_ll,
+                                        uint64_t max_pairs, uint64_t* n_pairs, char* err,
+                                        size_t err_len);
+/* Two-stage Metropolis-Hastings (Christen & Fox): the surrogate screens each
+ * proposal (stage 1) and only survivors are evaluated exactly (stage 2), so
+ * the chains target the exact tempered posterior.  Same arguments and
+ * outputs as session_run for proposal modes 0, 1 and 2 (MALA is refused);
+ * out_exact (may be NULL) receives per chain the number of exact
+ * evaluations (stage-1 acceptances).  The surrogate must have d = n_params. */
+GPUM_API int gpum_b200_session_run_da(gpum_b200_session* s, gpum_b200_mlp* surrogate,
+                                      const double* init, const double* proposal_sd,
+                                      const double* temperatures, uint32_t n_chains,
+                                      uint32_t n_iter, uint32_t seed, uint32_t proposal_mode,
+                                      double gamma, double de_noise, const double* proposal_l,
+                                      size_t n_l, int rng, float* out_draws, float* out_accept,
+                                      double* out_last_logpost, uint32_t* out_exact, char* err,
+                                      size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,138 @@
+"""Delayed acceptance on the B200: pair recording, the two-stage kernels
+against the CPU restatement (oracle/da_oracle.py) with the very surrogate the
+GPU uses, and the posterior of the API-level surrogate mode."""
+import numpy as np
+import pytest
+
+from gpumetropolis_b200 import api
+from gpumetropolis_b200 import workloads as W
+from gpumetropolis_b200.diagnostics import rhat
+from oracle import da_oracle
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _session(gpu, w):
+    m = w.model
+    return gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                       w.data, m.n_cols, w.n_obs)
+
+
+def _trained(gpu, s, w, init, sd, n_iter=100, steps=600, hidden=128, batch=1024):
+    """A surrogate trained on the pairs of one recorded exact run."""
+    C = init.shape[0]
+    s.record(n_iter * C)
+    s.run(init, sd, np.ones(C), n_iter, 5, 0)
+    theta, ll = s.recorded()
+    s.record(0)
+    net = gpu.Surrogate(w.model.n_params, hidden=hidden, batch=batch, seed=3)
+    net.fit_normalizer(theta.astype(np.float64), ll)
+    net.train(theta.astype(np.float64), ll, steps, lr=2e-3)
+    return net
+
+
+def test_recording_stores_every_exact_proposal(gpu):
+    w = W.make("logistic", n_obs=3000)
+    m = w.model
+    C, n = 48, 12
+    rng = np.random.default_rng(1)
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.02)
+    with _session(gpu, w) as s:
+        s.record(10 * C * n)
+        s.run(init, sd, np.ones(C), n, 7, 0)
+        theta, ll = s.recorded()
+        assert theta.shape == (n * C, m.n_params) and ll.shape == (n * C,)
+        want = O.loglik_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
+                              w.n_obs, theta.astype(np.float64))
+        np.testing.assert_allclose(ll, want, rtol=1e-6)
+        # a second run appends; the proposals of iteration 0 are slot 0..C-1
+        s.run(init, sd, np.ones(C), n, 8, 0)
+        theta2, ll2 = s.recorded()
+        assert theta2.shape[0] == 2 * n * C
+        np.testing.assert_array_equal(theta2[: n * C], theta)
+        # capacity bounds the store
+        s.record(C + 5)
+        s.run(init, sd, np.ones(C), n, 9, 0)
+        assert s.recorded()[0].shape[0] == C + 5
+        s.record(0)
+        assert s.recorded()[0].shape[0] == 0
+
+
+@pytest.mark.parametrize("temps_kind", ["cold", "tempered"])
+def test_two_stage_trajectories_match_oracle(gpu, temps_kind):
+    w = W.make("logistic", n_obs=2048, p=4)
+    m = w.model
+    rng = np.random.default_rng(2)
+    C, n_iter, seed = 12, 30, 21
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.04)
+    temps = np.ones(C) if temps_kind == "cold" else np.where(np.arange(C) % 3 == 0, 2.5, 1.0)
+    with _session(gpu, w) as s:
+        big = w.truth["beta"] + rng.normal(0, 0.05, (256, m.n_params))
+        net = _trained(gpu, s, w, big, np.full((256, m.n_params), 0.04))
+        try:
+            d, acc, last, exact = s.run_da(net, init, sd, temps, n_iter, seed, 0)
+            d = d.reshape((n_iter, C, m.n_params), order="F")
+            od, oacc, oexact, tie_at = da_oracle.run_da(
+                m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                w.data, m.n_cols, w.n_obs, init, sd, temps, n_iter, seed, net.predict)
+        finally:
+            net.close()
+    clean = tie_at == n_iter
+    assert clean.sum() >= C // 2
+    for c in range(C):
+        t = tie_at[c]
+        np.testing.assert_allclose(d[:t, c], od[:t, c], rtol=2e-6, atol=1e-6)
+    np.testing.assert_array_equal(exact[clean], oexact[clean])
+    np.testing.assert_allclose(acc[clean], oacc[clean] / n_iter, atol=1e-6)
+    # the surrogate screens: fewer exact evaluations than iterations
+    assert exact.sum() < C * n_iter
+
+
+def test_run_da_refuses_mala(gpu):
+    w = W.make("gaussian", n_obs=500)
+    C = 4
+    with _session(gpu, w) as s:
+        net = gpu.Surrogate(1, hidden=128, batch=128)
+        try:
+            with pytest.raises(gpu.GpumError, match="symmetric proposal"):
+                s.run_da(net, np.zeros((C, 1)), np.full((C, 1), 0.1), np.ones(C), 10, 1, 3)
+        finally:
+            net.close()
+
+
+def test_surrogate_mode_recovers_closed_form(gpu):
+    w = W.make("gaussian", n_obs=20000)
+    fit = api.gpu_metropolis(w.model, {"y": w.data[:, 0]}, init=np.full((128, 1), 3.0),
+                             proposal_sd=0.02, n_iter=3000, warmup=1500, seed=4,
+                             surrogate={"hidden": 128, "batch": 2048, "steps": 800})
+    info = fit.extra["surrogate"]
+    assert info["used"], info
+    assert 0.0 < info["exact_fraction"] < 0.9
+    d = fit.draws[:, :, 0]
+    n_eff = d.size / 20.0  # conservative: autocorrelation time <= 20 at this acceptance
+    mcse = d.std() / np.sqrt(n_eff)
+    assert abs(d.mean() - w.truth["post_mean"]) < 5 * mcse
+    assert abs(d.std() - w.truth["post_sd"]) < 0.1 * w.truth["post_sd"]
+    assert rhat(d, warmup=0) < 1.01
+
+
+def test_surrogate_mode_pt(gpu):
+    # y ~ N(|mu|, 1): two modes ~1500 nats apart, so chains start on both
+    # sides and swaps carry states to the cold chain (as test-pt.R:198-217)
+    rng = np.random.default_rng(5)
+    y = rng.normal(3.0, 1.0, 400)
+    from gpumetropolis_b200.dsl import gpum_model
+    m = gpum_model("~ log(exp(-0.5 * (y - mu)^2) + exp(-0.5 * (y + mu)^2))", params="mu",
+                   data="y")
+    init = np.linspace(-6, 6, 8).reshape(8, 1)
+    fit = api.gpu_metropolis(m, {"y": y}, init=init, proposal_sd=0.15,
+                             n_iter=4000, warmup=2000, method="pt", seed=6,
+                             surrogate={"hidden": 128, "batch": 1024, "steps": 600,
+                                        "min_pairs": 512})
+    assert fit.extra["surrogate"]["used"], fit.extra["surrogate"]
+    cold = fit.draws[:, 0, 0]
+    assert np.any(cold > 1.5) and np.any(cold < -1.5)
+    assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
