@@ -74,6 +74,8 @@ SIGNATURES = {
     "gpum_b200_mlp_destroy": (None, [C.c_void_p]),
     "gpum_b200_mlp_set_normalizer": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_double,
                                                C.c_double, _errp, _sz]),
+    "gpum_b200_mlp_set_whitening": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_double,
+                                              C.c_double, _errp, _sz]),
     "gpum_b200_mlp_train": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, C.c_uint32, C.c_double,
                                       _f32p, _errp, _sz]),
     "gpum_b200_mlp_predict": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
@@ -459,11 +461,30 @@ class Surrogate:
                                                       _p(xs, C.c_double), float(ymean),
                                                       float(ysd), err, _ERRLEN), err)
 
-    def fit_normalizer(self, theta, ll):
+    def set_whitening(self, xmean, xw, ymean, ysd):
+        xm, w = _f64(xmean), _f64(xw)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_set_whitening(self._h, _p(xm, C.c_double),
+                                                     _p(w, C.c_double), float(ymean),
+                                                     float(ysd), err, _ERRLEN), err)
+
+    def fit_normalizer(self, theta, ll, whiten=False):
+        """Standardise the target; inputs per coordinate, or (``whiten``)
+        by the inverse Cholesky factor of their covariance."""
         theta = np.asarray(theta, dtype=np.float64).reshape(-1, self.d)
+        ysd = float(np.std(ll)) or 1.0
+        if whiten and self.d > 1:
+            cov = np.cov(theta, rowvar=False)
+            cov = cov + np.eye(self.d) * 1e-10 * max(float(np.mean(np.diag(cov))), 1e-300)
+            try:
+                Linv = np.linalg.inv(np.linalg.cholesky(cov))
+            except np.linalg.LinAlgError:
+                pass
+            else:
+                self.set_whitening(theta.mean(axis=0), Linv, float(np.mean(ll)), ysd)
+                return
         sd = theta.std(axis=0)
         sd = np.where(sd > 0, sd, 1.0)
-        ysd = float(np.std(ll)) or 1.0
         self.set_normalizer(theta.mean(axis=0), sd, float(np.mean(ll)), ysd)
 
     def train(self, theta, ll, steps, lr=1e-3):

@@ -93,8 +93,14 @@ def _data_matrix(model: GpumModel, data):
     return np.ascontiguousarray(np.stack(cols, axis=1)), n
 
 
-SURROGATE_DEFAULTS = {"hidden": 256, "batch": 4096, "steps": 3000, "lr": 1e-3,
-                      "max_pairs": 1 << 20, "min_pairs": 2048, "seed": 1}
+# hidden/batch: network width and training batch (multiples of 128); steps/lr:
+# Adam steps at lr, then steps at lr/3 and lr/10; step_scale multiplies the
+# adapted random-walk proposal in the two-stage phase (screening makes
+# rejections cheap, so longer steps pay: Sherlock, Thiery & Golightly 2021);
+# whiten: inputs whitened by the pairs' covariance.
+SURROGATE_DEFAULTS = {"hidden": 256, "batch": 4096, "steps": 2000, "lr": 2e-3,
+                      "max_pairs": 1 << 20, "min_pairs": 2048, "seed": 1,
+                      "step_scale": 1.6, "whiten": True}
 
 
 class _Backend:
@@ -150,8 +156,10 @@ class _Backend:
         hold, train = idx[:n_hold], idx[n_hold:]
         net = _native.Surrogate(self.np, hidden=int(self.cfg["hidden"]),
                                 batch=int(self.cfg["batch"]), seed=int(self.cfg["seed"]))
-        net.fit_normalizer(theta[train], ll[train])
-        loss = net.train(theta[train], ll[train], int(self.cfg["steps"]), lr=float(self.cfg["lr"]))
+        net.fit_normalizer(theta[train], ll[train], whiten=bool(self.cfg["whiten"]))
+        steps, lr = int(self.cfg["steps"]), float(self.cfg["lr"])
+        for f in (1.0, 1.0 / 3.0, 0.1):
+            loss = net.train(theta[train], ll[train], steps, lr=lr * f)
         resid = net.predict(theta[hold]) - ll[hold]
         self.net = net
         self.info = {"used": True, "pairs": int(theta.shape[0]),
@@ -167,6 +175,11 @@ class _Backend:
             self.start_da()
         self._maybe_record(C, n_iter)
         if self.net is not None and proposal_mode != _native.MODE_MALA:
+            k = float(self.cfg["step_scale"])
+            if proposal_mode in (_native.MODE_RWM, _native.MODE_CHOL) and k != 1.0:
+                sd = np.asarray(sd, dtype=np.float64) * k
+                if proposal_l is not None:
+                    proposal_l = np.asarray(proposal_l, dtype=np.float64) * k
             d, acc, last, exact = self.session.run_da(
                 self.net, init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF, proposal_mode,
                 gamma, de_noise, proposal_l, rng=self.rng)

@@ -723,14 +723,17 @@ void da_step(gpum_b200_session* s) {
   const int rc = mlp_infer(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->stream, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
   cudaStream_t st = s->stream;
-  const unsigned cb = (unsigned)((C + 255) / 256);
-  da_stage1_kernel<<<cb, 256, 0, st>>>(s->A, s->D);
+  // 64-thread blocks spread the per-chain f64 work (prior, proposal) over
+  // more SMs; finalize runs one warp per chain.
+  const unsigned cb = (unsigned)((C + 63) / 64);
+  da_stage1_kernel<<<cb, 64, 0, st>>>(s->A, s->D);
   da_compact_kernel<<<1, 1024, 0, st>>>(s->A, s->D);
   da_pack_kernel<<<(unsigned)(((size_t)C * np + 255) / 256), 256, 0, st>>>(s->A, s->D);
   GPUM_CK(cudaGetLastError());
   s->launch_with(s->geo_da, s->E_da, PH_EVAL);
-  da_finalize_kernel<<<cb, 256, 0, st>>>(s->A, s->D, s->da_partials.p, s->geo_da.NOB,
-                                         s->geo_da.C_pad);
+  da_finalize_kernel<<<(unsigned)((C + 7) / 8), 256, 0, st>>>(
+      s->A, s->D, s->da_partials.p, s->geo_da.CG, s->geo_da.NCB * s->geo_da.NOB,
+      s->geo_da.ntiles, s->geo_da.C_pad);
   da_tick_kernel<<<1, 32, 0, st>>>(s->D);
   GPUM_CK(cudaGetLastError());
   s->launches += 5 + 5 * (uint64_t)s->da_chunks;
@@ -766,13 +769,21 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   s->da_active.ensure(1);
   s->da_iter.ensure(1);
   s->da_params.ensure((size_t)np * g.C_pad);
-  // The exact evaluation sees about a quarter of the chains (a tuned RWM
-  // accepts ~1/4 at stage 1): more observation blocks keep the GPU full.
-  s->geo_da = s->geometry((int)C, s->kc, std::max(1, g.NCB / 4));
-  s->da_partials.ensure((size_t)s->geo_da.NOB * s->geo_da.C_pad);
+  // The exact evaluation runs a fixed 1-D grid of 4 CTAs per resident slot
+  // (at least one per chain block); the kernel splits it into (live chain
+  // blocks x observation blocks) from the stage-1 survivor count on the
+  // device (da_obs_blocks).
+  s->geo_da = g;
+  {
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kc.fn, kThreads, g.smem);
+    s->geo_da.NCB = std::max(4 * num_sms() * std::max(occ, 1), g.NCB);
+    s->geo_da.NOB = 1;
+  }
+  const int max_nob = std::max(1, std::min(s->geo_da.NCB, std::max(g.ntiles, 1)));
+  s->da_partials.ensure((size_t)max_nob * s->geo_da.C_pad);
   GPUM_CK(cudaMemsetAsync(s->da_params.p, 0, sizeof(float) * np * g.C_pad, st));
   s->E_da = s->E;
-  s->E_da.tiles_per_cta = s->geo_da.tiles_per_cta;
   s->E_da.params = s->da_params.p;
   s->E_da.partials = s->da_partials.p;
   s->E_da.active = s->da_active.p;

@@ -76,6 +76,27 @@ struct EvalArgs {
   const uint32_t* active;  // if set: only the first *active points are live
 };
 
+// Delayed acceptance evaluates the first `live` points of the compacted array
+// with a fixed 1-D grid of `total` CTAs, whose split into chain blocks x
+// observation blocks is decided on the device from `live`, so the GPU stays
+// full whatever stage 1 accepted.  Returns the observation blocks used (0 if
+// nothing is live) and the tiles per CTA.
+__host__ __device__ inline int da_obs_blocks(int live, int CG, int total, int ntiles, int* tpc) {
+  const int busy = (live + CG - 1) / CG;
+  if (busy <= 0) {
+    *tpc = 0;
+    return 0;
+  }
+  if (ntiles <= 0) {
+    *tpc = 0;
+    return 1;
+  }
+  int nob = total / busy;
+  nob = nob < 1 ? 1 : (nob > ntiles ? ntiles : nob);
+  *tpc = (ntiles + nob - 1) / nob;
+  return (ntiles + *tpc - 1) / *tpc;
+}
+
 // ------------------------------------------------------ f64 prior, interpreted
 // The prior is a handful of ops once per chain per iteration; it is
 // interpreted in f64 from the source bytecode (semantics of
@@ -101,7 +122,14 @@ __device__ inline double prior_interp(const uint32_t* __restrict__ code, int n,
       case 9: st[sp - 1] = log(st[sp - 1]); break;
       case 10: st[sp - 1] = sqrt(st[sp - 1]); break;
       case 12: st[sp - 1] = lgamma(st[sp - 1]); break;
-      default: st[sp - 2] = pow(st[sp - 2], st[sp - 1]); --sp; break;
+      // x^2 squared exactly: the correctly rounded x*x, which is what the
+      // host libm's pow returns for an exponent of 2
+      default: {
+        const double a = st[sp - 2], b = st[sp - 1];
+        st[sp - 2] = b == 2.0 ? a * a : pow(a, b);
+        --sp;
+        break;
+      }
     }
   }
   return st[0];
@@ -345,9 +373,17 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   const int CG = E.CG, T = E.T, ncols = E.ncols, np = E.np;
   // Chain blocks vary fastest, so the CTAs that share an observation tile
   // run in the same wave and read it through L2 once.
-  const int cb = blockIdx.x, ob = blockIdx.y;
-  // Delayed acceptance evaluates a compacted prefix of live points only.
-  if (E.active && cb * CG >= (int)*E.active) return;
+  int cb = blockIdx.x, ob = blockIdx.y, tiles_per_cta = E.tiles_per_cta;
+  if (E.active) {  // delayed acceptance: geometry from the live count
+    const int live = (int)*E.active;
+    const int busy = (live + CG - 1) / CG;
+    const int nob = da_obs_blocks(live, CG, (int)(gridDim.x * gridDim.y), E.ntiles,
+                                  &tiles_per_cta);
+    const int id = (int)(blockIdx.y * gridDim.x + blockIdx.x);
+    if (busy == 0 || id >= busy * nob) return;
+    cb = id % busy;
+    ob = id / busy;
+  }
   const int WO = kWarps / E.WC;
   const int wc = warp % E.WC, wo = warp / E.WC;
 
@@ -363,8 +399,8 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
     psm[i] = E.params[(size_t)p * E.C_pad + (size_t)cb * CG + cl];
   }
 
-  const int t0 = ob * E.tiles_per_cta;
-  const int t1 = min(t0 + E.tiles_per_cta, E.ntiles);
+  const int t0 = ob * tiles_per_cta;
+  const int t1 = min(t0 + tiles_per_cta, E.ntiles);
   const int nt = max(t1 - t0, 0);
   const uint32_t tile_bytes = (uint32_t)(stage_floats * sizeof(float));
   // No tiles (or no data columns): the tensor map is never touched.

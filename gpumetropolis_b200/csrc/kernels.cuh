@@ -198,19 +198,31 @@ static __global__ void da_pack_kernel(ChainArgs A, DaArgs D) {
 }
 
 // Stage 2 for the survivors, the draw for every chain, the next proposal.
+// One warp per chain: the lanes add the chain's observation-block partials in
+// a fixed lane-strided order and a fixed shuffle tree (deterministic), lane 0
+// does the rest.
 static __global__ void da_finalize_kernel(ChainArgs A, DaArgs D, const double* __restrict__ partials,
-                                          int nob, int C_pad_eval) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+                                          int CG, int total, int ntiles, int C_pad_eval) {
+  const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (c >= A.n_chains) return;
+  const bool live = D.flag[c] != 0;
+  double ll = 0.0;
+  if (live) {
+    int tpc = 0;
+    const int nob = da_obs_blocks((int)D.active[0], CG, total, ntiles, &tpc);
+    const uint32_t k = D.slot[c];
+    for (int o = lane; o < nob; o += 32) ll += partials[(size_t)o * C_pad_eval + k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, off);
+  }
+  if (lane != 0) return;
   const int np = A.np;
   const uint32_t t = D.iter[0];
   double* x = A.state + (size_t)c * np;
   const double* y = A.prop + (size_t)c * np;
   Stream rs = make_stream(A, c);
-  if (D.flag[c]) {
-    const uint32_t k = D.slot[c];
-    double ll = 0.0;
-    for (int o = 0; o < nob; ++o) ll += partials[(size_t)o * C_pad_eval + k];
+  if (live) {
     const double plp = ll + D.prior_y[c];
     A.last_eval[c] = plp;
     const double u = da_uniform(rs, t, 0xFFFF0002u);

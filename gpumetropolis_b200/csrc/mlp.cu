@@ -78,24 +78,52 @@ __device__ __forceinline__ uint32_t pick(uint32_t seed, uint32_t step, uint32_t 
   return (uint32_t)(((uint64_t)r.x * n) >> 32);
 }
 
-// Batch rows: standardised inputs (bf16, padded with zeros) and targets.
+// Input transform of one row into Xh (bf16, zero padded to dp):
+//   per coordinate  v_j = (theta_j - xmean_j) * xinv_j            (xw == nullptr)
+//   whitening       v_j = sum_k xw[j][k] (theta_k - xmean_k)      (xw: d x d)
+// `cen` is block-shared scratch of d floats.  Called by every thread.
+template <class Src>
+__device__ __forceinline__ void mlp_input_row(Src theta_at, bool live, int d, int dp,
+                                              const float* __restrict__ xmean,
+                                              const float* __restrict__ xinv,
+                                              const float* __restrict__ xw, float* cen,
+                                              bf16* __restrict__ out) {
+  if (xw) {
+    for (int k = threadIdx.x; k < d; k += blockDim.x) cen[k] = live ? theta_at(k) - xmean[k] : 0.0f;
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < dp; j += blockDim.x) {
+    float v = 0.0f;
+    if (live && j < d) {
+      if (xw) {
+        const float* wr = xw + (size_t)j * d;
+        for (int k = 0; k < d; ++k) v = fmaf(wr[k], cen[k], v);
+      } else {
+        v = (theta_at(j) - xmean[j]) * xinv[j];
+      }
+    }
+    out[j] = __float2bfloat16(v);
+  }
+}
+
+// Batch rows: transformed inputs (bf16, padded with zeros) and targets.
 // idx_mode 0: rows 0..n-1 in order (inference / gradient check);
 //          1: Philox-random rows of the training set.
 __global__ void mlp_gather(const float* __restrict__ theta, const double* __restrict__ ll,
                            size_t n, int d, int dp, int B, int idx_mode, uint32_t seed,
                            uint32_t step, const float* __restrict__ xmean,
-                           const float* __restrict__ xinv, float ymean, float yinv,
-                           bf16* __restrict__ Xh, float* __restrict__ t) {
+                           const float* __restrict__ xinv, const float* __restrict__ xw,
+                           float ymean, float yinv, bf16* __restrict__ Xh,
+                           float* __restrict__ t) {
+  __shared__ float cen[256];
   const int row = blockIdx.x;
   if (row >= B) return;
   size_t src = idx_mode ? pick(seed, step, (uint32_t)row, (uint32_t)n) : (size_t)row;
   const bool live = src < n;
   if (!live) src = 0;
-  for (int j = threadIdx.x; j < dp; j += blockDim.x) {
-    float v = 0.0f;
-    if (live && j < d) v = (theta[src * d + j] - xmean[j]) * xinv[j];
-    Xh[(size_t)row * dp + j] = __float2bfloat16(v);
-  }
+  const float* th = theta + src * d;
+  mlp_input_row([&](int k) { return th[k]; }, live, d, dp, xmean, xinv, xw, cen,
+                Xh + (size_t)row * dp);
   if (threadIdx.x == 0 && t) t[row] = live && ll ? (float)((ll[src] - ymean) * yinv) : 0.0f;
 }
 
@@ -157,25 +185,59 @@ __global__ void mlp_transpose(const bf16* __restrict__ in, bf16* __restrict__ ou
   }
 }
 
-// out[j] = sum_b M[b][j] * (s ? s[b] : 1), fixed order over b.
-__global__ void mlp_colsum(const float* __restrict__ M, const float* __restrict__ s, int B, int H,
-                           float* __restrict__ out, int silu_in) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= H) return;
+// Column sums out[j] = scale_j * sum_b f(M[b][j]) * (s ? s[b] : 1) with
+// f = identity, silu or silu' (mode 0/1/2), in two fixed-order passes: blocks
+// of 32 columns x kColRows rows (8 warps, each a fixed row stride, then the
+// warps in order) write partials[chunk][j]; the second pass adds the chunks
+// in order.  Deterministic, and parallel over rows.
+constexpr int kColRows = 128;
+
+__global__ void mlp_colsum_part(const float* __restrict__ M, const float* __restrict__ s, int B,
+                                int H, int mode, float* __restrict__ part) {
+  __shared__ float red[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + lane;
+  const int b0 = blockIdx.y * kColRows, b1 = min(b0 + kColRows, B);
   float acc = 0.0f;
-  for (int b = 0; b < B; ++b) {
-    float v = M[(size_t)b * H + j];
-    if (silu_in) v = silu(v);
-    acc += s ? v * s[b] : v;
+  if (j < H) {
+    for (int b = b0 + w; b < b1; b += 8) {
+      float v = M[(size_t)b * H + j];
+      v = mode == 1 ? silu(v) : (mode == 2 ? dsilu(v) : v);
+      acc += s ? v * s[b] : v;
+    }
   }
-  out[j] = acc;
+  red[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && j < H) {
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += red[k][lane];
+    part[(size_t)blockIdx.y * H + j] = t;
+  }
 }
 
+__global__ void mlp_colsum_fin(const float* __restrict__ part, int nchunk, int H,
+                               const float* __restrict__ scale, float* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= H) return;
+  float t = 0.0f;
+  for (int c = 0; c < nchunk; ++c) t += part[(size_t)c * H + j];
+  out[j] = scale ? t * scale[j] : t;
+}
+
+// out[0] = sum of v[0..n), fixed order: 256 strided per-thread sums, then a
+// fixed shared-memory tree.  One block of 256 threads.
 __global__ void mlp_sum(const float* __restrict__ v, int n, float* __restrict__ out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  float acc = 0.0f;
-  for (int i = 0; i < n; ++i) acc += v[i];
-  out[0] = acc;
+  __shared__ float red[256];
+  float t = 0.0f;
+  for (int i = threadIdx.x; i < n; i += 256) t += v[i];
+  red[threadIdx.x] = t;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0];
 }
 
 // Adam (Kingma & Ba) with bias correction; also refreshes the bf16 copy and,
@@ -221,14 +283,14 @@ unsigned blocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 // Inference gather from f64 chain-major parameters [n][d].
 __global__ void mlp_gather64(const double* __restrict__ theta, int n, int d, int dp, int B,
                              const float* __restrict__ xmean, const float* __restrict__ xinv,
-                             bf16* __restrict__ Xh) {
+                             const float* __restrict__ xw, bf16* __restrict__ Xh) {
+  __shared__ float cen[256];
   const int row = blockIdx.x;
   if (row >= B) return;
-  for (int j = threadIdx.x; j < dp; j += blockDim.x) {
-    float v = 0.0f;
-    if (row < n && j < d) v = ((float)theta[(size_t)row * d + j] - xmean[j]) * xinv[j];
-    Xh[(size_t)row * dp + j] = __float2bfloat16(v);
-  }
+  const bool live = row < n;
+  const double* th = theta + (size_t)(live ? row : 0) * d;
+  mlp_input_row([&](int k) { return (float)th[k]; }, live, d, dp, xmean, xinv, xw, cen,
+                Xh + (size_t)row * dp);
 }
 
 __global__ void mlp_unscale(const float* __restrict__ y, int n, float ysd, float ymean,
@@ -252,8 +314,12 @@ struct gpum_b200_mlp {
   // activations and work buffers (batch rows)
   Buf<bf16> Xh, XTh, A1h, A1Th, A2h, dZ2h, dZ2Th, dZ1Th;
   Buf<float> Z1, Z2, t, yhat, rsq, dyhat, dA1, dZ1, loss, scratch;
+  Buf<float> colpart;  // [B / kColRows][H] column-sum partials
+  Buf<float> splitk;   // split-K GEMM partials
   // normaliser
-  Buf<float> xmean, xinv;
+  Buf<float> xmean, xinv, xw;  // xw: d x d whitening, used when `whiten`
+  bool whiten = false;
+  const float* xw_or_null() const { return whiten ? xw.p : nullptr; }
   float ymean = 0.0f, yinv = 1.0f, ysd = 1.0f;
   Buf<uint32_t> err;
   int adam_t = 0;
@@ -274,8 +340,20 @@ struct gpum_b200_mlp {
                                   (int)smem));
       smem_set[BN == 128] = true;
     }
-    dim3 grid(N / BN, M / kGemmBM);
-    tc_gemm_kernel<BN><<<grid, kGemmThreads, smem, st>>>(A, Bm, C, bias, act, M, N, K, err.p);
+    // Long-K products with few output tiles (the weight gradients, K = batch)
+    // split K across CTAs so the GPU is not left with a handful of CTAs.
+    int S = 1;
+    if (!bias && !act) {
+      const int tiles = (N / BN) * (M / kGemmBM);
+      while (S < 32 && tiles * S < 128 && K % (2 * S * kGemmBK) == 0 &&
+             (size_t)2 * S * M * N <= splitk.n)
+        S *= 2;
+    }
+    dim3 grid(N / BN, M / kGemmBM, S);
+    tc_gemm_kernel<BN><<<grid, kGemmThreads, smem, st>>>(A, Bm, S > 1 ? splitk.p : C, bias, act,
+                                                         M, N, K, K / S, err.p);
+    if (S > 1)
+      tc_splitk_sum<<<blocks((size_t)M * N), 256, 0, st>>>(splitk.p, S, (size_t)M * N, C);
     MLP_CK(cudaGetLastError());
   }
 
@@ -297,9 +375,9 @@ struct gpum_b200_mlp {
                                                      rsq.p, dyhat.p, dZ2h.p, dZ2Th.p, 1);
     MLP_CK(cudaGetLastError());
     // w3 and b3: dw3[j] = sum_b dyhat[b] silu(Z2[b][j]); db3 = sum dyhat
-    mlp_colsum<<<blocks(H), 256, 0, st>>>(Z2.p, dyhat.p, B, H, gw3.p, 1);
-    mlp_sum<<<1, 32, 0, st>>>(dyhat.p, B, gb3.p);
-    mlp_sum<<<1, 32, 0, st>>>(rsq.p, B, loss.p);
+    colsum(Z2.p, dyhat.p, 1, nullptr, gw3.p);
+    mlp_sum<<<1, 256, 0, st>>>(dyhat.p, B, gb3.p);
+    mlp_sum<<<1, 256, 0, st>>>(rsq.p, B, loss.p);
     // db2 = column sums of dZ2 (from its bf16 transpose would lose bits: use
     // the f32 row kernel output through dA1's buffer as scratch)
     mlp_transpose<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(A1h.p, A1Th.p, B, H);
@@ -308,14 +386,22 @@ struct gpum_b200_mlp {
     // db2 = sum_b dZ2[b][j]: recompute in f32 from Z2 and dyhat
     db2_from_head();
     mlp_dz1<<<blocks((size_t)B * H), 256, 0, st>>>(dA1.p, Z1.p, B, H, dZ1.p, dZ1Th.p);
-    mlp_colsum<<<blocks(H), 256, 0, st>>>(dZ1.p, nullptr, B, H, gb1.p, 0);
+    colsum(dZ1.p, nullptr, 0, nullptr, gb1.p);
     mlp_transpose<<<dim3(dp / 32, B / 32), dim3(32, 8), 0, st>>>(Xh.p, XTh.p, B, dp);
     gemm_any(dZ1Th.p, XTh.p, gW1.p, nullptr, nullptr, H, dp, B);  // dW1 = dZ1^T X
     MLP_CK(cudaGetLastError());
   }
 
-  // db2[j] = sum_b dyhat[b] w3[j] silu'(Z2[b][j]), fixed order over b.
-  void db2_from_head();
+  // db2[j] = w3[j] sum_b dyhat[b] silu'(Z2[b][j]), fixed order over b.
+  void db2_from_head() { colsum(Z2.p, dyhat.p, 2, w3.p, gb2.p); }
+
+  // Column sums of a B x H row-major matrix (mlp_colsum_part / _fin).
+  void colsum(const float* M, const float* sc, int mode, const float* scale, float* out) {
+    const int nchunk = (B + kColRows - 1) / kColRows;
+    mlp_colsum_part<<<dim3((H + 31) / 32, nchunk), 256, 0, st>>>(M, sc, B, H, mode, colpart.p);
+    mlp_colsum_fin<<<blocks(H), 256, 0, st>>>(colpart.p, nchunk, H, scale, out);
+    MLP_CK(cudaGetLastError());
+  }
 
   void adam(float lr) {
     ++adam_t;
@@ -348,15 +434,6 @@ struct gpum_b200_mlp {
 
 namespace {
 
-__global__ void mlp_db2(const float* __restrict__ Z2, const float* __restrict__ dyhat,
-                        const float* __restrict__ w3, int B, int H, float* __restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= H) return;
-  float acc = 0.0f;
-  for (int b = 0; b < B; ++b) acc += dyhat[b] * dsilu(Z2[(size_t)b * H + j]);
-  out[j] = acc * w3[j];
-}
-
 int mlp_guard(char* err, size_t len, const std::function<void()>& body) {
   try {
     body();
@@ -379,11 +456,6 @@ void need(bool ok, const char* msg, int code = GPUM_ERR_INVALID) {
 }
 
 }  // namespace
-
-void gpum_b200_mlp::db2_from_head() {
-  mlp_db2<<<blocks(H), 256, 0, st>>>(Z2.p, dyhat.p, w3.p, B, H, gb2.p);
-  MLP_CK(cudaGetLastError());
-}
 
 namespace {
 
@@ -422,12 +494,13 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
   try {
     for (int r0 = 0; r0 < n; r0 += m->B) {
       const int rows = std::min(m->B, n - r0);
-      mlp_gather64<<<m->B, 128, 0, st>>>(theta + (size_t)r0 * d, rows, d, m->dp, m->B,
-                                         m->xmean.p, m->xinv.p, m->Xh.p);
-      m->forward(m->B);
-      mlp_head<<<blocks((size_t)m->B * 32), 256, 0, st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr,
-                                                         m->B, m->H, m->B, m->yhat.p, nullptr,
-                                                         nullptr, nullptr, nullptr, 0);
+      const int Mi = (rows + kGemmBM - 1) / kGemmBM * kGemmBM;  // rows padded to the tile
+      mlp_gather64<<<Mi, 128, 0, st>>>(theta + (size_t)r0 * d, rows, d, m->dp, Mi, m->xmean.p,
+                                       m->xinv.p, m->xw_or_null(), m->Xh.p);
+      m->forward(Mi);
+      mlp_head<<<blocks((size_t)Mi * 32), 256, 0, st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr, Mi,
+                                                       m->H, Mi, m->yhat.p, nullptr, nullptr,
+                                                       nullptr, nullptr, 0);
       mlp_unscale<<<blocks(rows), 256, 0, st>>>(m->yhat.p, rows, m->ysd, m->ymean, out + r0);
       MLP_CK(cudaGetLastError());
     }
@@ -482,8 +555,11 @@ int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t s
     for (auto* b : {&m->Z1, &m->Z2, &m->dA1, &m->dZ1}) b->alloc((size_t)B * H);
     for (auto* b : {&m->t, &m->yhat, &m->rsq, &m->dyhat}) b->alloc(B);
     m->loss.alloc(1);
+    m->colpart.alloc((size_t)((B + kColRows - 1) / kColRows) * H);
+    m->splitk.alloc((size_t)32 * H * std::max(H, dp));
     m->xmean.alloc(d);
     m->xinv.alloc(d);
+    m->xw.alloc((size_t)d * d);
     m->err.alloc(1);
     MLP_CK(cudaMemsetAsync(m->err.p, 0, sizeof(uint32_t), m->st));
     // zero moments and padded rows
@@ -531,6 +607,34 @@ int gpum_b200_mlp_set_normalizer(gpum_b200_mlp* m, const double* xmean, const do
     MLP_CK(cudaMemcpyAsync(m->xinv.p, inv.data(), m->d * sizeof(float), cudaMemcpyHostToDevice,
                            m->st));
     MLP_CK(cudaStreamSynchronize(m->st));
+    m->whiten = false;
+    m->ymean = (float)ymean;
+    m->ysd = (float)ysd;
+    m->yinv = (float)(1.0 / ysd);
+  });
+}
+
+int gpum_b200_mlp_set_whitening(gpum_b200_mlp* m, const double* xmean, const double* xw,
+                                double ymean, double ysd, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && xmean && xw, "NULL argument");
+    need(std::isfinite(ymean) && ysd > 0 && std::isfinite(ysd), "ysd must be positive");
+    const int d = m->d;
+    std::vector<float> mu(d), w((size_t)d * d);
+    for (int j = 0; j < d; ++j) {
+      need(std::isfinite(xmean[j]), "xmean must be finite");
+      mu[j] = (float)xmean[j];
+    }
+    for (size_t i = 0; i < (size_t)d * d; ++i) {
+      need(std::isfinite(xw[i]), "the whitening matrix must be finite");
+      w[i] = (float)xw[i];
+    }
+    MLP_CK(cudaMemcpyAsync(m->xmean.p, mu.data(), d * sizeof(float), cudaMemcpyHostToDevice,
+                           m->st));
+    MLP_CK(cudaMemcpyAsync(m->xw.p, w.data(), (size_t)d * d * sizeof(float),
+                           cudaMemcpyHostToDevice, m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
+    m->whiten = true;
     m->ymean = (float)ymean;
     m->ysd = (float)ysd;
     m->yinv = (float)(1.0 / ysd);
@@ -548,7 +652,8 @@ int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll,
     std::vector<float> losses(steps);
     for (uint32_t s = 0; s < steps; ++s) {
       mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed,
-                                          m->step++, m->xmean.p, m->xinv.p, m->ymean, m->yinv,
+                                          m->step++, m->xmean.p, m->xinv.p, m->xw_or_null(),
+                                          m->ymean, m->yinv,
                                           m->Xh.p, m->t.p);
       m->forward(m->B);
       m->backward(m->B);
@@ -574,7 +679,8 @@ int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, doubl
     for (size_t r0 = 0; r0 < n; r0 += m->B) {
       const size_t rows = std::min<size_t>(m->B, n - r0);
       mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p + r0 * m->d, nullptr, rows, m->d, m->dp, m->B, 0,
-                                          0, 0, m->xmean.p, m->xinv.p, 0.0f, 1.0f, m->Xh.p,
+                                          0, 0, m->xmean.p, m->xinv.p, m->xw_or_null(), 0.0f,
+                                          1.0f, m->Xh.p,
                                           nullptr);
       m->forward(m->B);
       mlp_head<<<blocks((size_t)m->B * 32), 256, 0, m->st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr,
@@ -599,7 +705,8 @@ int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double*
     Buf<double> dll;
     upload_pairs(m, theta, ll, n, dth, dll);
     mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n, m->d, m->dp, m->B, 0, 0, 0, m->xmean.p,
-                                        m->xinv.p, m->ymean, m->yinv, m->Xh.p, m->t.p);
+                                        m->xinv.p, m->xw_or_null(), m->ymean, m->yinv, m->Xh.p,
+                                        m->t.p);
     m->forward(m->B);
     m->backward((int)n);
     const int H = m->H, dp = m->dp;
@@ -658,6 +765,7 @@ int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
     db.alloc(bh.size());
     dc.alloc((size_t)M * N);
     tmp.err.alloc(1);
+    tmp.splitk.alloc(std::min<size_t>((size_t)32 * M * N, (size_t)1 << 26));
     MLP_CK(cudaMemsetAsync(tmp.err.p, 0, sizeof(uint32_t), tmp.st));
     MLP_CK(cudaMemcpyAsync(da.p, ah.data(), ah.size() * 2, cudaMemcpyHostToDevice, tmp.st));
     MLP_CK(cudaMemcpyAsync(db.p, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice, tmp.st));

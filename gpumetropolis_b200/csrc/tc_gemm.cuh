@@ -12,6 +12,9 @@
 // before reusing shared memory.  The epilogue reads TMEM with tcgen05.ld
 // (warp w owns lanes 32w..32w+31 = rows), applies bias and SiLU, and stores.
 // M, N and K must be multiples of 128, BN and 64 (callers pad with zeros).
+// Split K: with gridDim.z = S > 1, CTA z reduces K columns [z*kz, z*kz + kz)
+// into its own partial C + z*M*N (no epilogue); the caller adds the S
+// partials in order (tc_splitk_sum), which keeps the result deterministic.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -98,7 +101,7 @@ template <int BN>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B,
                float* __restrict__ C, const float* __restrict__ bias,
-               __nv_bfloat16* __restrict__ act, int M, int N, int K, uint32_t* err) {
+               __nv_bfloat16* __restrict__ act, int M, int N, int K, int kz, uint32_t* err) {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "BN");
   constexpr uint32_t kTmemCols = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
   extern __shared__ __align__(1024) unsigned char gsm[];
@@ -108,6 +111,8 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * BN;
+  const int kbeg = (int)blockIdx.z * kz, kend = min(kbeg + kz, K);
+  C += (size_t)blockIdx.z * M * N;
 
   if (warp == 0) tmem_alloc(tslot, kTmemCols);
   if (tid == 0) {
@@ -123,7 +128,7 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
   const uint32_t lbo_a = (kGemmBM / 8) * 128, lbo_b = (BN / 8) * 128;
   bool ok = true;
 
-  for (int k0 = 0, it = 0; k0 < K; k0 += kGemmBK, ++it) {
+  for (int k0 = kbeg, it = 0; k0 < kend; k0 += kGemmBK, ++it) {
     // Stage the A (128 rows) and B (BN rows) slices: 16-byte chunks (8 bf16)
     // read coalesced along K, written to their core-matrix positions.
     for (int i = tid; i < kGemmBM * (kGemmBK / 8); i += kGemmThreads) {
@@ -145,7 +150,7 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
       for (int kk = 0; kk < kGemmBK / 16; ++kk) {
         const uint64_t ad = umma_smem_desc(sa_addr + 2 * kk * lbo_a, lbo_a, 128);
         const uint64_t bd = umma_smem_desc(sb_addr + 2 * kk * lbo_b, lbo_b, 128);
-        umma_bf16(tmem, ad, bd, idesc, (k0 > 0 || kk > 0) ? 1u : 0u);
+        umma_bf16(tmem, ad, bd, idesc, (k0 > kbeg || kk > 0) ? 1u : 0u);
       }
       umma_commit(bar);
     }
@@ -179,6 +184,16 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+// out[i] = sum_z part[z*n + i], z in order.
+static __global__ void tc_splitk_sum(const float* __restrict__ part, int S, size_t n,
+                                     float* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float t = 0.0f;
+  for (int z = 0; z < S; ++z) t += part[(size_t)z * n + i];
+  out[i] = t;
 }
 
 template <int BN>

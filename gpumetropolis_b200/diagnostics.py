@@ -2,6 +2,12 @@
 
 * :func:`ess` -- Geyer's initial positive sequence per chain, summed over
   chains (``R/diagnostics.R:36-59,96-99``), the package's own estimator;
+* :func:`ess_pooled` -- multi-chain ESS from the chain-averaged
+  autocovariance and the between-chain variance (Vehtari, Gelman, Simpson,
+  Carpenter & Buerkner 2021, without rank normalisation), with Geyer's
+  initial monotone sequence; robust where chains barely move, where the
+  per-chain estimator counts a constant chain as fully independent.  Not in
+  the reference; used to compare samplers' ESS per second;
 * :func:`rhat` -- split R-hat (``R/diagnostics.R:127-159``);
 * :func:`gaussian_mean_posterior` -- the closed form N(mean(y), sigma^2/n)
   (``R/diagnostics.R:246-257``).
@@ -55,6 +61,38 @@ def ess(draws, warmup: int | None = None) -> float:
     if w < 0 or w >= n:
         raise ValueError("`warmup` must be in [0, n_iter).")
     return float(sum(ess_chain(x[w:, c]) for c in range(x.shape[1])))
+
+
+def ess_pooled(draws) -> float:
+    """Multi-chain ESS of an ``(n_iter, n_chains)`` array (all draws kept)."""
+    x = np.asarray(draws, dtype=np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    n, m = x.shape
+    if n < 4:
+        return float(n * m)
+    xc = x - x.mean(axis=0)
+    L = 1 << int(np.ceil(np.log2(2 * n)))
+    f = np.fft.rfft(xc, L, axis=0)
+    acov = np.fft.irfft(f * np.conj(f), L, axis=0)[:n] / n       # (n, m), divisor n
+    acov_mean = acov.mean(axis=1)
+    W = acov_mean[0] * n / (n - 1)
+    B_over_n = x.mean(axis=0).var(ddof=1) if m > 1 else 0.0
+    var_plus = W * (n - 1) / n + B_over_n
+    if not var_plus > 0:
+        return 0.0
+    rho = 1.0 - (W - acov_mean) / var_plus
+    rho[0] = 1.0
+    k = (n - 1) // 2
+    P = rho[0:2 * k:2] + rho[1:2 * k:2]
+    # initial positive sequence, then made monotone
+    pos = np.nonzero(P <= 0)[0]
+    P = P[: pos[0]] if pos.size else P
+    if P.size == 0:
+        return float(n * m)
+    P = np.minimum.accumulate(P)
+    tau = max(-1.0 + 2.0 * P.sum(), 1.0 / np.log10(max(n * m, 10)))
+    return float(n * m / tau)
 
 
 def rhat(draws, warmup: int | None = None) -> float:

@@ -222,6 +222,11 @@ GPUM_API void gpum_b200_mlp_destroy(gpum_b200_mlp* m);
 GPUM_API int gpum_b200_mlp_set_normalizer(gpum_b200_mlp* m, const double* xmean,
                                           const double* xsd, double ymean, double ysd, char* err,
                                           size_t err_len);
+/* Whitening instead of per-coordinate scaling: the network sees
+ * xw (theta - xmean), xw a d x d row-major matrix (e.g. the inverse Cholesky
+ * factor of the training parameters' covariance). */
+GPUM_API int gpum_b200_mlp_set_whitening(gpum_b200_mlp* m, const double* xmean, const double* xw,
+                                         double ymean, double ysd, char* err, size_t err_len);
 /* `steps` Adam steps on random batches of the pairs (host arrays theta
  * n_pairs x d, ll n_pairs); out_loss (may be NULL) receives each step's mean
  * squared error in standardised units. */

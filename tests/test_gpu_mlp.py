@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 128, 192), (384, 64, 128),
-                                   (128, 256, 512)])
+                                   (128, 256, 512), (256, 64, 4096)])
 def test_tcgen05_gemm_matches_numpy(gpu, M, N, K):
     rng = np.random.default_rng(M + N + K)
     A = rng.standard_normal((M, K)).astype(np.float32)

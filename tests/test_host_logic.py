@@ -120,3 +120,19 @@ def test_gpu_metropolis_input_validation():
         gpu_metropolis(m, y, backend="cuda")
     with pytest.raises(GpumInputError, match="warmup"):
         gpu_metropolis(m, y, n_iter=10, warmup=10)
+
+
+def test_pooled_ess_on_ar1_and_stuck_chains():
+    from gpumetropolis_b200.diagnostics import ess_pooled
+    rng = np.random.default_rng(0)
+    n, m = 3000, 32
+    for phi in (0.0, 0.5, 0.9):
+        x = np.zeros((n, m))
+        e = rng.standard_normal((n, m))
+        for t in range(1, n):
+            x[t] = phi * x[t - 1] + e[t]
+        want = (1 - phi) / (1 + phi)
+        assert abs(ess_pooled(x) / (n * m) - want) < 0.12 * want + 0.01
+    # chains that never move carry one value each, not n
+    stuck = np.repeat(rng.standard_normal((1, m)), 400, axis=0)
+    assert ess_pooled(stuck) < 2 * m
