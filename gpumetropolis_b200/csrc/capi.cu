@@ -445,8 +445,7 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
   // Observations per tile: a multiple of 32 (one per lane), <= 256 (TMA box
   // limit), with a stage of at most 32 KB.
   if (n_cols > 0) {
-    const int T = (int)((8192 / n_cols) / 32 * 32);
-    s->T = std::max(32, std::min(256, T));
+    s->T = tile_obs(n_cols);
   } else {
     s->T = 256;
   }

@@ -12,6 +12,9 @@
 // is xo[j*T].
 #include "codegen.hpp"
 
+#include "program.hpp"
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -168,6 +171,24 @@ std::string op_expr(const Graph& g, int i, const std::string& a, const std::stri
   }
 }
 
+// Paired (float2) value of `i` from child names: two observations at once.
+std::string op_expr2(const Graph& g, int i, const std::string& a, const std::string& b) {
+  switch (g.n[i].op) {
+    case O_ADD: return "gm2_add(" + a + ", " + b + ")";
+    case O_SUB: return "gm2_sub(" + a + ", " + b + ")";
+    case O_MUL: return "gm2_mul(" + a + ", " + b + ")";
+    case O_DIV: return "gm2_div(" + a + ", " + b + ")";
+    case O_NEG: return "gm2_neg(" + a + ")";
+    case O_EXP: return "gm2_exp(" + a + ")";
+    case O_LOG: return "gm2_log(" + a + ")";
+    case O_SQRT: return "gm2_sqrt(" + a + ")";
+    case O_LGAMMA: return "gm2_lgamma(" + a + ")";
+    default:
+      if (is_const2(g, g.n[i].b)) return "gm2_mul(" + a + ", " + a + ")";
+      return "gm2_pow(" + a + ", " + b + ")";
+  }
+}
+
 // Local-derivative contributions of node i with adjoint `G` to its children,
 // as (child, expression) pairs (cpu_native.rs:217-277).
 std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const std::string& G,
@@ -209,7 +230,6 @@ std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const s
 int generate_model(const uint32_t* code, size_t n_code, const double* consts,
                    const uint32_t* prior_code, size_t n_prior, const double* prior_consts,
                    uint32_t n_params, uint32_t n_cols, GenModel* out, std::string* err) {
-  (void)n_cols;
   *out = GenModel();
   Graph g;
   const int root = g.build(code, n_code, consts);
@@ -253,6 +273,9 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   s << "#define GM_NP " << n_params << "\n";
   s << "#define GM_NH " << std::max(1, out->n_hoist) << "\n";
   s << "#define GM_ND " << std::max(1, out->n_data) << "\n";
+  // The tile height is fixed by the column count, so column offsets are
+  // compile-time immediates in the generated loads.
+  s << "#define GM_T " << tile_obs(n_cols) << "\n";
 
   // gm_data: data leaves and data-only subexpressions, per observation.
   s << "__device__ __forceinline__ void gm_data(const float* __restrict__ xo, int T, "
@@ -260,7 +283,7 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   for (int i = 0; i < N; ++i) {
     if (!live[i] || !is_d(i)) continue;
     const Node& x = g.n[i];
-    std::string e = x.op == O_D ? "xo[" + std::to_string(x.arg) + " * T]"
+    std::string e = x.op == O_D ? "xo[" + std::to_string(x.arg) + " * GM_T]"
                                 : op_expr(g, i, name[x.a], x.b >= 0 ? name[x.b] : "", true);
     s << "  const float " << name[i] << " = " << e << ";\n";
     if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
@@ -297,6 +320,73 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
        "const float* __restrict__ p, const float* __restrict__ h) {\n";
   emit_fwd(s);
   s << "  (void)d; (void)p; (void)h;\n  return " << rootv << ";\n}\n";
+
+  // Paired versions (two observations per call) of gm_data and gm_value.
+  // Leaves that do not depend on the observation (constants, parameters,
+  // hoisted values) appear as broadcast pairs; a product used only by one sum
+  // is fused into it (FFMA2), the contraction the scalar code gets from
+  // --fmad=true.
+  {
+    std::vector<int> uses(N, 0);
+    for (int i = 0; i < N; ++i) {
+      if (!live[i]) continue;
+      if (g.n[i].a >= 0) ++uses[g.n[i].a];
+      if (g.n[i].b >= 0) ++uses[g.n[i].b];
+    }
+    if (root >= 0) ++uses[root];
+    auto ref2 = [&](int i) -> std::string {
+      const Node& x = g.n[i];
+      if (x.op == O_C) return "gm2(" + flit(x.c) + ")";
+      if (x.op == O_P) return "pp[" + std::to_string(x.arg) + "]";
+      if (hslot[i] >= 0) return "hh[" + std::to_string(hslot[i]) + "]";
+      if (dslot[i] >= 0) return "d[" + std::to_string(dslot[i]) + "]";
+      return name[i];
+    };
+    auto data_ref2 = [&](int i) -> std::string {  // inside gm_data2
+      const Node& x = g.n[i];
+      if (x.op == O_C) return "gm2(" + flit(x.c) + ")";
+      return name[i];
+    };
+    s << "__device__ __forceinline__ void gm_data2(const float* __restrict__ xo, int T, "
+         "float2* __restrict__ d) {\n";
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_d(i)) continue;
+      const Node& x = g.n[i];
+      std::string e = x.op == O_D
+                          ? "*reinterpret_cast<const float2*>(xo + " + std::to_string(x.arg) +
+                                " * GM_T)"
+                          : op_expr2(g, i, data_ref2(x.a), x.b >= 0 ? data_ref2(x.b) : "");
+      s << "  const float2 " << name[i] << " = " << e << ";\n";
+      if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
+    }
+    s << "  (void)xo; (void)T; (void)d;\n}\n";
+    auto fusable = [&](int c) {
+      return c >= 0 && is_pd(c) && g.n[c].op == O_MUL && uses[c] == 1 && c != root;
+    };
+    std::vector<char> fused(N, 0);
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i) || g.n[i].op != O_ADD) continue;
+      if (fusable(g.n[i].a)) fused[g.n[i].a] = 1;
+      else if (fusable(g.n[i].b)) fused[g.n[i].b] = 1;
+    }
+    s << "__device__ __forceinline__ float2 gm_value2(const float2* __restrict__ d, "
+         "const float2* __restrict__ pp, const float2* __restrict__ hh) {\n";
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i)) continue;
+      if (fused[i]) continue;
+      const Node& x = g.n[i];
+      std::string e;
+      if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
+        const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
+        e = "gm2_fma(" + ref2(g.n[m].a) + ", " + ref2(g.n[m].b) + ", " + ref2(o) + ")";
+      } else {
+        e = op_expr2(g, i, ref2(x.a), x.b >= 0 ? ref2(x.b) : "");
+      }
+      s << "  const float2 " << name[i] << " = " << e << ";\n";
+    }
+    const std::string root2 = root < 0 ? std::string("gm2(0.0f)") : ref2(root);
+    s << "  (void)d; (void)pp; (void)hh;\n  return " << root2 << ";\n}\n";
+  }
 
   // Value + gradient: forward, then adjoints in reverse order.
   s << "__device__ __forceinline__ float gm_value_grad(const float* __restrict__ d, "

@@ -427,15 +427,36 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
       if (lane == 0) atomicOr(E.err, DEV_ERR_TMA_TIMEOUT);
     }
     const int obs0 = (t0 + k) * T;
-    for (int ol = lane + 32 * wo; ol < T; ol += 32 * WO) {
-      const int obs = obs0 + ol;
-      const bool valid = obs < E.n_obs;
-      body.eval(tile + ol, T, valid);
-      if (phase == PH_POINTWISE && valid) {
+    if constexpr (Body::kObsPerEval == 2) {
+      // observation pairs (2 pi, 2 pi + 1); T is even, so each pair is
+      // 8-byte aligned in every column of the tile
+      for (int pi = lane + 32 * wo; 2 * pi < T; pi += 32 * WO) {
+        const int obs = obs0 + 2 * pi;
+        const bool v0 = obs < E.n_obs, v1 = obs + 1 < E.n_obs;
+        body.eval2(tile + 2 * pi, T, v0, v1);
+        if (phase == PH_POINTWISE && v0) {
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-          const int c = cb * CG + wc * G + g;
-          if (c < E.n_points) E.pointwise[(size_t)c * E.n_obs + obs] = (double)body.last(g);
+          for (int g = 0; g < G; ++g) {
+            const int c = cb * CG + wc * G + g;
+            if (c < E.n_points) {
+              const float2 lv = body.last2(g);
+              E.pointwise[(size_t)c * E.n_obs + obs] = (double)lv.x;
+              if (v1) E.pointwise[(size_t)c * E.n_obs + obs + 1] = (double)lv.y;
+            }
+          }
+        }
+      }
+    } else {
+      for (int ol = lane + 32 * wo; ol < T; ol += 32 * WO) {
+        const int obs = obs0 + ol;
+        const bool valid = obs < E.n_obs;
+        body.eval(tile + ol, T, valid);
+        if (phase == PH_POINTWISE && valid) {
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const int c = cb * CG + wc * G + g;
+            if (c < E.n_points) E.pointwise[(size_t)c * E.n_obs + obs] = (double)body.last(g);
+          }
         }
       }
     }

@@ -13,20 +13,35 @@
 
 namespace gpum {
 
-// Each observation's FP32 value is accumulated into an FP64 sum (exact per
-// term, two instructions), so per-thread partial sums carry no FP32 error.
+// Per-thread sums: FP32 terms are added in blocks of kAccBlock into an FP32
+// partial, and each block's partial is added into an FP64 sum.  The FP32
+// error of a block is at most (kAccBlock - 1) ulp-scale of its terms and
+// does not grow with the number of observations; the f32 -> f64 conversion
+// and the f64 add (slow pipes) run once per block instead of per term.
+constexpr int kAccBlock = 8;
+
 struct Acc64 {
   double s;
-  __device__ __forceinline__ void init() { s = 0.0; }
-  __device__ __forceinline__ void add(float x) { s += (double)x; }
-  __device__ __forceinline__ double total() const { return s; }
+  float part;
+  __device__ __forceinline__ void init() {
+    s = 0.0;
+    part = 0.0f;
+  }
+  __device__ __forceinline__ void add(float x) { part += x; }
+  __device__ __forceinline__ void flush() {
+    s += (double)part;
+    part = 0.0f;
+  }
+  __device__ __forceinline__ double total() const { return s + (double)part; }
 };
 
 template <int G, bool GRAD>
 struct JitBody {
+  static constexpr int kObsPerEval = 1;
   float p[G][GM_NP];
   float h[G][GM_NH];
   Acc64 acc[G];
+  int cnt;  // terms in the open FP32 blocks
   float lastv[G];
   float gp[GRAD ? G : 1][GRAD ? GM_NP : 1];
   float gh[GRAD ? G : 1][GRAD ? GM_NH : 1];
@@ -40,6 +55,7 @@ struct JitBody {
       acc[g].init();
       lastv[g] = 0.0f;
     }
+    cnt = 0;
     if (GRAD) {
 #pragma unroll
       for (int g = 0; g < (GRAD ? G : 1); ++g) {
@@ -68,6 +84,11 @@ struct JitBody {
         if (valid) acc[g].add(v);
       }
     }
+    if (valid && ++cnt == kAccBlock) {
+      cnt = 0;
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[g].flush();
+    }
   }
 
   __device__ __forceinline__ float last(int g) const { return lastv[g]; }
@@ -85,6 +106,71 @@ struct JitBody {
   }
 };
 
+#if GM_PAIR
+// Value body over observation pairs: gm_data2 loads each column pair with one
+// 64-bit shared-memory load and gm_value2 runs the model on both
+// observations with two-wide FP32 instructions.  Parameters and hoisted
+// values are kept as broadcast pairs (p, p) so every instruction is paired.
+template <int G>
+struct JitBody2 {
+  static constexpr int kObsPerEval = 2;
+  float2 pp[G][GM_NP];
+  float2 hh[G][GM_NH];
+  double s[G];
+  float2 part[G];
+  float2 lastv[G];
+  int cnt;  // observation pairs in the open FP32 blocks
+
+  __device__ __forceinline__ void begin(const float* pc0, int CG) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      float p[GM_NP], h[GM_NH];
+#pragma unroll
+      for (int j = 0; j < GM_NP; ++j) p[j] = pc0[j * CG + g];
+      gm_hoist(p, h);
+#pragma unroll
+      for (int j = 0; j < GM_NP; ++j) pp[g][j] = make_float2(p[j], p[j]);
+#pragma unroll
+      for (int j = 0; j < GM_NH; ++j) hh[g][j] = make_float2(h[j], h[j]);
+      s[g] = 0.0;
+      part[g] = make_float2(0.0f, 0.0f);
+      lastv[g] = make_float2(0.0f, 0.0f);
+    }
+    cnt = 0;
+  }
+
+  // xo: the first observation of the pair (the second is xo + 1).
+  __device__ __forceinline__ void eval2(const float* xo, int T, bool v0, bool v1) {
+    float2 d[GM_ND];
+    gm_data2(xo, T, d);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const float2 v = gm_value2(d, pp[g], hh[g]);
+      lastv[g] = v;
+      if (v1) part[g] = __fadd2_rn(part[g], v);
+      else if (v0) part[g].x += v.x;
+    }
+    if (v0 && ++cnt == kAccBlock) {
+      cnt = 0;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        s[g] += (double)part[g].x + (double)part[g].y;
+        part[g] = make_float2(0.0f, 0.0f);
+      }
+    }
+  }
+
+  __device__ __forceinline__ float2 last2(int g) const { return lastv[g]; }
+  __device__ __forceinline__ void end() {}
+  __device__ __forceinline__ double total(int g, int) const {
+    return s[g] + ((double)part[g].x + (double)part[g].y);
+  }
+};
+using ValueBody = JitBody2<GM_G>;
+#else
+using ValueBody = JitBody<GM_G, false>;
+#endif
+
 // The generated f64 prior (value and reverse-mode gradient).
 struct JitPrior {
   __device__ static double value(const ChainArgs&, const double* p) { return gm_prior(p); }
@@ -96,12 +182,17 @@ struct JitPrior {
 }  // namespace gpum
 
 // Value-only kernel: PH_EVAL / PH_POINTWISE / RWM, DE and Cholesky steps.
-extern "C" __global__ void __launch_bounds__(gpum::kThreads, 1)
+// The paired body fits in 128 registers, so two CTAs (16 warps) share an SM.
+#if GM_PAIR
+#define GM_VALUE_MIN_CTAS 2
+#else
+#define GM_VALUE_MIN_CTAS 1
+#endif
+extern "C" __global__ void __launch_bounds__(gpum::kThreads, GM_VALUE_MIN_CTAS)
 gm_iter_value(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum::ChainArgs A,
               int phase) {
-  gpum::JitBody<GM_G, false> body;
-  gpum::run_iteration<GM_G, 1, gpum::JitBody<GM_G, false>, gpum::JitPrior>(&tmap, E, A, phase,
-                                                                           body);
+  gpum::ValueBody body;
+  gpum::run_iteration<GM_G, 1, gpum::ValueBody, gpum::JitPrior>(&tmap, E, A, phase, body);
 }
 
 // Value + gradient kernel: gradient batches and MALA steps.

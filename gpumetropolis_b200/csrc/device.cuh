@@ -169,4 +169,35 @@ struct Comp {
   }
 };
 
+// ------------------------------------------------- paired FP32 arithmetic
+// Two observations per lane: sm_100's two-wide FP32 instructions (FADD2,
+// FMUL2, FFMA2) round each half exactly like the scalar instruction.
+// Subtraction and negation are FFMA2 / FMUL2 by -1, which are exact.
+__device__ __forceinline__ float2 gm2(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 gm2_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 gm2_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 gm2_fma(float2 a, float2 b, float2 c) {
+  return __ffma2_rn(a, b, c);
+}
+__device__ __forceinline__ float2 gm2_sub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 gm2_neg(float2 a) {
+  return __fmul2_rn(a, make_float2(-1.0f, -1.0f));
+}
+__device__ __forceinline__ float2 gm2_div(float2 a, float2 b) {
+  return make_float2(a.x / b.x, a.y / b.y);
+}
+__device__ __forceinline__ float2 gm2_exp(float2 a) { return make_float2(expf(a.x), expf(a.y)); }
+__device__ __forceinline__ float2 gm2_log(float2 a) { return make_float2(logf(a.x), logf(a.y)); }
+__device__ __forceinline__ float2 gm2_sqrt(float2 a) {
+  return make_float2(sqrtf(a.x), sqrtf(a.y));
+}
+__device__ __forceinline__ float2 gm2_lgamma(float2 a) {
+  return make_float2(lgammaf(a.x), lgammaf(a.y));
+}
+__device__ __forceinline__ float2 gm2_pow(float2 a, float2 b) {
+  return make_float2(powf(a.x, b.x), powf(a.y, b.y));
+}
+
 }  // namespace gpum

@@ -67,4 +67,13 @@ int validate_program(const uint32_t* code, size_t n_code, size_t n_consts,
                      uint32_t n_params, uint32_t n_cols, bool allow_data,
                      int* depth, std::string* err);
 
+// Observations per shared-memory tile for a data set of n_cols columns: a
+// multiple of 32 (one per lane), at most 256 (the TMA box limit) and at most
+// 32 KB per stage.  The compiled engine bakes it into the generated loads.
+inline int tile_obs(uint32_t n_cols) {
+  if (n_cols == 0) return 256;
+  const int T = (int)((8192 / n_cols) / 32 * 32);
+  return T < 32 ? 32 : (T > 256 ? 256 : T);
+}
+
 }  // namespace gpum
