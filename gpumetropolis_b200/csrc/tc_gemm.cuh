@@ -128,19 +128,42 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
   const uint32_t lbo_a = (kGemmBM / 8) * 128, lbo_b = (BN / 8) * 128;
   bool ok = true;
 
+  // Staging: each thread owns kLA + kLB 16-byte chunks of a K slice.  All
+  // global loads of a slice are issued back to back into registers, and the
+  // next slice is loaded while the tensor core works on the current one.
+  constexpr int kChunks = kGemmBK / 8;  // 16-byte chunks per row of a slice
+  constexpr int kLA = kGemmBM * kChunks / kGemmThreads;
+  constexpr int kLB = BN * kChunks / kGemmThreads;
+  static_assert(kGemmBM * kChunks % kGemmThreads == 0 && BN * kChunks % kGemmThreads == 0, "");
+  uint4 ra[kLA], rb[kLB];
+  auto load_slice = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < kLA; ++q) {
+      const int i = tid + q * kGemmThreads, r = i / kChunks, c8 = (i % kChunks) * 8;
+      ra[q] = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * K + k0 + c8);
+    }
+#pragma unroll
+    for (int q = 0; q < kLB; ++q) {
+      const int i = tid + q * kGemmThreads, r = i / kChunks, c8 = (i % kChunks) * 8;
+      rb[q] = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * K + k0 + c8);
+    }
+  };
+  auto store_slice = [&]() {
+#pragma unroll
+    for (int q = 0; q < kLA; ++q) {
+      const int i = tid + q * kGemmThreads, r = i / kChunks, c8 = (i % kChunks) * 8;
+      *reinterpret_cast<uint4*>(sa + kmajor_offset(r, c8, kGemmBM)) = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < kLB; ++q) {
+      const int i = tid + q * kGemmThreads, r = i / kChunks, c8 = (i % kChunks) * 8;
+      *reinterpret_cast<uint4*>(sb + kmajor_offset(r, c8, BN)) = rb[q];
+    }
+  };
+  if (kbeg < kend) load_slice(kbeg);
+
   for (int k0 = kbeg, it = 0; k0 < kend; k0 += kGemmBK, ++it) {
-    // Stage the A (128 rows) and B (BN rows) slices: 16-byte chunks (8 bf16)
-    // read coalesced along K, written to their core-matrix positions.
-    for (int i = tid; i < kGemmBM * (kGemmBK / 8); i += kGemmThreads) {
-      const int r = i / (kGemmBK / 8), c8 = (i % (kGemmBK / 8)) * 8;
-      const uint4 v = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * K + k0 + c8);
-      *reinterpret_cast<uint4*>(sa + kmajor_offset(r, c8, kGemmBM)) = v;
-    }
-    for (int i = tid; i < BN * (kGemmBK / 8); i += kGemmThreads) {
-      const int r = i / (kGemmBK / 8), c8 = (i % (kGemmBK / 8)) * 8;
-      const uint4 v = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * K + k0 + c8);
-      *reinterpret_cast<uint4*>(sb + kmajor_offset(r, c8, BN)) = v;
-    }
+    store_slice();
     // Generic-proxy smem writes must be visible to the tensor core's async proxy.
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -154,6 +177,7 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
       }
       umma_commit(bar);
     }
+    if (k0 + kGemmBK < kend) load_slice(k0 + kGemmBK);  // overlaps the MMAs
     __syncwarp();
     if (!mbar_wait_bounded(bar, (uint32_t)(it & 1))) {
       ok = false;
@@ -164,20 +188,39 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
     if (!ok) break;
   }
 
-  // Epilogue: warp w reads TMEM lanes 32w..32w+31 (rows), 16 columns at a time.
+  // Epilogue: warp w reads TMEM lanes 32w..32w+31 (rows), 16 columns at a
+  // time, and writes each row's 16 values with 16-byte stores.
   if (ok) {
     const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-      float* crow = C + (size_t)row * N + n0 + c;
+      if (bias) {
+        const float4* b4 = reinterpret_cast<const float4*>(bias + n0 + c);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        float z = v[j];
-        if (bias) z += bias[n0 + c + j];
-        crow[j] = z;
-        if (act) act[(size_t)row * N + n0 + c + j] = __float2bfloat16(silu(z));
+        for (int q = 0; q < 4; ++q) {
+          const float4 b = b4[q];
+          v[4 * q] += b.x;
+          v[4 * q + 1] += b.y;
+          v[4 * q + 2] += b.z;
+          v[4 * q + 3] += b.w;
+        }
+      }
+      float4* c4 = reinterpret_cast<float4*>(C + (size_t)row * N + n0 + c);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) c4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      if (act) {
+        uint4 packed[2];
+        uint32_t* w32 = reinterpret_cast<uint32_t*>(packed);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(silu(v[2 * q]), silu(v[2 * q + 1]));
+          w32[q] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        uint4* a4 = reinterpret_cast<uint4*>(act + (size_t)row * N + n0 + c);
+        a4[0] = packed[0];
+        a4[1] = packed[1];
       }
     }
   }
