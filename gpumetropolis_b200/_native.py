@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libgpum_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_NODEVICE, ERR_DEVICE = range(7)
 ENGINE_INTERP, ENGINE_COMPILED, ENGINE_AUTO = 0, 1, 2
-MODE_RWM, MODE_DE, MODE_CHOL, MODE_MALA = 0, 1, 2, 3
+MODE_RWM, MODE_DE, MODE_CHOL, MODE_MALA, MODE_DE_SYNC = 0, 1, 2, 3, 4
 RNG_TRIPLE32, RNG_PHILOX = 0, 1
 _ERRLEN = 1024
 
@@ -104,6 +104,13 @@ SIGNATURES = {
     "gpum_b200_session_launches": (C.c_uint64, [C.c_void_p]),
     "gpum_b200_session_stream": (C.c_void_p, [C.c_void_p]),
     "gpum_b200_session_destroy": (None, [C.c_void_p]),
+    "gpum_b200_run_de_sync": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p, C.c_uint32,
+                                        C.c_uint64, _u32p, _sz, _f64p, _sz, _f64p, _f64p,
+                                        C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                        C.c_double, _f32p, _f32p, _f64p, _errp, _sz]),
+    "gpum_b200_session_run_de_sync": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_uint32,
+                                                C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                                C.c_int, _f32p, _f32p, _f64p, _errp, _sz]),
     "gpum_b200_session_record": (C.c_int, [C.c_void_p, C.c_uint64, _errp, _sz]),
     "gpum_b200_session_recorded": (C.c_int, [C.c_void_p, _f32p, _f64p, C.c_uint64,
                                              C.POINTER(C.c_uint64), _errp, _sz]),
@@ -195,6 +202,28 @@ def run(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, i
         _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
     _check(rc, err)
     return draws, acc, last
+
+
+def run_de_sync(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
+                proposal_sd, n_iter, seed, gamma, de_noise):
+    """One-shot path-B DE (``gpum_b200_run_de_sync``, the argument order of
+    ``rust_gpu_metropolis_de_sync``'s inputs)."""
+    code, pcode = _u32(code), _u32(prior_code)
+    consts, pconsts = _f64(consts), _f64(prior_consts)
+    data, init, sd = _f64(data), _f64(init), _f64(proposal_sd)
+    n_chains = init.size // n_params
+    draws = np.empty(max(n_iter * n_chains * n_params, 1), np.float32)
+    acc = np.empty(n_chains, np.float32)
+    last = np.empty(n_chains, np.float64)
+    err = C.create_string_buffer(_ERRLEN)
+    rc = load().gpum_b200_run_de_sync(
+        _p(code, C.c_uint32), code.size, _p(consts, C.c_double), consts.size, n_params,
+        _p(data, C.c_double), n_cols, n_obs, _p(pcode, C.c_uint32), pcode.size,
+        _p(pconsts, C.c_double), pconsts.size, _p(init, C.c_double), _p(sd, C.c_double),
+        n_chains, n_iter, seed & 0xFFFFFFFF, float(gamma), float(de_noise),
+        _p(draws, C.c_float), _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
+    _check(rc, err)
+    return draws[: n_iter * n_chains * n_params], acc, last
 
 
 def _batch(fname, code, consts, n_params, data, n_cols, n_obs, points, width):
@@ -302,6 +331,21 @@ class Session:
             n_iter, seed & 0xFFFFFFFF, proposal_mode, gamma, de_noise, _p(L, C.c_double),
             0 if L is None else L.size, rng, _p(draws, C.c_float), _p(acc, C.c_float),
             _p(last, C.c_double), err, _ERRLEN)
+        _check(rc, err)
+        return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def run_de_sync(self, init, proposal_sd, n_iter, seed, gamma, de_noise, rng=RNG_TRIPLE32):
+        """Per-generation DE (path B).  Returns (draws, accept, last_logpost)."""
+        init, sd = _f64(init), _f64(proposal_sd)
+        n_chains = init.size // self.n_params
+        draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
+        acc = np.empty(n_chains, np.float32)
+        last = np.empty(n_chains, np.float64)
+        err = C.create_string_buffer(_ERRLEN)
+        rc = self._lib.gpum_b200_session_run_de_sync(
+            self._h, _p(init, C.c_double), _p(sd, C.c_double), n_chains, n_iter,
+            seed & 0xFFFFFFFF, float(gamma), float(de_noise), rng, _p(draws, C.c_float),
+            _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
         _check(rc, err)
         return draws[: n_iter * n_chains * self.n_params], acc, last
 

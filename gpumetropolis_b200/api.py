@@ -279,9 +279,8 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
             raise GpumInputError("`de_noise` must be non-negative and finite.")
         if de_every is None:
             de_every = max(C, 10)
-        if de_sync:
-            raise GpumInputError("`de_sync = TRUE` (synchronous per-generation DE) is not "
-                                 "available on the b200 backend in this build.")
+        if de_sync and surrogate is not None and surrogate is not False:
+            raise GpumInputError("`surrogate` is not available with `de_sync = TRUE`.")
 
     scfg = None
     if surrogate is not None and surrogate is not False:
@@ -301,6 +300,18 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
             raise GpumInputError("`surrogate` must be None, True or a dict of options.")
 
     call = _Backend(model, data_mat, n_obs, rng_kind, scfg)
+    if method == "de" and de_sync:
+        # Path B (R/api.R:464-497): per-generation DE over the whole run,
+        # trim-only warmup, proposal_sd the fixed jitter base.
+        try:
+            d, acc, _ = call.session.run_de_sync(init_mat, sd_mat, n_iter, int(seed), gamma,
+                                                 de_noise, rng=rng_kind)
+        finally:
+            call.close()
+        draws = d.reshape((n_iter, n_chains, npar), order="F")
+        return GpumFit(draws[warmup:], acc.astype(np.float64), model, n_iter - warmup, n_iter,
+                       warmup, n_chains, npar, backend, int(seed), "de", None,
+                       {"gamma": gamma, "de_noise": de_noise, "de_sync": True})
     if scfg is not None:
         every = {"pt": swap_every, "de": de_every}.get(method)
         w_eff = warmup if every is None else max(0, min(-(-n_iter // every), warmup // every)) * every

@@ -187,6 +187,7 @@ struct gpum_b200_session {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   int graph_len = 0;
+  uint64_t graph_launches = 0;  // kernel nodes per graph replay
   uint64_t launches = 0;
   // Training pairs for the surrogate (exact runs only).
   DBuf<float> rec_theta;
@@ -328,6 +329,18 @@ struct gpum_b200_session {
   }
 
   void launch(int phase) { launch_with(geo, E, phase); }
+
+  // One Metropolis iteration: for path-B DE the proposals of the generation
+  // come first, in their own kernel (every chain reads the population).
+  void step() {
+    if (A.mode == MODE_DESYNC) {
+      desync_propose_kernel<<<(unsigned)((n_chains + 127) / 128), 128, 0, stream>>>(
+          A, params.p, geo.C_pad);
+      GPUM_CK(cudaGetLastError());
+      ++launches;
+    }
+    launch(PH_STEP);
+  }
 
   void launch_with(const Geometry& g, EvalArgs& e, int phase) {
     const dim3 grid(g.NCB, g.NOB);
@@ -490,7 +503,9 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   require(s != nullptr, "session is NULL");
   require(C >= 1, "n_chains must be at least 1");
   require(init && sd && temps, "init, proposal_sd and temperatures must be non-NULL");
-  require(mode <= 3, "proposal_mode must be 0 (rwm), 1 (de), 2 (cholesky) or 3 (mala)");
+  require(mode <= 4,
+          "proposal_mode must be 0 (rwm), 1 (de), 2 (cholesky), 3 (mala) or 4 (de_sync)");
+  require(mode != 4 || C >= 3, "de_sync needs at least 3 chains (two distinct partners)");
   require(rng == GPUM_RNG_TRIPLE32 || rng == GPUM_RNG_PHILOX, "rng must be 0 or 1");
   const size_t np = s->np;
   const bool mala = mode == 3;
@@ -565,7 +580,11 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
   A.draws = s->draws.p;
   A.n_iter = max_iter;
   A.seed = seed;
-  A.mode = mode == 0 ? MODE_RWM : (mode == 2 ? MODE_CHOL : (mala ? MODE_MALA : MODE_DE));
+  A.mode = mode == 0 ? MODE_RWM
+         : mode == 2 ? MODE_CHOL
+         : mala      ? MODE_MALA
+         : mode == 4 ? MODE_DESYNC
+                     : MODE_DE;
   A.rng = rng;
   A.gamma = gamma;
   A.de_noise = de_noise;
@@ -599,15 +618,17 @@ void advance(gpum_b200_session* s, uint32_t n) {
   constexpr int kGraphLen = 32;
   if (n >= (uint32_t)kGraphLen && !s->gexec) {
     GPUM_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = s->launches;
     try {
-      for (int i = 0; i < kGraphLen; ++i) s->launch(PH_STEP);
+      for (int i = 0; i < kGraphLen; ++i) s->step();
     } catch (...) {
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(s->stream, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
-    s->launches -= kGraphLen;  // counted per replay below
+    s->graph_launches = s->launches - before;  // counted per replay below
+    s->launches = before;
     GPUM_CK(cudaStreamEndCapture(s->stream, &s->graph));
     GPUM_CK(cudaGraphInstantiate(&s->gexec, s->graph, 0));
     s->graph_len = kGraphLen;
@@ -615,10 +636,10 @@ void advance(gpum_b200_session* s, uint32_t n) {
   uint32_t left = n;
   while (s->gexec && left >= (uint32_t)s->graph_len) {
     GPUM_CK(cudaGraphLaunch(s->gexec, s->stream));
-    s->launches += s->graph_len;
+    s->launches += s->graph_launches;
     left -= s->graph_len;
   }
-  for (; left > 0; --left) s->launch(PH_STEP);
+  for (; left > 0; --left) s->step();
   s->n_done += n;
 }
 
@@ -1049,6 +1070,43 @@ int gpum_b200_grad_batch(const uint32_t* code, size_t n_code, const double* cons
                          char* err, size_t err_len) {
   return one_shot_batch(code, n_code, consts, n_consts, n_params, data, n_cols, n_obs, points,
                         n_points, out, err, err_len, B_GRAD);
+}
+
+int gpum_b200_session_run_de_sync(gpum_b200_session* s, const double* init, const double* sd,
+                                  uint32_t n_chains, uint32_t n_iter, uint32_t seed,
+                                  double gamma, double de_noise, int rng, float* out_draws,
+                                  float* out_accept, double* out_last, char* err,
+                                  size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(n_chains >= 1, "n_chains must be at least 1");
+    const std::vector<double> temps(n_chains, 1.0);  // path B is untempered
+    prepare(s, init, sd, temps.data(), n_chains, n_iter, seed, 4, gamma, de_noise, nullptr, 0,
+            rng);
+    advance(s, n_iter);
+    fetch(s, out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_run_de_sync(const uint32_t* code, size_t n_code, const double* consts,
+                          size_t n_consts, uint32_t n_params, const double* data,
+                          uint32_t n_cols, uint64_t n_obs, const uint32_t* prior_code,
+                          size_t n_prior, const double* prior_consts, size_t n_prior_consts,
+                          const double* init, const double* sd, uint32_t n_chains,
+                          uint32_t n_iter, uint32_t seed, double gamma, double de_noise,
+                          float* out_draws, float* out_accept, double* out_last, char* err,
+                          size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(n_chains >= 1, "n_chains must be at least 1");
+    std::unique_ptr<gpum_b200_session> s(create_session(code, n_code, consts, n_consts,
+                                                        prior_code, n_prior, prior_consts,
+                                                        n_prior_consts, n_params, data, n_cols,
+                                                        n_obs));
+    const std::vector<double> temps(n_chains, 1.0);
+    prepare(s.get(), init, sd, temps.data(), n_chains, n_iter, seed, 4, gamma, de_noise,
+            nullptr, 0, GPUM_RNG_TRIPLE32);
+    advance(s.get(), n_iter);
+    fetch(s.get(), out_draws, out_accept, out_last, nullptr);
+  });
 }
 
 int gpum_b200_session_record(gpum_b200_session* s, uint64_t capacity, char* err,

@@ -25,7 +25,7 @@ constexpr int kMaxStackF64 = 32;
 
 enum Phase : int { PH_EVAL = 0, PH_INIT = 1, PH_STEP = 2, PH_POINTWISE = 3 };
 enum RngKind : int { RNG_TRIPLE32 = 0, RNG_PHILOX = 1 };
-enum ModeKind : int { MODE_RWM = 0, MODE_DE = 1, MODE_CHOL = 2, MODE_MALA = 3 };
+enum ModeKind : int { MODE_RWM = 0, MODE_DE = 1, MODE_CHOL = 2, MODE_MALA = 3, MODE_DESYNC = 4 };
 
 // Chain state of a run, all device pointers.
 struct ChainArgs {
@@ -269,6 +269,32 @@ __device__ inline void propose(const ChainArgs& A, int c, Stream& rs, float* par
   for (int j = 0; j < np; ++j) params[(size_t)j * C_pad + c] = (float)y[j];
 }
 
+// Synchronous per-generation DE (path B, cpu_native.rs:400-506): the
+// difference vector comes from the current population, so this runs in its
+// own kernel after every chain's previous accept.  Partners a != c and
+// b != c, a (cpu_native.rs:430-440); g = 1 with probability 0.1, else gamma.
+__device__ inline void propose_desync(const ChainArgs& A, int c, Stream& rs, float* params,
+                                      int C_pad) {
+  const int n = A.n_chains, np = A.np;
+  int a = (int)(rs.next() * (double)n);
+  if (a >= n) a = n - 1;
+  if (a == c) a = (a + 1) % n;
+  int b = (int)(rs.next() * (double)n);
+  if (b >= n) b = n - 1;
+  while (b == c || b == a) b = (b + 1) % n;  // n >= 3 is checked by the host
+  const double g = rs.next() < 0.1 ? 1.0 : A.gamma;
+  const double* x = A.state + (size_t)c * np;
+  const double* pa = A.state + (size_t)a * np;
+  const double* pb = A.state + (size_t)b * np;
+  const double* sd = A.sd + (size_t)c * np;
+  double* y = A.prop + (size_t)c * np;
+  for (int j = 0; j < np; ++j) {
+    const double z = rs.normal();
+    y[j] = x[j] + g * (pa[j] - pb[j]) + A.de_noise * sd[j] * z;
+    params[(size_t)j * C_pad + c] = (float)y[j];
+  }
+}
+
 // Accept/reject + record + propose for chain c.  `ll` is the data-term sum;
 // with MALA the data-term gradient has been summed into A.gy (STEP) or A.gx
 // (INIT).  Prior::value(A, p) and Prior::value_grad(A, p, g) give the f64
@@ -286,7 +312,7 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
                                  : Prior::value(A, x));
     A.cur[c] = lp;
     A.last_eval[c] = lp;
-    if (A.n_iter > 0) {
+    if (A.n_iter > 0 && A.mode != MODE_DESYNC) {  // path B proposes in its own kernel
       rs.it = 0;
       propose(A, c, rs, params, C_pad);
     }
@@ -338,7 +364,7 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
     }
     if (t < A.n_iter)
       for (int j = 0; j < np; ++j) A.draws[((size_t)t * np + j) * C_pad + c] = (float)x[j];
-    if (t + 1 < A.n_iter) {
+    if (t + 1 < A.n_iter && A.mode != MODE_DESYNC) {
       rs.it = t + 1;
       rs.k = 0;
       propose(A, c, rs, params, C_pad);

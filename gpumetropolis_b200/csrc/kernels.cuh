@@ -106,6 +106,21 @@ static __global__ void draws_layout_kernel(const float* __restrict__ in, float* 
 // so the target is unchanged; only stage-1 survivors are evaluated exactly.
 namespace gpum {
 
+// Path-B DE proposals of generation A.iter[0] for every chain (one thread per
+// chain), between the previous generation's accepts and this generation's
+// evaluation.  All chain blocks have the same iteration count here.
+static __global__ void desync_propose_kernel(ChainArgs A, float* params, int C_pad) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.n_chains) return;
+  const uint32_t t = A.iter[0];
+  if (t >= A.n_iter) return;
+  Stream rs = make_stream(A, c);
+  rs.it = t;
+  rs.k = 0;
+  propose_desync(A, c, rs, params, C_pad);
+  A.ctr[c] = rs.ctr;
+}
+
 struct DaArgs {
   double* sll_x;     // [C] surrogate log-likelihood at the state
   double* sll_y;     // [C] surrogate log-likelihood at the proposal

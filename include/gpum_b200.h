@@ -49,6 +49,8 @@ extern "C" {
 #define GPUM_MODE_DE 1          /* differential evolution on the init snapshot */
 #define GPUM_MODE_CHOL 2        /* random walk with per-chain Cholesky factor  */
 #define GPUM_MODE_MALA 3        /* Metropolis-adjusted Langevin                */
+#define GPUM_MODE_DE_SYNC 4     /* per-generation DE, path B (sessions only;   *
+                                 * cpu_native.rs:400-506)                      */
 
 /* evaluation engines (gpum_b200_session_set_engine) */
 #define GPUM_ENGINE_INTERP 0    /* register-stack bytecode interpreter          */
@@ -139,6 +141,22 @@ GPUM_API int gpum_b200_loglik_batch_noalloc(const uint32_t* code, size_t n_code,
                                             double* d_out, void* stream, char* err,
                                             size_t err_len);
 
+/* Synchronous per-generation differential evolution (path B): every
+ * proposal of generation t reads the population after generation t-1;
+ * untempered; proposal_sd is the jitter base; needs n_chains >= 3.  Same
+ * arguments and outputs as rust_gpu_metropolis_de_sync (lib.rs:215-259,
+ * cpu_native.rs:400-506), in this header's layouts, with the reference's
+ * triple32 stream. */
+GPUM_API int gpum_b200_run_de_sync(const uint32_t* code, size_t n_code, const double* consts,
+                                   size_t n_consts, uint32_t n_params, const double* data,
+                                   uint32_t n_cols, uint64_t n_obs, const uint32_t* prior_code,
+                                   size_t n_prior, const double* prior_consts,
+                                   size_t n_prior_consts, const double* init,
+                                   const double* proposal_sd, uint32_t n_chains,
+                                   uint32_t n_iter, uint32_t seed, double gamma,
+                                   double de_noise, float* out_draws, float* out_accept,
+                                   double* out_last_logpost, char* err, size_t err_len);
+
 /* ------------------------------------------------------------- sessions --
  * A session keeps the model and the data resident on the GPU, so batches of a
  * host-orchestrated run (adaptive warmup, PT, DE snapshots) do not re-upload
@@ -159,6 +177,14 @@ GPUM_API int gpum_b200_session_run(gpum_b200_session* s, const double* init, con
                           const double* proposal_l, size_t n_l, int rng, float* out_draws,
                           float* out_accept, double* out_last_logpost, char* err,
                           size_t err_len);
+
+/* gpum_b200_run_de_sync on a session; rng selects the stream. */
+GPUM_API int gpum_b200_session_run_de_sync(gpum_b200_session* s, const double* init,
+                                           const double* proposal_sd, uint32_t n_chains,
+                                           uint32_t n_iter, uint32_t seed, double gamma,
+                                           double de_noise, int rng, float* out_draws,
+                                           float* out_accept, double* out_last_logpost,
+                                           char* err, size_t err_len);
 
 /* Select the evaluation engine (GPUM_ENGINE_*); the default is AUTO.
  * Gradients (MALA, grad_batch) always use the compiled engine. */

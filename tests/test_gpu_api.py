@@ -91,6 +91,27 @@ def test_de_recovers_correlated_bivariate(gpu):
     assert rhat(fit["mu1"], warmup=0) < 1.05
 
 
+def test_de_sync_recovers_correlated_bivariate(gpu):
+    # path B (R/api.R:464-497): per-generation population, trim-only warmup
+    rng = np.random.default_rng(3)
+    rho = 0.9
+    S = np.array([[1, rho], [rho, 1]])
+    y = rng.standard_normal((500, 2)) @ np.linalg.cholesky(S).T + np.array([2.0, -1.0])
+    Si = np.linalg.inv(S)
+    f = (f"~ -0.5 * ({Si[0, 0]:.6f}*(y1-mu1)^2 + 2*{Si[0, 1]:.6f}*(y1-mu1)*(y2-mu2)"
+         f" + {Si[1, 1]:.6f}*(y2-mu2)^2)")
+    m = gpum_model(f, ["mu1", "mu2"], ["y1", "y2"])
+    fit = gpu_metropolis(m, {"y1": y[:, 0], "y2": y[:, 1]}, n_iter=8000, n_chains=16,
+                         method="de", de_sync=True, seed=2)
+    assert fit.extra["de_sync"] and fit.adaptation is None
+    assert fit.draws.shape == (4000, 16, 2) and fit.warmup == 4000
+    d1, d2 = fit["mu1"].ravel(), fit["mu2"].ravel()
+    assert abs(d1.mean() - y[:, 0].mean()) < 0.02
+    assert abs(d2.mean() - y[:, 1].mean()) < 0.02
+    assert abs(np.corrcoef(d1, d2)[0, 1] - rho) < 0.05
+    assert rhat(fit["mu1"], warmup=0) < 1.05
+
+
 def test_mala_recovers_gaussian_at_its_target_rate(gpu):
     # test-mala.R:35-46 (runs on the GPU here; the reference refuses a GPU)
     rng = np.random.default_rng(1)

@@ -165,3 +165,40 @@ def test_device_resident_stepping_matches_one_call(gpu):
         d2, a2, l2, n = s.fetch()
     assert n == 90
     assert np.array_equal(d1, d2) and np.array_equal(a1, a2) and np.array_equal(l1, l2)
+
+
+@pytest.mark.parametrize("engine", [0, 1], ids=["interp", "compiled"])
+def test_de_sync_generations_follow_the_oracle(gpu, engine):
+    # path B: every proposal reads the previous generation of the whole
+    # population (cpu_native.rs:400-506), so one flipped decision would
+    # change every later generation; with the triple32 stream the GPU
+    # population follows the CPU restatement exactly
+    w = W.make("gaussian", n_obs=2000)
+    C, n_iter, seed = 8, 200, 13
+    rng = np.random.default_rng(4)
+    init = (w.data.mean() + rng.normal(0, 0.1, C)).reshape(C, 1)
+    sd = np.full((C, 1), 0.05)
+    with gpu.Session(*_model_args(w), engine=engine) as s:
+        d_g, a_g, l_g = s.run_de_sync(init, sd, n_iter, seed, 0.8, 0.01)
+    d_o, a_o, l_o = O.run_de_sync(*_model_args(w), init, sd, n_iter, seed, 0.8, 0.01)
+    np.testing.assert_array_equal(a_g, a_o)
+    np.testing.assert_allclose(d_g, d_o, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(l_g, l_o, rtol=1e-6)
+    assert 0.05 < a_g.mean() < 0.95
+
+
+def test_de_sync_one_shot_entry_matches_session(gpu):
+    w = W.make("gaussian", n_obs=1500)
+    m = w.model
+    C, n_iter = 6, 50
+    init = np.linspace(3.0, 3.8, C).reshape(C, 1)
+    sd = np.full((C, 1), 0.05)
+    d1, a1, l1 = gpu.run_de_sync(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                                 m.n_params, w.data, m.n_cols, w.n_obs, init, sd, n_iter, 3,
+                                 0.7, 0.02)
+    with gpu.Session(*_model_args(w)) as s:
+        d2, a2, l2 = s.run_de_sync(init, sd, n_iter, 3, 0.7, 0.02)
+        with pytest.raises(gpu.GpumError, match="at least 3 chains"):
+            s.run_de_sync(init[:2], sd[:2], 10, 3, 0.7, 0.02)
+    np.testing.assert_array_equal(d1, d2)
+    np.testing.assert_array_equal(a1, a2)
