@@ -111,6 +111,8 @@ SIGNATURES = {
     "gpum_b200_session_run_de_sync": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_uint32,
                                                 C.c_uint32, C.c_uint32, C.c_double, C.c_double,
                                                 C.c_int, _f32p, _f32p, _f64p, _errp, _sz]),
+    "gpum_b200_session_set_likelihood_powers": (C.c_int, [C.c_void_p, _f64p, _sz, _errp,
+                                                          _sz]),
     "gpum_b200_session_record": (C.c_int, [C.c_void_p, C.c_uint64, _errp, _sz]),
     "gpum_b200_session_recorded": (C.c_int, [C.c_void_p, _f32p, _f64p, C.c_uint64,
                                              C.POINTER(C.c_uint64), _errp, _sz]),
@@ -348,6 +350,17 @@ class Session:
             _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
         _check(rc, err)
         return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def set_likelihood_powers(self, beta=None):
+        """Per-chain likelihood powers for later runs (None clears)."""
+        err = C.create_string_buffer(_ERRLEN)
+        if beta is None:
+            _check(self._lib.gpum_b200_session_set_likelihood_powers(self._h, None, 0, err,
+                                                                     _ERRLEN), err)
+            return
+        b = _f64(beta)
+        _check(self._lib.gpum_b200_session_set_likelihood_powers(
+            self._h, _p(b, C.c_double), b.size, err, _ERRLEN), err)
 
     def record(self, capacity):
         """Store the (theta, log-likelihood) pair of every exactly evaluated

@@ -383,3 +383,140 @@ def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmu
     kept = draws[warmup:] if warmup > 0 else draws
     return GpumFit(kept, acc, model, n_iter - warmup, n_iter, warmup, C, npar, backend, seed,
                    method)
+
+
+# ------------------------------------------------------------ evidence (TI)
+@dataclass
+class GpumEvidence:
+    log_evidence: float
+    betas: np.ndarray
+    expected_loglik: np.ndarray
+    n_rungs: int
+    power: float
+    accept_rate: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+    def __repr__(self):
+        return (f"<gpum_evidence>\n  log marginal likelihood {self.log_evidence:.3f}\n"
+                f"  thermodynamic integration over {self.n_rungs} rungs (power {self.power:g})")
+
+
+@dataclass
+class GpumBayesFactor:
+    bf10: float
+    log_bf10: float
+    log_evidence1: float
+    log_evidence0: float
+    interpretation: str
+
+
+def gpum_evidence(model: GpumModel, data=None, n_rungs=24, power=5, n_iter=4000, n_chains=8,
+                  warmup=None, seed=1, backend="b200", max_points_per_rung=20000,
+                  rng="triple32") -> GpumEvidence:
+    """Log marginal likelihood by thermodynamic integration (``R/bayes.R:279-338``).
+
+    Power posteriors ``p_beta ∝ p(y|θ)^beta p(θ)`` on the grid
+    ``beta = (k / n_rungs)^power``; the log evidence is the trapezoidal
+    integral over beta of E_beta[log p(y|θ)] (Gelman & Meng 1998; Friel &
+    Pettitt 2008).  The reference samples the rungs one after another with a
+    "power model" each; here every rung is a group of ``n_chains`` chains of
+    one batched run on the device (per-chain likelihood powers), with
+    adaptive random-walk proposals fitted per chain (a DE pool or a pooled
+    covariance would mix rungs whose targets differ).  E_beta[log p(y|θ)] is
+    the mean of ``loglik_batch`` over each rung's kept draws."""
+    if not isinstance(model, GpumModel):
+        raise GpumInputError("`model` must be a gpum_model from gpum_model().")
+    if backend not in ("b200", "auto"):
+        raise GpumInputError(f"backend '{backend}' is not available in this build. "
+                             "Available: b200")
+    if model.prior.code.size == 0:
+        raise GpumInputError("Evidence requires a proper prior; this model has none. The "
+                             "marginal likelihood is undefined for a flat or absent prior.")
+    n_rungs, n_chains, n_iter = int(n_rungs), int(n_chains), int(n_iter)
+    if n_rungs < 1 or n_chains < 1:
+        raise GpumInputError("`n_rungs` and `n_chains` must be positive.")
+    warmup = n_iter // 2 if warmup is None else int(warmup)
+    if warmup < 1 or warmup >= n_iter:
+        raise GpumInputError("`warmup` must be in [1, n_iter).")
+    rng_kind = {"triple32": _native.RNG_TRIPLE32, "philox": _native.RNG_PHILOX}[rng]
+    data_mat, n_obs = _data_matrix(model, data)
+    npar = model.n_params
+    betas = (np.arange(n_rungs + 1) / n_rungs) ** float(power)
+    C = (n_rungs + 1) * n_chains
+    beta_c = np.repeat(betas, n_chains)              # chain r*n_chains + k is on rung r
+    g = np.random.Generator(np.random.PCG64(int(seed)))
+    init = g.standard_normal((C, npar))
+    call = _Backend(model, data_mat, n_obs, rng_kind)
+    try:
+        s = call.session
+        s.set_likelihood_powers(beta_c)
+        ones = np.ones(C)
+        # Warmup: batches of diagonal RWM, per-chain Welford covariance and
+        # Robbins-Monro scale (R/adaptive.R:101-254 without the pooled
+        # covariance), statistics restarted at the half.
+        n_batches = min(40, max(10, warmup // 50), warmup)
+        sizes = np.full(n_batches, warmup // n_batches)
+        sizes[-1] += warmup - sizes.sum()
+        states = AD.Welford.init(C, npar, np.full(npar, 0.01))
+        scale0 = 2.38 / np.sqrt(npar)
+        scales = np.full(C, scale0)
+        sd = np.full((C, npar), 0.1)
+        target = AD.target_accept(npar)
+        cur = init
+        for b in range(1, n_batches + 1):
+            d, acc, _ = s.run(cur, sd, ones, int(sizes[b - 1]), int(seed) + b - 1, 0, rng=rng_kind)
+            d = d.reshape((int(sizes[b - 1]), C, npar), order="F")
+            states.update(d)
+            bi = b - n_batches // 2 if b > n_batches // 2 else b
+            scales = AD.robbins_monro_scale(scales, acc, bi, npar, target)
+            cur = d[-1].copy()
+            if b == n_batches // 2:
+                diag = np.maximum(np.diagonal(states.covariance(), axis1=1, axis2=2), 1e-12)
+                states = AD.Welford.init(C, npar, diag.mean(axis=0))
+            cov = states.covariance()
+            sd = scales[:, None] * np.sqrt(np.maximum(np.diagonal(cov, axis1=1, axis2=2), 1e-12))
+        # Sampling with per-chain Cholesky factors of the warmup covariance.
+        samp = n_iter - warmup
+        if npar > 1:
+            cov = states.covariance()
+            L = np.stack([scales[c] * AD.cholesky_reg(cov[c]) for c in range(C)])
+            d, acc, _ = s.run(cur, sd, ones, samp, int(seed) + n_batches, 2, proposal_l=L,
+                              rng=rng_kind)
+        else:
+            d, acc, _ = s.run(cur, sd, ones, samp, int(seed) + n_batches, 0, rng=rng_kind)
+        d = d.reshape((samp, C, npar), order="F")
+        s.set_likelihood_powers(None)
+        expected = np.empty(n_rungs + 1)
+        for r in range(n_rungs + 1):
+            pts = d[:, r * n_chains:(r + 1) * n_chains, :].reshape(-1, npar)
+            if pts.shape[0] > max_points_per_rung:
+                pts = pts[np.linspace(0, pts.shape[0] - 1, max_points_per_rung).astype(int)]
+            expected[r] = float(np.mean(s.loglik_batch(pts)))
+    finally:
+        call.close()
+    log_ev = float(np.sum(0.5 * (expected[1:] + expected[:-1]) * np.diff(betas)))
+    return GpumEvidence(log_ev, betas, expected, n_rungs, float(power), acc.astype(np.float64))
+
+
+def _jeffreys(b: float) -> str:
+    if b < 1:
+        return f"favours model0 ({_jeffreys(1 / b)} reversed)"
+    if b < 3:
+        return "barely worth mention"
+    if b < 10:
+        return "substantial"
+    if b < 30:
+        return "strong"
+    if b < 100:
+        return "very strong"
+    return "decisive"
+
+
+def gpum_bayes_factor(model1: GpumModel, model0: GpumModel, data=None,
+                      **kw) -> GpumBayesFactor:
+    """B_10 = p(y | model1) / p(y | model0) by thermodynamic integration
+    (``R/bayes.R:374-393``); keyword arguments go to :func:`gpum_evidence`."""
+    e1 = gpum_evidence(model1, data, **kw)
+    e0 = gpum_evidence(model0, data, **kw)
+    log_bf = e1.log_evidence - e0.log_evidence
+    bf = float(np.exp(log_bf))
+    return GpumBayesFactor(bf, log_bf, e1.log_evidence, e0.log_evidence, _jeffreys(bf))

@@ -202,6 +202,9 @@ struct gpum_b200_session {
   DaArgs D{};
   gpum_b200_mlp* da_mlp = nullptr;
   int da_chunks = 0;
+  // Per-chain likelihood powers for later runs (power posteriors).
+  DBuf<double> beta;
+  size_t n_beta = 0;
 
   ~gpum_b200_session() {
     drop_graph();
@@ -599,6 +602,11 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
     A.my = s->my.p;
     A.vbuf = s->vbuf.p;
   }
+  if (s->n_beta > 0) {
+    require(s->n_beta == C, "likelihood powers were set for " + std::to_string(s->n_beta) +
+                                " chains, the run has " + std::to_string(C));
+    A.beta = s->beta.p;
+  }
   if (s->rec_cap > 0) {
     A.rec_theta = s->rec_theta.p;
     A.rec_ll = s->rec_ll.p;
@@ -767,6 +775,7 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   require(mlp != nullptr, "surrogate is NULL");
   require(mode <= 2, "delayed acceptance needs a symmetric proposal: mode 0 (rwm), 1 (de) or 2 "
                      "(cholesky)");
+  require(s->n_beta == 0, "delayed acceptance does not support likelihood powers");
   const uint64_t keep_cap = s->rec_cap;
   s->rec_cap = 0;  // stage-1 rejections leave no exact pair to record
   try {
@@ -1106,6 +1115,28 @@ int gpum_b200_run_de_sync(const uint32_t* code, size_t n_code, const double* con
             nullptr, 0, GPUM_RNG_TRIPLE32);
     advance(s.get(), n_iter);
     fetch(s.get(), out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_session_set_likelihood_powers(gpum_b200_session* s, const double* beta,
+                                            size_t n_chains, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    s->drop_graph();
+    s->prepared = false;
+    if (beta == nullptr || n_chains == 0) {
+      s->n_beta = 0;
+      s->beta.release();
+      return;
+    }
+    for (size_t c = 0; c < n_chains; ++c)
+      require(std::isfinite(beta[c]) && beta[c] >= 0.0,
+              "likelihood powers must be finite and non-negative");
+    s->beta.ensure(n_chains);
+    GPUM_CK(cudaMemcpyAsync(s->beta.p, beta, sizeof(double) * n_chains, cudaMemcpyHostToDevice,
+                            s->stream));
+    GPUM_CK(cudaStreamSynchronize(s->stream));
+    s->n_beta = n_chains;
   });
 }
 

@@ -62,6 +62,9 @@ struct ChainArgs {
   float* rec_theta;     // [rec_cap][np] or nullptr
   double* rec_ll;       // [rec_cap]
   uint64_t rec_base, rec_cap;
+  // Power posteriors (thermodynamic integration): chain c targets
+  // beta[c] * loglik + prior; nullptr means beta = 1.
+  const double* beta;
 };
 
 struct EvalArgs {
@@ -307,8 +310,9 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
   Stream rs = make_stream(A, c);
   const bool mala = A.mode == MODE_MALA;
   double* x = A.state + (size_t)c * np;
+  const double bl = A.beta ? A.beta[c] * ll : ll;  // likelihood power
   if (phase == PH_INIT) {
-    const double lp = ll + (mala ? Prior::value_grad(A, x, A.gx + (size_t)c * np)
+    const double lp = bl + (mala ? Prior::value_grad(A, x, A.gx + (size_t)c * np)
                                  : Prior::value(A, x));
     A.cur[c] = lp;
     A.last_eval[c] = lp;
@@ -318,7 +322,7 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
     }
   } else {
     const double* y = A.prop + (size_t)c * np;
-    const double plp = ll + (mala ? Prior::value_grad(A, y, A.gy + (size_t)c * np)
+    const double plp = bl + (mala ? Prior::value_grad(A, y, A.gy + (size_t)c * np)
                                   : Prior::value(A, y));
     A.last_eval[c] = plp;
     if (A.rec_ll) {
@@ -537,11 +541,12 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
     for (uint32_t o = 0; o < nob; ++o) ll += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W]);
     if (A.mode == MODE_MALA) {
       double* gsum = (phase == PH_INIT ? A.gx : A.gy) + (size_t)c * np;
+      const double b = A.beta ? A.beta[c] : 1.0;
       for (int j = 0; j < np; ++j) {
         double v = 0.0;
         for (uint32_t o = 0; o < nob; ++o)
           v += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W + 1 + j]);
-        gsum[j] = v;
+        gsum[j] = b * v;
       }
     }
     finalize_chain<Prior>(A, c, cb, ll, phase, const_cast<float*>(E.params), E.C_pad);

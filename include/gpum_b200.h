@@ -275,6 +275,16 @@ GPUM_API int gpum_b200_mlp_get_params(gpum_b200_mlp* m, float* out, char* err, s
 GPUM_API int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
                                       const float* B, float* C, char* err, size_t err_len);
 
+/* Power posteriors for thermodynamic integration: later runs on this session
+ * target beta[c] * log-likelihood + log-prior for chain c (the prior is not
+ * tempered; the acceptance temperature still applies).  The reference builds
+ * one "power model" per rung (R/bayes.R:266-277) and runs the rungs one after
+ * another; here all rungs run as chains of one batch.  NULL / 0 clears; runs
+ * must then have exactly n_chains chains.  Not available with run_da. */
+GPUM_API int gpum_b200_session_set_likelihood_powers(gpum_b200_session* s, const double* beta,
+                                                     size_t n_chains, char* err,
+                                                     size_t err_len);
+
 /* ------------------------------------------------- delayed acceptance --
  * No counterpart in the reference.  Training pairs come from exact runs:
  * with recording on, every proposal an exact step (session_run / advance)

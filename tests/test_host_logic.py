@@ -136,3 +136,11 @@ def test_pooled_ess_on_ar1_and_stuck_chains():
     # chains that never move carry one value each, not n
     stuck = np.repeat(rng.standard_normal((1, m)), 400, axis=0)
     assert ess_pooled(stuck) < 2 * m
+
+
+def test_evidence_needs_a_proper_prior():
+    # test-bayes.R:77-82
+    from gpumetropolis_b200.api import gpum_evidence
+    flat = gpum_model("~ -((y - mu)^2) / 8", "mu", "y")
+    with pytest.raises(GpumInputError, match="proper prior"):
+        gpum_evidence(flat, {"y": np.zeros(10)})
