@@ -269,6 +269,28 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     return name[i];
   };
 
+  // Use counts, and LOG(1 + EXP(a)) chains whose inner nodes feed nothing
+  // else: the value functions evaluate them as one accurate softplus(a).
+  std::vector<int> uses(N, 0);
+  for (int i = 0; i < N; ++i) {
+    if (!live[i]) continue;
+    if (g.n[i].a >= 0) ++uses[g.n[i].a];
+    if (g.n[i].b >= 0) ++uses[g.n[i].b];
+  }
+  if (root >= 0) ++uses[root];
+  std::vector<int> softplus_arg(N, -1);
+  std::vector<char> softplus_inner(N, 0);
+  auto is_one = [&](int i) { return i >= 0 && g.n[i].op == O_C && g.n[i].c == 1.0; };
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || !is_pd(i) || g.n[i].op != O_LOG) continue;
+    const int j = g.n[i].a;
+    if (!is_pd(j) || g.n[j].op != O_ADD || uses[j] != 1) continue;
+    const int k = is_one(g.n[j].a) ? g.n[j].b : (is_one(g.n[j].b) ? g.n[j].a : -1);
+    if (k < 0 || !is_pd(k) || g.n[k].op != O_EXP || uses[k] != 1) continue;
+    softplus_arg[i] = g.n[k].a;
+    softplus_inner[j] = softplus_inner[k] = 1;
+  }
+
   std::ostringstream s;
   s << "#define GM_NP " << n_params << "\n";
   s << "#define GM_NH " << std::max(1, out->n_hoist) << "\n";
@@ -305,20 +327,25 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   for (int i : need_h) s << "  h[" << hslot[i] << "] = " << name[i] << ";\n";
   s << "  (void)p; (void)h;\n}\n";
 
-  // Per-observation forward code.
-  auto emit_fwd = [&](std::ostringstream& o) {
+  // Per-observation forward code (`fused`: with the softplus rewrite, for
+  // the value functions; the gradient keeps every node).
+  auto emit_fwd = [&](std::ostringstream& o, bool fused) {
     for (int i = 0; i < N; ++i) {
       if (!live[i] || !is_pd(i)) continue;
+      if (fused && softplus_inner[i]) continue;
       const Node& x = g.n[i];
       o << "  const float " << name[i] << " = "
-        << op_expr(g, i, ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "", true) << ";\n";
+        << (fused && softplus_arg[i] >= 0
+                ? "gm_softplus(" + ref_obs(softplus_arg[i]) + ")"
+                : op_expr(g, i, ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "", true))
+        << ";\n";
       ++out->n_fwd;
     }
   };
   const std::string rootv = root < 0 ? std::string("0.0f") : ref_obs(root);
   s << "__device__ __forceinline__ float gm_value(const float* __restrict__ d, "
        "const float* __restrict__ p, const float* __restrict__ h) {\n";
-  emit_fwd(s);
+  emit_fwd(s, true);
   s << "  (void)d; (void)p; (void)h;\n  return " << rootv << ";\n}\n";
 
   // Paired versions (two observations per call) of gm_data and gm_value.
@@ -327,13 +354,6 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   // is fused into it (FFMA2), the contraction the scalar code gets from
   // --fmad=true.
   {
-    std::vector<int> uses(N, 0);
-    for (int i = 0; i < N; ++i) {
-      if (!live[i]) continue;
-      if (g.n[i].a >= 0) ++uses[g.n[i].a];
-      if (g.n[i].b >= 0) ++uses[g.n[i].b];
-    }
-    if (root >= 0) ++uses[root];
     auto ref2 = [&](int i) -> std::string {
       const Node& x = g.n[i];
       if (x.op == O_C) return "gm2(" + flit(x.c) + ")";
@@ -373,10 +393,12 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
          "const float2* __restrict__ pp, const float2* __restrict__ hh) {\n";
     for (int i = 0; i < N; ++i) {
       if (!live[i] || !is_pd(i)) continue;
-      if (fused[i]) continue;
+      if (fused[i] || softplus_inner[i]) continue;
       const Node& x = g.n[i];
       std::string e;
-      if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
+      if (softplus_arg[i] >= 0) {
+        e = "gm2_softplus(" + ref2(softplus_arg[i]) + ")";
+      } else if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
         const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
         e = "gm2_fma(" + ref2(g.n[m].a) + ", " + ref2(g.n[m].b) + ", " + ref2(o) + ")";
       } else {
@@ -395,7 +417,7 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   {
     std::ostringstream f;
     const int nf = out->n_fwd;
-    emit_fwd(f);
+    emit_fwd(f, false);
     out->n_fwd = nf;
     s << f.str();
     // adjoint accumulators of per-observation nodes

@@ -115,3 +115,32 @@ def test_mala_and_rwm_on_compiled_engine_recover_gaussian(gpu):
             e = ess(dr, warmup=0)
             assert abs(dr.mean() - w.data.mean()) < 5 * dr.std() / math.sqrt(e)
             assert rhat(dr, warmup=0) < 1.01
+
+
+def test_softplus_rewrite_is_accurate(gpu):
+    # LOG(1 + EXP(z)) is evaluated as max(z, 0) + log1p(e^-|z|) in the value
+    # kernels.  Per observation it is compared with an exact f64 softplus of
+    # the same FP32 argument z = fl32(a * x): relative error of a few FP32
+    # ulp wherever softplus(z) is a normal FP32 number (the naive f64 form of
+    # the oracle rounds to 0 once e^z < 1e-16, so it is not the yardstick
+    # here); the sums are still checked against the oracle.
+    from gpumetropolis_b200.dsl import gpum_model
+    m = gpum_model("~ log(1 + exp(a * x))", "a", "x")
+    x = np.concatenate([np.linspace(-95, 95, 4001), np.linspace(-3, 3, 4001),
+                        [0.0, 1e-30, -1e-30, 87.0, -87.0, 200.0, -200.0]])
+    x = x.astype(np.float32).astype(np.float64)
+    a = np.array([1.0, -0.5])
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, 1,
+                     x.reshape(-1, 1), 1, x.size, engine=1) as s:
+        got = s.loglik_pointwise(a.reshape(-1, 1)).reshape(2, -1)
+        tot = s.loglik_batch(a.reshape(-1, 1))
+    z = (a[:, None].astype(np.float32) * x[None, :].astype(np.float32)).astype(np.float64)
+    exact = np.logaddexp(0.0, z)
+    assert np.all(np.isfinite(got))
+    normal = exact > 1e-30
+    rel = np.abs(got[normal] - exact[normal]) / exact[normal]
+    assert rel.max() < 6e-7, rel.max()
+    assert np.abs(got[~normal] - exact[~normal]).max() < 1e-30
+    want = O.loglik_pointwise(m.loglik.code, m.loglik.consts, 1, x.reshape(-1, 1), 1, x.size,
+                              a.reshape(-1, 1)).reshape(2, -1)
+    np.testing.assert_allclose(tot, want.sum(axis=1), rtol=1e-6)
