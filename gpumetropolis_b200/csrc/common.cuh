@@ -460,7 +460,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
     if constexpr (Body::kObsPerEval == 2) {
       // observation pairs (2 pi, 2 pi + 1); T is even, so each pair is
       // 8-byte aligned in every column of the tile
-      for (int pi = lane + 32 * wo; 2 * pi < T; pi += 32 * WO) {
+      auto pair = [&](int pi) {
         const int obs = obs0 + 2 * pi;
         const bool v0 = obs < E.n_obs, v1 = obs + 1 < E.n_obs;
         body.eval2(tile + 2 * pi, T, v0, v1);
@@ -475,6 +475,15 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
             }
           }
         }
+      };
+      constexpr int kT = Body::kTileObs;  // compile-time tile height, or 0
+      if (kT > 0 && kT % 64 == 0 && WO == 1) {
+        // every warp covers the tile: a fixed trip count, unrolled so the
+        // compiler can overlap one pair's loads with another's arithmetic
+#pragma unroll
+        for (int it = 0; it < (kT > 0 ? kT : 64) / 64; ++it) pair(lane + 32 * it);
+      } else {
+        for (int pi = lane + 32 * wo; 2 * pi < T; pi += 32 * WO) pair(pi);
       }
     } else {
       for (int ol = lane + 32 * wo; ol < T; ol += 32 * WO) {

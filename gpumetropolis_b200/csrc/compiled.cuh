@@ -114,6 +114,7 @@ struct JitBody {
 template <int G>
 struct JitBody2 {
   static constexpr int kObsPerEval = 2;
+  static constexpr int kTileObs = GM_T;
   float2 pp[G][GM_NP];
   float2 hh[G][GM_NH];
   double s[G];
