@@ -57,8 +57,8 @@ ROW_BYTES = 17 * 4          # one f32 observation row
 def _args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=30)
-    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--n-obs", type=int, default=1 << 20)
     p.add_argument("--chains", type=int, default=1024)
@@ -124,21 +124,29 @@ def cpu_sample(w, seconds, chains_cap):
 
 
 class Clocks:
-    """nvidia-smi sampled every 200 ms during the timed region."""
+    """nvidia-smi sampled every 100 ms; the summary keeps the samples whose
+    timestamps fall inside the marked (timed) window."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -154,22 +162,36 @@ class Clocks:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
+        import datetime
         for line in out.strip().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                self.rows.append(f)
+            if len(f) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                ts = None
+            self.rows.append((ts, f[1:]))
 
     def summary(self):
         rows = getattr(self, "rows", [])
-        if not rows:
+        window = "timed region"
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for ts, r in rows if ts is not None and self.t0 - 0.05 <= ts <= self.t1 + 0.05]
+        else:
+            inside = []
+        if not inside:
+            inside = [r for _, r in rows]
+            window = "whole sampler lifetime (no sample fell inside the timed region)"
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(inside), "window": window}
 
 
 def da_measure(w, C, n_warm, n_samp, seed=11):
@@ -301,6 +323,8 @@ def run_b200(a):
     torch.cuda.synchronize()
     l0 = sess.launches
     with Clocks(local) as clk:
+        time.sleep(0.5)  # let the sampler start before the timed region
+        clk.mark_start()
         t0 = time.perf_counter()
         with torch.cuda.stream(stream):
             for k in range(K):
@@ -310,6 +334,7 @@ def run_b200(a):
                 ends[k].record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        clk.mark_end()
     launches = sess.launches - l0
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     dev_ms = float(step_ms.sum())
