@@ -40,6 +40,7 @@ namespace gpum {
 int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
               std::string* err);
 int mlp_batch_rows(const gpum_b200_mlp* m);
+int mlp_infer_launches(const gpum_b200_mlp* m, int n);
 }  // namespace gpum
 
 static_assert(sizeof(CUtensorMap) == sizeof(TmapDesc), "tensor map size");
@@ -764,7 +765,7 @@ void da_step(gpum_b200_session* s) {
       s->geo_da.ntiles, s->geo_da.C_pad);
   da_tick_kernel<<<1, 32, 0, st>>>(s->D);
   GPUM_CK(cudaGetLastError());
-  s->launches += 5 + 5 * (uint64_t)s->da_chunks;
+  s->launches += 5 + (uint64_t)s->da_chunks;
 }
 
 void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const double* sd,
@@ -834,8 +835,8 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   std::string e;
   int rc = mlp_infer(mlp, s->state.p, (int)C, np, s->sll_x.p, st, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
-  s->da_chunks = (int)((C + mlp_batch_rows(mlp) - 1) / mlp_batch_rows(mlp));
-  s->launches += 5 * (uint64_t)s->da_chunks;
+  s->da_chunks = mlp_infer_launches(mlp, (int)C);  // launches per surrogate call
+  s->launches += (uint64_t)s->da_chunks;
   da_setup_kernel<<<(C + 255) / 256, 256, 0, st>>>(s->A, D);
   GPUM_CK(cudaGetLastError());
   ++s->launches;

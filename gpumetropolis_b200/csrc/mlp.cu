@@ -299,6 +299,181 @@ __global__ void mlp_unscale(const float* __restrict__ y, int n, float ysd, float
   if (i < n) out[i] = (double)y[i] * ysd + ymean;
 }
 
+// Fused inference for 128 rows per CTA (128 threads, one row per thread in
+// the transform and epilogues), for d <= 64 (dp = 64) and H in {128, 256}:
+//   X = transform(theta) -> shared (bf16, K-major core matrices)
+//   Z1 = X W1^T  (tcgen05, M = 128, N = H, K = 64, accumulators in TMEM)
+//   A1 = silu(Z1 + b1) -> shared (bf16, the K-major A operand of layer 2)
+//   Z2 = A1 W2^T (tcgen05, K = H in 64-wide slices; the W2 slice is staged in
+//        shared memory, the next one prefetched into registers meanwhile)
+//   y  = silu(Z2 + b2) . w3 + b3;  out = y * ysd + ymean   (f64)
+// Shared memory: X 16 KB | W1 H x 64 | A1 (H / 64) x 16 KB | W2 slice H x 64.
+// The whitening scratch (centred inputs, 128 x 64 f32) lives in A1's space
+// before layer 1 is read out.  Waits are bounded; a timeout sets the error
+// word and skips the epilogues.
+constexpr int kInfRows = 128;
+
+__host__ __device__ constexpr size_t mlp_infer_smem(int H) {
+  return (size_t)kInfRows * 64 * 2 + (size_t)H * 64 * 2 + (size_t)(H / 64) * kInfRows * 64 * 2 +
+         (size_t)H * 64 * 2 + 64;
+}
+
+__global__ void __launch_bounds__(kInfRows, 1)
+mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
+                const float* __restrict__ xmean, const float* __restrict__ xinv,
+                const float* __restrict__ xw, const bf16* __restrict__ W1h,
+                const float* __restrict__ b1, const bf16* __restrict__ W2h,
+                const float* __restrict__ b2, const float* __restrict__ w3,
+                const float* __restrict__ b3, float ysd, float ymean, double* __restrict__ out,
+                uint32_t* err) {
+  extern __shared__ __align__(1024) unsigned char fsm[];
+  constexpr int kSlice = kInfRows * 64 * 2;  // one 128 x 64 bf16 slice
+  unsigned char* sx = fsm;
+  unsigned char* sw1 = sx + kSlice;
+  unsigned char* sa1 = sw1 + (size_t)H * 128;
+  unsigned char* sw2 = sa1 + (size_t)(H / 64) * kSlice;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sw2 + (size_t)H * 128);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = blockIdx.x * kInfRows + tid;
+  const bool live = row < n;
+  const int KH = H / 64;
+
+  if (warp == 0) tmem_alloc(tslot, 256);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+
+  // Inputs: one row per thread.  Centred values go to a swizzled scratch
+  // (conflict-free column access) for the whitening products.
+  {
+    const double* th = theta + (size_t)(live ? row : 0) * d;
+    float* cen = reinterpret_cast<float*>(sa1);
+    for (int j = 0; j < d; ++j)
+      cen[tid * 64 + ((j + tid) & 63)] = live ? (float)th[j] - xmean[j] : 0.0f;
+    for (int k8 = 0; k8 < 64; k8 += 8) {
+      __align__(16) bf16 v8[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k = k8 + q;
+        float v = 0.0f;
+        if (live && k < d) {
+          if (xw) {
+            const float* wr = xw + (size_t)k * d;
+            for (int j = 0; j < d; ++j) v = fmaf(wr[j], cen[tid * 64 + ((j + tid) & 63)], v);
+          } else {
+            v = cen[tid * 64 + ((k + tid) & 63)] * xinv[k];
+          }
+        }
+        v8[q] = __float2bfloat16(v);
+      }
+      *reinterpret_cast<uint4*>(sx + kmajor_offset(tid, k8, kInfRows)) =
+          *reinterpret_cast<const uint4*>(v8);
+    }
+  }
+  // W1 (H x 64) into its K-major layout.
+  for (int i = tid; i < H * 8; i += kInfRows) {
+    const int r = i >> 3, c8 = (i & 7) * 8;
+    *reinterpret_cast<uint4*>(sw1 + kmajor_offset(r, c8, H)) =
+        *reinterpret_cast<const uint4*>(W1h + (size_t)r * 64 + c8);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(kInfRows, H);
+  const uint32_t lbo_x = (kInfRows / 8) * 128, lbo_h = (uint32_t)(H / 8) * 128;
+  if (tid == 0) {
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+      umma_bf16(tmem, umma_smem_desc(smem_addr(sx) + 2 * kk * lbo_x, lbo_x, 128),
+                umma_smem_desc(smem_addr(sw1) + 2 * kk * lbo_h, lbo_h, 128), idesc,
+                kk > 0 ? 1u : 0u);
+    umma_commit(bar);
+  }
+  // W2 slice prefetch into registers while layer 1 runs (H x 64 per slice).
+  constexpr int kMaxPf = 256 * 8 / kInfRows;  // 16 chunks per thread at H = 256
+  uint4 pf[kMaxPf];
+  const int npf = H * 8 / kInfRows;
+  auto load_w2 = [&](int s) {
+#pragma unroll
+    for (int q = 0; q < kMaxPf; ++q) {
+      if (q < npf) {
+        const int i = tid + q * kInfRows, r = i >> 3, c8 = (i & 7) * 8;
+        pf[q] = *reinterpret_cast<const uint4*>(W2h + (size_t)r * H + s * 64 + c8);
+      }
+    }
+  };
+  auto store_w2 = [&]() {
+#pragma unroll
+    for (int q = 0; q < kMaxPf; ++q) {
+      if (q < npf) {
+        const int i = tid + q * kInfRows, r = i >> 3, c8 = (i & 7) * 8;
+        *reinterpret_cast<uint4*>(sw2 + kmajor_offset(r, c8, H)) = pf[q];
+      }
+    }
+  };
+  load_w2(0);
+  int ok = mbar_wait_bounded(bar, 0u) ? 1 : 0;
+  ok = __syncthreads_and(ok);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  if (ok) {
+    // Layer-1 epilogue: A1 = silu(Z1 + b1) as bf16 into the layer-2 A operand.
+    for (int c = 0; c < H; c += 16) {
+      float v[16];
+      tmem_ld16(trow + (uint32_t)c, v);
+      __align__(16) bf16 a8[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) a8[j] = __float2bfloat16(silu(v[j] + b1[c + j]));
+      unsigned char* base = sa1 + (size_t)(c / 64) * kSlice;
+      *reinterpret_cast<uint4*>(base + kmajor_offset(tid, c % 64, kInfRows)) =
+          *reinterpret_cast<const uint4*>(a8);
+      *reinterpret_cast<uint4*>(base + kmajor_offset(tid, c % 64 + 8, kInfRows)) =
+          *reinterpret_cast<const uint4*>(a8 + 8);
+    }
+  }
+  // Layer 2 over the K slices of A1 / W2.
+  for (int s = 0; s < KH && ok; ++s) {
+    store_w2();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        umma_bf16(tmem,
+                  umma_smem_desc(smem_addr(sa1 + (size_t)s * kSlice) + 2 * kk * lbo_x, lbo_x, 128),
+                  umma_smem_desc(smem_addr(sw2) + 2 * kk * lbo_h, lbo_h, 128), idesc,
+                  (s > 0 || kk > 0) ? 1u : 0u);
+      umma_commit(bar);
+    }
+    if (s + 1 < KH) load_w2(s + 1);
+    ok = mbar_wait_bounded(bar, (uint32_t)((s + 1) & 1)) ? 1 : 0;
+    ok = __syncthreads_and(ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (ok) {
+    float acc = 0.0f;
+    for (int c = 0; c < H; c += 16) {
+      float v[16];
+      tmem_ld16(trow + (uint32_t)c, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc = fmaf(silu(v[j] + b2[c + j]), w3[c + j], acc);
+    }
+    if (live) out[row] = (double)(acc + b3[0]) * ysd + ymean;
+  } else if (tid == 0) {
+    atomicOr(err, DEV_ERR_MMA_TIMEOUT);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
 }  // namespace
 
 struct gpum_b200_mlp {
@@ -324,6 +499,10 @@ struct gpum_b200_mlp {
   Buf<uint32_t> err;
   int adam_t = 0;
   bool smem_set[2] = {false, false};
+  bool infer_smem_set = false;
+
+  // The fused inference kernel covers d <= 64 and H in {128, 256}.
+  bool fused_inference() const { return dp == 64 && (H == 128 || H == 256); }
 
   ~gpum_b200_mlp() {
     if (st) cudaStreamDestroy(st);
@@ -480,6 +659,11 @@ namespace gpum {
 
 int mlp_batch_rows(const gpum_b200_mlp* m) { return m->B; }
 
+// Kernel launches one mlp_infer call of n rows makes.
+int mlp_infer_launches(const gpum_b200_mlp* m, int n) {
+  return m->fused_inference() ? 1 : 5 * ((n + m->B - 1) / m->B);
+}
+
 // Surrogate log-likelihood of n f64 parameter vectors (device, chain-major)
 // into out (device), enqueued on `st`.  Used by the delayed-acceptance loop.
 int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
@@ -492,6 +676,22 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
   m->st = st;
   int rc = GPUM_OK;
   try {
+    if (m->fused_inference()) {
+      const size_t smem = mlp_infer_smem(m->H);
+      if (!m->infer_smem_set) {
+        MLP_CK(cudaFuncSetAttribute(mlp_infer_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+        m->infer_smem_set = true;
+      }
+      if (n > 0) {
+        mlp_infer_fused<<<(unsigned)((n + kInfRows - 1) / kInfRows), kInfRows, smem, st>>>(
+            theta, n, d, m->H, m->xmean.p, m->xinv.p, m->xw_or_null(), m->W1h.p, m->b1.p,
+            m->W2h.p, m->b2.p, m->w3.p, m->b3.p, m->ysd, m->ymean, out, m->err.p);
+        MLP_CK(cudaGetLastError());
+      }
+      m->st = keep;
+      return GPUM_OK;
+    }
     for (int r0 = 0; r0 < n; r0 += m->B) {
       const int rows = std::min(m->B, n - r0);
       const int Mi = (rows + kGemmBM - 1) / kGemmBM * kGemmBM;  // rows padded to the tile
@@ -672,26 +872,19 @@ int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, doubl
                           size_t err_len) {
   return mlp_guard(err, err_len, [&] {
     need(m && theta && out, "NULL argument");
-    Buf<float> dth;
-    Buf<double> none;
-    upload_pairs(m, theta, nullptr, n, dth, none);
-    std::vector<float> y(m->B);
-    for (size_t r0 = 0; r0 < n; r0 += m->B) {
-      const size_t rows = std::min<size_t>(m->B, n - r0);
-      mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p + r0 * m->d, nullptr, rows, m->d, m->dp, m->B, 0,
-                                          0, 0, m->xmean.p, m->xinv.p, m->xw_or_null(), 0.0f,
-                                          1.0f, m->Xh.p,
-                                          nullptr);
-      m->forward(m->B);
-      mlp_head<<<blocks((size_t)m->B * 32), 256, 0, m->st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr,
-                                                            m->B, m->H, m->B, m->yhat.p, nullptr,
-                                                            nullptr, nullptr, nullptr, 0);
-      MLP_CK(cudaGetLastError());
-      MLP_CK(cudaMemcpyAsync(y.data(), m->yhat.p, rows * sizeof(float), cudaMemcpyDeviceToHost,
-                             m->st));
-      MLP_CK(cudaStreamSynchronize(m->st));
-      for (size_t i = 0; i < rows; ++i) out[r0 + i] = (double)y[i] * m->ysd + m->ymean;
-    }
+    need(n <= (1u << 24), "more than 2^24 points");
+    if (n == 0) return;
+    // The same device path as the delayed-acceptance loop (mlp_infer).
+    Buf<double> dth, dout;
+    dth.alloc(n * m->d);
+    dout.alloc(n);
+    MLP_CK(cudaMemcpyAsync(dth.p, theta, n * m->d * sizeof(double), cudaMemcpyHostToDevice,
+                           m->st));
+    std::string e;
+    const int rc = gpum::mlp_infer(m, dth.p, (int)n, m->d, dout.p, m->st, &e);
+    if (rc != GPUM_OK) throw MlpFail{rc, e};
+    MLP_CK(cudaMemcpyAsync(out, dout.p, n * sizeof(double), cudaMemcpyDeviceToHost, m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
     m->check_err();
   });
 }

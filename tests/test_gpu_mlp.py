@@ -69,3 +69,29 @@ def test_training_fits_a_loglik_surface(gpu):
     s2.fit_normalizer(theta, ll)
     losses2 = s2.train(theta, ll, steps=20, lr=2e-3)
     assert np.array_equal(losses[:20], losses2)   # fixed-order reductions: repeatable
+
+
+@pytest.mark.parametrize("d,H,whiten", [(5, 128, False), (17, 256, True), (17, 256, False),
+                                        (65, 512, False)])
+def test_inference_matches_cpu_oracle(gpu, d, H, whiten):
+    # d <= 64 with H in {128, 256} runs the fused tcgen05 inference kernel,
+    # the others the layer-by-layer path; both against the numpy forward
+    theta, ll = _quadratic_pairs(d, 1000, 4)
+    s = gpu.Surrogate(d, hidden=H, batch=512, seed=5)
+    s.fit_normalizer(theta, ll, whiten=whiten)
+    s.train(theta, ll, steps=40, lr=2e-3)
+    got = s.predict(theta[:300])
+    th = theta[:300].astype(np.float32)
+    mu = theta.mean(axis=0).astype(np.float32)
+    if whiten:
+        cov = np.cov(theta, rowvar=False)
+        cov = cov + np.eye(d) * 1e-10 * max(float(np.mean(np.diag(cov))), 1e-300)
+        W = np.linalg.inv(np.linalg.cholesky(cov)).astype(np.float32)
+        X = MO.f32((th - mu) @ W.T)
+    else:
+        X = MO.f32((th - mu) * (1.0 / theta.std(axis=0)).astype(np.float32))
+    ym, ys = float(np.mean(ll)), float(np.std(ll))
+    ref = MO.predict(s.params(), d, H, X) * MO.f32(ys) + MO.f32(ym)
+    scale = np.std(ref)
+    assert np.max(np.abs(got - ref)) < 2e-2 * scale, np.max(np.abs(got - ref)) / scale
+    assert np.corrcoef(got, ref)[0, 1] > 0.9999
