@@ -299,26 +299,30 @@ __global__ void mlp_unscale(const float* __restrict__ y, int n, float ysd, float
   if (i < n) out[i] = (double)y[i] * ysd + ymean;
 }
 
-// Fused inference for 128 rows per CTA (128 threads, one row per thread in
-// the transform and epilogues), for d <= 64 (dp = 64) and H in {128, 256}:
+// Fused inference for 128 rows per CTA, for d <= 64 (dp = 64) and H in
+// {128, 256}, with 512 threads: warp w serves TMEM lane quarter w % 4 (rows
+// 32 (w % 4) + lane) and hidden-column quarter w / 4, so both epilogues are
+// spread over 16 warps.
 //   X = transform(theta) -> shared (bf16, K-major core matrices)
 //   Z1 = X W1^T  (tcgen05, M = 128, N = H, K = 64, accumulators in TMEM)
 //   A1 = silu(Z1 + b1) -> shared (bf16, the K-major A operand of layer 2)
-//   Z2 = A1 W2^T (tcgen05, K = H in 64-wide slices; the W2 slice is staged in
+//   Z2 = A1 W2^T (tcgen05, K = H in 64-wide slices; each W2 slice staged in
 //        shared memory, the next one prefetched into registers meanwhile)
-//   y  = silu(Z2 + b2) . w3 + b3;  out = y * ysd + ymean   (f64)
+//   y  = silu(Z2 + b2) . w3 + b3 (four column-quarter partials added in
+//        order);  out = y * ysd + ymean   (f64)
 // Shared memory: X 16 KB | W1 H x 64 | A1 (H / 64) x 16 KB | W2 slice H x 64.
-// The whitening scratch (centred inputs, 128 x 64 f32) lives in A1's space
-// before layer 1 is read out.  Waits are bounded; a timeout sets the error
-// word and skips the epilogues.
+// The whitening scratch (centred inputs, 128 x 64 f32) and the head
+// partials live in A1's space when it is free.  Waits are bounded; a timeout
+// sets the error word and skips the epilogues.
 constexpr int kInfRows = 128;
+constexpr int kInfThreads = 512;
 
 __host__ __device__ constexpr size_t mlp_infer_smem(int H) {
   return (size_t)kInfRows * 64 * 2 + (size_t)H * 64 * 2 + (size_t)(H / 64) * kInfRows * 64 * 2 +
          (size_t)H * 64 * 2 + 64;
 }
 
-__global__ void __launch_bounds__(kInfRows, 1)
+__global__ void __launch_bounds__(kInfThreads, 1)
 mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
                 const float* __restrict__ xmean, const float* __restrict__ xinv,
                 const float* __restrict__ xw, const bf16* __restrict__ W1h,
@@ -334,9 +338,10 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
   unsigned char* sw2 = sa1 + (size_t)(H / 64) * kSlice;
   uint64_t* bar = reinterpret_cast<uint64_t*>(sw2 + (size_t)H * 128);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int row = blockIdx.x * kInfRows + tid;
-  const bool live = row < n;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rloc = (warp & 3) * 32 + lane;  // this thread's TMEM lane = row
+  const int quarter = warp >> 2;            // hidden-column quarter
+  const int row0 = blockIdx.x * kInfRows;
   const int KH = H / 64;
 
   if (warp == 0) tmem_alloc(tslot, 256);
@@ -345,14 +350,17 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
     mbar_fence_init();
   }
 
-  // Inputs: one row per thread.  Centred values go to a swizzled scratch
-  // (conflict-free column access) for the whitening products.
+  // Inputs: row rloc, input columns [16 quarter, 16 quarter + 16).  The
+  // centred values go to a swizzled scratch (conflict-free column access).
+  float* cen = reinterpret_cast<float*>(sa1);
   {
+    const int row = row0 + rloc;
+    const bool live = row < n;
     const double* th = theta + (size_t)(live ? row : 0) * d;
-    float* cen = reinterpret_cast<float*>(sa1);
-    for (int j = 0; j < d; ++j)
-      cen[tid * 64 + ((j + tid) & 63)] = live ? (float)th[j] - xmean[j] : 0.0f;
-    for (int k8 = 0; k8 < 64; k8 += 8) {
+    for (int j = quarter; j < d; j += 4)
+      cen[rloc * 64 + ((j + rloc) & 63)] = live ? (float)th[j] - xmean[j] : 0.0f;
+    __syncthreads();
+    for (int k8 = quarter * 16; k8 < quarter * 16 + 16; k8 += 8) {
       __align__(16) bf16 v8[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -361,19 +369,19 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
         if (live && k < d) {
           if (xw) {
             const float* wr = xw + (size_t)k * d;
-            for (int j = 0; j < d; ++j) v = fmaf(wr[j], cen[tid * 64 + ((j + tid) & 63)], v);
+            for (int j = 0; j < d; ++j) v = fmaf(wr[j], cen[rloc * 64 + ((j + rloc) & 63)], v);
           } else {
-            v = cen[tid * 64 + ((k + tid) & 63)] * xinv[k];
+            v = cen[rloc * 64 + ((k + rloc) & 63)] * xinv[k];
           }
         }
         v8[q] = __float2bfloat16(v);
       }
-      *reinterpret_cast<uint4*>(sx + kmajor_offset(tid, k8, kInfRows)) =
+      *reinterpret_cast<uint4*>(sx + kmajor_offset(rloc, k8, kInfRows)) =
           *reinterpret_cast<const uint4*>(v8);
     }
   }
   // W1 (H x 64) into its K-major layout.
-  for (int i = tid; i < H * 8; i += kInfRows) {
+  for (int i = tid; i < H * 8; i += kInfThreads) {
     const int r = i >> 3, c8 = (i & 7) * 8;
     *reinterpret_cast<uint4*>(sw1 + kmajor_offset(r, c8, H)) =
         *reinterpret_cast<const uint4*>(W1h + (size_t)r * 64 + c8);
@@ -394,14 +402,14 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
     umma_commit(bar);
   }
   // W2 slice prefetch into registers while layer 1 runs (H x 64 per slice).
-  constexpr int kMaxPf = 256 * 8 / kInfRows;  // 16 chunks per thread at H = 256
+  constexpr int kMaxPf = 256 * 8 / kInfThreads;  // 4 chunks per thread at H = 256
   uint4 pf[kMaxPf];
-  const int npf = H * 8 / kInfRows;
+  const int npf = H * 8 / kInfThreads;
   auto load_w2 = [&](int s) {
 #pragma unroll
     for (int q = 0; q < kMaxPf; ++q) {
       if (q < npf) {
-        const int i = tid + q * kInfRows, r = i >> 3, c8 = (i & 7) * 8;
+        const int i = tid + q * kInfThreads, r = i >> 3, c8 = (i & 7) * 8;
         pf[q] = *reinterpret_cast<const uint4*>(W2h + (size_t)r * H + s * 64 + c8);
       }
     }
@@ -410,7 +418,7 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
 #pragma unroll
     for (int q = 0; q < kMaxPf; ++q) {
       if (q < npf) {
-        const int i = tid + q * kInfRows, r = i >> 3, c8 = (i & 7) * 8;
+        const int i = tid + q * kInfThreads, r = i >> 3, c8 = (i & 7) * 8;
         *reinterpret_cast<uint4*>(sw2 + kmajor_offset(r, c8, H)) = pf[q];
       }
     }
@@ -420,19 +428,20 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+  const int cq = H / 4;  // hidden columns per quarter (64 or 32)
+  const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   if (ok) {
     // Layer-1 epilogue: A1 = silu(Z1 + b1) as bf16 into the layer-2 A operand.
-    for (int c = 0; c < H; c += 16) {
+    for (int c = quarter * cq; c < quarter * cq + cq; c += 16) {
       float v[16];
       tmem_ld16(trow + (uint32_t)c, v);
       __align__(16) bf16 a8[16];
 #pragma unroll
       for (int j = 0; j < 16; ++j) a8[j] = __float2bfloat16(silu(v[j] + b1[c + j]));
       unsigned char* base = sa1 + (size_t)(c / 64) * kSlice;
-      *reinterpret_cast<uint4*>(base + kmajor_offset(tid, c % 64, kInfRows)) =
+      *reinterpret_cast<uint4*>(base + kmajor_offset(rloc, c % 64, kInfRows)) =
           *reinterpret_cast<const uint4*>(a8);
-      *reinterpret_cast<uint4*>(base + kmajor_offset(tid, c % 64 + 8, kInfRows)) =
+      *reinterpret_cast<uint4*>(base + kmajor_offset(rloc, c % 64 + 8, kInfRows)) =
           *reinterpret_cast<const uint4*>(a8 + 8);
     }
   }
@@ -457,17 +466,27 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
     ok = __syncthreads_and(ok);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  // Head: partial dot products per column quarter, added in quarter order.
+  // A1's space is free once the last layer-2 MMA has completed.
+  float* part = reinterpret_cast<float*>(sa1);
   if (ok) {
     float acc = 0.0f;
-    for (int c = 0; c < H; c += 16) {
+    for (int c = quarter * cq; c < quarter * cq + cq; c += 16) {
       float v[16];
       tmem_ld16(trow + (uint32_t)c, v);
 #pragma unroll
       for (int j = 0; j < 16; ++j) acc = fmaf(silu(v[j] + b2[c + j]), w3[c + j], acc);
     }
-    if (live) out[row] = (double)(acc + b3[0]) * ysd + ymean;
+    part[quarter * kInfRows + rloc] = acc;
   } else if (tid == 0) {
     atomicOr(err, DEV_ERR_MMA_TIMEOUT);
+  }
+  __syncthreads();
+  if (ok && quarter == 0) {
+    const int row = row0 + rloc;
+    const float y = ((part[rloc] + part[kInfRows + rloc]) + part[2 * kInfRows + rloc]) +
+                    part[3 * kInfRows + rloc];
+    if (row < n) out[row] = (double)(y + b3[0]) * ysd + ymean;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -684,7 +703,7 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
         m->infer_smem_set = true;
       }
       if (n > 0) {
-        mlp_infer_fused<<<(unsigned)((n + kInfRows - 1) / kInfRows), kInfRows, smem, st>>>(
+        mlp_infer_fused<<<(unsigned)((n + kInfRows - 1) / kInfRows), kInfThreads, smem, st>>>(
             theta, n, d, m->H, m->xmean.p, m->xinv.p, m->xw_or_null(), m->W1h.p, m->b1.p,
             m->W2h.p, m->b2.p, m->w3.p, m->b3.p, m->ysd, m->ymean, out, m->err.p);
         MLP_CK(cudaGetLastError());
