@@ -23,6 +23,7 @@
 #include <cstring>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -149,6 +150,7 @@ struct Geometry {
   int G, WC, CG, NCB, C_pad, NOB, tiles_per_cta, ntiles;
   size_t smem;
 };
+
 
 }  // namespace
 

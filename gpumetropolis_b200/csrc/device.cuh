@@ -263,6 +263,16 @@ __device__ __forceinline__ float2 gm2_softplus(float2 a) {
   return make_float2(a.x == a.x ? r.x : a.x, a.y == a.y ? r.y : a.y);
 }
 
+__device__ __forceinline__ float2 gm2_digamma(float2 a) {
+  return make_float2(gm_digammaf(a.x), gm_digammaf(a.y));
+}
+// Adjoint of a^b with respect to the exponent: G v log(a) where a > 0, else 0
+// (the reference's guard, cpu_native.rs:271-274).
+__device__ __forceinline__ float2 gm2_powexp_adj(float2 G, float2 v, float2 a) {
+  return make_float2(a.x > 0.0f ? G.x * v.x * logf(a.x) : 0.0f,
+                     a.y > 0.0f ? G.y * v.y * logf(a.y) : 0.0f);
+}
+
 __device__ __forceinline__ float2 gm2_pow(float2 a, float2 b) {
   return make_float2(powf(a.x, b.x), powf(a.y, b.y));
 }

@@ -180,20 +180,24 @@ int build_cubin_uncached(const std::string& src, std::vector<char>* out, std::st
 
 }  // namespace
 
-void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair) {
+void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pairg) {
   // The paired body keeps G x (parameters + hoisted values) broadcast pairs
   // in registers: use it while that stays within 96 registers.
   const int w = np + std::max(nh, 1);
   *pair = w <= 48;
   if (*pair) *G = w <= 24 ? 2 : 1;
   else *G = np <= 24 ? 4 : (np <= 48 ? 2 : 1);
-  *GG = np <= 16 ? 2 : 1;
+  // The paired gradient body also keeps the adjoint pairs: one chain per
+  // thread, while parameters + hoisted values stay within 32.
+  *pairg = w <= 32;
+  *GG = *pairg ? 1 : (np <= 16 ? 2 : 1);
 }
 
-std::string jit_source(const GenModel& gm, int G, int GG, bool pair) {
+std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg) {
   std::string s;
   s += "#include \"device.cuh\"\n";
   s += "#define GM_PAIR " + std::string(pair ? "1" : "0") + "\n";
+  s += "#define GM_PAIRG " + std::string(pairg ? "1" : "0") + "\n";
   s += "#define GM_G " + std::to_string(G) + "\n";
   s += "#define GM_GG " + std::to_string(GG) + "\n";
   s += "namespace gpum {\n";
@@ -205,19 +209,19 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair) {
 
 int jit_compile_check(const GenModel& gm, size_t* cubin_bytes, std::string* err) {
   int G = 1, GG = 1;
-  bool pair = false;
-  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair);
+  bool pair = false, pairg = false;
+  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair, &pairg);
   std::vector<char> cubin;
-  if (build_cubin(jit_source(gm, G, GG, pair), &cubin, err)) return 1;
+  if (build_cubin(jit_source(gm, G, GG, pair, pairg), &cubin, err)) return 1;
   if (cubin_bytes) *cubin_bytes = cubin.size();
   return 0;
 }
 
 int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   int G = 1, GG = 1;
-  bool pair = false;
-  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair);
-  const std::string src = jit_source(gm, G, GG, pair);
+  bool pair = false, pairg = false;
+  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair, &pairg);
+  const std::string src = jit_source(gm, G, GG, pair, pairg);
   const size_t key = std::hash<std::string>()(src);
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = cache().find(key);
@@ -244,6 +248,7 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.G = G;
   e.model.GG = GG;
   e.model.pair = pair;
+  e.model.pairg = pairg;
   e.model.np = gm.np;
   e.model.compile_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

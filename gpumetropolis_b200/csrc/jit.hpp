@@ -17,6 +17,7 @@ struct CompiledModel {
   cudaKernel_t k_grad = nullptr;    // gm_iter_grad
   int G = 1, GG = 1;                // chains per thread of each kernel
   bool pair = false;                // value kernel evaluates observation pairs
+  bool pairg = false;               // gradient kernel evaluates observation pairs
   int np = 0;
   double compile_seconds = 0.0;
 };
@@ -24,14 +25,14 @@ struct CompiledModel {
 // Chains per thread for the value and gradient kernels, and whether the
 // value kernel uses the paired-observation body, by parameter and hoisted
 // value counts.
-void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair);
+void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pairg);
 
 // Returns 0 and a loaded model, or 1 with a message (NVRTC missing, compile
 // error, load error).
 int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err);
 
 // The full NVRTC source a model compiles from (for tests and diagnostics).
-std::string jit_source(const GenModel& gm, int G, int GG, bool pair);
+std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg);
 
 // Compile only (no GPU needed): returns 0 and the cubin size, or 1 + message.
 int jit_compile_check(const GenModel& gm, size_t* cubin_bytes, std::string* err);
