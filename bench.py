@@ -287,9 +287,8 @@ def run_b200(a):
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from gpumetropolis_b200 import replicas as R
+    rank, world, local = R.rank_env()
     if world > 1:
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -311,7 +310,7 @@ def run_b200(a):
     sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
                            m.n_params, w.data, m.n_cols, w.n_obs, engine=a.engine)
     engine = {0: "interpreter", 1: "compiled"}[sess.engine]
-    sess.prepare(init, sd, temps, Wm + K, 1 + rank, 0, rng=_native.RNG_PHILOX)
+    sess.prepare(init, sd, temps, Wm + K, R.replica_seed(1, rank), 0, rng=_native.RNG_PHILOX)
     sess.advance(Wm)
     sess.sync()
     stream = torch.cuda.ExternalStream(sess.stream, device=dev)
@@ -339,13 +338,11 @@ def run_b200(a):
     step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
     dev_ms = float(step_ms.sum())
     if world > 1:
-        t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
+        dev_ms = R.max_over_ranks(dev_ms, device=dev)
         dist.barrier()
     _, acc, _, _ = sess.fetch(want_draws=False)
     sess.close()
-    value = world * K * C * N / (dev_ms / 1e3)
+    value = R.whole_job_rate(K * C * N, world, dev_ms / 1e3)
     ms_step = dev_ms / K
 
     clocks = clk.summary()
