@@ -23,7 +23,6 @@
 #include <cstring>
 #include <functional>
 #include <memory>
-#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -40,7 +39,6 @@ namespace gpum {
 // Surrogate inference on device parameters (mlp.cu).
 int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
               std::string* err);
-int mlp_batch_rows(const gpum_b200_mlp* m);
 int mlp_infer_launches(const gpum_b200_mlp* m, int n);
 }  // namespace gpum
 
@@ -204,7 +202,7 @@ struct gpum_b200_session {
   EvalArgs E_da{};
   DaArgs D{};
   gpum_b200_mlp* da_mlp = nullptr;
-  int da_chunks = 0;
+  int da_mlp_launches = 0;  // kernel launches per surrogate call
   // Per-chain likelihood powers for later runs (power posteriors).
   DBuf<double> beta;
   size_t n_beta = 0;
@@ -258,9 +256,7 @@ struct gpum_b200_session {
     return k;
   }
 
-  // `busy_blocks`: chain blocks expected to do work (delayed acceptance
-  // evaluates a compacted subset); 0 means all of them.
-  Geometry geometry(int n, const KernelChoice& k, int busy_blocks = 0) const {
+  Geometry geometry(int n, const KernelChoice& k) const {
     Geometry g{};
     g.G = k.G;
     const int groups = (n + g.G - 1) / g.G;
@@ -275,8 +271,7 @@ struct gpum_b200_session {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
     if (occ < 1) occ = 1;
     const int slots = num_sms() * occ;
-    const int busy = busy_blocks > 0 ? std::min(busy_blocks, g.NCB) : g.NCB;
-    int nob = std::max(1, (4 * slots) / busy);
+    int nob = std::max(1, (4 * slots) / g.NCB);
     nob = std::min(nob, std::max(1, g.ntiles));
     g.tiles_per_cta = g.ntiles > 0 ? (g.ntiles + nob - 1) / nob : 0;
     g.NOB = g.ntiles > 0 ? (g.ntiles + g.tiles_per_cta - 1) / g.tiles_per_cta : 1;
@@ -767,7 +762,7 @@ void da_step(gpum_b200_session* s) {
       s->geo_da.ntiles, s->geo_da.C_pad);
   da_tick_kernel<<<1, 32, 0, st>>>(s->D);
   GPUM_CK(cudaGetLastError());
-  s->launches += 5 + (uint64_t)s->da_chunks;
+  s->launches += 5 + (uint64_t)s->da_mlp_launches;
 }
 
 void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const double* sd,
@@ -833,12 +828,12 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   D.full = s->params.p;
   D.C_pad = g.C_pad;
   s->da_mlp = mlp;
-  s->da_chunks = 0;
+  s->da_mlp_launches = 0;
   std::string e;
   int rc = mlp_infer(mlp, s->state.p, (int)C, np, s->sll_x.p, st, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
-  s->da_chunks = mlp_infer_launches(mlp, (int)C);  // launches per surrogate call
-  s->launches += (uint64_t)s->da_chunks;
+  s->da_mlp_launches = mlp_infer_launches(mlp, (int)C);
+  s->launches += (uint64_t)s->da_mlp_launches;
   da_setup_kernel<<<(C + 255) / 256, 256, 0, st>>>(s->A, D);
   GPUM_CK(cudaGetLastError());
   ++s->launches;

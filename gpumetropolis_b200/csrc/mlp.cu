@@ -676,8 +676,6 @@ void upload_pairs(gpum_b200_mlp* m, const double* theta, const double* ll, size_
 
 namespace gpum {
 
-int mlp_batch_rows(const gpum_b200_mlp* m) { return m->B; }
-
 // Kernel launches one mlp_infer call of n rows makes.
 int mlp_infer_launches(const gpum_b200_mlp* m, int n) {
   return m->fused_inference() ? 1 : 5 * ((n + m->B - 1) / m->B);
