@@ -111,6 +111,9 @@ SIGNATURES = {
     "gpum_b200_session_run_de_sync": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_uint32,
                                                 C.c_uint32, C.c_uint32, C.c_double, C.c_double,
                                                 C.c_int, _f32p, _f32p, _f64p, _errp, _sz]),
+    "gpum_b200_session_draw_moments": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, _f64p,
+                                                 _f64p, _f64p, _f64p, _errp, _sz]),
+    "gpum_b200_session_state": (C.c_int, [C.c_void_p, _f64p, _errp, _sz]),
     "gpum_b200_session_set_likelihood_powers": (C.c_int, [C.c_void_p, _f64p, _sz, _errp,
                                                           _sz]),
     "gpum_b200_session_record": (C.c_int, [C.c_void_p, C.c_uint64, _errp, _sz]),
@@ -350,6 +353,26 @@ class Session:
             _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
         _check(rc, err)
         return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def draw_moments(self, t0, n):
+        """(chain_mean (C, np), chain_m2 (C, np), pool_mean (np,), pool_m2 (np, np)) of
+        the draws of iterations [t0, t0 + n) of the prepared run."""
+        nc, d = self.n_chains, self.n_params
+        cm, c2 = np.empty((nc, d)), np.empty((nc, d))
+        pm, p2 = np.empty(d), np.empty((d, d))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_draw_moments(
+            self._h, int(t0), int(n), _p(cm, C.c_double), _p(c2, C.c_double),
+            _p(pm, C.c_double), _p(p2, C.c_double), err, _ERRLEN), err)
+        return cm, c2, pm, p2
+
+    def state(self):
+        """Current chain states (C, np)."""
+        out = np.empty((self.n_chains, self.n_params))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_state(self._h, _p(out, C.c_double), err, _ERRLEN),
+               err)
+        return out
 
     def set_likelihood_powers(self, beta=None):
         """Per-chain likelihood powers for later runs (None clears)."""

@@ -76,10 +76,16 @@ class Welford:
             return self
         mb = x.mean(axis=0)
         dev = x - mb
-        m2b = np.einsum("ncd,nce->cde", dev, dev)
+        return self.merge(nb, mb, np.einsum("ncd,nce->cde", dev, dev))
+
+    def merge(self, nb, mb, m2b):
+        """Merge a batch given by its size, means (C, d) and cross-deviation
+        sums (C, d, d) -- Chan, Golub & LeVeque's pairwise update."""
+        if nb == 0:
+            return self
         na = self.n.astype(np.float64)
         n = na + nb
-        delta = mb - self.mean
+        delta = np.asarray(mb, dtype=np.float64) - self.mean
         self.mean = self.mean + delta * (nb / n)[:, None]
         self.m2 = self.m2 + m2b + np.einsum("cd,ce->cde", delta, delta) * (na * nb / n)[:, None,
                                                                                          None]
@@ -89,6 +95,78 @@ class Welford:
     def covariance(self):
         cov = self.m2 / np.maximum(self.n - 1, 1)[:, None, None]
         return np.where((self.n < 2)[:, None, None], self.sigma, cov)
+
+
+@dataclass
+class WelfordDiag:
+    """Per-chain running means and variances only: the per-chain adaptation
+    uses nothing but the diagonal (``R/adaptive.R:150-160``).  ``m2`` is
+    (C, d)."""
+    n: np.ndarray
+    mean: np.ndarray
+    m2: np.ndarray
+    sigma: np.ndarray
+
+    @classmethod
+    def init(cls, n_chains: int, d: int, sigma_diag):
+        sd = np.broadcast_to(np.asarray(sigma_diag, dtype=np.float64), (n_chains, d)).copy()
+        return cls(np.zeros(n_chains, np.int64), np.zeros((n_chains, d)),
+                   np.zeros((n_chains, d)), sd)
+
+    def update(self, x):
+        x = np.asarray(x, dtype=np.float64)
+        nb = x.shape[0]
+        if nb == 0:
+            return self
+        mb = x.mean(axis=0)
+        return self.merge(nb, mb, ((x - mb) ** 2).sum(axis=0))
+
+    def merge(self, nb, mb, m2b):
+        if nb == 0:
+            return self
+        na = self.n.astype(np.float64)
+        n = na + nb
+        delta = np.asarray(mb, dtype=np.float64) - self.mean
+        self.mean = self.mean + delta * (nb / n)[:, None]
+        self.m2 = self.m2 + m2b + delta * delta * (na * nb / n)[:, None]
+        self.n = self.n + nb
+        return self
+
+    def variances(self):
+        var = self.m2 / np.maximum(self.n - 1, 1)[:, None]
+        return np.where((self.n < 2)[:, None], self.sigma, var)
+
+
+@dataclass
+class BatchMoments:
+    """What the adaptation needs from a batch of draws (n, C, d)."""
+    n: int
+    chain_mean: np.ndarray   # (C, d)
+    chain_m2: np.ndarray     # (C, d) sums of squared deviations
+    pool_mean: np.ndarray    # (d,)
+    pool_m2: np.ndarray      # (d, d) sums of cross deviations over n * C draws
+    last: np.ndarray         # (C, d) the final states
+
+
+def moments_of(draws) -> BatchMoments:
+    """Host version of the device moment reduction (for backends that return
+    draws)."""
+    x = np.asarray(draws, dtype=np.float64)
+    n = x.shape[0]
+    cm = x.mean(axis=0)
+    pool = x.reshape(-1, x.shape[2])
+    pm = pool.mean(axis=0)
+    dev = pool - pm
+    return BatchMoments(n, cm, ((x - cm) ** 2).sum(axis=0), pm, dev.T @ dev, x[-1].copy())
+
+
+def _run_batch(call, init, sd, n, seed, mode, L):
+    """One warmup batch: device moments when the backend has them (no draws
+    copied), else moments of the returned draws."""
+    if hasattr(call, "run_moments"):
+        return call.run_moments(init, sd, n, seed, None, mode, 0.0, 0.0, L)
+    draws, acc, _ = call(init, sd, n, seed, None, mode, 0.0, 0.0, L)
+    return moments_of(draws), acc
 
 
 @dataclass
@@ -115,7 +193,7 @@ def am_orchestrate_warmup(call: Callable, np_: int, n_chains: int, init_mat, pro
     sizes = np.full(n_batches, k, dtype=np.int64)
     sizes[-1] += warmup - n_batches * k
     C = n_chains
-    states = Welford.init(C, np_, np.asarray(proposal_sd) ** 2)
+    states = WelfordDiag.init(C, np_, np.asarray(proposal_sd) ** 2)
     scale0 = 1.65 / np_ ** (1.0 / 6.0) if langevin else 2.38 / np.sqrt(np_)
     scales = np.full(C, scale0)
     cur_init = np.array(init_mat, dtype=np.float64, copy=True)
@@ -133,21 +211,20 @@ def am_orchestrate_warmup(call: Callable, np_: int, n_chains: int, init_mat, pro
     for b in range(1, n_batches + 1):
         use_L = np_ > 1 and cur_L is not None
         pm = 3 if langevin else (2 if use_L else 0)
-        draws, acc, _ = call(cur_init, cur_sd, int(sizes[b - 1]), seed + b - 1, None, pm, 0.0,
-                             0.0, cur_L if use_L else None)
-        states.update(draws)
-        pool.update(draws.reshape(-1, 1, np_))
+        mo, acc = _run_batch(call, cur_init, cur_sd, int(sizes[b - 1]), seed + b - 1, pm,
+                             cur_L if use_L else None)
+        states.merge(mo.n, mo.chain_mean, mo.chain_m2)
+        pool.merge(mo.n * C, mo.pool_mean[None], mo.pool_m2[None])
         bi = b - reset_batch if b > reset_batch else b
         scales = robbins_monro_scale(scales, acc, bi, np_, target)
-        cur_init = draws[-1].copy()
-        cov = states.covariance()
-        diag_sd = np.sqrt(np.maximum(np.diagonal(cov, axis1=1, axis2=2), 1e-12))
+        cur_init = mo.last
+        diag_sd = np.sqrt(np.maximum(states.variances(), 1e-12))
         cur_sd = scales[:, None] * diag_sd
         acc_hist[:, b - 1] = acc
         if b == reset_batch:
             diag_now = np.maximum(np.diag(pool.covariance()[0]), 1e-12)
             pool = Welford.init(1, np_, diag_now)
-            states = Welford.init(C, np_, diag_now)
+            states = WelfordDiag.init(C, np_, diag_now)
             scales = np.full(C, scale0)
         if np_ > 1:
             if pool.n[0] >= 2:
@@ -229,7 +306,7 @@ def pt_orchestrate(call, np_, n_chains, init_mat, proposal_sd, temperatures, n_i
     wb = max(0, min(nb, warmup // swap_every))
     wused = int(sizes[:wb].sum()) if wb > 0 else 0
     C = n_chains
-    states = Welford.init(C, np_, np.asarray(proposal_sd) ** 2)
+    states = WelfordDiag.init(C, np_, np.asarray(proposal_sd) ** 2)
     scales = np.ones(C)
     cur_init = np.array(init_mat, dtype=np.float64, copy=True)
     cur_sd = np.array(proposal_sd, dtype=np.float64, copy=True)
@@ -256,9 +333,7 @@ def pt_orchestrate(call, np_, n_chains, init_mat, proposal_sd, temperatures, n_i
         if in_warm and adapt:
             states.update(draws)
             scales = robbins_monro_scale(scales, acc, b, np_)
-            cov = states.covariance()
-            cur_sd = scales[:, None] * np.sqrt(np.maximum(np.diagonal(cov, axis1=1, axis2=2),
-                                                          1e-12))
+            cur_sd = scales[:, None] * np.sqrt(np.maximum(states.variances(), 1e-12))
         cur_init = draws[-1].copy()
         if pairs > 0:
             order = (np.arange(1, pairs + 1, 2) if b % 2 == 1
@@ -291,7 +366,7 @@ def de_orchestrate(call, np_, n_chains, init_mat, proposal_sd, gamma, de_noise, 
     wb = max(0, min(nb, warmup // de_every))
     wused = int(sizes[:wb].sum()) if wb > 0 else 0
     C = n_chains
-    states = Welford.init(C, np_, np.asarray(proposal_sd) ** 2)
+    states = WelfordDiag.init(C, np_, np.asarray(proposal_sd) ** 2)
     cur_init = np.array(init_mat, dtype=np.float64, copy=True)
     cur_sd = np.array(proposal_sd, dtype=np.float64, copy=True)
     samp = max(1, n_iter - wused)
@@ -314,8 +389,7 @@ def de_orchestrate(call, np_, n_chains, init_mat, proposal_sd, gamma, de_noise, 
             filled += bs
         if in_warm and adapt:
             states.update(draws)
-            cov = states.covariance()
-            cur_sd = np.sqrt(np.maximum(np.diagonal(cov, axis1=1, axis2=2), 1e-12))
+            cur_sd = np.sqrt(np.maximum(states.variances(), 1e-12))
         cur_init = draws[-1].copy()
         disp[:, b - 1] = cur_init.std(axis=0, ddof=1) if C > 1 else np.nan
     rate = acc_sum / iters if iters > 0 else acc

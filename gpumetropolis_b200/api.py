@@ -192,6 +192,26 @@ class _Backend:
         self.consumed += int(n_iter)
         return d.reshape((int(n_iter), C, self.np), order="F"), acc.astype(np.float64), last
 
+    def run_moments(self, init, sd, n_iter, seed, temperatures=None, proposal_mode=0,
+                    gamma=0.0, de_noise=0.0, proposal_l=None):
+        """A warmup batch that returns the moments of its draws (computed on
+        the device) instead of the draws: (BatchMoments, accept rates)."""
+        init = np.asarray(init, dtype=np.float64)
+        C = init.shape[0]
+        temps = np.ones(C) if temperatures is None else np.asarray(temperatures, np.float64)
+        if self.cfg is not None and self.da_at is not None and self.consumed >= self.da_at:
+            self.start_da()
+        self._maybe_record(C, n_iter)
+        s = self.session
+        s.prepare(init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF, proposal_mode, gamma,
+                  de_noise, proposal_l, rng=self.rng)
+        s.advance(int(n_iter))
+        cm, c2, pm, p2 = s.draw_moments(0, int(n_iter))
+        last = s.state()
+        _, acc, _, _ = s.fetch(want_draws=False)
+        self.consumed += int(n_iter)
+        return AD.BatchMoments(int(n_iter), cm, c2, pm, p2, last), acc.astype(np.float64)
+
     def da_summary(self):
         out = dict(self.info)
         if self.da_iters:

@@ -203,6 +203,7 @@ struct gpum_b200_session {
   DaArgs D{};
   gpum_b200_mlp* da_mlp = nullptr;
   int da_mlp_launches = 0;  // kernel launches per surrogate call
+  DBuf<double> mom;  // draw moments scratch
   // Per-chain likelihood powers for later runs (power posteriors).
   DBuf<double> beta;
   size_t n_beta = 0;
@@ -1113,6 +1114,48 @@ int gpum_b200_run_de_sync(const uint32_t* code, size_t n_code, const double* con
             nullptr, 0, GPUM_RNG_TRIPLE32);
     advance(s.get(), n_iter);
     fetch(s.get(), out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_session_draw_moments(gpum_b200_session* s, uint32_t t0, uint32_t n,
+                                   double* chain_mean, double* chain_m2, double* pool_mean,
+                                   double* pool_m2, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s && s->prepared, "session has no prepared run");
+    require(n >= 1 && (uint64_t)t0 + n <= s->n_done, "iterations beyond those advanced");
+    require(chain_mean && chain_m2 && pool_mean && pool_m2, "output pointers are NULL");
+    const int C = s->n_chains, np = (int)s->np;
+    cudaStream_t st = s->stream;
+    s->mom.ensure((size_t)2 * C * np + np + (size_t)np * np);
+    double* dmean = s->mom.p;
+    double* dm2 = dmean + (size_t)C * np;
+    double* pmean = dm2 + (size_t)C * np;
+    double* pm2 = pmean + np;
+    const int CP = s->geo.C_pad;
+    moments_chain_kernel<<<(unsigned)(((size_t)C * np + 255) / 256), 256, 0, st>>>(
+        s->draws.p, np, C, CP, (int)t0, (int)n, dmean, dm2);
+    moments_pool_mean_kernel<<<np, 256, 0, st>>>(s->draws.p, np, C, CP, (int)t0, (int)n, pmean);
+    moments_pool_m2_kernel<<<np * np, 256, 0, st>>>(s->draws.p, np, C, CP, (int)t0, (int)n,
+                                                    pmean, pm2);
+    GPUM_CK(cudaGetLastError());
+    s->launches += 3;
+    GPUM_CK(cudaMemcpyAsync(chain_mean, dmean, sizeof(double) * C * np, cudaMemcpyDeviceToHost,
+                            st));
+    GPUM_CK(cudaMemcpyAsync(chain_m2, dm2, sizeof(double) * C * np, cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaMemcpyAsync(pool_mean, pmean, sizeof(double) * np, cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaMemcpyAsync(pool_m2, pm2, sizeof(double) * np * np, cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaStreamSynchronize(st));
+  });
+}
+
+int gpum_b200_session_state(gpum_b200_session* s, double* out_state, char* err,
+                            size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s && s->prepared, "session has no prepared run");
+    require(out_state != nullptr, "output pointer is NULL");
+    GPUM_CK(cudaMemcpyAsync(out_state, s->state.p, sizeof(double) * s->n_chains * s->np,
+                            cudaMemcpyDeviceToHost, s->stream));
+    GPUM_CK(cudaStreamSynchronize(s->stream));
   });
 }
 

@@ -106,6 +106,80 @@ static __global__ void draws_layout_kernel(const float* __restrict__ in, float* 
 // so the target is unchanged; only stage-1 survivors are evaluated exactly.
 namespace gpum {
 
+// ------------------------------------------------- draw moments (adaptation)
+// Moments of the draws of iterations [t0, t0 + n) in the internal layout
+// [n_iter][np][C_pad], all in f64 and in a fixed order: per chain and
+// parameter the mean and the sum of squared deviations (two passes), the
+// pooled mean per parameter, and the pooled sums of cross deviations.
+static __global__ void moments_chain_kernel(const float* __restrict__ draws, int np, int C,
+                                            int C_pad, int t0, int n, double* __restrict__ mean,
+                                            double* __restrict__ m2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np * C) return;
+  const int j = i / C, c = i % C;  // consecutive threads: consecutive chains
+  double sm = 0.0;
+  for (int t = 0; t < n; ++t) sm += (double)draws[((size_t)(t0 + t) * np + j) * C_pad + c];
+  const double mu = sm / n;
+  double q = 0.0;
+  for (int t = 0; t < n; ++t) {
+    const double dv = (double)draws[((size_t)(t0 + t) * np + j) * C_pad + c] - mu;
+    q += dv * dv;
+  }
+  mean[(size_t)c * np + j] = mu;
+  m2[(size_t)c * np + j] = q;
+}
+
+// One block per parameter: pooled mean of the n x C values (fixed-order
+// strided sums, then a fixed shared-memory tree).
+static __global__ void moments_pool_mean_kernel(const float* __restrict__ draws, int np, int C,
+                                                int C_pad, int t0, int n,
+                                                double* __restrict__ pmean) {
+  __shared__ double red[256];
+  const int j = blockIdx.x;
+  const size_t total = (size_t)n * C;
+  double sm = 0.0;
+  for (size_t k = threadIdx.x; k < total; k += blockDim.x) {
+    const size_t t = k / C, c = k % C;
+    sm += (double)draws[((t0 + t) * np + j) * C_pad + c];
+  }
+  red[threadIdx.x] = sm;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) pmean[j] = red[0] / (double)total;
+}
+
+// One block per (j, k >= j): pooled sum of (x_j - m_j)(x_k - m_k).
+static __global__ void moments_pool_m2_kernel(const float* __restrict__ draws, int np, int C,
+                                              int C_pad, int t0, int n,
+                                              const double* __restrict__ pmean,
+                                              double* __restrict__ pm2) {
+  __shared__ double red[256];
+  const int j = blockIdx.x / np, k = blockIdx.x % np;
+  if (k < j) return;  // uniform per block
+  const size_t total = (size_t)n * C;
+  const double mj = pmean[j], mk = pmean[k];
+  double sm = 0.0;
+  for (size_t q = threadIdx.x; q < total; q += blockDim.x) {
+    const size_t t = q / C, c = q % C;
+    const double a = (double)draws[((t0 + t) * np + j) * C_pad + c] - mj;
+    const double b = (double)draws[((t0 + t) * np + k) * C_pad + c] - mk;
+    sm += a * b;
+  }
+  red[threadIdx.x] = sm;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pm2[(size_t)j * np + k] = red[0];
+    pm2[(size_t)k * np + j] = red[0];
+  }
+}
+
 // Path-B DE proposals of generation A.iter[0] for every chain (one thread per
 // chain), between the previous generation's accepts and this generation's
 // evaluation.  All chain blocks have the same iteration count here.

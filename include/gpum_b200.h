@@ -223,6 +223,21 @@ GPUM_API int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, flo
                             double* out_last_logpost, uint32_t* n_done, char* err,
                             size_t err_len);
 
+/* Moments of the draws of iterations [t0, t0 + n) of the prepared run, for
+ * adaptive warmup without copying the draws (R/adaptive.R:101-254 only uses
+ * these): per chain the mean and the sum of squared deviations of each
+ * parameter (chain-major n_chains x n_params), the pooled mean (n_params) and
+ * the pooled sums of cross deviations (n_params x n_params) over the
+ * n x n_chains draws; f64, fixed summation order.  No reference counterpart
+ * (the reference returns every draw to R). */
+GPUM_API int gpum_b200_session_draw_moments(gpum_b200_session* s, uint32_t t0, uint32_t n,
+                                            double* chain_mean, double* chain_m2,
+                                            double* pool_mean, double* pool_m2, char* err,
+                                            size_t err_len);
+/* The current chain states (n_chains x n_params, f64). */
+GPUM_API int gpum_b200_session_state(gpum_b200_session* s, double* out_state, char* err,
+                                     size_t err_len);
+
 /* The session's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events with the session's launches. */
 GPUM_API void* gpum_b200_session_stream(const gpum_b200_session* s);

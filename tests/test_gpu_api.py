@@ -132,3 +132,29 @@ def test_nonfinite_start_and_proposals(gpu):
     assert np.all(np.isfinite(d)) and d.min() > 0 and abs(d.mean() - 2) < 0.4
     fit = gpu_metropolis(m, {"y": [0.0]}, init=[[-1.0]], proposal_sd=0.3, n_iter=500, seed=1)
     assert fit.draws.shape == (250, 1, 1)
+
+
+def test_device_moments_match_the_draws(gpu):
+    # the adaptive warmup reduces each batch on the device instead of copying
+    # its draws; the moments equal those of the draws themselves
+    from gpumetropolis_b200 import adaptive as AD
+    from gpumetropolis_b200 import workloads as W
+    w = W.make("logistic", n_obs=3000)
+    m = w.model
+    C, n = 40, 30
+    rng = np.random.default_rng(2)
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.02)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                     w.data, m.n_cols, w.n_obs) as s:
+        s.prepare(init, sd, np.ones(C), n, 4, 0)
+        s.advance(n)
+        cm, c2, pm, p2 = s.draw_moments(0, n)
+        last = s.state()
+        d, _, _, _ = s.fetch()
+    ref = AD.moments_of(d.reshape((n, C, m.n_params), order="F"))
+    np.testing.assert_allclose(cm, ref.chain_mean, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(c2, ref.chain_m2, rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(pm, ref.pool_mean, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(p2, ref.pool_m2, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(last, ref.last, rtol=1e-6)  # draws are stored in f32

@@ -144,3 +144,21 @@ def test_evidence_needs_a_proper_prior():
     flat = gpum_model("~ -((y - mu)^2) / 8", "mu", "y")
     with pytest.raises(GpumInputError, match="proper prior"):
         gpum_evidence(flat, {"y": np.zeros(10)})
+
+
+def test_batch_moments_merge_like_the_row_updates():
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(40, 6, 3)) * np.array([1.0, 3.0, 0.2])
+    wd = AD.WelfordDiag.init(6, 3, np.ones(3))
+    wf = AD.Welford.init(1, 3, np.ones(3))
+    for b in range(4):
+        mo = AD.moments_of(x[10 * b:10 * (b + 1)])
+        wd.merge(mo.n, mo.chain_mean, mo.chain_m2)
+        wf.merge(mo.n * 6, mo.pool_mean[None], mo.pool_m2[None])
+        assert np.array_equal(mo.last, x[10 * b + 9])
+    np.testing.assert_allclose(wd.variances(), x.var(axis=0, ddof=1), rtol=1e-12)
+    np.testing.assert_allclose(wf.covariance()[0], np.cov(x.reshape(-1, 3), rowvar=False),
+                               rtol=1e-12)
+    full = AD.Welford.init(6, 3, np.ones(3)).update(x)
+    np.testing.assert_allclose(np.diagonal(full.covariance(), axis1=1, axis2=2),
+                               wd.variances(), rtol=1e-12)
