@@ -111,6 +111,10 @@ SIGNATURES = {
     "gpum_b200_session_run_de_sync": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_uint32,
                                                 C.c_uint32, C.c_uint32, C.c_double, C.c_double,
                                                 C.c_int, _f32p, _f32p, _f64p, _errp, _sz]),
+    "gpum_b200_session_set_exchange": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, _errp,
+                                                 _sz]),
+    "gpum_b200_session_exchange_stats": (C.c_int, [C.c_void_p, _u32p, _u32p, _u32p, _errp,
+                                                   _sz]),
     "gpum_b200_session_draw_moments": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, _f64p,
                                                  _f64p, _f64p, _f64p, _errp, _sz]),
     "gpum_b200_session_state": (C.c_int, [C.c_void_p, _f64p, _errp, _sz]),
@@ -325,7 +329,7 @@ class Session:
     def run(self, init, proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0,
             de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
         init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
-        n_chains = init.size // self.n_params
+        n_chains = self.n_chains = init.size // self.n_params
         L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
         draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
         acc = np.empty(n_chains, np.float32)
@@ -353,6 +357,23 @@ class Session:
             _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
         _check(rc, err)
         return draws[: n_iter * n_chains * self.n_params], acc, last
+
+    def set_exchange(self, ladder_len=0, swap_every=1):
+        """Device replica exchange for later runs (ladder_len 0: off)."""
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_set_exchange(self._h, int(ladder_len),
+                                                        int(swap_every), err, _ERRLEN), err)
+
+    def exchange_stats(self):
+        """(attempts (C,), accepted (C,), n_exchanges) of the prepared run."""
+        att = np.zeros(self.n_chains, np.uint32)
+        acc = np.zeros(self.n_chains, np.uint32)
+        n = np.zeros(1, np.uint32)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_exchange_stats(
+            self._h, _p(att, C.c_uint32), _p(acc, C.c_uint32), _p(n, C.c_uint32), err,
+            _ERRLEN), err)
+        return att, acc, int(n[0])
 
     def draw_moments(self, t0, n):
         """(chain_mean (C, np), chain_m2 (C, np), pool_mean (np,), pool_m2 (np, np)) of

@@ -227,12 +227,19 @@ class _Backend:
 def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_iter=2000,
                    n_chains=4, warmup=None, adapt=True, method="rwm", temperatures=None,
                    swap_every=None, gamma=None, de_noise=1e-3, de_every=None, de_sync=False,
-                   seed=1, backend="b200", rng="triple32", surrogate=None) -> GpumFit:
+                   seed=1, backend="b200", rng="triple32", surrogate=None, swap_on_device=False,
+                   ladder_len=None) -> GpumFit:
     """Run the batched Metropolis sampler on the B200 backend (``R/api.R:247-599``).
 
     ``surrogate``: None/False (exact Metropolis, the reference's behaviour),
     True, or a dict overriding ``SURROGATE_DEFAULTS`` -- delayed acceptance
-    in the sampling phase (rwm, pt, de; needs warmup > 0)."""
+    in the sampling phase (rwm, pt, de; needs warmup > 0).
+
+    ``swap_on_device`` (pt): exchanges run on the GPU after every
+    ``swap_every`` iterations inside one run instead of between host batches;
+    the chains form ladders of ``ladder_len`` consecutive chains (default: one
+    ladder of all chains, as the reference), temperatures repeating per
+    ladder."""
     if not isinstance(model, GpumModel):
         raise GpumInputError("`model` must be a gpum_model from gpum_model().")
     if backend not in ("b200", "auto"):
@@ -276,8 +283,12 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
     C = n_chains
     temps = None
     if method == "pt":
+        ladder_len = C if ladder_len is None else int(ladder_len)
+        if swap_on_device and (ladder_len < 2 or C % ladder_len != 0):
+            raise GpumInputError("`ladder_len` must be at least 2 and divide `n_chains`.")
         if temperatures is None:
-            temps = AD.pt_default_ladder(C)
+            temps = (np.tile(AD.pt_default_ladder(ladder_len), C // ladder_len)
+                     if swap_on_device else AD.pt_default_ladder(C))
         else:
             temps = np.asarray(temperatures, dtype=np.float64).ravel()
             if temps.size != C:
@@ -320,6 +331,16 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
             raise GpumInputError("`surrogate` must be None, True or a dict of options.")
 
     call = _Backend(model, data_mat, n_obs, rng_kind, scfg)
+    if method == "pt" and swap_on_device:
+        if scfg is not None:
+            call.close()
+            raise GpumInputError("`surrogate` is not available with `swap_on_device = TRUE`.")
+        try:
+            return _pt_device(model, call, npar, n_chains, init_mat, sd_mat, temps, n_iter,
+                              warmup, int(swap_every), ladder_len, bool(adapt), int(seed),
+                              backend)
+        finally:
+            call.close()
     if method == "de" and de_sync:
         # Path B (R/api.R:464-497): per-generation DE over the whole run,
         # trim-only warmup, proposal_sd the fixed jitter base.
@@ -346,6 +367,44 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
         return fit
     finally:
         call.close()
+
+
+def _pt_device(model, call, npar, C, init_mat, sd_mat, temps, n_iter, warmup, swap_every,
+               ladder_len, adapt, seed, backend):
+    """Parallel tempering with the exchanges on the device: adaptive warmup
+    batches (per-chain Robbins-Monro scales and variances as in the host
+    orchestration, R/adaptive.R:330-355, from device moments) with exchanges
+    inside each batch, then one sampling run with an exchange every
+    ``swap_every`` iterations."""
+    s = call.session
+    s.set_exchange(ladder_len, swap_every)
+    cur, sd = np.array(init_mat, dtype=np.float64), np.array(sd_mat, dtype=np.float64)
+    scales = np.ones(C)
+    sizes = np.zeros(0, np.int64)
+    if warmup > 0:
+        nb = min(40, max(10, warmup // 50), warmup) if adapt else 1
+        sizes = np.full(nb, warmup // nb, dtype=np.int64)
+        sizes[-1] += warmup - sizes.sum()
+        states = AD.WelfordDiag.init(C, npar, sd ** 2)
+        for b, n in enumerate(sizes, start=1):
+            mo, acc = call.run_moments(cur, sd, int(n), seed + b - 1, temps, 0)
+            cur = mo.last
+            if adapt:
+                states.merge(mo.n, mo.chain_mean, mo.chain_m2)
+                scales = AD.robbins_monro_scale(scales, acc, b, npar)
+                sd = scales[:, None] * np.sqrt(np.maximum(states.variances(), 1e-12))
+    samp = n_iter - warmup
+    d, acc, _ = call(cur, sd, samp, seed + sizes.size, temps, 0)
+    att, ok, n_ex = s.exchange_stats()
+    s.set_exchange(0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rate = np.where(att > 0, ok / np.maximum(att, 1), np.nan)
+    return GpumFit(d, acc, model, samp, n_iter, warmup, C, npar, backend, seed, "pt",
+                   {"final_proposal_sd": sd, "final_scales": scales,
+                    "n_batches": int(sizes.size), "batch_sizes": sizes} if adapt else None,
+                   {"temperatures": temps, "swap_every": swap_every, "ladder_len": ladder_len,
+                    "swap_on_device": True, "exchanges": n_ex,
+                    "exchange_rate": rate[: C - 1]})
 
 
 def _route(model, call, method, npar, C, init_mat, sd_mat, n_iter, warmup, warmup_auto, adapt,

@@ -204,6 +204,9 @@ struct gpum_b200_session {
   gpum_b200_mlp* da_mlp = nullptr;
   int da_mlp_launches = 0;  // kernel launches per surrogate call
   DBuf<double> mom;  // draw moments scratch
+  // Replica exchange on the device (0 = off).
+  int pt_K = 0, pt_every = 0;
+  DBuf<uint32_t> pt_att, pt_acc, pt_n;
   // Per-chain likelihood powers for later runs (power posteriors).
   DBuf<double> beta;
   size_t n_beta = 0;
@@ -342,6 +345,12 @@ struct gpum_b200_session {
       ++launches;
     }
     launch(PH_STEP);
+    if (pt_K > 0) {
+      PtArgs P{pt_K, pt_every, pt_n.p, pt_att.p, pt_acc.p, params.p, geo.C_pad};
+      pt_exchange_kernel<<<(unsigned)((n_chains + 127) / 128), 128, 0, stream>>>(A, P);
+      GPUM_CK(cudaGetLastError());
+      ++launches;
+    }
   }
 
   void launch_with(const Geometry& g, EvalArgs& e, int phase) {
@@ -606,6 +615,17 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
                                 " chains, the run has " + std::to_string(C));
     A.beta = s->beta.p;
   }
+  if (s->pt_K > 0) {
+    require(C % (uint32_t)s->pt_K == 0,
+            "n_chains must be a multiple of the ladder length for device exchanges");
+    require(mode != 4, "device exchanges are not available with de_sync");
+    s->pt_att.ensure(C);
+    s->pt_acc.ensure(C);
+    s->pt_n.ensure(1);
+    GPUM_CK(cudaMemsetAsync(s->pt_att.p, 0, sizeof(uint32_t) * C, st));
+    GPUM_CK(cudaMemsetAsync(s->pt_acc.p, 0, sizeof(uint32_t) * C, st));
+    GPUM_CK(cudaMemsetAsync(s->pt_n.p, 0, sizeof(uint32_t), st));
+  }
   if (s->rec_cap > 0) {
     A.rec_theta = s->rec_theta.p;
     A.rec_ll = s->rec_ll.p;
@@ -775,6 +795,8 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   require(mode <= 2, "delayed acceptance needs a symmetric proposal: mode 0 (rwm), 1 (de) or 2 "
                      "(cholesky)");
   require(s->n_beta == 0, "delayed acceptance does not support likelihood powers");
+  require(s->pt_K == 0, "delayed acceptance does not run device exchanges; exchange between "
+                        "run_da calls instead");
   const uint64_t keep_cap = s->rec_cap;
   s->rec_cap = 0;  // stage-1 rejections leave no exact pair to record
   try {
@@ -1114,6 +1136,39 @@ int gpum_b200_run_de_sync(const uint32_t* code, size_t n_code, const double* con
             nullptr, 0, GPUM_RNG_TRIPLE32);
     advance(s.get(), n_iter);
     fetch(s.get(), out_draws, out_accept, out_last, nullptr);
+  });
+}
+
+int gpum_b200_session_set_exchange(gpum_b200_session* s, uint32_t ladder_len,
+                                   uint32_t swap_every, char* err, size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    require(ladder_len == 0 || (ladder_len >= 2 && swap_every >= 1),
+            "ladder_len must be 0 (off) or >= 2, with swap_every >= 1");
+    s->drop_graph();
+    s->prepared = false;
+    s->pt_K = (int)ladder_len;
+    s->pt_every = ladder_len ? (int)swap_every : 0;
+  });
+}
+
+int gpum_b200_session_exchange_stats(gpum_b200_session* s, uint32_t* attempts,
+                                     uint32_t* accepted, uint32_t* n_exchanges, char* err,
+                                     size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s && s->prepared, "session has no prepared run");
+    require(s->pt_K > 0, "device exchanges are off");
+    const size_t C = (size_t)s->n_chains;
+    if (attempts)
+      GPUM_CK(cudaMemcpyAsync(attempts, s->pt_att.p, sizeof(uint32_t) * C,
+                              cudaMemcpyDeviceToHost, s->stream));
+    if (accepted)
+      GPUM_CK(cudaMemcpyAsync(accepted, s->pt_acc.p, sizeof(uint32_t) * C,
+                              cudaMemcpyDeviceToHost, s->stream));
+    if (n_exchanges)
+      GPUM_CK(cudaMemcpyAsync(n_exchanges, s->pt_n.p, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              s->stream));
+    GPUM_CK(cudaStreamSynchronize(s->stream));
   });
 }
 

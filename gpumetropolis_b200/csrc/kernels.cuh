@@ -180,6 +180,70 @@ static __global__ void moments_pool_m2_kernel(const float* __restrict__ draws, i
   }
 }
 
+// ------------------------------------------------------ parallel tempering
+// Replica exchange on the device (the reference swaps on the host between
+// batches, R/adaptive.R:272-413): after every `every`-th iteration, the
+// adjacent pairs (i, i + 1) of each ladder -- contiguous groups of K chains
+// with the temperatures along the group -- of one parity (alternating from
+// exchange to exchange, starting with the even pairs) exchange states with
+// probability min(1, exp(delta)), delta = (lp[i+1] - lp[i]) (1/T[i] - 1/T[i+1])
+// on the untempered log posteriors.  The proposals already drawn for the
+// next iteration were centred on the old states, so both chains of an
+// exchanged pair draw new ones.  Uniforms: Philox keyed by (seed, exchange,
+// pair).  One thread per pair; the pairs of one parity are disjoint.
+struct PtArgs {
+  int K;               // ladder length
+  int every;           // iterations between exchanges
+  uint32_t* n_swaps;   // [1] exchanges done
+  uint32_t* att;       // [C] attempts of pair (c, c + 1)
+  uint32_t* acc;       // [C] accepted exchanges of pair (c, c + 1)
+  float* params;       // [np][C_pad] evaluation points of the next iteration
+  int C_pad;
+};
+
+static __global__ void pt_exchange_kernel(ChainArgs A, PtArgs P) {
+  const uint32_t t = A.iter[0];  // iterations done (all chain blocks agree here)
+  if (t == 0 || t % (uint32_t)P.every != 0 || t >= A.n_iter) return;
+  const uint32_t s = t / (uint32_t)P.every;  // exchange number, from 1
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int C = A.n_chains, np = A.np;
+  if (i == 0) P.n_swaps[0] = s;
+  if (i + 1 >= C || (i % P.K) == P.K - 1) return;     // not a pair of one ladder
+  if (((i % P.K) & 1) != (int)((s + 1) & 1)) return;  // odd exchanges: even pairs
+  const double lpa = A.cur[i], lpb = A.cur[i + 1];
+  const double delta = (lpb - lpa) * (1.0 / A.temp[i] - 1.0 / A.temp[i + 1]);
+  const U4 r = philox4x32_10(U4{(uint32_t)i, s, 0x50545357u, 0u}, A.seed, 0x3C6EF372u);
+  const double u = u53(r.x, r.y);
+  P.att[i] += 1;
+  if (!(isfinite(delta) && log(u) < delta)) return;
+  P.acc[i] += 1;
+  double* xa = A.state + (size_t)i * np;
+  double* xb = A.state + (size_t)(i + 1) * np;
+  for (int j = 0; j < np; ++j) {
+    const double tmp = xa[j];
+    xa[j] = xb[j];
+    xb[j] = tmp;
+  }
+  A.cur[i] = lpb;
+  A.cur[i + 1] = lpa;
+  if (A.mode == MODE_MALA) {  // the cached gradients belong to the states
+    double* ga = A.gx + (size_t)i * np;
+    double* gb = A.gx + (size_t)(i + 1) * np;
+    for (int j = 0; j < np; ++j) {
+      const double tmp = ga[j];
+      ga[j] = gb[j];
+      gb[j] = tmp;
+    }
+  }
+  for (int c = i; c <= i + 1; ++c) {
+    Stream rs = make_stream(A, c);
+    rs.it = t;
+    rs.k = 0x40000000u;  // counters apart from the iteration's own proposal
+    propose(A, c, rs, P.params, P.C_pad);
+    A.ctr[c] = rs.ctr;
+  }
+}
+
 // Path-B DE proposals of generation A.iter[0] for every chain (one thread per
 // chain), between the previous generation's accepts and this generation's
 // evaluation.  All chain blocks have the same iteration count here.

@@ -223,6 +223,22 @@ GPUM_API int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, flo
                             double* out_last_logpost, uint32_t* n_done, char* err,
                             size_t err_len);
 
+/* Replica exchange on the device for later runs: chains form ladders of
+ * ladder_len consecutive chains (their temperatures along the ladder, n_chains
+ * a multiple of ladder_len); after every swap_every-th iteration the adjacent
+ * pairs of one parity (alternating, even pairs first) exchange states with
+ * the reference's probability min(1, exp((lp[i+1] - lp[i]) (1/T[i] -
+ * 1/T[i+1]))) (R/adaptive.R:362-387, there between host batches); exchanged
+ * chains draw fresh proposals.  Philox uniforms.  ladder_len 0 turns it off. */
+GPUM_API int gpum_b200_session_set_exchange(gpum_b200_session* s, uint32_t ladder_len,
+                                            uint32_t swap_every, char* err, size_t err_len);
+/* Per pair (c, c+1) the attempted and accepted exchanges of the prepared run
+ * (n_chains entries each; entries that are no pair stay 0) and the number of
+ * exchange steps.  Any output pointer may be NULL. */
+GPUM_API int gpum_b200_session_exchange_stats(gpum_b200_session* s, uint32_t* attempts,
+                                              uint32_t* accepted, uint32_t* n_exchanges,
+                                              char* err, size_t err_len);
+
 /* Moments of the draws of iterations [t0, t0 + n) of the prepared run, for
  * adaptive warmup without copying the draws (R/adaptive.R:101-254 only uses
  * these): per chain the mean and the sum of squared deviations of each

@@ -158,3 +158,44 @@ def test_device_moments_match_the_draws(gpu):
     np.testing.assert_allclose(pm, ref.pool_mean, rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(p2, ref.pool_m2, rtol=1e-9, atol=1e-12)
     np.testing.assert_allclose(last, ref.last, rtol=1e-6)  # draws are stored in f32
+
+
+def test_device_exchanges_permute_equal_temperature_ladders(gpu):
+    # all temperatures equal: delta = 0, so every attempted exchange happens;
+    # with negligible moves the draws show the exact permutations (even pairs
+    # at the first exchange, odd pairs at the second)
+    w = W.make("gaussian", n_obs=500)
+    m = w.model
+    C, n_iter = 8, 12
+    init = np.arange(1, C + 1, dtype=np.float64).reshape(C, 1)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, 1, w.data,
+                     1, w.n_obs) as s:
+        s.set_exchange(4, 5)        # two ladders of 4 chains
+        d, _, _ = s.run(init, np.full((C, 1), 1e-12), np.ones(C), n_iter, 3, 0,
+                        rng=gpu.RNG_PHILOX)
+        att, ok, n_ex = s.exchange_stats()
+    d = d.reshape((n_iter, C), order="F")
+    np.testing.assert_allclose(d[4], init[:, 0], atol=1e-6)
+    even = [1, 0, 3, 2, 5, 4, 7, 6]                 # pairs (0,1),(2,3) in each ladder
+    np.testing.assert_allclose(d[5], d[4][even], atol=1e-6)
+    odd = [0, 2, 1, 3, 4, 6, 5, 7]                  # pair (1,2) in each ladder
+    np.testing.assert_allclose(d[10], d[9][odd], atol=1e-6)
+    np.testing.assert_allclose(d[11], d[10], atol=1e-6)
+    assert n_ex == 2
+    np.testing.assert_array_equal(att, [1, 1, 1, 0, 1, 1, 1, 0])
+    np.testing.assert_array_equal(ok, att)
+
+
+def test_pt_with_device_exchanges_covers_both_modes(gpu):
+    rng = np.random.default_rng(1)
+    y = rng.normal(3.0, 1.0, 400)
+    m = gpum_model("~ log(exp(-((y - mu)^2) / 2) + exp(-((y + mu)^2) / 2))", "mu", "y")
+    init = np.tile(np.linspace(-6, 6, 8), 4).reshape(32, 1)
+    fit = gpu_metropolis(m, {"y": y}, init=init, proposal_sd=0.15, n_iter=4000, method="pt",
+                         seed=2, swap_on_device=True, ladder_len=8, swap_every=10)
+    assert fit.extra["swap_on_device"] and fit.extra["exchanges"] == 199  # t = 10 .. 1990
+    cold = fit.draws[:, ::8, 0].ravel()               # rung 0 of each ladder
+    assert np.any(cold > 1.5) and np.any(cold < -1.5)
+    assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
+    r = fit.extra["exchange_rate"]
+    assert np.nanmax(r) > 0.2 and np.nanmin(r) >= 0.0

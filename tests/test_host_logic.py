@@ -120,6 +120,10 @@ def test_gpu_metropolis_input_validation():
         gpu_metropolis(m, y, backend="cuda")
     with pytest.raises(GpumInputError, match="warmup"):
         gpu_metropolis(m, y, n_iter=10, warmup=10)
+    with pytest.raises(GpumInputError, match="ladder_len"):
+        gpu_metropolis(m, y, n_chains=8, method="pt", swap_on_device=True, ladder_len=3)
+    with pytest.raises(GpumInputError, match="ladder_len"):
+        gpu_metropolis(m, y, n_chains=8, method="pt", swap_on_device=True, ladder_len=1)
 
 
 def test_pooled_ess_on_ar1_and_stuck_chains():
