@@ -480,8 +480,19 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
       if (kT > 0 && kT % 64 == 0 && WO == 1) {
         // every warp covers the tile: a fixed trip count, unrolled so the
         // compiler can overlap one pair's loads with another's arithmetic
+        bool done = false;
+        if constexpr (kT > 0) {
+          if (phase != PH_POINTWISE && obs0 + kT <= E.n_obs) {  // a full tile
 #pragma unroll
-        for (int it = 0; it < (kT > 0 ? kT : 64) / 64; ++it) pair(lane + 32 * it);
+            for (int it = 0; it < kT / 64; ++it) body.eval2_full(tile + 2 * (lane + 32 * it));
+            body.flush();
+            done = true;
+          }
+        }
+        if (!done) {
+#pragma unroll
+          for (int it = 0; it < (kT > 0 ? kT : 64) / 64; ++it) pair(lane + 32 * it);
+        }
       } else {
         for (int pi = lane + 32 * wo; 2 * pi < T; pi += 32 * WO) pair(pi);
       }

@@ -161,6 +161,24 @@ struct JitBody2 {
     }
   }
 
+  // A pair of a full tile outside pointwise output: no validity tests, no
+  // block counter; the caller flushes once per tile.
+  __device__ __forceinline__ void eval2_full(const float* xo) {
+    float2 d[GM_ND];
+    gm_data2(xo, GM_T, d);
+#pragma unroll
+    for (int g = 0; g < G; ++g) part[g] = __fadd2_rn(part[g], gm_value2(d, pp[g], hh[g]));
+  }
+  // Close the open FP32 blocks into the FP64 sums.
+  __device__ __forceinline__ void flush() {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      s[g] += (double)part[g].x + (double)part[g].y;
+      part[g] = make_float2(0.0f, 0.0f);
+    }
+    cnt = 0;
+  }
+
   __device__ __forceinline__ float2 last2(int g) const { return lastv[g]; }
   __device__ __forceinline__ void end() {}
   __device__ __forceinline__ double total(int g, int) const {

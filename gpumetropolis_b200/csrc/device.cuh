@@ -172,42 +172,57 @@ struct Comp {
 // ------------------------------------------------------------- softplus
 // softplus(a) = log(1 + e^a), which codegen substitutes for LOG(1 + EXP(a)):
 //   softplus(a) = max(a, 0) + log1p(u),  u = e^(-|a|) in (0, 1],
-//   u = 2^t with t = -|a| log2(e) carried as t_hi + t_lo (fma split of the
-//       product), 2^t_hi from the hardware ex2, times (1 + t_lo ln 2);
-//   log1p(u) = 2 atanh(s), s = u / (2 + u) in (0, 1/3]:
-//       2s (1 + s^2/3 + s^4/5 + ... + s^14/15), the omitted tail < 2^-28 s.
+//   u = 2^t e^r with t = fl(-|a| log2(e)) and the residual r = -|a| - t ln 2
+//       (Cody & Waite reduction: ln 2 = LN2_HI + LN2_LO, two FMAs), 2^t from
+//       the hardware ex2 and e^r = 1 + r (|r| < 6e-6, so r^2/2 < 2e-11);
+//   log1p(u) = 2 atanh(s), s = u / (2 + u) in (0, 1/3]; with w = 2s =
+//       u / (1 + u/2) and q = w^2:  w (1 + q/12 + q^2/80 + ... + q^6/53248),
+//       the coefficients 1 / ((2k+1) 4^k) of the atanh series in w, the
+//       omitted tail < 1.5e-8 w.
 // Unlike log(1 + exp(a)) in FP32 this keeps full relative accuracy where
-// e^a underflows against 1.  NaN propagates; +inf -> +inf; -inf -> 0.
+// e^a underflows against 1.  NaN propagates (max.NaN); +inf -> +inf;
+// -inf -> 0.
 __device__ __forceinline__ float gm_ex2_approx(float t) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(t));
   return y;
 }
-
-__device__ __forceinline__ float gm_log1p_atanh(float u) {
-  const float s = __fdividef(u, 2.0f + u);
-  const float s2 = s * s;
-  float p = 1.0f / 15.0f;
-  p = fmaf(p, s2, 1.0f / 13.0f);
-  p = fmaf(p, s2, 1.0f / 11.0f);
-  p = fmaf(p, s2, 1.0f / 9.0f);
-  p = fmaf(p, s2, 1.0f / 7.0f);
-  p = fmaf(p, s2, 1.0f / 5.0f);
-  p = fmaf(p, s2, 1.0f / 3.0f);
-  const float s_2 = s + s;
-  return fmaf(s_2, s2 * p, s_2);
+__device__ __forceinline__ float gm_rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gm_max_nan(float a, float b) {
+  float y;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+  return y;
 }
 
+#define GM_SP_L2E 1.44269502162933349609375f        // log2(e) rounded to float
+#define GM_SP_LN2_HI 0.693147182464599609375f       // ln(2) rounded to float
+#define GM_SP_LN2_LO (-1.904654212125934e-09f)      // ln(2) - GM_SP_LN2_HI
+#define GM_SP_C1 (1.0f / 12.0f)
+#define GM_SP_C2 (1.0f / 80.0f)
+#define GM_SP_C3 (1.0f / 448.0f)
+#define GM_SP_C4 (1.0f / 2304.0f)
+#define GM_SP_C5 (1.0f / 11264.0f)
+#define GM_SP_C6 (1.0f / 53248.0f)
+
 __device__ __forceinline__ float gm_softplus(float a) {
-  const float kL2E = 1.44269502162933349609375f;  // log2(e) rounded to float
-  const float kL2E_LO = 1.925962989e-08f;         // log2(e) - kL2E
-  const float na = fmaxf(-fabsf(a), -126.0f);      // e^-126 underflows to 0 anyway
-  const float th = na * kL2E;
-  const float tl = fmaf(na, kL2E, -th) + na * kL2E_LO;
-  float u = gm_ex2_approx(th);
-  u = fmaf(u, tl * 0.693147180559945309f, u);
-  const float r = fmaxf(a, 0.0f) + gm_log1p_atanh(u);
-  return a == a ? r : a;
+  const float na = fmaxf(-fabsf(a), -126.0f);  // e^-126 underflows to 0 anyway
+  const float t = na * GM_SP_L2E;
+  const float r = fmaf(t, -GM_SP_LN2_LO, fmaf(t, -GM_SP_LN2_HI, na));
+  const float u0 = gm_ex2_approx(t);
+  const float u = fmaf(u0, r, u0);
+  const float w = u * gm_rcp_approx(fmaf(u, 0.5f, 1.0f));
+  const float q = w * w;
+  float p = GM_SP_C6;
+  p = fmaf(p, q, GM_SP_C5);
+  p = fmaf(p, q, GM_SP_C4);
+  p = fmaf(p, q, GM_SP_C3);
+  p = fmaf(p, q, GM_SP_C2);
+  p = fmaf(p, q, GM_SP_C1);
+  return gm_max_nan(a, 0.0f) + fmaf(w, q * p, w);
 }
 
 // ------------------------------------------------- paired FP32 arithmetic
@@ -237,30 +252,27 @@ __device__ __forceinline__ float2 gm2_sqrt(float2 a) {
 __device__ __forceinline__ float2 gm2_lgamma(float2 a) {
   return make_float2(lgammaf(a.x), lgammaf(a.y));
 }
-// Paired softplus: the argument split, the correction and the atanh series
-// run on FFMA2/FMUL2/FADD2; the hardware 2^x and the reciprocal per half.
+// Paired softplus (the scalar gm_softplus step for step): the reduction,
+// the correction and the series on FFMA2/FMUL2/FADD2; the hardware 2^x,
+// reciprocal and NaN-propagating max per half.
 __device__ __forceinline__ float2 gm2_softplus(float2 a) {
-  const float2 kL2E = gm2(1.44269502162933349609375f);
-  const float2 kL2E_LO = gm2(1.925962989e-08f);
   const float2 na = make_float2(fmaxf(-fabsf(a.x), -126.0f), fmaxf(-fabsf(a.y), -126.0f));
-  const float2 th = __fmul2_rn(na, kL2E);
-  const float2 tl = __ffma2_rn(na, kL2E_LO, __ffma2_rn(na, kL2E, gm2_neg(th)));
-  float2 u = make_float2(gm_ex2_approx(th.x), gm_ex2_approx(th.y));
-  u = __ffma2_rn(u, __fmul2_rn(tl, gm2(0.693147180559945309f)), u);
-  const float2 den = __fadd2_rn(u, gm2(2.0f));
-  const float2 s = make_float2(__fdividef(u.x, den.x), __fdividef(u.y, den.y));
-  const float2 s2 = __fmul2_rn(s, s);
-  float2 p = gm2(1.0f / 15.0f);
-  p = __ffma2_rn(p, s2, gm2(1.0f / 13.0f));
-  p = __ffma2_rn(p, s2, gm2(1.0f / 11.0f));
-  p = __ffma2_rn(p, s2, gm2(1.0f / 9.0f));
-  p = __ffma2_rn(p, s2, gm2(1.0f / 7.0f));
-  p = __ffma2_rn(p, s2, gm2(1.0f / 5.0f));
-  p = __ffma2_rn(p, s2, gm2(1.0f / 3.0f));
-  const float2 s_2 = __fadd2_rn(s, s);
-  const float2 l = __ffma2_rn(s_2, __fmul2_rn(s2, p), s_2);
-  const float2 r = __fadd2_rn(make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)), l);
-  return make_float2(a.x == a.x ? r.x : a.x, a.y == a.y ? r.y : a.y);
+  const float2 t = __fmul2_rn(na, gm2(GM_SP_L2E));
+  const float2 r =
+      __ffma2_rn(t, gm2(-GM_SP_LN2_LO), __ffma2_rn(t, gm2(-GM_SP_LN2_HI), na));
+  const float2 u0 = make_float2(gm_ex2_approx(t.x), gm_ex2_approx(t.y));
+  const float2 u = __ffma2_rn(u0, r, u0);
+  const float2 den = __ffma2_rn(u, gm2(0.5f), gm2(1.0f));
+  const float2 w = __fmul2_rn(u, make_float2(gm_rcp_approx(den.x), gm_rcp_approx(den.y)));
+  const float2 q = __fmul2_rn(w, w);
+  float2 p = gm2(GM_SP_C6);
+  p = __ffma2_rn(p, q, gm2(GM_SP_C5));
+  p = __ffma2_rn(p, q, gm2(GM_SP_C4));
+  p = __ffma2_rn(p, q, gm2(GM_SP_C3));
+  p = __ffma2_rn(p, q, gm2(GM_SP_C2));
+  p = __ffma2_rn(p, q, gm2(GM_SP_C1));
+  const float2 l = __ffma2_rn(w, __fmul2_rn(q, p), w);
+  return __fadd2_rn(make_float2(gm_max_nan(a.x, 0.0f), gm_max_nan(a.y, 0.0f)), l);
 }
 
 __device__ __forceinline__ float2 gm2_digamma(float2 a) {
