@@ -419,14 +419,29 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       if (fusable(g.n[i].a)) fused[g.n[i].a] = 1;
       else if (fusable(g.n[i].b)) fused[g.n[i].b] = 1;
     }
+    // x * y - softplus(a), with the product and the softplus feeding nothing
+    // else, is one gm2_fma_nsoftplus (value functions only).
+    std::vector<char> nsp_fold(N, 0), nsp_skip(N, 0);
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i) || g.n[i].op != O_SUB) continue;
+      const int a = g.n[i].a, b = g.n[i].b;
+      if (!fusable(a) || fused[a] || b < 0 || softplus_arg[b] < 0 || uses[b] != 1 || b == root)
+        continue;
+      nsp_fold[i] = 1;
+      nsp_skip[a] = nsp_skip[b] = 1;
+    }
     s << "__device__ __forceinline__ float2 gm_value2(const float2* __restrict__ d, "
          "const float2* __restrict__ pp, const float2* __restrict__ hh) {\n";
     for (int i = 0; i < N; ++i) {
       if (!live[i] || !is_pd(i)) continue;
-      if (fused[i] || softplus_inner[i]) continue;
+      if (fused[i] || softplus_inner[i] || nsp_skip[i]) continue;
       const Node& x = g.n[i];
       std::string e;
-      if (softplus_arg[i] >= 0) {
+      if (nsp_fold[i]) {
+        const Node& m = g.n[x.a];
+        e = "gm2_fma_nsoftplus(" + ref2(m.a) + ", " + ref2(m.b) + ", " +
+            ref2(softplus_arg[x.b]) + ")";
+      } else if (softplus_arg[i] >= 0) {
         e = "gm2_softplus(" + ref2(softplus_arg[i]) + ")";
       } else if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
         const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;

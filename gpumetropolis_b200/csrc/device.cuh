@@ -176,9 +176,11 @@ struct Comp {
 //       (Cody & Waite reduction: ln 2 = LN2_HI + LN2_LO, two FMAs), 2^t from
 //       the hardware ex2 and e^r = 1 + r (|r| < 6e-6, so r^2/2 < 2e-11);
 //   log1p(u) = 2 atanh(s), s = u / (2 + u) in (0, 1/3]; with w = 2s =
-//       u / (1 + u/2) and q = w^2:  w (1 + q/12 + q^2/80 + ... + q^6/53248),
-//       the coefficients 1 / ((2k+1) 4^k) of the atanh series in w, the
-//       omitted tail < 1.5e-8 w.
+//       u / (1 + u/2) and q = w^2 in [0, 4/9]:  w (1 + q P(q)), P the
+//       degree-3 minimax fit (discrete Chebyshev approximation by linear
+//       programming on 4001 points, weighted to the relative error of
+//       log1p) of the atanh series sum_k q^(k-1) / ((2k+1) 4^k); its
+//       relative error in log1p is below 5e-9.
 // Unlike log(1 + exp(a)) in FP32 this keeps full relative accuracy where
 // e^a underflows against 1.  NaN propagates (max.NaN); +inf -> +inf;
 // -inf -> 0.
@@ -197,16 +199,19 @@ __device__ __forceinline__ float gm_max_nan(float a, float b) {
   asm("max.NaN.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
   return y;
 }
+__device__ __forceinline__ float gm_min_nan(float a, float b) {
+  float y;
+  asm("min.NaN.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+  return y;
+}
 
 #define GM_SP_L2E 1.44269502162933349609375f        // log2(e) rounded to float
 #define GM_SP_LN2_HI 0.693147182464599609375f       // ln(2) rounded to float
 #define GM_SP_LN2_LO (-1.904654212125934e-09f)      // ln(2) - GM_SP_LN2_HI
-#define GM_SP_C1 (1.0f / 12.0f)
-#define GM_SP_C2 (1.0f / 80.0f)
-#define GM_SP_C3 (1.0f / 448.0f)
-#define GM_SP_C4 (1.0f / 2304.0f)
-#define GM_SP_C5 (1.0f / 11264.0f)
-#define GM_SP_C6 (1.0f / 53248.0f)
+#define GM_SP_P0 8.333302289e-02f
+#define GM_SP_P1 1.250672713e-02f
+#define GM_SP_P2 2.187641105e-03f
+#define GM_SP_P3 5.471091135e-04f
 
 __device__ __forceinline__ float gm_softplus(float a) {
   const float na = fmaxf(-fabsf(a), -126.0f);  // e^-126 underflows to 0 anyway
@@ -216,12 +221,10 @@ __device__ __forceinline__ float gm_softplus(float a) {
   const float u = fmaf(u0, r, u0);
   const float w = u * gm_rcp_approx(fmaf(u, 0.5f, 1.0f));
   const float q = w * w;
-  float p = GM_SP_C6;
-  p = fmaf(p, q, GM_SP_C5);
-  p = fmaf(p, q, GM_SP_C4);
-  p = fmaf(p, q, GM_SP_C3);
-  p = fmaf(p, q, GM_SP_C2);
-  p = fmaf(p, q, GM_SP_C1);
+  float p = GM_SP_P3;
+  p = fmaf(p, q, GM_SP_P2);
+  p = fmaf(p, q, GM_SP_P1);
+  p = fmaf(p, q, GM_SP_P0);
   return gm_max_nan(a, 0.0f) + fmaf(w, q * p, w);
 }
 
@@ -254,8 +257,9 @@ __device__ __forceinline__ float2 gm2_lgamma(float2 a) {
 }
 // Paired softplus (the scalar gm_softplus step for step): the reduction,
 // the correction and the series on FFMA2/FMUL2/FADD2; the hardware 2^x,
-// reciprocal and NaN-propagating max per half.
-__device__ __forceinline__ float2 gm2_softplus(float2 a) {
+// reciprocal and NaN-propagating max per half.  gm2_log1p_nexp is the
+// second addend log1p(e^-|a|).
+__device__ __forceinline__ float2 gm2_log1p_nexp(float2 a) {
   const float2 na = make_float2(fmaxf(-fabsf(a.x), -126.0f), fmaxf(-fabsf(a.y), -126.0f));
   const float2 t = __fmul2_rn(na, gm2(GM_SP_L2E));
   const float2 r =
@@ -265,14 +269,22 @@ __device__ __forceinline__ float2 gm2_softplus(float2 a) {
   const float2 den = __ffma2_rn(u, gm2(0.5f), gm2(1.0f));
   const float2 w = __fmul2_rn(u, make_float2(gm_rcp_approx(den.x), gm_rcp_approx(den.y)));
   const float2 q = __fmul2_rn(w, w);
-  float2 p = gm2(GM_SP_C6);
-  p = __ffma2_rn(p, q, gm2(GM_SP_C5));
-  p = __ffma2_rn(p, q, gm2(GM_SP_C4));
-  p = __ffma2_rn(p, q, gm2(GM_SP_C3));
-  p = __ffma2_rn(p, q, gm2(GM_SP_C2));
-  p = __ffma2_rn(p, q, gm2(GM_SP_C1));
-  const float2 l = __ffma2_rn(w, __fmul2_rn(q, p), w);
-  return __fadd2_rn(make_float2(gm_max_nan(a.x, 0.0f), gm_max_nan(a.y, 0.0f)), l);
+  float2 p = gm2(GM_SP_P3);
+  p = __ffma2_rn(p, q, gm2(GM_SP_P2));
+  p = __ffma2_rn(p, q, gm2(GM_SP_P1));
+  p = __ffma2_rn(p, q, gm2(GM_SP_P0));
+  return __ffma2_rn(w, __fmul2_rn(q, p), w);
+}
+__device__ __forceinline__ float2 gm2_softplus(float2 a) {
+  const float2 m = make_float2(gm_max_nan(a.x, 0.0f), gm_max_nan(a.y, 0.0f));
+  return __fadd2_rn(m, gm2_log1p_nexp(a));
+}
+// x * y - softplus(a) as FFMA2(x, y, min(-a, 0) - log1p(e^-|a|)), the NaN-
+// propagating min giving -max(a, 0): one rounding fewer than the product and
+// the difference apart, and no separate negation.
+__device__ __forceinline__ float2 gm2_fma_nsoftplus(float2 x, float2 y, float2 a) {
+  const float2 nm = make_float2(gm_min_nan(-a.x, 0.0f), gm_min_nan(-a.y, 0.0f));
+  return __ffma2_rn(x, y, __ffma2_rn(gm2_log1p_nexp(a), gm2(-1.0f), nm));
 }
 
 __device__ __forceinline__ float2 gm2_digamma(float2 a) {
