@@ -316,8 +316,11 @@ struct JitPrior {
 }  // namespace gpum
 
 // Value-only kernel: PH_EVAL / PH_POINTWISE / RWM, DE and Cholesky steps.
-// The paired body fits in 128 registers, so two CTAs (16 warps) share an SM.
-#if GM_PAIR
+// CTAs per SM the registers must allow (GM_VALUE_CTAS from the host: three
+// for narrow paired models, 80 registers; two for the other paired ones).
+#ifdef GM_VALUE_CTAS
+#define GM_VALUE_MIN_CTAS GM_VALUE_CTAS
+#elif GM_PAIR
 #define GM_VALUE_MIN_CTAS 2
 #else
 #define GM_VALUE_MIN_CTAS 1

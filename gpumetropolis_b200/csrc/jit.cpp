@@ -200,6 +200,12 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg)
   s += "#define GM_PAIRG " + std::string(pairg ? "1" : "0") + "\n";
   s += "#define GM_G " + std::to_string(G) + "\n";
   s += "#define GM_GG " + std::to_string(GG) + "\n";
+  // Narrow paired models with two chains per thread (2 x (parameters +
+  // hoisted values) <= 40 broadcast pairs) fit in 80 registers without
+  // spills: three CTAs, 24 warps per SM.
+  const int w = gm.np + std::max(gm.n_hoist, 1);
+  s += "#define GM_VALUE_CTAS " +
+       std::to_string(pair ? (G == 2 && G * w <= 40 ? 3 : 2) : 1) + "\n";
   s += "namespace gpum {\n";
   s += gm.source;
   s += "}  // namespace gpum\nusing namespace gpum;\n";
