@@ -346,7 +346,7 @@ class Session:
     def run_de_sync(self, init, proposal_sd, n_iter, seed, gamma, de_noise, rng=RNG_TRIPLE32):
         """Per-generation DE (path B).  Returns (draws, accept, last_logpost)."""
         init, sd = _f64(init), _f64(proposal_sd)
-        n_chains = init.size // self.n_params
+        n_chains = self.n_chains = init.size // self.n_params
         draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
         acc = np.empty(n_chains, np.float32)
         last = np.empty(n_chains, np.float64)
@@ -430,7 +430,7 @@ class Session:
         """Delayed-acceptance run with `surrogate` (a Surrogate) as stage 1.
         Returns (draws, accept, last_logpost, exact_evals per chain)."""
         init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
-        n_chains = init.size // self.n_params
+        n_chains = self.n_chains = init.size // self.n_params
         L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
         draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
         acc = np.empty(n_chains, np.float32)

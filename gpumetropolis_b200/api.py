@@ -332,13 +332,16 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
 
     call = _Backend(model, data_mat, n_obs, rng_kind, scfg)
     if method == "pt" and swap_on_device:
-        if scfg is not None:
-            call.close()
-            raise GpumInputError("`surrogate` is not available with `swap_on_device = TRUE`.")
+        if scfg is not None:  # exact pairs from the second half of warmup
+            call.record_at = warmup // 2
+            call.da_at = warmup
         try:
-            return _pt_device(model, call, npar, n_chains, init_mat, sd_mat, temps, n_iter,
-                              warmup, int(swap_every), ladder_len, bool(adapt), int(seed),
-                              backend)
+            fit = _pt_device(model, call, npar, n_chains, init_mat, sd_mat, temps, n_iter,
+                             warmup, int(swap_every), ladder_len, bool(adapt), int(seed),
+                             backend)
+            if scfg is not None:
+                fit.extra["surrogate"] = call.da_summary()
+            return fit
         finally:
             call.close()
     if method == "de" and de_sync:
@@ -375,7 +378,9 @@ def _pt_device(model, call, npar, C, init_mat, sd_mat, temps, n_iter, warmup, sw
     batches (per-chain Robbins-Monro scales and variances as in the host
     orchestration, R/adaptive.R:330-355, from device moments) with exchanges
     inside each batch, then one sampling run with an exchange every
-    ``swap_every`` iterations."""
+    ``swap_every`` iterations (two-stage when the backend has a surrogate
+    schedule: trained on the warmup's exact pairs, exchanges on the exact
+    log posteriors)."""
     s = call.session
     s.set_exchange(ladder_len, swap_every)
     cur, sd = np.array(init_mat, dtype=np.float64), np.array(sd_mat, dtype=np.float64)

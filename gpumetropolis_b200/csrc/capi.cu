@@ -346,7 +346,8 @@ struct gpum_b200_session {
     }
     launch(PH_STEP);
     if (pt_K > 0) {
-      PtArgs P{pt_K, pt_every, pt_n.p, pt_att.p, pt_acc.p, params.p, geo.C_pad};
+      PtArgs P{pt_K, pt_every, A.iter, nullptr, nullptr, pt_n.p, pt_att.p, pt_acc.p,
+               params.p, geo.C_pad};
       pt_exchange_kernel<<<(unsigned)((n_chains + 127) / 128), 128, 0, stream>>>(A, P);
       GPUM_CK(cudaGetLastError());
       ++launches;
@@ -784,6 +785,13 @@ void da_step(gpum_b200_session* s) {
   da_tick_kernel<<<1, 32, 0, st>>>(s->D);
   GPUM_CK(cudaGetLastError());
   s->launches += 5 + (uint64_t)s->da_mlp_launches;
+  if (s->pt_K > 0) {  // exchanges on the exact log posteriors, caches swapped along
+    PtArgs P{s->pt_K,   s->pt_every,  s->D.iter, s->D.sll_x, s->D.prior_x,
+             s->pt_n.p, s->pt_att.p, s->pt_acc.p, s->D.full,  s->D.C_pad};
+    pt_exchange_kernel<<<(unsigned)((C + 127) / 128), 128, 0, st>>>(s->A, P);
+    GPUM_CK(cudaGetLastError());
+    ++s->launches;
+  }
 }
 
 void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const double* sd,
@@ -795,8 +803,6 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   require(mode <= 2, "delayed acceptance needs a symmetric proposal: mode 0 (rwm), 1 (de) or 2 "
                      "(cholesky)");
   require(s->n_beta == 0, "delayed acceptance does not support likelihood powers");
-  require(s->pt_K == 0, "delayed acceptance does not run device exchanges; exchange between "
-                        "run_da calls instead");
   const uint64_t keep_cap = s->rec_cap;
   s->rec_cap = 0;  // stage-1 rejections leave no exact pair to record
   try {
@@ -1156,9 +1162,11 @@ int gpum_b200_session_exchange_stats(gpum_b200_session* s, uint32_t* attempts,
                                      uint32_t* accepted, uint32_t* n_exchanges, char* err,
                                      size_t err_len) {
   return guard(err, err_len, [&] {
-    require(s && s->prepared, "session has no prepared run");
+    require(s != nullptr, "session is NULL");
     require(s->pt_K > 0, "device exchanges are off");
     const size_t C = (size_t)s->n_chains;
+    require(C > 0 && s->pt_att.p && s->pt_att.n >= C,
+            "no run with device exchanges since they were set");
     if (attempts)
       GPUM_CK(cudaMemcpyAsync(attempts, s->pt_att.p, sizeof(uint32_t) * C,
                               cudaMemcpyDeviceToHost, s->stream));

@@ -118,7 +118,8 @@ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
   return c;
 }
 
-// 53-bit uniform in (0, 1) from two 32-bit words.
+// 53-bit uniform in (0, 1] from two 32-bit words (the top value, 2^53 - 1/2
+// over 2^53, rounds to 1).
 __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
   const uint64_t m = ((uint64_t)a << 21) ^ (uint64_t)(b >> 11);
   return ((double)(m & ((1ull << 53) - 1)) + 0.5) * (1.0 / 9007199254740992.0);

@@ -194,6 +194,9 @@ static __global__ void moments_pool_m2_kernel(const float* __restrict__ draws, i
 struct PtArgs {
   int K;               // ladder length
   int every;           // iterations between exchanges
+  const uint32_t* iter;  // [1] iterations done (the step's or the DA loop's counter)
+  double* sll_x;       // [C] delayed acceptance: surrogate value at the state, or null
+  double* prior_x;     // [C] delayed acceptance: prior at the state, or null
   uint32_t* n_swaps;   // [1] exchanges done
   uint32_t* att;       // [C] attempts of pair (c, c + 1)
   uint32_t* acc;       // [C] accepted exchanges of pair (c, c + 1)
@@ -202,7 +205,7 @@ struct PtArgs {
 };
 
 static __global__ void pt_exchange_kernel(ChainArgs A, PtArgs P) {
-  const uint32_t t = A.iter[0];  // iterations done (all chain blocks agree here)
+  const uint32_t t = P.iter[0];  // iterations done (all chain blocks agree here)
   if (t == 0 || t % (uint32_t)P.every != 0 || t >= A.n_iter) return;
   const uint32_t s = t / (uint32_t)P.every;  // exchange number, from 1
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -226,6 +229,13 @@ static __global__ void pt_exchange_kernel(ChainArgs A, PtArgs P) {
   }
   A.cur[i] = lpb;
   A.cur[i + 1] = lpa;
+  if (P.sll_x) {  // the two-stage loop's cached values follow their states
+    const double s0 = P.sll_x[i], p0 = P.prior_x[i];
+    P.sll_x[i] = P.sll_x[i + 1];
+    P.prior_x[i] = P.prior_x[i + 1];
+    P.sll_x[i + 1] = s0;
+    P.prior_x[i + 1] = p0;
+  }
   if (A.mode == MODE_MALA) {  // the cached gradients belong to the states
     double* ga = A.gx + (size_t)i * np;
     double* gb = A.gx + (size_t)(i + 1) * np;

@@ -232,9 +232,11 @@ GPUM_API int gpum_b200_session_fetch(gpum_b200_session* s, float* out_draws, flo
  * chains draw fresh proposals.  Philox uniforms.  ladder_len 0 turns it off. */
 GPUM_API int gpum_b200_session_set_exchange(gpum_b200_session* s, uint32_t ladder_len,
                                             uint32_t swap_every, char* err, size_t err_len);
-/* Per pair (c, c+1) the attempted and accepted exchanges of the prepared run
- * (n_chains entries each; entries that are no pair stay 0) and the number of
- * exchange steps.  Any output pointer may be NULL. */
+/* Per pair (c, c+1) the attempted and accepted exchanges of the last run
+ * (prepared, run or run_da; n_chains entries each; entries that are no pair
+ * stay 0) and the number of exchange steps.  In a delayed-acceptance run the
+ * exchanges use the exact log posteriors, and the surrogate value and prior
+ * cached for each state move with it.  Any output pointer may be NULL. */
 GPUM_API int gpum_b200_session_exchange_stats(gpum_b200_session* s, uint32_t* attempts,
                                               uint32_t* accepted, uint32_t* n_exchanges,
                                               char* err, size_t err_len);
@@ -334,7 +336,8 @@ GPUM_API int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, 
  * the chains target the exact tempered posterior.  Same arguments and
  * outputs as session_run for proposal modes 0, 1 and 2 (MALA is refused);
  * out_exact (may be NULL) receives per chain the number of exact
- * evaluations (stage-1 acceptances).  The surrogate must have d = n_params. */
+ * evaluations (stage-1 acceptances).  The surrogate must have d = n_params.
+ * Device exchanges (session_set_exchange) run as in session_run. */
 GPUM_API int gpum_b200_session_run_da(gpum_b200_session* s, gpum_b200_mlp* surrogate,
                                       const double* init, const double* proposal_sd,
                                       const double* temperatures, uint32_t n_chains,

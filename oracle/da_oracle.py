@@ -14,6 +14,16 @@ stream are the reference's random-walk ones (``cpu_native.rs:726-735``,
 then per iteration the stage-1 uniform, the stage-2 uniform (only when stage 1
 accepted), and the next proposal's normals.  The surrogate is a callable, so
 the test can hand in the very network the GPU uses.  Used by tests only.
+
+With ``exchange=(ladder_len, every)`` it adds the device replica exchange:
+after every ``every``-th iteration the adjacent pairs of one parity within
+each ladder of ``ladder_len`` consecutive chains (pairs 0-1, 2-3, ... at odd
+exchange numbers, 1-2, 3-4, ... at even ones, as ``R/adaptive.R:362-387``)
+swap states with probability min(1, exp((lp[i+1] - lp[i]) (1/T[i] -
+1/T[i+1]))) on the exact log posteriors; the uniform is Philox4x32-10
+(Salmon, Moraes, Dror & Shaw, "Parallel random numbers: as easy as 1, 2,
+3", SC 2011) keyed by (seed, exchange number, pair); both chains of an
+exchanged pair draw a new proposal from their own streams.
 """
 from __future__ import annotations
 
@@ -49,14 +59,44 @@ class _Stream:
         return math.sqrt(-2.0 * math.log(u1)) * math.cos(6.283185307179586 * u2)
 
 
+_M32 = 0xFFFFFFFF
+
+
+def philox4x32_10(c, k0, k1):
+    """Philox4x32 with 10 rounds on the counter (c0, c1, c2, c3), key (k0, k1)."""
+    c0, c1, c2, c3 = (x & _M32 for x in c)
+    for _ in range(10):
+        p0 = 0xD2511F53 * c0
+        p1 = 0xCD9E8D57 * c2
+        c0, c1, c2, c3 = ((p1 >> 32) ^ c1 ^ k0) & _M32, p1 & _M32, ((p0 >> 32) ^ c3 ^ k1) & _M32, \
+            p0 & _M32
+        k0 = (k0 + 0x9E3779B9) & _M32
+        k1 = (k1 + 0xBB67AE85) & _M32
+    return c0, c1, c2, c3
+
+
+def u53(a, b):
+    """Uniform in (0, 1] from the top 53 bits of two 32-bit words (the top
+    value rounds to 1 in f64, as on the device)."""
+    m = ((a << 21) ^ (b >> 11)) & ((1 << 53) - 1)
+    return (m + 0.5) / 9007199254740992.0
+
+
+def exchange_uniform(seed, exchange, pair):
+    r = philox4x32_10((pair, exchange, 0x50545357, 0), seed & _M32, 0x3C6EF372)
+    return u53(r[0], r[1])
+
+
 def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
-           proposal_sd, temperatures, n_iter, seed, surrogate, tie=1e-4):
+           proposal_sd, temperatures, n_iter, seed, surrogate, tie=1e-4, exchange=None):
     """Random-walk delayed acceptance for every chain.
 
     ``surrogate(theta (n x np)) -> (n,)``.  Returns ``(draws (n_iter, C, np),
     accepts (C,), exact_evals (C,), tie_at (C,))``; ``tie_at[c]`` is the first
     iteration whose decision lay within ``tie`` of its threshold (the chain's
-    later draws are not comparable), or n_iter."""
+    later draws are not comparable), or n_iter.  With ``exchange`` the tuple
+    also holds ``(attempts (C,), accepted (C,))`` per pair (c, c + 1), and a
+    tie in an exchange decision marks both chains of the pair."""
     init = np.asarray(init, dtype=np.float64).reshape(-1, n_params)
     C = init.shape[0]
     sd = np.asarray(proposal_sd, dtype=np.float64).reshape(C, n_params)
@@ -83,6 +123,33 @@ def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs
                 y[c, j] = x[c, j] + sd[c, j] * streams[c].normal()
         return y
 
+    att = np.zeros(C, dtype=np.int64)
+    ok = np.zeros(C, dtype=np.int64)
+
+    def exchange_step(t_done, y):
+        K, every = exchange
+        if t_done % every or t_done >= n_iter:
+            return
+        s = t_done // every
+        for i in range(C - 1):
+            if i % K == K - 1 or (i % K) % 2 != (s + 1) % 2:
+                continue
+            lpa, lpb = llx[i] + px[i], llx[i + 1] + px[i + 1]
+            delta = (lpb - lpa) * (1.0 / temps[i] - 1.0 / temps[i + 1])
+            lu = math.log(exchange_uniform(seed, s, i))
+            att[i] += 1
+            if abs(lu - delta) < tie:
+                for c in (i, i + 1):
+                    tie_at[c] = min(tie_at[c], t_done)
+            if not (math.isfinite(delta) and lu < delta):
+                continue
+            ok[i] += 1
+            for arr in (x, llx, px, sx):
+                arr[[i, i + 1]] = arr[[i + 1, i]]
+            for c in (i, i + 1):
+                for j in range(n_params):
+                    y[c, j] = x[c, j] + sd[c, j] * streams[c].normal()
+
     y = propose()
     for t in range(n_iter):
         sy = np.asarray(surrogate(y), dtype=np.float64)
@@ -106,4 +173,8 @@ def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs
         draws[t] = x
         if t + 1 < n_iter:
             y = propose()
+            if exchange is not None:
+                exchange_step(t + 1, y)
+    if exchange is not None:
+        return draws, accepts, exact_n, tie_at, (att, ok)
     return draws, accepts, exact_n, tie_at

@@ -136,3 +136,65 @@ def test_surrogate_mode_pt(gpu):
     cold = fit.draws[:, 0, 0]
     assert np.any(cold > 1.5) and np.any(cold < -1.5)
     assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
+
+
+def test_two_stage_with_device_exchanges_matches_oracle(gpu):
+    # three ladders of four tempered chains, an exchange after every third
+    # iteration: same trajectories and exchange counts as the oracle, whose
+    # exchange step also moves each state's cached surrogate value and prior
+    w = W.make("logistic", n_obs=2048, p=4)
+    m = w.model
+    rng = np.random.default_rng(3)
+    C, K, every, n_iter, seed = 12, 4, 3, 30, 33
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.04)
+    temps = np.tile([1.0, 1.3, 1.7, 2.2], C // K)
+    with _session(gpu, w) as s:
+        big = w.truth["beta"] + rng.normal(0, 0.05, (256, m.n_params))
+        net = _trained(gpu, s, w, big, np.full((256, m.n_params), 0.04))
+        try:
+            s.set_exchange(K, every)
+            d, acc, last, exact = s.run_da(net, init, sd, temps, n_iter, seed, 0)
+            att, ok, n_ex = s.exchange_stats()
+            s.set_exchange(0)
+            d = d.reshape((n_iter, C, m.n_params), order="F")
+            od, oacc, oexact, tie_at, (oatt, ook) = da_oracle.run_da(
+                m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                w.data, m.n_cols, w.n_obs, init, sd, temps, n_iter, seed, net.predict,
+                exchange=(K, every))
+        finally:
+            net.close()
+    assert n_ex == (n_iter - 1) // every
+    np.testing.assert_array_equal(att, np.tile([5, 4, 5, 0], C // K))  # 5 odd, 4 even exchanges
+    np.testing.assert_array_equal(att, oatt)
+    t_min = int(tie_at.min())  # exchanges spread a tie to other chains: compare before it
+    assert t_min >= 9, t_min
+    np.testing.assert_allclose(d[:t_min], od[:t_min], rtol=2e-6, atol=1e-6)
+    if t_min == n_iter:
+        np.testing.assert_array_equal(ok, ook)
+        np.testing.assert_array_equal(exact, oexact)
+    assert ook.sum() > 0
+
+
+def test_surrogate_mode_pt_with_device_exchanges(gpu):
+    # four ladders of eight rungs on the |mu| target, two-stage sampling with
+    # the exchanges on the device
+    rng = np.random.default_rng(5)
+    y = rng.normal(3.0, 1.0, 400)
+    from gpumetropolis_b200.dsl import gpum_model
+    m = gpum_model("~ log(exp(-0.5 * (y - mu)^2) + exp(-0.5 * (y + mu)^2))", params="mu",
+                   data="y")
+    init = np.tile(np.linspace(-6, 6, 8), 4).reshape(32, 1)
+    fit = api.gpu_metropolis(m, {"y": y}, init=init, proposal_sd=0.15, n_iter=4000,
+                             warmup=2000, method="pt", seed=6, swap_on_device=True,
+                             ladder_len=8, swap_every=10,
+                             surrogate={"hidden": 128, "batch": 1024, "steps": 600,
+                                        "min_pairs": 512})
+    info = fit.extra["surrogate"]
+    assert info["used"], info
+    assert info["exact_fraction"] < 1.0
+    assert fit.extra["exchanges"] == 199  # t = 10 .. 1990 of the sampling run
+    cold = fit.draws[:, ::8, 0].ravel()
+    assert np.any(cold > 1.5) and np.any(cold < -1.5)
+    assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
+    assert np.nanmax(fit.extra["exchange_rate"]) > 0.2

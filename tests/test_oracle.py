@@ -144,3 +144,18 @@ def test_de_and_de_sync_recover_correlated_target():
     dr = d.reshape((3000, C, 2), order="F")[1000:]
     assert abs(dr[..., 0].mean() - y[:, 0].mean()) < 0.02
     assert abs(np.corrcoef(dr[..., 0].ravel(), dr[..., 1].ravel())[0, 1] - rho) < 0.05
+
+
+def test_philox_known_answers():
+    # Philox4x32-10 known-answer vectors of the Random123 distribution
+    # (counter, key -> output); the exchange uniforms of the delayed-
+    # acceptance oracle come from this function.
+    from oracle.da_oracle import philox4x32_10, u53
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+             ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF),
+              (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+             ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+              (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1))]
+    for c, k, want in cases:
+        assert philox4x32_10(c, *k) == want
+    assert 0.0 < u53(0, 0) < 1e-15 and u53(0xFFFFFFFF, 0xFFFFFFFF) == 1.0
