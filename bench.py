@@ -70,6 +70,10 @@ def _args():
     p.add_argument("--no-da", action="store_true")
     p.add_argument("--da-warmup", type=int, default=1000)
     p.add_argument("--da-iters", type=int, default=1000)
+    p.add_argument("--configs", action="store_true",
+                   help="instead of the headline line: time the Poisson (MALA), mixture (PT "
+                        "ladders) and Student-t (DE) configurations at full size, one JSON "
+                        "line each")
     return p.parse_args()
 
 
@@ -501,10 +505,81 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_configs(a, n_warm=2, n_timed=6):
+    """Full-size timing of the other configurations: per configuration one
+    session, `n_warm` untimed iterations, then `n_timed` single-iteration
+    advances, each after an L2 flush and bracketed by CUDA events on the
+    session's stream."""
+    import torch
+
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200 import workloads as W
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    dev = torch.device("cuda", 0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for name in ("poisson", "mixture", "student_t"):
+        w = W.make(name)
+        m = w.model
+        C, N, npar = w.n_chains, w.n_obs, m.n_params
+        rng = np.random.default_rng(7)
+        temps = np.ones(C)
+        gamma, ladder = 0.0, 0
+        if name == "poisson":
+            mode, centre, jitter, step = _native.MODE_MALA, w.truth["beta"], 0.01, 2e-4
+            method = "mala (paired value + adjoint kernel gm_iter_grad)"
+        elif name == "mixture":
+            mode, jitter, step = _native.MODE_RWM, 0.01, 5e-4
+            centre = np.array([math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)])
+            ladder = 16
+            temps = np.tile(np.geomspace(1.0, 64.0, ladder), C // ladder)
+            method = "rwm, 512 ladders of 16 geometric temperatures 1..64, device exchanges every 10"
+        else:
+            mode, jitter, step = _native.MODE_DE, 0.01, 1e-4
+            centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
+            gamma = 2.38 / math.sqrt(2 * npar)
+            method = "de (scalar wide-model body gm_iter_value)"
+        init = centre + rng.normal(0.0, jitter, (C, npar))
+        sd = np.full((C, npar), step)
+        sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                               npar, w.data, m.n_cols, N)
+        if ladder:
+            sess.set_exchange(ladder, 10)
+        sess.prepare(init, sd, temps, n_warm + n_timed, 3, mode, gamma, 1e-3,
+                     rng=_native.RNG_PHILOX)
+        sess.advance(n_warm)
+        sess.sync()
+        stream = torch.cuda.ExternalStream(sess.stream, device=dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(n_timed)]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for s0, s1 in ev:
+                flush.zero_()
+                s0.record(stream)
+                sess.advance(1)
+                s1.record(stream)
+        torch.cuda.synchronize()
+        ms = float(np.mean([s0.elapsed_time(s1) for s0, s1 in ev]))
+        _, acc, last, _ = sess.fetch(want_draws=False)
+        sess.close()
+        print(json.dumps({
+            "config": name, "n_chains": C, "n_obs": N, "n_params": npar, "method": method,
+            "ms_per_iter": round(ms, 3), "chain_obs_per_s": C * N / (ms / 1e3),
+            "all_finite": bool(np.all(np.isfinite(last))),
+            "timing": f"{n_timed} single-iteration advances after {n_warm} warm-up, L2 "
+                      "flushed before each, CUDA events on the session stream"}), flush=True)
+        del w
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.configs:
+        run_configs(a)
     else:
         run_b200(a)
 
