@@ -540,7 +540,7 @@ def run_configs(a, n_warm=2, n_timed=6):
             mode, jitter, step = _native.MODE_DE, 0.01, 1e-4
             centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
             gamma = 2.38 / math.sqrt(2 * npar)
-            method = "de (scalar wide-model body gm_iter_value)"
+            method = "de (chain-lane value body gm_iter_value)"
         init = centre + rng.normal(0.0, jitter, (C, npar))
         sd = np.full((C, npar), step)
         sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,

@@ -140,8 +140,9 @@ int num_sms() {
 struct KernelChoice {
   bool compiled = false;
   const void* fn = nullptr;  // __global__ pointer or cudaKernel_t
-  int G = 8;                 // chains per thread
+  int G = 8;                 // chains per thread (per warp for a chain-lane body)
   int W = 1;                 // values per chain (1, or 1 + np with the gradient)
+  bool lanes = false;        // chain-lane body: G = 32 chains per warp group
 };
 
 struct Geometry {
@@ -249,7 +250,8 @@ struct gpum_b200_session {
                           " the compiled engine: " + cm_error};
       k.compiled = true;
       k.fn = need_grad ? (const void*)cm.k_grad : (const void*)cm.k_value;
-      k.G = need_grad ? cm.GG : cm.G;
+      k.lanes = !need_grad && cm.lanes;
+      k.G = need_grad ? cm.GG : (k.lanes ? 32 : cm.G);
       k.W = need_grad ? 1 + (int)np : 1;
     } else {
       k.compiled = false;
@@ -270,7 +272,7 @@ struct gpum_b200_session {
     g.NCB = (n + g.CG - 1) / g.CG;
     g.C_pad = g.NCB * g.CG;
     g.ntiles = (int)((n_obs + T - 1) / T);
-    g.smem = skel_smem_bytes(T, (int)ncols, (int)np, g.CG, g.G, k.W);
+    g.smem = skel_smem_bytes(T, (int)ncols, (int)np, g.CG, g.G, k.W, k.lanes);
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
     if (occ < 1) occ = 1;

@@ -339,8 +339,42 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
                                 : op_expr(g, i, name[x.a], x.b >= 0 ? name[x.b] : "", true);
     s << "  const float " << name[i] << " = " << e << ";\n";
     if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
+    if (x.op != O_D) ++out->n_data_ops;
   }
   s << "  (void)xo; (void)T; (void)d;\n}\n";
+
+  // gm_data4l: four consecutive observations xo .. xo + 3 for the chain-lane
+  // body, one 16-byte load per column (every lane reads the same address, a
+  // broadcast); xo is 16-byte aligned (a multiple of 4 observations into a
+  // tile whose column stride GM_T * 4 is a multiple of 128 bytes).
+  s << "__device__ __forceinline__ void gm_data4l(const float* __restrict__ xo, "
+       "float* __restrict__ d0, float* __restrict__ d1, float* __restrict__ d2, "
+       "float* __restrict__ d3) {\n";
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || !is_d(i)) continue;
+    const Node& x = g.n[i];
+    if (x.op == O_D) {
+      s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
+        << x.arg << " * GM_T);\n";
+      for (int k = 0; k < 4; ++k)
+        s << "  const float " << name[i] << "_" << k << " = q_" << name[i] << "."
+          << "xyzw"[k] << ";\n";
+    } else {
+      for (int k = 0; k < 4; ++k) {
+        auto arg = [&](int c) -> std::string {
+          if (c < 0) return "";
+          if (g.n[c].op == O_C) return name[c];
+          return name[c] + "_" + std::to_string(k);
+        };
+        s << "  const float " << name[i] << "_" << k << " = "
+          << op_expr(g, i, arg(x.a), arg(x.b), true) << ";\n";
+      }
+    }
+    if (dslot[i] >= 0)
+      for (int k = 0; k < 4; ++k)
+        s << "  d" << k << "[" << dslot[i] << "] = " << name[i] << "_" << k << ";\n";
+  }
+  s << "  (void)xo; (void)d0; (void)d1; (void)d2; (void)d3;\n}\n";
 
   // gm_hoist: parameter-only subexpressions, once per chain.
   auto emit_hoist_body = [&](std::ostringstream& o) {
@@ -377,6 +411,57 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
        "const float* __restrict__ p, const float* __restrict__ h) {\n";
   emit_fwd(s, true);
   s << "  (void)d; (void)p; (void)h;\n  return " << rootv << ";\n}\n";
+
+  // gm_value4l: four consecutive observations xo .. xo + 3 (the chain-lane
+  // body), evaluated node by node in lockstep so that only the running
+  // values stay live; each data column is loaded (16 bytes, a broadcast) at
+  // its first use.  Models with data-only operations take gm_data4l and
+  // gm_value four times instead.
+  s << "__device__ __forceinline__ void gm_value4l(const float* __restrict__ xo, "
+       "const float* __restrict__ p, const float* __restrict__ h, "
+       "float* __restrict__ out) {\n";
+  if (out->n_data_ops > 0) {
+    s << "  float d0[GM_ND], d1[GM_ND], d2[GM_ND], d3[GM_ND];\n"
+         "  gm_data4l(xo, d0, d1, d2, d3);\n"
+         "  out[0] = gm_value(d0, p, h);\n  out[1] = gm_value(d1, p, h);\n"
+         "  out[2] = gm_value(d2, p, h);\n  out[3] = gm_value(d3, p, h);\n";
+  } else {
+    std::vector<char> loaded(N, 0);
+    auto ref4 = [&](int i, int k) -> std::string {
+      const Node& x = g.n[i];
+      if (x.op == O_C) return name[i];
+      if (hslot[i] >= 0) return "h[" + std::to_string(hslot[i]) + "]";
+      if (x.op == O_P) return name[i];
+      if (x.op == O_D) {
+        if (!loaded[i]) {
+          s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
+            << x.arg << " * GM_T);\n";
+          loaded[i] = 1;
+        }
+        return "q_" + name[i] + "." + "xyzw"[k];
+      }
+      return name[i] + "_" + std::to_string(k);
+    };
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i) || softplus_inner[i]) continue;
+      const Node& x = g.n[i];
+      std::string a[4], b[4];
+      for (int k = 0; k < 4; ++k) {  // loads first, so they precede the four uses
+        const int ca = softplus_arg[i] >= 0 ? softplus_arg[i] : x.a;
+        a[k] = ref4(ca, k);
+        if (softplus_arg[i] < 0 && x.b >= 0) b[k] = ref4(x.b, k);
+      }
+      for (int k = 0; k < 4; ++k)
+        s << "  const float " << name[i] << "_" << k << " = "
+          << (softplus_arg[i] >= 0 ? "gm_softplus(" + a[k] + ")"
+                                   : op_expr(g, i, a[k], b[k], true))
+          << ";\n";
+    }
+    for (int k = 0; k < 4; ++k)
+      s << "  out[" << k << "] = " << (root < 0 ? std::string("0.0f") : ref4(root, k))
+        << ";\n";
+  }
+  s << "  (void)xo; (void)p; (void)h;\n}\n";
 
   // Paired versions (two observations per call) of gm_data and gm_value.
   // Leaves that do not depend on the observation (constants, parameters,

@@ -379,15 +379,24 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
 
 // --------------------------------------------------------- kernel skeleton
 // Shared-memory carve-up (the host's smem_bytes() must agree):
-//   2 data stages [ncols][T] f32 | params [np][CG] f32 (rounded to 4) |
-//   reduction [kWarps][G][width] f64 | 2 mbarriers | ticket.
+//   2 data stages [ncols][T] f32 | params [np][CG] f32 (rounded to 4; none
+//   for chain-lane bodies, whose lanes read their parameters from global
+//   memory) | reduction [kWarps][G][width] f64 | 2 mbarriers | ticket.
+__host__ __device__ inline size_t skel_param_floats(int np, int CG, bool lanes) {
+  return lanes ? 0 : (((size_t)np * CG + 3) & ~(size_t)3);
+}
 __host__ __device__ inline size_t skel_smem_bytes(int T, int ncols, int np, int CG, int G,
-                                                  int width) {
-  return 2 * (size_t)T * ncols * 4 + (((size_t)np * CG + 3) & ~(size_t)3) * 4 +
+                                                  int width, bool lanes = false) {
+  return 2 * (size_t)T * ncols * 4 + skel_param_floats(np, CG, lanes) * 4 +
          (size_t)kWarps * G * width * 8 + 2 * 8 + 16;
 }
 
 // Body contract (G chains per thread):
+//   bool kChainLanes                       false: lanes are observations (below);
+//                                          true: lanes are chains, G = 32 counts
+//                                          the chains of a warp, and the body has
+//                                          begin_lanes(pc, C_pad), eval4(xo, nv),
+//                                          last4(k) instead of begin/eval/last
 //   void begin(const float* pc0, int CG)   pc0 = this thread's first chain in
 //                                          the [np][CG] parameter tile
 //   void eval(const float* xo, int T, bool valid)  one observation
@@ -419,14 +428,17 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
 
   const size_t stage_floats = (size_t)T * ncols;
   float* xs = reinterpret_cast<float*>(smem_raw);
+  constexpr bool kLanes = Body::kChainLanes;
   float* psm = xs + 2 * stage_floats;
-  double* red = reinterpret_cast<double*>(psm + (((size_t)np * CG + 3) & ~(size_t)3));
+  double* red = reinterpret_cast<double*>(psm + skel_param_floats(np, CG, kLanes));
   uint64_t* bars = reinterpret_cast<uint64_t*>(red + (size_t)kWarps * G * W);
   uint32_t* s_ticket = reinterpret_cast<uint32_t*>(bars + 2);
 
-  for (int i = tid; i < np * CG; i += kThreads) {
-    const int p = i / CG, cl = i % CG;
-    psm[i] = E.params[(size_t)p * E.C_pad + (size_t)cb * CG + cl];
+  if constexpr (!kLanes) {
+    for (int i = tid; i < np * CG; i += kThreads) {
+      const int p = i / CG, cl = i % CG;
+      psm[i] = E.params[(size_t)p * E.C_pad + (size_t)cb * CG + cl];
+    }
   }
 
   const int t0 = ob * tiles_per_cta;
@@ -448,7 +460,10 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
       tma_load_2d(xs + s * stage_floats, tmap, &bars[s], (t0 + s) * T, 0);
     }
   }
-  body.begin(psm + wc * G, CG);
+  if constexpr (kLanes)
+    body.begin_lanes(E.params + (size_t)cb * CG + (size_t)wc * 32 + lane, E.C_pad);
+  else
+    body.begin(psm + wc * G, CG);
 
   for (int k = 0; k < nt; ++k) {
     const int st = k & 1;
@@ -457,7 +472,24 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
       if (lane == 0) atomicOr(E.err, DEV_ERR_TMA_TIMEOUT);
     }
     const int obs0 = (t0 + k) * T;
-    if constexpr (Body::kObsPerEval == 2) {
+    if constexpr (kLanes) {
+      // quads of observations (o .. o + 3), the WO warps of a chain group
+      // taking every WO-th quad; all lanes read the same addresses
+      for (int o = 4 * wo; o < T; o += 4 * WO) {
+        const long long left = (long long)E.n_obs - (obs0 + o);
+        if (left <= 0) break;
+        const int nv = left >= 4 ? 4 : (int)left;
+        body.eval4(tile + o, nv);
+        if (phase == PH_POINTWISE) {
+          const int c = cb * CG + wc * 32 + lane;
+          if (c < E.n_points) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)  // constant indices keep the values in registers
+              if (q < nv) E.pointwise[(size_t)c * E.n_obs + obs0 + o + q] = (double)body.last4(q);
+          }
+        }
+      }
+    } else if constexpr (Body::kObsPerEval == 2) {
       // observation pairs (2 pi, 2 pi + 1); T is even, so each pair is
       // 8-byte aligned in every column of the tile
       auto pair = [&](int pi) {
@@ -523,17 +555,21 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   // tree), then the WO warps that share a chain group, in warp order.
 #pragma unroll
   for (int w = 0; w < W; ++w) {
-    double tot[G];
+    if constexpr (kLanes) {  // each lane holds its own chain's sum (G == 32)
+      red[((size_t)warp * G + lane) * W + w] = body.total(0, w);
+    } else {
+      double tot[G];
 #pragma unroll
-    for (int g = 0; g < G; ++g) tot[g] = body.total(g, w);
+      for (int g = 0; g < G; ++g) tot[g] = body.total(g, w);
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
+      for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
-      for (int g = 0; g < G; ++g) tot[g] += __shfl_down_sync(0xffffffffu, tot[g], off);
-    }
-    if (lane == 0) {
+        for (int g = 0; g < G; ++g) tot[g] += __shfl_down_sync(0xffffffffu, tot[g], off);
+      }
+      if (lane == 0) {
 #pragma unroll
-      for (int g = 0; g < G; ++g) red[((size_t)warp * G + g) * W + w] = tot[g];
+        for (int g = 0; g < G; ++g) red[((size_t)warp * G + g) * W + w] = tot[g];
+      }
     }
   }
   __syncthreads();

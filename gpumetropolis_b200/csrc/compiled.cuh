@@ -37,6 +37,7 @@ struct Acc64 {
 
 template <int G, bool GRAD>
 struct JitBody {
+  static constexpr bool kChainLanes = false;
   static constexpr int kObsPerEval = 1;
   float p[G][GM_NP];
   float h[G][GM_NH];
@@ -113,6 +114,7 @@ struct JitBody {
 // values are kept as broadcast pairs (p, p) so every instruction is paired.
 template <int G>
 struct JitBody2 {
+  static constexpr bool kChainLanes = false;
   static constexpr int kObsPerEval = 2;
   static constexpr int kTileObs = GM_T;
   float2 pp[G][GM_NP];
@@ -186,8 +188,63 @@ struct JitBody2 {
   }
 };
 using ValueBody = JitBody2<GM_G>;
+constexpr int kValueG = GM_G;
+#elif GM_LANES
+// Value body for wide models, one chain per lane: the lanes of a warp are 32
+// chains, so every lane reads the same observation values (a shared-memory
+// broadcast) and one 16-byte load per column serves four observations of all
+// 32 chains.  Parameters come straight from the [np][C_pad] evaluation
+// points; terms are added in FP32 blocks of eight observations, each block
+// into an FP64 sum.
+struct JitLanes {
+  static constexpr bool kChainLanes = true;
+  static constexpr int kObsPerEval = 4;
+  static constexpr int kTileObs = GM_T;
+  float p[GM_NP];
+  float h[GM_NH];
+  double s;
+  float part;
+  int cnt;  // quads in the open FP32 block
+  float lastv[4];
+
+  __device__ __forceinline__ void begin_lanes(const float* pc, int C_pad) {
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) p[j] = pc[(size_t)j * C_pad];
+    gm_hoist(p, h);
+    s = 0.0;
+    part = 0.0f;
+    cnt = 0;
+  }
+
+  // Observations xo .. xo + 3, of which the first nv are valid.
+  __device__ __forceinline__ void eval4(const float* xo, int nv) {
+    float v[4];
+    gm_value4l(xo, p, h, v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) lastv[k] = v[k];
+    if (nv == 4) {
+      part = ((part + lastv[0]) + lastv[1]) + (lastv[2] + lastv[3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (k < nv) part += lastv[k];
+    }
+    if (++cnt == 2) {
+      s += (double)part;
+      part = 0.0f;
+      cnt = 0;
+    }
+  }
+
+  __device__ __forceinline__ float last4(int k) const { return lastv[k]; }
+  __device__ __forceinline__ void end() {}
+  __device__ __forceinline__ double total(int, int) const { return s + (double)part; }
+};
+using ValueBody = JitLanes;
+constexpr int kValueG = 32;  // chains per warp group, as the host counts them
 #else
 using ValueBody = JitBody<GM_G, false>;
+constexpr int kValueG = GM_G;
 #endif
 
 #if GM_PAIRG
@@ -197,6 +254,7 @@ using ValueBody = JitBody<GM_G, false>;
 // valid runs the scalar gm_value_grad on that observation.
 template <int G>
 struct JitBody2G {
+  static constexpr bool kChainLanes = false;
   static constexpr int kObsPerEval = 2;
   static constexpr int kTileObs = 0;  // not unrolled: the body is large
   float2 pp[G][GM_NP];
@@ -329,7 +387,8 @@ extern "C" __global__ void __launch_bounds__(gpum::kThreads, GM_VALUE_MIN_CTAS)
 gm_iter_value(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum::ChainArgs A,
               int phase) {
   gpum::ValueBody body;
-  gpum::run_iteration<GM_G, 1, gpum::ValueBody, gpum::JitPrior>(&tmap, E, A, phase, body);
+  gpum::run_iteration<gpum::kValueG, 1, gpum::ValueBody, gpum::JitPrior>(&tmap, E, A, phase,
+                                                                          body);
 }
 
 // Value + gradient kernel: gradient batches and MALA steps.

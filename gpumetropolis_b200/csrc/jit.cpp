@@ -193,9 +193,15 @@ void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pa
   *GG = *pairg ? 1 : (np <= 16 ? 2 : 1);
 }
 
+bool jit_value_lanes(const GenModel& gm, bool pair) {
+  return !pair && gm.n_data_ops == 0 && gm.np + std::max(gm.n_hoist, 1) <= 160;
+}
+
 std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg) {
+  const bool lanes = jit_value_lanes(gm, pair);
   std::string s;
   s += "#include \"device.cuh\"\n";
+  s += "#define GM_LANES " + std::string(lanes ? "1" : "0") + "\n";
   s += "#define GM_PAIR " + std::string(pair ? "1" : "0") + "\n";
   s += "#define GM_PAIRG " + std::string(pairg ? "1" : "0") + "\n";
   s += "#define GM_G " + std::to_string(G) + "\n";
@@ -204,8 +210,10 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg)
   // hoisted values) <= 40 broadcast pairs) fit in 80 registers without
   // spills: three CTAs, 24 warps per SM.
   const int w = gm.np + std::max(gm.n_hoist, 1);
+  // Chain lanes: two CTAs while parameters + hoisted values stay within 80.
   s += "#define GM_VALUE_CTAS " +
-       std::to_string(pair ? (G == 2 && G * w <= 40 ? 3 : 2) : 1) + "\n";
+       std::to_string(pair ? (G == 2 && G * w <= 40 ? 3 : 2) : (lanes && w <= 80 ? 2 : 1)) +
+       "\n";
   s += "namespace gpum {\n";
   s += gm.source;
   s += "}  // namespace gpum\nusing namespace gpum;\n";
@@ -255,6 +263,7 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.GG = GG;
   e.model.pair = pair;
   e.model.pairg = pairg;
+  e.model.lanes = jit_value_lanes(gm, pair);
   e.model.np = gm.np;
   e.model.compile_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

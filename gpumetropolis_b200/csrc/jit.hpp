@@ -18,6 +18,7 @@ struct CompiledModel {
   int G = 1, GG = 1;                // chains per thread of each kernel
   bool pair = false;                // value kernel evaluates observation pairs
   bool pairg = false;               // gradient kernel evaluates observation pairs
+  bool lanes = false;               // value kernel: one chain per lane (G counts 32)
   int np = 0;
   double compile_seconds = 0.0;
 };
@@ -26,6 +27,12 @@ struct CompiledModel {
 // value kernel uses the paired-observation body, by parameter and hoisted
 // value counts.
 void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pairg);
+
+// Whether the value kernel maps chains to lanes (wide models: every lane
+// reads the same observation values, broadcast): models the paired body does
+// not take, without data-only operations (each lane would repeat them), and
+// with parameters + hoisted values that fit the registers.
+bool jit_value_lanes(const GenModel& gm, bool pair);
 
 // Returns 0 and a loaded model, or 1 with a message (NVRTC missing, compile
 // error, load error).

@@ -11,6 +11,7 @@ namespace gpum {
 
 template <int G, int D>
 struct InterpBody {
+  static constexpr bool kChainLanes = false;
   static constexpr int kObsPerEval = 1;
   const EvalProg& pg;
   const float* pc0;

@@ -47,13 +47,18 @@ def _normals(seed, c, n, start=0):
     return np.array(z), k
 
 
-def test_single_step_decisions_match(gpu):
-    w = W.make("logistic", n_obs=4096)
+@pytest.mark.parametrize("name,n_obs,C,step", [("logistic", 4096, 512, 0.01),
+                                                ("student_t", 1031, 300, 0.006)])
+def test_single_step_decisions_match(gpu, name, n_obs, C, step):
+    # student_t (65 parameters) runs the chain-lane value body: 300 chains are
+    # two ragged blocks of 256 chains
+    w = W.make(name, n_obs=n_obs)
     m = w.model
-    C, seed = 512, 11
+    seed = 11
     rng = np.random.default_rng(0)
-    init = w.truth["beta"] + rng.normal(0, 0.02, (C, m.n_params))
-    sd = np.full((C, m.n_params), 0.01)
+    centre = w.truth["beta"] if name == "logistic" else np.append(w.truth["beta"], np.log(1.5))
+    init = centre + rng.normal(0, 0.02 if name == "logistic" else 0.002, (C, m.n_params))
+    sd = np.full((C, m.n_params), step)
     temps = np.where(np.arange(C) % 2 == 0, 1.0, 3.0)
     d_g, a_g, l_g = gpu.run(*_model_args(w), init, sd, temps, 1, seed, 0)
     d_o, a_o, l_o = O.run(*_model_args(w), init, sd, temps, 1, seed, 0)
