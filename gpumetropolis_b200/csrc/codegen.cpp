@@ -286,6 +286,19 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   if (root >= 0 && is_h(root)) need_h.insert(root);
   if (root >= 0 && is_d(root)) need_d.insert(root);
   for (int i : need_h) hslot[i] = out->n_hoist++;
+  // Division by a parameter-only value (exp(ls), a parameter, ...): the value
+  // functions multiply by its reciprocal, hoisted once per chain into a slot
+  // of its own (the gradient keeps the division and its adjoints).
+  std::vector<int> rslot(N, -1);
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || g.n[i].dep != (DEP_P | DEP_D) || g.n[i].op != O_DIV) continue;
+    const int b = g.n[i].b;
+    if (b >= 0 && g.n[b].dep == DEP_P && rslot[b] < 0) rslot[b] = out->n_hoist++;
+  }
+  auto recip = [&](int i) {  // hoisted reciprocal slot of node i's divisor, or -1
+    const Node& x = g.n[i];
+    return x.op == O_DIV && x.b >= 0 ? rslot[x.b] : -1;
+  };
   for (int i : need_d) dslot[i] = out->n_data++;
   for (int i = 0; i < N; ++i) {
     const Node& x = g.n[i];
@@ -389,6 +402,8 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
        "float* __restrict__ h) {\n";
   emit_hoist_body(s);
   for (int i : need_h) s << "  h[" << hslot[i] << "] = " << name[i] << ";\n";
+  for (int i = 0; i < N; ++i)
+    if (rslot[i] >= 0) s << "  h[" << rslot[i] << "] = 1.0f / " << name[i] << ";\n";
   s << "  (void)p; (void)h;\n}\n";
 
   // Per-observation forward code (`fused`: with the softplus rewrite, for
@@ -401,7 +416,9 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       o << "  const float " << name[i] << " = "
         << (fused && softplus_arg[i] >= 0
                 ? "gm_softplus(" + ref_obs(softplus_arg[i]) + ")"
-                : op_expr(g, i, ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "", true))
+                : fused && recip(i) >= 0
+                      ? "(" + ref_obs(x.a) + " * h[" + std::to_string(recip(i)) + "])"
+                      : op_expr(g, i, ref_obs(x.a), x.b >= 0 ? ref_obs(x.b) : "", true))
         << ";\n";
       ++out->n_fwd;
     }
@@ -454,6 +471,7 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       for (int k = 0; k < 4; ++k)
         s << "  const float " << name[i] << "_" << k << " = "
           << (softplus_arg[i] >= 0 ? "gm_softplus(" + a[k] + ")"
+              : recip(i) >= 0      ? "(" + a[k] + " * h[" + std::to_string(recip(i)) + "])"
                                    : op_expr(g, i, a[k], b[k], true))
           << ";\n";
     }
@@ -528,6 +546,8 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
             ref2(softplus_arg[x.b]) + ")";
       } else if (softplus_arg[i] >= 0) {
         e = "gm2_softplus(" + ref2(softplus_arg[i]) + ")";
+      } else if (recip(i) >= 0) {
+        e = "gm2_mul(" + ref2(x.a) + ", hh[" + std::to_string(recip(i)) + "])";
       } else if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
         const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
         e = "gm2_fma(" + ref2(g.n[m].a) + ", " + ref2(g.n[m].b) + ", " + ref2(o) + ")";

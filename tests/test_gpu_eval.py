@@ -145,5 +145,7 @@ def test_session_reuse_and_determinism(gpu):
         b = s.loglik_batch(pts)
         c = s.loglik_batch(pts[:3])
     assert np.array_equal(a, b)        # fixed-order reductions: bitwise repeatable
-    # another launch geometry partitions the observations differently
-    np.testing.assert_allclose(a[:3], c, rtol=1e-9)
+    # another launch geometry partitions the observations differently, so
+    # the FP32 blocks (about 1,250 here, each rounding ~1e-6 of a ~20-unit
+    # partial) differ: ~4e-5 absolute on a ~2.7e4 total, ~1.5e-9 relative
+    np.testing.assert_allclose(a[:3], c, rtol=5e-9)
