@@ -153,6 +153,23 @@ struct Geometry {
 
 }  // namespace
 
+// Tensor map of column-major f32 data (n_cols columns of leading dimension
+// ld >= n_obs, a multiple of 4): boxes of T observations x all columns.
+void encode_cols_tmap(float* base, uint64_t n_obs, uint32_t n_cols, int64_t ld, int T,
+                      TmapDesc* out) {
+  CUtensorMap tm;
+  cuuint64_t gdim[2] = {(cuuint64_t)n_obs, (cuuint64_t)n_cols};
+  cuuint64_t gstride[1] = {(cuuint64_t)ld * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)T, (cuuint32_t)n_cols};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, gdim, gstride, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    throw Failure{GPUM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")"};
+  std::memcpy(out, &tm, sizeof tm);
+}
+
 struct gpum_b200_session {
   cudaStream_t stream = nullptr;
   UProg ll;
@@ -171,6 +188,13 @@ struct gpum_b200_session {
   int64_t ld = 0;
   DBuf<float> data;
   TmapDesc tmap;
+  // The compiled engine's data when its model materializes data-only
+  // operations (cm.n_mat > 0): the data columns, then one column per
+  // operation, with its own tile height and tensor map.
+  DBuf<float> data_c;
+  TmapDesc tmap_c;
+  int T_c = 256;
+  uint32_t ncols_c = 0;
   DBuf<uint32_t> d_prior_code;
   DBuf<double> d_prior_consts;
   DBuf<uint32_t> d_err;
@@ -234,9 +258,29 @@ struct gpum_b200_session {
       cm_error = e.empty() ? "compiled engine unavailable" : e;
       return false;
     }
+    if (cm.n_mat > 0 && ncols > 0 && n_obs > 0) materialize();
     cm_ready = true;
     return true;
   }
+
+  // Extra columns for the compiled model's data-only operations, computed
+  // once on the device by the model's own gm_materialize.
+  void materialize() {
+    ncols_c = ncols + (uint32_t)cm.n_mat;
+    T_c = tile_obs(ncols_c);
+    data_c.ensure((size_t)ld * ncols_c);
+    GPUM_CK(cudaMemcpyAsync(data_c.p, data.p, sizeof(float) * (size_t)ld * ncols,
+                            cudaMemcpyDeviceToDevice, stream));
+    float* cols = data_c.p;
+    long long nobs = (long long)n_obs, lld = (long long)ld;
+    void* args[] = {(void*)&cols, (void*)&nobs, (void*)&lld};
+    GPUM_CK(cudaLaunchKernel((const void*)cm.k_mat, dim3((unsigned)((n_obs + 255) / 256)),
+                             dim3(256), args, 0, stream));
+    ++launches;
+    encode_cols_tmap(data_c.p, n_obs, ncols_c, ld, T_c, &tmap_c);
+    GPUM_CK(cudaStreamSynchronize(stream));
+  }
+  bool ext(const KernelChoice& k) const { return k.compiled && cm.n_mat > 0; }
 
   KernelChoice choose(bool need_grad) {
     KernelChoice k;
@@ -271,8 +315,10 @@ struct gpum_b200_session {
     g.CG = g.WC * g.G;
     g.NCB = (n + g.CG - 1) / g.CG;
     g.C_pad = g.NCB * g.CG;
-    g.ntiles = (int)((n_obs + T - 1) / T);
-    g.smem = skel_smem_bytes(T, (int)ncols, (int)np, g.CG, g.G, k.W, k.lanes);
+    const int Tk = ext(k) ? T_c : T;
+    g.ntiles = (int)((n_obs + Tk - 1) / Tk);
+    g.smem = skel_smem_bytes(Tk, (int)(ext(k) ? ncols_c : ncols), (int)np, g.CG, g.G, k.W,
+                             k.lanes);
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
     if (occ < 1) occ = 1;
@@ -308,8 +354,8 @@ struct gpum_b200_session {
     GPUM_CK(cudaMemsetAsync(tickets.p, 0, sizeof(uint32_t) * geo.NCB, stream));
     E = EvalArgs{};
     E.n_obs = (int)n_obs;
-    E.ncols = (int)ncols;
-    E.T = T;
+    E.ncols = (int)(ext(kc) ? ncols_c : ncols);
+    E.T = ext(kc) ? T_c : T;
     E.ntiles = geo.ntiles;
     E.tiles_per_cta = geo.tiles_per_cta;
     E.CG = geo.CG;
@@ -359,7 +405,7 @@ struct gpum_b200_session {
   void launch_with(const Geometry& g, EvalArgs& e, int phase) {
     const dim3 grid(g.NCB, g.NOB);
     if (kc.compiled) {
-      void* args[] = {(void*)&tmap, (void*)&e, (void*)&A, (void*)&phase};
+      void* args[] = {(void*)(ext(kc) ? &tmap_c : &tmap), (void*)&e, (void*)&A, (void*)&phase};
       GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, g.smem, stream));
     } else {
       launch_interp(variant, grid, g.smem, stream, *prog, tmap, e, A, phase);
@@ -495,18 +541,7 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
       GPUM_CK(cudaGetLastError());
     }
     GPUM_CK(cudaStreamSynchronize(s->stream));
-    CUtensorMap tm;
-    cuuint64_t gdim[2] = {(cuuint64_t)n_obs, (cuuint64_t)n_cols};
-    cuuint64_t gstride[1] = {(cuuint64_t)s->ld * sizeof(float)};
-    cuuint32_t box[2] = {(cuuint32_t)s->T, (cuuint32_t)n_cols};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->data.p, gdim, gstride,
-                             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS)
-      throw Failure{GPUM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")"};
-    std::memcpy(&s->tmap, &tm, sizeof tm);
+    encode_cols_tmap(s->data.p, n_obs, n_cols, s->ld, s->T, &s->tmap);
   }
   return s.release();
 }

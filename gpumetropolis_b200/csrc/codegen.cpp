@@ -300,6 +300,14 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     return x.op == O_DIV && x.b >= 0 ? rslot[x.b] : -1;
   };
   for (int i : need_d) dslot[i] = out->n_data++;
+  // Data-only operations that per-observation code reads (lgamma(y + 1),
+  // x^2, ...) are computed once per session into extra f32 columns n_cols,
+  // n_cols + 1, ... (gm_mat_obs below); every per-observation function then
+  // loads them like data columns.  col_of(i): the column of a data value.
+  std::vector<int> mcol(N, -1);
+  for (int i : need_d)
+    if (g.n[i].op != O_D) mcol[i] = (int)n_cols + out->n_mat++;
+  auto col_of = [&](int i) { return g.n[i].op == O_D ? (int)g.n[i].arg : mcol[i]; };
   for (int i = 0; i < N; ++i) {
     const Node& x = g.n[i];
     if (x.op == O_C) name[i] = flit(x.c);
@@ -340,20 +348,31 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   s << "#define GM_ND " << std::max(1, out->n_data) << "\n";
   // The tile height is fixed by the column count, so column offsets are
   // compile-time immediates in the generated loads.
-  s << "#define GM_T " << tile_obs(n_cols) << "\n";
+  s << "#define GM_T " << tile_obs(n_cols + (uint32_t)out->n_mat) << "\n";
+  s << "#define GM_NCOLS " << n_cols << "\n";
+  s << "#define GM_NMAT " << std::max(1, out->n_mat) << "\n";
+  s << "#define GM_HAS_MAT " << (out->n_mat > 0 ? 1 : 0) << "\n";
 
-  // gm_data: data leaves and data-only subexpressions, per observation.
-  s << "__device__ __forceinline__ void gm_data(const float* __restrict__ xo, int T, "
-       "float* __restrict__ d) {\n";
+  // gm_mat_obs: the materialized data-only operations of one observation
+  // from its data columns (x[j * ld]), computed as the per-observation code
+  // would compute them.
+  s << "__device__ __forceinline__ void gm_mat_obs(const float* __restrict__ x, long long ld, "
+       "float* __restrict__ m) {\n";
   for (int i = 0; i < N; ++i) {
     if (!live[i] || !is_d(i)) continue;
     const Node& x = g.n[i];
-    std::string e = x.op == O_D ? "xo[" + std::to_string(x.arg) + " * GM_T]"
+    std::string e = x.op == O_D ? "x[" + std::to_string(x.arg) + " * ld]"
                                 : op_expr(g, i, name[x.a], x.b >= 0 ? name[x.b] : "", true);
     s << "  const float " << name[i] << " = " << e << ";\n";
-    if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
-    if (x.op != O_D) ++out->n_data_ops;
+    if (mcol[i] >= 0) s << "  m[" << mcol[i] - (int)n_cols << "] = " << name[i] << ";\n";
   }
+  s << "  (void)x; (void)ld; (void)m;\n}\n";
+
+  // gm_data: the data values per-observation code reads, one observation.
+  s << "__device__ __forceinline__ void gm_data(const float* __restrict__ xo, int T, "
+       "float* __restrict__ d) {\n";
+  for (int i : need_d)
+    s << "  d[" << dslot[i] << "] = xo[" << col_of(i) << " * GM_T];\n";
   s << "  (void)xo; (void)T; (void)d;\n}\n";
 
   // gm_data4l: four consecutive observations xo .. xo + 3 for the chain-lane
@@ -363,29 +382,11 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   s << "__device__ __forceinline__ void gm_data4l(const float* __restrict__ xo, "
        "float* __restrict__ d0, float* __restrict__ d1, float* __restrict__ d2, "
        "float* __restrict__ d3) {\n";
-  for (int i = 0; i < N; ++i) {
-    if (!live[i] || !is_d(i)) continue;
-    const Node& x = g.n[i];
-    if (x.op == O_D) {
-      s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
-        << x.arg << " * GM_T);\n";
-      for (int k = 0; k < 4; ++k)
-        s << "  const float " << name[i] << "_" << k << " = q_" << name[i] << "."
-          << "xyzw"[k] << ";\n";
-    } else {
-      for (int k = 0; k < 4; ++k) {
-        auto arg = [&](int c) -> std::string {
-          if (c < 0) return "";
-          if (g.n[c].op == O_C) return name[c];
-          return name[c] + "_" + std::to_string(k);
-        };
-        s << "  const float " << name[i] << "_" << k << " = "
-          << op_expr(g, i, arg(x.a), arg(x.b), true) << ";\n";
-      }
-    }
-    if (dslot[i] >= 0)
-      for (int k = 0; k < 4; ++k)
-        s << "  d" << k << "[" << dslot[i] << "] = " << name[i] << "_" << k << ";\n";
+  for (int i : need_d) {
+    s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
+      << col_of(i) << " * GM_T);\n";
+    for (int k = 0; k < 4; ++k)
+      s << "  d" << k << "[" << dslot[i] << "] = q_" << name[i] << "." << "xyzw"[k] << ";\n";
   }
   s << "  (void)xo; (void)d0; (void)d1; (void)d2; (void)d3;\n}\n";
 
@@ -432,27 +433,21 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   // gm_value4l: four consecutive observations xo .. xo + 3 (the chain-lane
   // body), evaluated node by node in lockstep so that only the running
   // values stay live; each data column is loaded (16 bytes, a broadcast) at
-  // its first use.  Models with data-only operations take gm_data4l and
-  // gm_value four times instead.
+  // its first use (materialized data-only operations included).
   s << "__device__ __forceinline__ void gm_value4l(const float* __restrict__ xo, "
        "const float* __restrict__ p, const float* __restrict__ h, "
        "float* __restrict__ out) {\n";
-  if (out->n_data_ops > 0) {
-    s << "  float d0[GM_ND], d1[GM_ND], d2[GM_ND], d3[GM_ND];\n"
-         "  gm_data4l(xo, d0, d1, d2, d3);\n"
-         "  out[0] = gm_value(d0, p, h);\n  out[1] = gm_value(d1, p, h);\n"
-         "  out[2] = gm_value(d2, p, h);\n  out[3] = gm_value(d3, p, h);\n";
-  } else {
+  {
     std::vector<char> loaded(N, 0);
     auto ref4 = [&](int i, int k) -> std::string {
       const Node& x = g.n[i];
       if (x.op == O_C) return name[i];
       if (hslot[i] >= 0) return "h[" + std::to_string(hslot[i]) + "]";
       if (x.op == O_P) return name[i];
-      if (x.op == O_D) {
+      if (dslot[i] >= 0) {
         if (!loaded[i]) {
           s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
-            << x.arg << " * GM_T);\n";
+            << col_of(i) << " * GM_T);\n";
           loaded[i] = 1;
         }
         return "q_" + name[i] + "." + "xyzw"[k];
@@ -495,23 +490,11 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       if (dslot[i] >= 0) return "d[" + std::to_string(dslot[i]) + "]";
       return name[i];
     };
-    auto data_ref2 = [&](int i) -> std::string {  // inside gm_data2
-      const Node& x = g.n[i];
-      if (x.op == O_C) return "gm2(" + flit(x.c) + ")";
-      return name[i];
-    };
     s << "__device__ __forceinline__ void gm_data2(const float* __restrict__ xo, int T, "
          "float2* __restrict__ d) {\n";
-    for (int i = 0; i < N; ++i) {
-      if (!live[i] || !is_d(i)) continue;
-      const Node& x = g.n[i];
-      std::string e = x.op == O_D
-                          ? "*reinterpret_cast<const float2*>(xo + " + std::to_string(x.arg) +
-                                " * GM_T)"
-                          : op_expr2(g, i, data_ref2(x.a), x.b >= 0 ? data_ref2(x.b) : "");
-      s << "  const float2 " << name[i] << " = " << e << ";\n";
-      if (dslot[i] >= 0) s << "  d[" << dslot[i] << "] = " << name[i] << ";\n";
-    }
+    for (int i : need_d)
+      s << "  d[" << dslot[i] << "] = *reinterpret_cast<const float2*>(xo + " << col_of(i)
+        << " * GM_T);\n";
     s << "  (void)xo; (void)T; (void)d;\n}\n";
     auto fusable = [&](int c) {
       return c >= 0 && is_pd(c) && g.n[c].op == O_MUL && uses[c] == 1 && c != root;

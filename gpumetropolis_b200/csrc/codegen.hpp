@@ -26,7 +26,7 @@ struct GenModel {
   int n_hoist = 0;        // per-chain hoisted values
   int n_data = 0;         // per-observation data registers
   int n_fwd = 0;          // per-observation forward nodes
-  int n_data_ops = 0;     // data-only operations (not plain data leaves)
+  int n_mat = 0;          // data-only operations materialized as extra columns
   bool has_grad = false;
 };
 

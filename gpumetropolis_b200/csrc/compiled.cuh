@@ -373,6 +373,19 @@ struct JitPrior {
 
 }  // namespace gpum
 
+// Materialized data-only operations: one thread per observation reads the
+// data columns (column-major, leading dimension ld) and writes the operations'
+// values into columns GM_NCOLS .. GM_NCOLS + n_mat - 1 of the same array.
+extern "C" __global__ void gm_materialize(float* __restrict__ cols, long long n_obs,
+                                          long long ld) {
+  const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!GM_HAS_MAT || o >= n_obs) return;
+  float m[GM_NMAT];
+  gpum::gm_mat_obs(cols + o, ld, m);
+#pragma unroll
+  for (int k = 0; k < GM_NMAT; ++k) cols[(size_t)(GM_NCOLS + k) * ld + o] = m[k];
+}
+
 // Value-only kernel: PH_EVAL / PH_POINTWISE / RWM, DE and Cholesky steps.
 // CTAs per SM the registers must allow (GM_VALUE_CTAS from the host: three
 // for narrow paired models, 80 registers; two for the other paired ones).

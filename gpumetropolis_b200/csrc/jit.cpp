@@ -194,7 +194,7 @@ void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pa
 }
 
 bool jit_value_lanes(const GenModel& gm, bool pair) {
-  return !pair && gm.n_data_ops == 0 && gm.np + std::max(gm.n_hoist, 1) <= 160;
+  return !pair && gm.np + std::max(gm.n_hoist, 1) <= 160;
 }
 
 std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg) {
@@ -254,7 +254,8 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
     return 1;
   }
   if (cudaLibraryGetKernel(&e.model.k_value, e.lib, "gm_iter_value") != cudaSuccess ||
-      cudaLibraryGetKernel(&e.model.k_grad, e.lib, "gm_iter_grad") != cudaSuccess) {
+      cudaLibraryGetKernel(&e.model.k_grad, e.lib, "gm_iter_grad") != cudaSuccess ||
+      cudaLibraryGetKernel(&e.model.k_mat, e.lib, "gm_materialize") != cudaSuccess) {
     *err = "compiled model is missing its kernels";
     cudaLibraryUnload(e.lib);
     return 1;
@@ -264,6 +265,7 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.pair = pair;
   e.model.pairg = pairg;
   e.model.lanes = jit_value_lanes(gm, pair);
+  e.model.n_mat = gm.n_mat;
   e.model.np = gm.np;
   e.model.compile_seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -15,6 +15,8 @@ namespace gpum {
 struct CompiledModel {
   cudaKernel_t k_value = nullptr;   // gm_iter_value
   cudaKernel_t k_grad = nullptr;    // gm_iter_grad
+  cudaKernel_t k_mat = nullptr;     // gm_materialize (extra data columns)
+  int n_mat = 0;                    // materialized data-only operations
   int G = 1, GG = 1;                // chains per thread of each kernel
   bool pair = false;                // value kernel evaluates observation pairs
   bool pairg = false;               // gradient kernel evaluates observation pairs
@@ -30,8 +32,8 @@ void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pa
 
 // Whether the value kernel maps chains to lanes (wide models: every lane
 // reads the same observation values, broadcast): models the paired body does
-// not take, without data-only operations (each lane would repeat them), and
-// with parameters + hoisted values that fit the registers.
+// not take, with parameters + hoisted values that fit the registers (data-only
+// operations are materialized columns, so no lane repeats them).
 bool jit_value_lanes(const GenModel& gm, bool pair);
 
 // Returns 0 and a loaded model, or 1 with a message (NVRTC missing, compile

@@ -144,3 +144,37 @@ def test_softplus_rewrite_is_accurate(gpu):
     want = O.loglik_pointwise(m.loglik.code, m.loglik.consts, 1, x.reshape(-1, 1), 1, x.size,
                               a.reshape(-1, 1)).reshape(2, -1)
     np.testing.assert_allclose(tot, want.sum(axis=1), rtol=1e-6)
+
+
+def test_materialized_data_columns(gpu):
+    # log(y), x^2 and lgamma(y + 1) depend on the data only: the compiled
+    # engine computes them once per session into three extra columns (y + 1 is
+    # an intermediate, not a column) and loads them per observation; the
+    # interpreter on the same session reads the original columns
+    rng = np.random.default_rng(4)
+    n = 3001
+    y = rng.lognormal(0.5, 0.7, n)
+    x = rng.normal(0.0, 1.0, n)
+    m = gpum_model("~ -((log(y) - mu - b * x^2)^2) / (2 * exp(2 * ls)) - ls - log(y)"
+                   " - lgamma(y + 1)", ["mu", "b", "ls"], ["y", "x"])
+    data = np.column_stack([y, x])
+    pts = np.array([0.5, 0.0, math.log(0.7)]) + rng.normal(0, 0.05, (40, 3))
+    args = (m.loglik.code, m.loglik.consts, 3, data, 2, n)
+    ref = O.loglik_batch(*args, pts)
+    ref_pw = O.loglik_pointwise(*args, pts[:4])
+    ref_g = O.grad_batch(*args, pts[:6]).reshape(6, -1)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, 3, data, 2,
+                     n, engine=1) as s:
+        got = s.loglik_batch(pts)
+        pw = s.loglik_pointwise(pts[:4])
+        g = s.grad_batch(pts[:6]).reshape(6, -1)
+        s.set_engine(0)
+        got_i = s.loglik_batch(pts)
+        s.set_engine(1)
+        again = s.loglik_batch(pts)
+    np.testing.assert_allclose(got, ref, rtol=1e-6)
+    np.testing.assert_allclose(pw, ref_pw, rtol=2e-5, atol=2e-5)
+    err = np.linalg.norm(g - ref_g, axis=1) / np.linalg.norm(ref_g, axis=1)
+    assert err.max() < 2e-5, err
+    np.testing.assert_allclose(got_i, ref, rtol=1e-6)
+    np.testing.assert_array_equal(again, got)
