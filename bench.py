@@ -74,6 +74,11 @@ def _args():
                    help="instead of the headline line: time the Poisson (MALA), mixture (PT "
                         "ladders) and Student-t (DE) configurations at full size, one JSON "
                         "line each")
+    p.add_argument("--configs-obs-shift", type=int, default=0,
+                   help="with --configs: divide each configuration's observation count by "
+                        "2^S (small cases for profiler captures)")
+    p.add_argument("--configs-only", default="poisson,mixture,student_t",
+                   help="with --configs: comma-separated configurations to run")
     return p.parse_args()
 
 
@@ -520,8 +525,10 @@ def run_configs(a, n_warm=2, n_timed=6):
         raise SystemExit("gpum_b200: no usable sm_100 device")
     dev = torch.device("cuda", 0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    for name in ("poisson", "mixture", "student_t"):
-        w = W.make(name)
+    import inspect
+    for name in a.configs_only.split(","):
+        full = inspect.signature(W.ALL[name]).parameters["n_obs"].default
+        w = W.make(name, n_obs=max(1024, full >> max(a.configs_obs_shift, 0)))
         m = w.model
         C, N, npar = w.n_chains, w.n_obs, m.n_params
         rng = np.random.default_rng(7)

@@ -404,8 +404,12 @@ gm_iter_value(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpu
                                                                           body);
 }
 
-// Value + gradient kernel: gradient batches and MALA steps.
-extern "C" __global__ void __launch_bounds__(gpum::kThreads, 1)
+// Value + gradient kernel: gradient batches and MALA steps (GM_GRAD_CTAS
+// from the host: CTAs per SM the registers must allow).
+#ifndef GM_GRAD_CTAS
+#define GM_GRAD_CTAS 1
+#endif
+extern "C" __global__ void __launch_bounds__(gpum::kThreads, GM_GRAD_CTAS)
 gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum::ChainArgs A,
              int phase) {
   gpum::GradBody body;

@@ -210,6 +210,8 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg)
   // hoisted values) <= 40 broadcast pairs) fit in 80 registers without
   // spills: three CTAs, 24 warps per SM.
   const int w = gm.np + std::max(gm.n_hoist, 1);
+  // Paired gradient body of at most 25 parameters + hoisted values: two CTAs.
+  s += "#define GM_GRAD_CTAS " + std::to_string(pairg && w <= 25 ? 2 : 1) + "\n";
   // Chain lanes: two CTAs while parameters + hoisted values stay within 80.
   s += "#define GM_VALUE_CTAS " +
        std::to_string(pair ? (G == 2 && G * w <= 40 ? 3 : 2) : (lanes && w <= 80 ? 2 : 1)) +
