@@ -77,8 +77,9 @@ def _args():
     p.add_argument("--configs-obs-shift", type=int, default=0,
                    help="with --configs: divide each configuration's observation count by "
                         "2^S (small cases for profiler captures)")
-    p.add_argument("--configs-only", default="poisson,mixture,student_t",
-                   help="with --configs: comma-separated configurations to run")
+    p.add_argument("--configs-only", default="poisson,mixture,student_t,student_t_mala",
+                   help="with --configs: comma-separated configurations to run "
+                        "(student_t_mala: the Student-t configuration with MALA)")
     return p.parse_args()
 
 
@@ -526,7 +527,8 @@ def run_configs(a, n_warm=2, n_timed=6):
     dev = torch.device("cuda", 0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     import inspect
-    for name in a.configs_only.split(","):
+    for label in a.configs_only.split(","):
+        name = label.replace("_mala", "")
         full = inspect.signature(W.ALL[name]).parameters["n_obs"].default
         w = W.make(name, n_obs=max(1024, full >> max(a.configs_obs_shift, 0)))
         m = w.model
@@ -543,6 +545,10 @@ def run_configs(a, n_warm=2, n_timed=6):
             ladder = 16
             temps = np.tile(np.geomspace(1.0, 64.0, ladder), C // ladder)
             method = "rwm, 512 ladders of 16 geometric temperatures 1..64, device exchanges every 10"
+        elif label == "student_t_mala":
+            mode, jitter, step = _native.MODE_MALA, 0.01, 1e-4
+            centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
+            method = "mala (value + adjoint kernel gm_iter_grad, scalar wide-model body)"
         else:
             mode, jitter, step = _native.MODE_DE, 0.01, 1e-4
             centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
@@ -573,7 +579,7 @@ def run_configs(a, n_warm=2, n_timed=6):
         _, acc, last, _ = sess.fetch(want_draws=False)
         sess.close()
         print(json.dumps({
-            "config": name, "n_chains": C, "n_obs": N, "n_params": npar, "method": method,
+            "config": label, "n_chains": C, "n_obs": N, "n_params": npar, "method": method,
             "ms_per_iter": round(ms, 3), "chain_obs_per_s": C * N / (ms / 1e3),
             "all_finite": bool(np.all(np.isfinite(last))),
             "timing": f"{n_timed} single-iteration advances after {n_warm} warm-up, L2 "

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <set>
 #include <sstream>
@@ -342,6 +343,79 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     softplus_inner[j] = softplus_inner[k] = 1;
   }
 
+  // LOG(X + Y) with X, Y scaled exponentials (EXP(a), EXP(a) * c, c * EXP(a)
+  // or EXP(a) / c; c a parameter-only or constant weight that is positive by
+  // construction) feeding nothing else: the value functions evaluate it as
+  // logaddexp(a +- log c1, b +- log c2), the log weights hoisted per chain.
+  std::vector<int> pos_memo(N, -1);
+  std::function<bool(int)> positive = [&](int i) -> bool {
+    if (i < 0) return false;
+    if (pos_memo[i] >= 0) return pos_memo[i] != 0;
+    const Node& x = g.n[i];
+    bool r = false;
+    if (x.op == O_C) r = x.c > 0.0;
+    else if (x.dep != DEP_P) r = false;
+    else if (x.op == O_EXP) r = true;
+    else if (x.op == O_ADD || x.op == O_MUL || x.op == O_DIV) r = positive(x.a) && positive(x.b);
+    else if (x.op == O_SQRT) r = positive(x.a);
+    pos_memo[i] = r ? 1 : 0;
+    return r;
+  };
+  struct ScaledExp {
+    int expo = -1, exp_node = -1, weight = -1, sign = 1;
+  };
+  auto scaled_exp = [&](int X, ScaledExp* o) -> bool {
+    if (X < 0 || !is_pd(X) || uses[X] != 1) return false;
+    const Node& x = g.n[X];
+    auto is_exp = [&](int e) { return e >= 0 && g.n[e].op == O_EXP && is_pd(e) && uses[e] == 1; };
+    if (x.op == O_EXP && is_exp(X)) {
+      *o = ScaledExp{x.a, X, -1, 1};
+      return true;
+    }
+    if (x.op == O_MUL) {
+      for (int side = 0; side < 2; ++side) {
+        const int e = side ? x.b : x.a, c = side ? x.a : x.b;
+        if (is_exp(e) && positive(c)) {
+          *o = ScaledExp{g.n[e].a, e, c, 1};
+          return true;
+        }
+      }
+    }
+    if (x.op == O_DIV && is_exp(x.a) && positive(x.b)) {
+      *o = ScaledExp{g.n[x.a].a, x.a, x.b, -1};
+      return true;
+    }
+    return false;
+  };
+  std::vector<ScaledExp> lse_x(N), lse_y(N);
+  std::vector<char> lse(N, 0), lse_skip(N, 0);
+  std::vector<int> lslot(N, -1);
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || !is_pd(i) || g.n[i].op != O_LOG || softplus_arg[i] >= 0) continue;
+    const int j = g.n[i].a;
+    if (j < 0 || !is_pd(j) || g.n[j].op != O_ADD || uses[j] != 1) continue;
+    ScaledExp X, Y;
+    if (!scaled_exp(g.n[j].a, &X) || !scaled_exp(g.n[j].b, &Y)) continue;
+    lse[i] = 1;
+    lse_x[i] = X;
+    lse_y[i] = Y;
+    lse_skip[j] = lse_skip[g.n[j].a] = lse_skip[g.n[j].b] = 1;
+    lse_skip[X.exp_node] = lse_skip[Y.exp_node] = 1;
+    for (int w : {X.weight, Y.weight})
+      if (w >= 0 && g.n[w].op != O_C && lslot[w] < 0) lslot[w] = out->n_hoist++;
+  }
+  // The term a +- log c of a scaled exponential, for a given reference to a.
+  auto lse_term = [&](const ScaledExp& e, const std::string& a, bool paired,
+                      const std::string& hname) -> std::string {
+    if (e.weight < 0) return a;
+    const Node& w = g.n[e.weight];
+    const std::string lw =
+        w.op == O_C ? (paired ? "gm2(" + flit(std::log(w.c)) + ")" : flit(std::log(w.c)))
+                    : hname + "[" + std::to_string(lslot[e.weight]) + "]";
+    if (paired) return std::string(e.sign > 0 ? "gm2_add(" : "gm2_sub(") + a + ", " + lw + ")";
+    return "(" + a + (e.sign > 0 ? " + " : " - ") + lw + ")";
+  };
+
   std::ostringstream s;
   s << "#define GM_NP " << n_params << "\n";
   s << "#define GM_NH " << std::max(1, out->n_hoist) << "\n";
@@ -405,6 +479,8 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   for (int i : need_h) s << "  h[" << hslot[i] << "] = " << name[i] << ";\n";
   for (int i = 0; i < N; ++i)
     if (rslot[i] >= 0) s << "  h[" << rslot[i] << "] = 1.0f / " << name[i] << ";\n";
+  for (int i = 0; i < N; ++i)
+    if (lslot[i] >= 0) s << "  h[" << lslot[i] << "] = logf(" << name[i] << ");\n";
   s << "  (void)p; (void)h;\n}\n";
 
   // Per-observation forward code (`fused`: with the softplus rewrite, for
@@ -412,8 +488,15 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
   auto emit_fwd = [&](std::ostringstream& o, bool fused) {
     for (int i = 0; i < N; ++i) {
       if (!live[i] || !is_pd(i)) continue;
-      if (fused && softplus_inner[i]) continue;
+      if (fused && (softplus_inner[i] || lse_skip[i])) continue;
       const Node& x = g.n[i];
+      if (fused && lse[i]) {
+        o << "  const float " << name[i] << " = gm_logaddexp("
+          << lse_term(lse_x[i], ref_obs(lse_x[i].expo), false, "h") << ", "
+          << lse_term(lse_y[i], ref_obs(lse_y[i].expo), false, "h") << ");\n";
+        ++out->n_fwd;
+        continue;
+      }
       o << "  const float " << name[i] << " = "
         << (fused && softplus_arg[i] >= 0
                 ? "gm_softplus(" + ref_obs(softplus_arg[i]) + ")"
@@ -455,8 +538,19 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       return name[i] + "_" + std::to_string(k);
     };
     for (int i = 0; i < N; ++i) {
-      if (!live[i] || !is_pd(i) || softplus_inner[i]) continue;
+      if (!live[i] || !is_pd(i) || softplus_inner[i] || lse_skip[i]) continue;
       const Node& x = g.n[i];
+      if (lse[i]) {
+        std::string ta[4], tb[4];
+        for (int k = 0; k < 4; ++k) {
+          ta[k] = lse_term(lse_x[i], ref4(lse_x[i].expo, k), false, "h");
+          tb[k] = lse_term(lse_y[i], ref4(lse_y[i].expo, k), false, "h");
+        }
+        for (int k = 0; k < 4; ++k)
+          s << "  const float " << name[i] << "_" << k << " = gm_logaddexp(" << ta[k] << ", "
+            << tb[k] << ");\n";
+        continue;
+      }
       std::string a[4], b[4];
       for (int k = 0; k < 4; ++k) {  // loads first, so they precede the four uses
         const int ca = softplus_arg[i] >= 0 ? softplus_arg[i] : x.a;
@@ -520,10 +614,13 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
          "const float2* __restrict__ pp, const float2* __restrict__ hh) {\n";
     for (int i = 0; i < N; ++i) {
       if (!live[i] || !is_pd(i)) continue;
-      if (fused[i] || softplus_inner[i] || nsp_skip[i]) continue;
+      if (fused[i] || softplus_inner[i] || nsp_skip[i] || lse_skip[i]) continue;
       const Node& x = g.n[i];
       std::string e;
-      if (nsp_fold[i]) {
+      if (lse[i]) {
+        e = "gm2_logaddexp(" + lse_term(lse_x[i], ref2(lse_x[i].expo), true, "hh") + ", " +
+            lse_term(lse_y[i], ref2(lse_y[i].expo), true, "hh") + ")";
+      } else if (nsp_fold[i]) {
         const Node& m = g.n[x.a];
         e = "gm2_fma_nsoftplus(" + ref2(m.a) + ", " + ref2(m.b) + ", " +
             ref2(softplus_arg[x.b]) + ")";

@@ -214,7 +214,8 @@ __device__ __forceinline__ float gm_min_nan(float a, float b) {
 #define GM_SP_P2 2.187641105e-03f
 #define GM_SP_P3 5.471091135e-04f
 
-__device__ __forceinline__ float gm_softplus(float a) {
+// log1p(e^-|a|), the second addend of softplus(a).
+__device__ __forceinline__ float gm_log1p_nexp(float a) {
   const float na = fmaxf(-fabsf(a), -126.0f);  // e^-126 underflows to 0 anyway
   const float t = na * GM_SP_L2E;
   const float r = fmaf(t, -GM_SP_LN2_LO, fmaf(t, -GM_SP_LN2_HI, na));
@@ -226,7 +227,22 @@ __device__ __forceinline__ float gm_softplus(float a) {
   p = fmaf(p, q, GM_SP_P2);
   p = fmaf(p, q, GM_SP_P1);
   p = fmaf(p, q, GM_SP_P0);
-  return gm_max_nan(a, 0.0f) + fmaf(w, q * p, w);
+  return fmaf(w, q * p, w);
+}
+
+__device__ __forceinline__ float gm_softplus(float a) {
+  return gm_max_nan(a, 0.0f) + gm_log1p_nexp(a);
+}
+
+// log(e^p + e^q) = max(p, q) + log1p(e^-|p - q|), which codegen substitutes
+// for LOG(c1 EXP(a) + c2 EXP(b)) with positive parameter-only weights (p = a
+// + log c1, q = b + log c2): no exponential of the terms themselves, so no
+// FP32 underflow to log(0) where the reference's f64 sum is still finite.
+// NaN propagates; both terms -inf gives -inf.
+__device__ __forceinline__ float gm_logaddexp(float p, float q) {
+  const float m = gm_max_nan(p, q);
+  const float r = m + gm_log1p_nexp(p - q);
+  return m < -3.402823466e38f ? m : r;  // m is -inf
 }
 
 // ------------------------------------------------- paired FP32 arithmetic
@@ -279,6 +295,12 @@ __device__ __forceinline__ float2 gm2_log1p_nexp(float2 a) {
 __device__ __forceinline__ float2 gm2_softplus(float2 a) {
   const float2 m = make_float2(gm_max_nan(a.x, 0.0f), gm_max_nan(a.y, 0.0f));
   return __fadd2_rn(m, gm2_log1p_nexp(a));
+}
+// Paired gm_logaddexp.
+__device__ __forceinline__ float2 gm2_logaddexp(float2 p, float2 q) {
+  const float2 m = make_float2(gm_max_nan(p.x, q.x), gm_max_nan(p.y, q.y));
+  const float2 r = __fadd2_rn(m, gm2_log1p_nexp(__ffma2_rn(q, gm2(-1.0f), p)));
+  return make_float2(m.x < -3.402823466e38f ? m.x : r.x, m.y < -3.402823466e38f ? m.y : r.y);
 }
 // x * y - softplus(a) as FFMA2(x, y, min(-a, 0) - log1p(e^-|a|)), the NaN-
 // propagating min giving -max(a, 0): one rounding fewer than the product and

@@ -178,3 +178,24 @@ def test_materialized_data_columns(gpu):
     assert err.max() < 2e-5, err
     np.testing.assert_allclose(got_i, ref, rtol=1e-6)
     np.testing.assert_array_equal(again, got)
+
+
+def test_log_sum_of_exponentials_rewrite(gpu):
+    # log(c1 e^a + c2 e^b) with positive parameter-only weights is evaluated
+    # as logaddexp(a + log c1, b + log c2): finite where FP32 e^a and e^b both
+    # underflow (|y| far in the tails) and the oracle's f64 sum is finite
+    from gpumetropolis_b200 import workloads as W
+    w = W.make("mixture", n_obs=200)
+    m = w.model
+    y = np.concatenate([np.linspace(-40, 40, 801), w.data[:200, 0]])
+    pts = np.array([[math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)],
+                    [0.4, -1.0, 2.0, -0.3, 0.2]])
+    args = (m.loglik.code, m.loglik.consts, m.n_params, y.reshape(-1, 1), 1, y.size)
+    ref = O.loglik_pointwise(*args, pts).reshape(2, -1)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                     y.reshape(-1, 1), 1, y.size, engine=1) as s:
+        got = s.loglik_pointwise(pts).reshape(2, -1)
+        tot = s.loglik_batch(pts)
+    assert np.all(np.isfinite(ref)) and np.all(np.isfinite(got))
+    np.testing.assert_allclose(got, ref, rtol=2e-6, atol=1e-5)
+    np.testing.assert_allclose(tot, ref.sum(axis=1), rtol=1e-6)
