@@ -74,6 +74,12 @@ def _args():
                    help="instead of the headline line: time the Poisson (MALA), mixture (PT "
                         "ladders) and Student-t (DE) configurations at full size, one JSON "
                         "line each")
+    p.add_argument("--pt-da", action="store_true",
+                   help="instead of the headline line: exact vs surrogate delayed-acceptance "
+                        "ESS/s on the mixture configuration (512 ladders of 16 temperatures, "
+                        "device exchanges), one JSON line")
+    p.add_argument("--pt-da-warmup", type=int, default=400)
+    p.add_argument("--pt-da-iters", type=int, default=400)
     p.add_argument("--configs-obs-shift", type=int, default=0,
                    help="with --configs: divide each configuration's observation count by "
                         "2^S (small cases for profiler captures)")
@@ -587,10 +593,114 @@ def run_configs(a, n_warm=2, n_timed=6):
         del w
 
 
+def run_pt_da(a, K=16, every=10, seed=21):
+    """Mixture configuration, PT + surrogate delayed acceptance: 8192 chains
+    as 512 ladders of K geometric temperatures 1..64 with device exchanges
+    every `every` iterations; adaptive warmup (per-chain Robbins-Monro scales
+    and variances from device moments) whose second half records the exact
+    pairs (at most 2^18) for the 5-256-256-1 surrogate; then, from the same
+    state, exact sampling and two-stage sampling of equal length, timed by
+    the wall clock around each blocking run (draws copied back in both).
+    ESS: multi-chain over the 512 temperature-1 chains, per parameter."""
+    import torch
+
+    from gpumetropolis_b200 import _native, api
+    from gpumetropolis_b200 import adaptive as AD
+    from gpumetropolis_b200 import workloads as W
+    from gpumetropolis_b200.build import build
+    from gpumetropolis_b200.diagnostics import ess_pooled
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    torch.cuda.set_device(0)
+    w = W.make("mixture")
+    m = w.model
+    C, npar = w.n_chains, m.n_params
+    temps = np.tile(np.geomspace(1.0, 64.0, K), C // K)
+    cfg = dict(api.SURROGATE_DEFAULTS)
+    cfg["max_pairs"] = 1 << 18
+    call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, cfg)
+    try:
+        s = call.session
+        s.set_exchange(K, every)
+        rng = np.random.default_rng(seed)
+        centre = np.array([math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)])
+        cur = centre + rng.normal(0.0, 0.01, (C, npar))
+        sd = np.full((C, npar), 1e-3) * np.sqrt(temps)[:, None]
+        n_warm, n_samp = a.pt_da_warmup, a.pt_da_iters
+        call.record_at = n_warm // 2
+        nb = min(40, max(10, n_warm // 50), n_warm)
+        sizes = np.full(nb, n_warm // nb, dtype=np.int64)
+        sizes[-1] += n_warm - sizes.sum()
+        states = AD.WelfordDiag.init(C, npar, sd ** 2)
+        scales = np.ones(C)
+        t = time.perf_counter()
+        for b, n in enumerate(sizes, start=1):
+            mo, acc = call.run_moments(cur, sd, int(n), seed + b, temps, 0)
+            cur = mo.last
+            states.merge(mo.n, mo.chain_mean, mo.chain_m2)
+            scales = AD.robbins_monro_scale(scales, acc, b, npar)
+            sd = scales[:, None] * np.sqrt(np.maximum(states.variances(), 1e-12))
+        t_warm = time.perf_counter() - t
+        t = time.perf_counter()
+        call.start_da()
+        t_train = time.perf_counter() - t
+        if call.net is None:
+            print(json.dumps({"pt_da": {"used": False, "reason": call.info.get("reason")}}))
+            return
+
+        def timed(f):
+            s.sync()
+            t0 = time.perf_counter()
+            r = f()
+            return r, time.perf_counter() - t0
+
+        (d_ex, acc_ex, _), t_ex = timed(lambda: s.run(cur, sd, temps, n_samp, seed + 100, 0,
+                                                      rng=_native.RNG_PHILOX))
+        att, ok_ex, _ = s.exchange_stats()
+        e0 = call.exact_evals
+        (d_da, acc_da, _), t_da = timed(lambda: call(cur, sd, n_samp, seed + 200, temps, 0))
+        _, ok_da, _ = s.exchange_stats()
+        exact_frac = (call.exact_evals - e0) / (n_samp * C)
+        d_ex = d_ex.reshape((n_samp, C, npar), order="F").astype(np.float64)[:, ::K, :]
+        d_da = np.asarray(d_da, dtype=np.float64)[:, ::K, :]
+        e_ex = np.array([ess_pooled(d_ex[:, :, j]) for j in range(npar)])
+        e_da = np.array([ess_pooled(d_da[:, :, j]) for j in range(npar)])
+        mc_ex = d_ex.reshape(-1, npar).std(axis=0) / np.sqrt(e_ex)
+        mc_da = d_da.reshape(-1, npar).std(axis=0) / np.sqrt(e_da)
+        z = np.abs(d_ex.mean(axis=(0, 1)) - d_da.mean(axis=(0, 1))) / np.sqrt(mc_ex**2 + mc_da**2)
+        r_ex, r_da = e_ex.min() / t_ex, e_da.min() / t_da
+        with np.errstate(invalid="ignore", divide="ignore"):
+            x_ex = float(np.nansum(ok_ex) / max(np.sum(att), 1))
+            x_da = float(np.nansum(ok_da) / max(np.sum(att), 1))
+        print(json.dumps({"pt_da": {
+            "config": "mixture N=2^22, 8192 chains = 512 ladders x 16 geometric temperatures "
+                      "1..64, device exchanges every %d iterations, surrogate 5-%d-%d-1 on "
+                      "<= 2^18 warmup pairs" % (every, cfg["hidden"], cfg["hidden"]),
+            "warmup_iters": n_warm, "sampling_iters": n_samp, "warmup_s": round(t_warm, 3),
+            "train_s": round(t_train, 3), "surrogate": call.da_summary(),
+            "exact": {"seconds": round(t_ex, 3), "accept_cold": float(np.mean(acc_ex[::K])),
+                      "exchange_rate": x_ex, "ess_min": float(e_ex.min()),
+                      "ess_mean": float(e_ex.mean()), "ess_per_s_min": r_ex},
+            "da": {"seconds": round(t_da, 3), "accept_cold": float(np.mean(acc_da[::K])),
+                   "exchange_rate": x_da, "exact_fraction": exact_frac,
+                   "ess_min": float(e_da.min()), "ess_mean": float(e_da.mean()),
+                   "ess_per_s_min": r_da},
+            "gain_ess_per_s_min": r_da / r_ex,
+            "gain_ess_per_s_mean": float((e_da.mean() / t_da) / (e_ex.mean() / t_ex)),
+            "posterior_mean_max_z": float(z.max()),
+            "ess": "multi-chain over the 512 temperature-1 chains, per parameter"}}),
+            flush=True)
+    finally:
+        call.close()
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.pt_da:
+        run_pt_da(a)
     elif a.configs:
         run_configs(a)
     else:
