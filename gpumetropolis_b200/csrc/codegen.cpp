@@ -1,15 +1,22 @@
 // codegen.cpp -- bytecode -> CUDA C model functions (see codegen.hpp).
 //
 // Generated interface (all __device__ __forceinline__):
+//   void   gm_mat_obs(const float* x, long long ld, float* m)  materialized
+//          data-only operations of one observation (once per session)
 //   void   gm_data(const float* xo, int T, float* d)     per observation
+//   void   gm_data2(const float* xo, int T, float2* d)   observation pair
 //   void   gm_hoist(const float* p, float* h)            per chain
 //   float  gm_value(const float* d, const float* p, const float* h)
+//   float2 gm_value2(const float2* d, const float2* pp, const float2* hh)
+//   void   gm_value4l(const float* xo, const float* p, const float* h,
+//                     float* out)  four observations, chain-lane body
 //   float  gm_value_grad(d, p, h, float* gp, float* gh)  gp/gh accumulated
+//   float2 gm_value_grad2(d, pp, hh, float2* gp2, float2* gh2)
 //   void   gm_hoist_grad(const float* p, const float* gh, float* gp)
 //   double gm_prior(const double* p)
 //   double gm_prior_grad(const double* p, double* g)     g accumulated
 // `xo` points at this lane's observation in the shared-memory tile; column j
-// is xo[j*T].
+// is xo[j*GM_T] (data columns, then the materialized columns).
 #include "codegen.hpp"
 
 #include "program.hpp"
@@ -449,21 +456,6 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     s << "  d[" << dslot[i] << "] = xo[" << col_of(i) << " * GM_T];\n";
   s << "  (void)xo; (void)T; (void)d;\n}\n";
 
-  // gm_data4l: four consecutive observations xo .. xo + 3 for the chain-lane
-  // body, one 16-byte load per column (every lane reads the same address, a
-  // broadcast); xo is 16-byte aligned (a multiple of 4 observations into a
-  // tile whose column stride GM_T * 4 is a multiple of 128 bytes).
-  s << "__device__ __forceinline__ void gm_data4l(const float* __restrict__ xo, "
-       "float* __restrict__ d0, float* __restrict__ d1, float* __restrict__ d2, "
-       "float* __restrict__ d3) {\n";
-  for (int i : need_d) {
-    s << "  const float4 q_" << name[i] << " = *reinterpret_cast<const float4*>(xo + "
-      << col_of(i) << " * GM_T);\n";
-    for (int k = 0; k < 4; ++k)
-      s << "  d" << k << "[" << dslot[i] << "] = q_" << name[i] << "." << "xyzw"[k] << ";\n";
-  }
-  s << "  (void)xo; (void)d0; (void)d1; (void)d2; (void)d3;\n}\n";
-
   // gm_hoist: parameter-only subexpressions, once per chain.
   auto emit_hoist_body = [&](std::ostringstream& o) {
     for (int i = 0; i < N; ++i) {
@@ -515,8 +507,10 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
 
   // gm_value4l: four consecutive observations xo .. xo + 3 (the chain-lane
   // body), evaluated node by node in lockstep so that only the running
-  // values stay live; each data column is loaded (16 bytes, a broadcast) at
-  // its first use (materialized data-only operations included).
+  // values stay live; each data column is loaded (16 bytes, a broadcast: every
+  // lane reads the same address) at its first use, materialized data-only
+  // operations included.  xo is 16-byte aligned: a multiple of 4 observations
+  // into a tile whose column stride GM_T * 4 is a multiple of 128 bytes.
   s << "__device__ __forceinline__ void gm_value4l(const float* __restrict__ xo, "
        "const float* __restrict__ p, const float* __restrict__ h, "
        "float* __restrict__ out) {\n";
