@@ -604,32 +604,34 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       nsp_fold[i] = 1;
       nsp_skip[a] = nsp_skip[b] = 1;
     }
+    // The paired value of node i with the references R (rewrites included);
+    // value_node(i): whether the paired value function evaluates node i.
+    auto value_node = [&](int i) {
+      return live[i] && is_pd(i) && !fused[i] && !softplus_inner[i] && !nsp_skip[i] &&
+             !lse_skip[i];
+    };
+    auto value2_expr = [&](int i, const std::function<std::string(int)>& R) -> std::string {
+      const Node& x = g.n[i];
+      if (lse[i])
+        return "gm2_logaddexp(" + lse_term(lse_x[i], R(lse_x[i].expo), true, "hh") + ", " +
+               lse_term(lse_y[i], R(lse_y[i].expo), true, "hh") + ")";
+      if (nsp_fold[i]) {
+        const Node& m = g.n[x.a];
+        return "gm2_fma_nsoftplus(" + R(m.a) + ", " + R(m.b) + ", " + R(softplus_arg[x.b]) + ")";
+      }
+      if (softplus_arg[i] >= 0) return "gm2_softplus(" + R(softplus_arg[i]) + ")";
+      if (recip(i) >= 0) return "gm2_mul(" + R(x.a) + ", hh[" + std::to_string(recip(i)) + "])";
+      if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
+        const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
+        return "gm2_fma(" + R(g.n[m].a) + ", " + R(g.n[m].b) + ", " + R(o) + ")";
+      }
+      return op_expr2(g, i, R(x.a), x.b >= 0 ? R(x.b) : "");
+    };
     s << "__device__ __forceinline__ float2 gm_value2(const float2* __restrict__ d, "
          "const float2* __restrict__ pp, const float2* __restrict__ hh) {\n";
-    for (int i = 0; i < N; ++i) {
-      if (!live[i] || !is_pd(i)) continue;
-      if (fused[i] || softplus_inner[i] || nsp_skip[i] || lse_skip[i]) continue;
-      const Node& x = g.n[i];
-      std::string e;
-      if (lse[i]) {
-        e = "gm2_logaddexp(" + lse_term(lse_x[i], ref2(lse_x[i].expo), true, "hh") + ", " +
-            lse_term(lse_y[i], ref2(lse_y[i].expo), true, "hh") + ")";
-      } else if (nsp_fold[i]) {
-        const Node& m = g.n[x.a];
-        e = "gm2_fma_nsoftplus(" + ref2(m.a) + ", " + ref2(m.b) + ", " +
-            ref2(softplus_arg[x.b]) + ")";
-      } else if (softplus_arg[i] >= 0) {
-        e = "gm2_softplus(" + ref2(softplus_arg[i]) + ")";
-      } else if (recip(i) >= 0) {
-        e = "gm2_mul(" + ref2(x.a) + ", hh[" + std::to_string(recip(i)) + "])";
-      } else if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
-        const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
-        e = "gm2_fma(" + ref2(g.n[m].a) + ", " + ref2(g.n[m].b) + ", " + ref2(o) + ")";
-      } else {
-        e = op_expr2(g, i, ref2(x.a), x.b >= 0 ? ref2(x.b) : "");
-      }
-      s << "  const float2 " << name[i] << " = " << e << ";\n";
-    }
+    for (int i = 0; i < N; ++i)
+      if (value_node(i))
+        s << "  const float2 " << name[i] << " = " << value2_expr(i, ref2) << ";\n";
     const std::string root2 = root < 0 ? std::string("gm2(0.0f)") : ref2(root);
     s << "  (void)d; (void)pp; (void)hh;\n  return " << root2 << ";\n}\n";
 
