@@ -554,7 +554,7 @@ def run_configs(a, n_warm=2, n_timed=6):
         elif label == "student_t_mala":
             mode, jitter, step = _native.MODE_MALA, 0.01, 1e-4
             centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
-            method = "mala (value + adjoint kernel gm_iter_grad, scalar wide-model body)"
+            method = "mala (value + adjoint kernel gm_iter_grad, chain-lane body)"
         else:
             mode, jitter, step = _native.MODE_DE, 0.01, 1e-4
             centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])

@@ -294,8 +294,8 @@ struct gpum_b200_session {
                           " the compiled engine: " + cm_error};
       k.compiled = true;
       k.fn = need_grad ? (const void*)cm.k_grad : (const void*)cm.k_value;
-      k.lanes = !need_grad && cm.lanes;
-      k.G = need_grad ? cm.GG : (k.lanes ? 32 : cm.G);
+      k.lanes = need_grad ? cm.lanes_grad : cm.lanes;
+      k.G = k.lanes ? 32 : (need_grad ? cm.GG : cm.G);
       k.W = need_grad ? 1 + (int)np : 1;
     } else {
       k.compiled = false;

@@ -743,6 +743,98 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     s << "  (void)d; (void)p; (void)h; (void)gp; (void)gh;\n  return " << rootv << ";\n}\n";
   }
 
+  // gm_value_grad4l: values and adjoints of four consecutive observations
+  // xo .. xo + 3 for the chain-lane gradient body, node by node in lockstep
+  // (forward as gm_value_grad, no value rewrites).  The reverse sweep reloads
+  // the data columns it needs (gm_lds4v) rather than keeping the forward's
+  // loads live.  Observations k >= nv (a partial last quad) read observation
+  // 0's data and enter the sweep with adjoint 0.
+  s << "__device__ __forceinline__ void gm_value_grad4l(const float* __restrict__ xo, int nv, "
+       "const float* __restrict__ p, const float* __restrict__ h, float* __restrict__ gp, "
+       "float* __restrict__ gh, float* __restrict__ out) {\n";
+  {
+    std::vector<char> fl(N, 0), rl(N, 0);
+    auto data4 = [&](int i, int k, bool reload) -> std::string {
+      std::vector<char>& L = reload ? rl : fl;
+      const std::string q = (reload ? "r_" : "q_") + name[i];
+      if (!L[i]) {
+        s << "  const float4 " << q << " = "
+          << (reload ? "gm_lds4v(" : "*reinterpret_cast<const float4*>(") << "xo + " << col_of(i)
+          << " * GM_T);\n";
+        s << "  const float " << q << "_0 = " << q << ".x;\n";
+        for (int j = 1; j < 4; ++j)
+          s << "  const float " << q << "_" << j << " = nv > " << j << " ? " << q << "."
+            << "xyzw"[j] << " : " << q << ".x;\n";
+        L[i] = 1;
+      }
+      return q + "_" + std::to_string(k);
+    };
+    auto ref4g = [&](int i, int k, bool reload) -> std::string {
+      const Node& x = g.n[i];
+      if (x.op == O_C || x.op == O_P) return name[i];
+      if (hslot[i] >= 0) return "h[" + std::to_string(hslot[i]) + "]";
+      if (dslot[i] >= 0) return data4(i, k, reload);
+      return name[i] + "_" + std::to_string(k);
+    };
+    for (int i = 0; i < N; ++i) {
+      if (!live[i] || !is_pd(i)) continue;
+      const Node& x = g.n[i];
+      std::string a[4], b[4];
+      for (int k = 0; k < 4; ++k) {
+        a[k] = ref4g(x.a, k, false);
+        if (x.b >= 0) b[k] = ref4g(x.b, k, false);
+      }
+      for (int k = 0; k < 4; ++k)
+        s << "  const float " << name[i] << "_" << k << " = " << op_expr(g, i, a[k], b[k], true)
+          << ";\n";
+    }
+    for (int i = 0; i < N; ++i)
+      if (live[i] && is_pd(i))
+        for (int k = 0; k < 4; ++k) s << "  float g" << i << "_" << k << " = 0.0f;\n";
+    std::vector<char> has_adj(N, 0);
+    auto sink4 = [&](int c, const std::string* e) {
+      if (c < 0 || !(g.n[c].dep & DEP_P)) return;
+      for (int k = 0; k < 4; ++k) {
+        if (g.n[c].op == O_P) s << "  gp[" << g.n[c].arg << "] += " << e[k] << ";\n";
+        else if (hslot[c] >= 0) s << "  gh[" << hslot[c] << "] += " << e[k] << ";\n";
+        else
+          s << "  g" << c << "_" << k << (has_adj[c] ? " += " : " = ") << e[k] << ";\n";
+      }
+      if (g.n[c].op != O_P && hslot[c] < 0) has_adj[c] = 1;
+    };
+    if (root >= 0 && (g.n[root].dep & DEP_P)) {
+      std::string w[4];
+      for (int k = 0; k < 4; ++k)
+        w[k] = k == 0 ? "1.0f" : "(nv > " + std::to_string(k) + " ? 1.0f : 0.0f)";
+      if (is_pd(root)) {
+        for (int k = 0; k < 4; ++k) s << "  g" << root << "_" << k << " = " << w[k] << ";\n";
+        has_adj[root] = 1;
+      } else {
+        sink4(root, w);
+      }
+    }
+    for (int i = N - 1; i >= 0; --i) {
+      if (!live[i] || !is_pd(i)) continue;
+      const Node& x = g.n[i];
+      std::vector<std::vector<std::pair<int, std::string>>> ce(4);
+      for (int k = 0; k < 4; ++k) {
+        const std::string G = "g" + std::to_string(i) + "_" + std::to_string(k);
+        const std::string v = name[i] + "_" + std::to_string(k);
+        ce[k] = adjoints(g, i, G, v, ref4g(x.a, k, true), x.b >= 0 ? ref4g(x.b, k, true) : "",
+                         true);
+      }
+      for (size_t j = 0; j < ce[0].size(); ++j) {
+        std::string e[4];
+        for (int k = 0; k < 4; ++k) e[k] = ce[k][j].second;
+        sink4(ce[0][j].first, e);
+      }
+    }
+    for (int k = 0; k < 4; ++k)
+      s << "  out[" << k << "] = " << (root < 0 ? std::string("0.0f") : ref4g(root, k, false))
+        << ";\n";
+  }
+  s << "  (void)xo; (void)nv; (void)p; (void)h; (void)gp; (void)gh;\n}\n";
+
   // Chain rule through the hoisted parameter-only nodes, once per chain.
   s << "__device__ __forceinline__ void gm_hoist_grad(const float* __restrict__ p, "
        "const float* __restrict__ gh, float* __restrict__ gp) {\n";

@@ -397,6 +397,11 @@ __host__ __device__ inline size_t skel_smem_bytes(int T, int ncols, int np, int 
 //                                          the chains of a warp, and the body has
 //                                          begin_lanes(pc, C_pad), eval4(xo, nv),
 //                                          last4(k) instead of begin/eval/last
+//   bool kLanesAcc (chain lanes)           true: the body accumulates values
+//                                          1 .. W-1 in its own row of the
+//                                          reduction buffer (begin_lanes_acc(pc,
+//                                          C_pad, row), flush_tile() after each
+//                                          tile); only value 0 is written here
 //   void begin(const float* pc0, int CG)   pc0 = this thread's first chain in
 //                                          the [np][CG] parameter tile
 //   void eval(const float* xo, int T, bool valid)  one observation
@@ -460,10 +465,15 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
       tma_load_2d(xs + s * stage_floats, tmap, &bars[s], (t0 + s) * T, 0);
     }
   }
-  if constexpr (kLanes)
-    body.begin_lanes(E.params + (size_t)cb * CG + (size_t)wc * 32 + lane, E.C_pad);
-  else
+  if constexpr (kLanes) {
+    const float* pc = E.params + (size_t)cb * CG + (size_t)wc * 32 + lane;
+    if constexpr (Body::kLanesAcc)
+      body.begin_lanes_acc(pc, E.C_pad, red + ((size_t)warp * G + lane) * W);
+    else
+      body.begin_lanes(pc, E.C_pad);
+  } else {
     body.begin(psm + wc * G, CG);
+  }
 
   for (int k = 0; k < nt; ++k) {
     const int st = k & 1;
@@ -489,6 +499,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
           }
         }
       }
+      if constexpr (Body::kLanesAcc) body.flush_tile();
     } else if constexpr (Body::kObsPerEval == 2) {
       // observation pairs (2 pi, 2 pi + 1); T is even, so each pair is
       // 8-byte aligned in every column of the tile
@@ -556,7 +567,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
 #pragma unroll
   for (int w = 0; w < W; ++w) {
     if constexpr (kLanes) {  // each lane holds its own chain's sum (G == 32)
-      red[((size_t)warp * G + lane) * W + w] = body.total(0, w);
+      if (!Body::kLanesAcc || w == 0) red[((size_t)warp * G + lane) * W + w] = body.total(0, w);
     } else {
       double tot[G];
 #pragma unroll

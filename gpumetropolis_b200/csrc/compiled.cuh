@@ -198,6 +198,7 @@ constexpr int kValueG = GM_G;
 // into an FP64 sum.
 struct JitLanes {
   static constexpr bool kChainLanes = true;
+  static constexpr bool kLanesAcc = false;
   static constexpr int kObsPerEval = 4;
   static constexpr int kTileObs = GM_T;
   float p[GM_NP];
@@ -359,8 +360,106 @@ struct JitBody2G {
   }
 };
 using GradBody = JitBody2G<GM_GG>;
+constexpr int kGradG = GM_GG;
+#elif GM_LANESG
+// Value + gradient body for wide models, one chain per lane (the chain-lane
+// layout of JitLanes): gm_value_grad4l on four observations per broadcast
+// load; each lane's FP32 parameter adjoints of one tile are added into its
+// own FP64 row of the reduction buffer in shared memory (acc, W = 1 + np
+// values, zeroed at the start), hoisted-value adjoints into FP64 registers,
+// and pushed through the hoisted nodes once at the end.
+struct JitLanesG {
+  static constexpr bool kChainLanes = true;
+  static constexpr bool kLanesAcc = true;
+  static constexpr int kObsPerEval = 4;
+  static constexpr int kTileObs = GM_T;
+  float p[GM_NP];
+  float h[GM_NH];
+  float gp[GM_NP];
+  float gh[GM_NH];
+  double ghd[GM_NH];
+  double* acc;
+  double s;
+  float part;
+  int cnt;
+  float lastv[4];
+
+  __device__ __forceinline__ void begin_lanes_acc(const float* pc, int C_pad, double* row) {
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) {
+      p[j] = pc[(size_t)j * C_pad];
+      gp[j] = 0.0f;
+    }
+    gm_hoist(p, h);
+#pragma unroll
+    for (int j = 0; j < GM_NH; ++j) {
+      gh[j] = 0.0f;
+      ghd[j] = 0.0;
+    }
+    acc = row;
+    for (int w = 0; w < 1 + GM_NP; ++w) acc[w] = 0.0;
+    s = 0.0;
+    part = 0.0f;
+    cnt = 0;
+  }
+
+  __device__ __forceinline__ void eval4(const float* xo, int nv) {
+    float v[4];
+    if (nv == 4) gm_value_grad4l(xo, 4, p, h, gp, gh, v);
+    else gm_value_grad4l(xo, nv, p, h, gp, gh, v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) lastv[k] = v[k];
+    if (nv == 4) {
+      part = ((part + v[0]) + v[1]) + (v[2] + v[3]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (k < nv) part += v[k];
+    }
+    if (++cnt == 2) {
+      s += (double)part;
+      part = 0.0f;
+      cnt = 0;
+    }
+  }
+
+  // After each tile: the tile's FP32 adjoints into the FP64 accumulators.
+  __device__ __forceinline__ void flush_tile() {
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) {
+      acc[1 + j] += (double)gp[j];
+      gp[j] = 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < GM_NH; ++j) {
+      ghd[j] += (double)gh[j];
+      gh[j] = 0.0f;
+    }
+  }
+
+  __device__ __forceinline__ float last4(int k) const { return lastv[k]; }
+
+  __device__ __forceinline__ void end() {
+    flush_tile();
+    float ghf[GM_NH], gx[GM_NP];
+#pragma unroll
+    for (int j = 0; j < GM_NH; ++j) ghf[j] = (float)ghd[j];
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) gx[j] = 0.0f;
+    gm_hoist_grad(p, ghf, gx);
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) acc[1 + j] += (double)gx[j];
+  }
+
+  __device__ __forceinline__ double total(int, int w) const {
+    return w == 0 ? s + (double)part : acc[w];
+  }
+};
+using GradBody = JitLanesG;
+constexpr int kGradG = 32;  // chains per warp group, as the host counts them
 #else
 using GradBody = JitBody<GM_GG, true>;
+constexpr int kGradG = GM_GG;
 #endif
 
 // The generated f64 prior (value and reverse-mode gradient).
@@ -413,6 +512,7 @@ extern "C" __global__ void __launch_bounds__(gpum::kThreads, GM_GRAD_CTAS)
 gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum::ChainArgs A,
              int phase) {
   gpum::GradBody body;
-  gpum::run_iteration<GM_GG, 1 + GM_NP, gpum::GradBody, gpum::JitPrior>(&tmap, E, A, phase,
+  gpum::run_iteration<gpum::kGradG, 1 + GM_NP, gpum::GradBody, gpum::JitPrior>(&tmap, E, A,
+                                                                            phase,
                                                                         body);
 }

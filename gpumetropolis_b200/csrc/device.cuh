@@ -69,6 +69,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// 16-byte shared-memory load that the compiler may not merge with an earlier
+// load of the same address (a reload instead of keeping the value live).
+__device__ __forceinline__ float4 gm_lds4v(const float* p) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(smem_addr(p)));
+  return v;
+}
+
 // 2-D tiled TMA load (no multicast): box at (x, y) of `map` into smem `dst`,
 // completion counted on `bar`.  x * elemsize must be a multiple of 16 bytes.
 __device__ __forceinline__ void tma_load_2d(void* dst, const TmapDesc* map, uint64_t* bar,

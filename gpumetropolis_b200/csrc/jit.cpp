@@ -197,11 +197,17 @@ bool jit_value_lanes(const GenModel& gm, bool pair) {
   return !pair && gm.np + std::max(gm.n_hoist, 1) <= 160;
 }
 
+bool jit_grad_lanes(const GenModel& gm, bool pairg) {
+  return !pairg && gm.np + std::max(gm.n_hoist, 1) <= 100;
+}
+
 std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg) {
   const bool lanes = jit_value_lanes(gm, pair);
+  const bool lanes_grad = jit_grad_lanes(gm, pairg);
   std::string s;
   s += "#include \"device.cuh\"\n";
   s += "#define GM_LANES " + std::string(lanes ? "1" : "0") + "\n";
+  s += "#define GM_LANESG " + std::string(lanes_grad ? "1" : "0") + "\n";
   s += "#define GM_PAIR " + std::string(pair ? "1" : "0") + "\n";
   s += "#define GM_PAIRG " + std::string(pairg ? "1" : "0") + "\n";
   s += "#define GM_G " + std::to_string(G) + "\n";
@@ -267,6 +273,7 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.pair = pair;
   e.model.pairg = pairg;
   e.model.lanes = jit_value_lanes(gm, pair);
+  e.model.lanes_grad = jit_grad_lanes(gm, pairg);
   e.model.n_mat = gm.n_mat;
   e.model.np = gm.np;
   e.model.compile_seconds =

@@ -21,6 +21,7 @@ struct CompiledModel {
   bool pair = false;                // value kernel evaluates observation pairs
   bool pairg = false;               // gradient kernel evaluates observation pairs
   bool lanes = false;               // value kernel: one chain per lane (G counts 32)
+  bool lanes_grad = false;          // gradient kernel: one chain per lane
   int np = 0;
   double compile_seconds = 0.0;
 };
@@ -35,6 +36,11 @@ void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pa
 // not take, with parameters + hoisted values that fit the registers (data-only
 // operations are materialized columns, so no lane repeats them).
 bool jit_value_lanes(const GenModel& gm, bool pair);
+
+// Whether the gradient kernel maps chains to lanes: models the paired
+// gradient body does not take, whose parameters + hoisted values (values and
+// adjoints in registers) stay within 100.
+bool jit_grad_lanes(const GenModel& gm, bool pairg);
 
 // Returns 0 and a loaded model, or 1 with a message (NVRTC missing, compile
 // error, load error).

@@ -199,3 +199,22 @@ def test_log_sum_of_exponentials_rewrite(gpu):
     assert np.all(np.isfinite(ref)) and np.all(np.isfinite(got))
     np.testing.assert_allclose(got, ref, rtol=2e-6, atol=1e-5)
     np.testing.assert_allclose(tot, ref.sum(axis=1), rtol=1e-6)
+
+
+@pytest.mark.parametrize("n_pts", [300, 5])
+def test_grad_batch_chain_lanes(gpu, n_pts):
+    # the Student-t model (65 parameters) runs the chain-lane gradient body:
+    # 300 points are two blocks of 256 chains, 5 points share one warp group
+    # whose warps split the observation quads; 20,011 observations make many
+    # tiles per CTA (per-tile FP64 flushes) and a ragged last quad
+    w = W.make("student_t", n_obs=20011)
+    m = w.model
+    rng = np.random.default_rng(6)
+    base = np.append(w.truth["beta"], math.log(1.5))
+    pts = base + rng.normal(0, 0.02, (n_pts, m.n_params))
+    ref = O.grad_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols, w.n_obs,
+                       pts).reshape(n_pts, -1)
+    got = gpu.grad_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
+                         w.n_obs, pts).reshape(n_pts, -1)
+    err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err.max() < 2e-5, err.max()
