@@ -198,10 +198,12 @@ std::string op_expr2(const Graph& g, int i, const std::string& a, const std::str
 }
 
 // Local-derivative contributions of node i with adjoint `G` to its children,
-// as (child, expression) pairs (cpu_native.rs:217-277).
+// as (child, expression) pairs (cpu_native.rs:217-277).  `rb`, when given, is
+// the reciprocal of a DIV node's divisor (the divisions become products).
 std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const std::string& G,
                                                   const std::string& v, const std::string& a,
-                                                  const std::string& b, bool f32) {
+                                                  const std::string& b, bool f32,
+                                                  const std::string& rb = "") {
   const Node& x = g.n[i];
   const std::string one = f32 ? "1.0f" : "1.0";
   const std::string half = f32 ? "0.5f" : "0.5";
@@ -212,7 +214,12 @@ std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const s
     case O_ADD: out = {{x.a, G}, {x.b, G}}; break;
     case O_SUB: out = {{x.a, G}, {x.b, "(-" + G + ")"}}; break;
     case O_MUL: out = {{x.a, G + " * " + b}, {x.b, G + " * " + a}}; break;
-    case O_DIV: out = {{x.a, G + " / " + b}, {x.b, "(-" + G + " * " + v + " / " + b + ")"}}; break;
+    case O_DIV:
+      if (!rb.empty())
+        out = {{x.a, G + " * " + rb}, {x.b, "(-" + G + " * " + v + " * " + rb + ")"}};
+      else
+        out = {{x.a, G + " / " + b}, {x.b, "(-" + G + " * " + v + " / " + b + ")"}};
+      break;
     case O_NEG: out = {{x.a, "(-" + G + ")"}}; break;
     case O_EXP: out = {{x.a, G + " * " + v}}; break;
     case O_LOG: out = {{x.a, G + " / " + a}}; break;
@@ -784,8 +791,10 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
         a[k] = ref4g(x.a, k, false);
         if (x.b >= 0) b[k] = ref4g(x.b, k, false);
       }
+      const std::string rb = recip(i) >= 0 ? "h[" + std::to_string(recip(i)) + "]" : "";
       for (int k = 0; k < 4; ++k)
-        s << "  const float " << name[i] << "_" << k << " = " << op_expr(g, i, a[k], b[k], true)
+        s << "  const float " << name[i] << "_" << k << " = "
+          << (rb.empty() ? op_expr(g, i, a[k], b[k], true) : "(" + a[k] + " * " + rb + ")")
           << ";\n";
     }
     for (int i = 0; i < N; ++i)
@@ -821,7 +830,7 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
         const std::string G = "g" + std::to_string(i) + "_" + std::to_string(k);
         const std::string v = name[i] + "_" + std::to_string(k);
         ce[k] = adjoints(g, i, G, v, ref4g(x.a, k, true), x.b >= 0 ? ref4g(x.b, k, true) : "",
-                         true);
+                         true, recip(i) >= 0 ? "h[" + std::to_string(recip(i)) + "]" : "");
       }
       for (size_t j = 0; j < ce[0].size(); ++j) {
         std::string e[4];
