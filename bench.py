@@ -544,7 +544,7 @@ def run_configs(a, n_warm=2, n_timed=6):
         gamma, ladder = 0.0, 0
         if name == "poisson":
             mode, centre, jitter, step = _native.MODE_MALA, w.truth["beta"], 0.01, 2e-4
-            method = "mala (paired value + adjoint kernel gm_iter_grad)"
+            method = "mala (value + adjoint kernel gm_iter_grad, chain-lane body)"
         elif name == "mixture":
             mode, jitter, step = _native.MODE_RWM, 0.01, 5e-4
             centre = np.array([math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)])

@@ -11,7 +11,8 @@
 //   void   gm_value4l(const float* xo, const float* p, const float* h,
 //                     float* out)  four observations, chain-lane body
 //   float  gm_value_grad(d, p, h, float* gp, float* gh)  gp/gh accumulated
-//   float2 gm_value_grad2(d, pp, hh, float2* gp2, float2* gh2)
+//   void   gm_value_grad4l(const float* xo, int nv, p, h, float* gp, float* gh,
+//                          float* out)  four observations, chain-lane body
 //   void   gm_hoist_grad(const float* p, const float* gh, float* gp)
 //   double gm_prior(const double* p)
 //   double gm_prior_grad(const double* p, double* g)     g accumulated
@@ -238,36 +239,6 @@ std::vector<std::pair<int, std::string>> adjoints(const Graph& g, int i, const s
       break;
   }
   return out;
-}
-
-// Paired adjoint contributions of node i (adjoint pair `G`) to its children:
-// either a product (mx * my, accumulated with FFMA2) or an expression.
-struct Adj2 {
-  int child;
-  std::string mx, my, expr;
-};
-
-std::vector<Adj2> adjoints2(const Graph& g, int i, const std::string& G, const std::string& v,
-                            const std::string& a, const std::string& b) {
-  const Node& x = g.n[i];
-  switch (x.op) {
-    case O_ADD: return {{x.a, "", "", G}, {x.b, "", "", G}};
-    case O_SUB: return {{x.a, "", "", G}, {x.b, "", "", "gm2_neg(" + G + ")"}};
-    case O_MUL: return {{x.a, G, b, ""}, {x.b, G, a, ""}};
-    case O_DIV:
-      return {{x.a, "", "", "gm2_div(" + G + ", " + b + ")"},
-              {x.b, "", "", "gm2_neg(gm2_div(gm2_mul(" + G + ", " + v + "), " + b + "))"}};
-    case O_NEG: return {{x.a, "", "", "gm2_neg(" + G + ")"}};
-    case O_EXP: return {{x.a, G, v, ""}};
-    case O_LOG: return {{x.a, "", "", "gm2_div(" + G + ", " + a + ")"}};
-    case O_SQRT: return {{x.a, "", "", "gm2_div(gm2_mul(" + G + ", gm2(0.5f)), " + v + ")"}};
-    case O_LGAMMA: return {{x.a, G, "gm2_digamma(" + a + ")", ""}};
-    default:
-      if (is_const2(g, x.b)) return {{x.a, "gm2_mul(" + G + ", gm2(2.0f))", a, ""}};
-      return {{x.a, "gm2_mul(" + G + ", " + b + ")", "gm2_pow(" + a + ", gm2_sub(" + b +
-                                                          ", gm2(1.0f)))", ""},
-              {x.b, "", "", "gm2_powexp_adj(" + G + ", " + v + ", " + a + ")"}};
-  }
 }
 
 }  // namespace
@@ -641,67 +612,6 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
         s << "  const float2 " << name[i] << " = " << value2_expr(i, ref2) << ";\n";
     const std::string root2 = root < 0 ? std::string("gm2(0.0f)") : ref2(root);
     s << "  (void)d; (void)pp; (void)hh;\n  return " << root2 << ";\n}\n";
-
-    // Paired value + gradient: forward node by node (no rewrites, as the
-    // scalar gradient), then paired adjoints; parameter and hoisted-value
-    // adjoints accumulate into gp2 / gh2 pairs (one sum per observation lane).
-    s << "__device__ __forceinline__ float2 gm_value_grad2(const float2* __restrict__ d, "
-         "const float2* __restrict__ pp, const float2* __restrict__ hh, "
-         "float2* __restrict__ gp2, float2* __restrict__ gh2) {\n";
-    // (a product feeding only a sum is fused: no adjoint reads its value)
-    for (int i = 0; i < N; ++i) {
-      if (!live[i] || !is_pd(i) || fused[i]) continue;
-      const Node& x = g.n[i];
-      std::string e;
-      if (x.op == O_ADD && (fused[x.a] || (x.b >= 0 && fused[x.b]))) {
-        const int m = fused[x.a] ? x.a : x.b, o = fused[x.a] ? x.b : x.a;
-        e = "gm2_fma(" + ref2(g.n[m].a) + ", " + ref2(g.n[m].b) + ", " + ref2(o) + ")";
-      } else {
-        e = op_expr2(g, i, ref2(x.a), x.b >= 0 ? ref2(x.b) : "");
-      }
-      s << "  const float2 " << name[i] << " = " << e << ";\n";
-    }
-    std::vector<char> has_adj2(N, 0);
-    for (int i = 0; i < N; ++i)
-      if (live[i] && is_pd(i)) s << "  float2 g" << i << " = gm2(0.0f);\n";
-    auto acc_into = [&](const std::string& target, const Adj2& e) {
-      if (!e.mx.empty())
-        s << "  " << target << " = gm2_fma(" << e.mx << ", " << e.my << ", " << target << ");\n";
-      else
-        s << "  " << target << " = gm2_add(" << target << ", " << e.expr << ");\n";
-    };
-    auto sink2 = [&](const Adj2& e) {
-      const int c = e.child;
-      if (c < 0 || !(g.n[c].dep & DEP_P)) return;
-      if (g.n[c].op == O_P) {
-        acc_into("gp2[" + std::to_string(g.n[c].arg) + "]", e);
-      } else if (hslot[c] >= 0) {
-        acc_into("gh2[" + std::to_string(hslot[c]) + "]", e);
-      } else if (!has_adj2[c]) {  // first contribution assigns
-        s << "  g" << c << " = "
-          << (e.mx.empty() ? e.expr : "gm2_mul(" + e.mx + ", " + e.my + ")") << ";\n";
-        has_adj2[c] = 1;
-      } else {
-        acc_into("g" + std::to_string(c), e);
-      }
-    };
-    if (root >= 0 && (g.n[root].dep & DEP_P)) {
-      if (is_pd(root)) {
-        s << "  g" << root << " = gm2(1.0f);\n";
-        has_adj2[root] = 1;
-      } else {
-        sink2({root, "", "", "gm2(1.0f)"});
-      }
-    }
-    for (int i = N - 1; i >= 0; --i) {
-      if (!live[i] || !is_pd(i)) continue;
-      const Node& x = g.n[i];
-      for (auto& e : adjoints2(g, i, "g" + std::to_string(i), name[i], ref2(x.a),
-                               x.b >= 0 ? ref2(x.b) : ""))
-        sink2(e);
-    }
-    s << "  (void)d; (void)pp; (void)hh; (void)gp2; (void)gh2;\n  return " << root2
-      << ";\n}\n";
   }
 
   // Value + gradient: forward, then adjoints in reverse order.

@@ -248,120 +248,7 @@ using ValueBody = JitBody<GM_G, false>;
 constexpr int kValueG = GM_G;
 #endif
 
-#if GM_PAIRG
-// Value + gradient over observation pairs (gm_value_grad2): parameter and
-// hoisted-value adjoints accumulate in one FP32 sum per observation lane and
-// are combined at the end; a last pair with only its first observation
-// valid runs the scalar gm_value_grad on that observation.
-template <int G>
-struct JitBody2G {
-  static constexpr bool kChainLanes = false;
-  static constexpr int kObsPerEval = 2;
-  static constexpr int kTileObs = 0;  // not unrolled: the body is large
-  float2 pp[G][GM_NP];
-  float2 hh[G][GM_NH];
-  float2 gp2[G][GM_NP];
-  float2 gh2[G][GM_NH];
-  double s[G];
-  float2 part[G];
-  float2 lastv[G];
-  int cnt;
-
-  __device__ __forceinline__ void begin(const float* pc0, int CG) {
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      float p[GM_NP], h[GM_NH];
-#pragma unroll
-      for (int j = 0; j < GM_NP; ++j) p[j] = pc0[j * CG + g];
-      gm_hoist(p, h);
-#pragma unroll
-      for (int j = 0; j < GM_NP; ++j) {
-        pp[g][j] = make_float2(p[j], p[j]);
-        gp2[g][j] = make_float2(0.0f, 0.0f);
-      }
-#pragma unroll
-      for (int j = 0; j < GM_NH; ++j) {
-        hh[g][j] = make_float2(h[j], h[j]);
-        gh2[g][j] = make_float2(0.0f, 0.0f);
-      }
-      s[g] = 0.0;
-      part[g] = make_float2(0.0f, 0.0f);
-      lastv[g] = make_float2(0.0f, 0.0f);
-    }
-    cnt = 0;
-  }
-
-  __device__ __forceinline__ void eval2(const float* xo, int T, bool v0, bool v1) {
-    float2 d[GM_ND];
-    gm_data2(xo, T, d);
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      if (v1) {
-        const float2 v = gm_value_grad2(d, pp[g], hh[g], gp2[g], gh2[g]);
-        lastv[g] = v;
-        part[g] = __fadd2_rn(part[g], v);
-      } else if (v0) {
-        float ds[GM_ND], p[GM_NP], h[GM_NH], gps[GM_NP], ghs[GM_NH];
-#pragma unroll
-        for (int k = 0; k < GM_ND; ++k) ds[k] = d[k].x;
-#pragma unroll
-        for (int j = 0; j < GM_NP; ++j) {
-          p[j] = pp[g][j].x;
-          gps[j] = 0.0f;
-        }
-#pragma unroll
-        for (int j = 0; j < GM_NH; ++j) {
-          h[j] = hh[g][j].x;
-          ghs[j] = 0.0f;
-        }
-        const float v = gm_value_grad(ds, p, h, gps, ghs);
-#pragma unroll
-        for (int j = 0; j < GM_NP; ++j) gp2[g][j].x += gps[j];
-#pragma unroll
-        for (int j = 0; j < GM_NH; ++j) gh2[g][j].x += ghs[j];
-        lastv[g] = make_float2(v, 0.0f);
-        part[g].x += v;
-      }
-    }
-    if (v0 && ++cnt == kAccBlock) {
-      cnt = 0;
-#pragma unroll
-      for (int g = 0; g < G; ++g) {
-        s[g] += (double)part[g].x + (double)part[g].y;
-        part[g] = make_float2(0.0f, 0.0f);
-      }
-    }
-  }
-
-  __device__ __forceinline__ float2 last2(int g) const { return lastv[g]; }
-
-  // Combine the two lanes and push the hoisted adjoints to the parameters;
-  // the totals are left in gp2[g][j].x.
-  __device__ __forceinline__ void end() {
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      float p[GM_NP], gp[GM_NP], gh[GM_NH];
-#pragma unroll
-      for (int j = 0; j < GM_NP; ++j) {
-        p[j] = pp[g][j].x;
-        gp[j] = gp2[g][j].x + gp2[g][j].y;
-      }
-#pragma unroll
-      for (int j = 0; j < GM_NH; ++j) gh[j] = gh2[g][j].x + gh2[g][j].y;
-      gm_hoist_grad(p, gh, gp);
-#pragma unroll
-      for (int j = 0; j < GM_NP; ++j) gp2[g][j].x = gp[j];
-    }
-  }
-
-  __device__ __forceinline__ double total(int g, int w) const {
-    if (w == 0) return s[g] + ((double)part[g].x + (double)part[g].y);
-    return (double)gp2[g][w - 1].x;
-  }
-};
-using GradBody = JitBody2G<GM_GG>;
-constexpr int kGradG = GM_GG;
-#elif GM_LANESG
+#if GM_LANESG
 // Value + gradient body for wide models, one chain per lane (the chain-lane
 // layout of JitLanes): gm_value_grad4l on four observations per broadcast
 // load; each lane's FP32 parameter adjoints of one tile are added into its

@@ -180,36 +180,32 @@ int build_cubin_uncached(const std::string& src, std::vector<char>* out, std::st
 
 }  // namespace
 
-void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pairg) {
+void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair) {
   // The paired body keeps G x (parameters + hoisted values) broadcast pairs
   // in registers: use it while that stays within 96 registers.
   const int w = np + std::max(nh, 1);
   *pair = w <= 48;
   if (*pair) *G = w <= 24 ? 2 : 1;
   else *G = np <= 24 ? 4 : (np <= 48 ? 2 : 1);
-  // The paired gradient body also keeps the adjoint pairs: one chain per
-  // thread, while parameters + hoisted values stay within 32.
-  *pairg = w <= 32;
-  *GG = *pairg ? 1 : (np <= 16 ? 2 : 1);
+  // Chains per thread of the scalar gradient body (models too wide for the
+  // chain-lane gradient body).
+  *GG = np <= 16 ? 2 : 1;
 }
 
 bool jit_value_lanes(const GenModel& gm, bool pair) {
   return !pair && gm.np + std::max(gm.n_hoist, 1) <= 160;
 }
 
-bool jit_grad_lanes(const GenModel& gm, bool pairg) {
-  return !pairg && gm.np + std::max(gm.n_hoist, 1) <= 100;
-}
+bool jit_grad_lanes(const GenModel& gm) { return gm.np + std::max(gm.n_hoist, 1) <= 100; }
 
-std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg) {
+std::string jit_source(const GenModel& gm, int G, int GG, bool pair) {
   const bool lanes = jit_value_lanes(gm, pair);
-  const bool lanes_grad = jit_grad_lanes(gm, pairg);
+  const bool lanes_grad = jit_grad_lanes(gm);
   std::string s;
   s += "#include \"device.cuh\"\n";
   s += "#define GM_LANES " + std::string(lanes ? "1" : "0") + "\n";
   s += "#define GM_LANESG " + std::string(lanes_grad ? "1" : "0") + "\n";
   s += "#define GM_PAIR " + std::string(pair ? "1" : "0") + "\n";
-  s += "#define GM_PAIRG " + std::string(pairg ? "1" : "0") + "\n";
   s += "#define GM_G " + std::to_string(G) + "\n";
   s += "#define GM_GG " + std::to_string(GG) + "\n";
   // Narrow paired models with two chains per thread (2 x (parameters +
@@ -217,7 +213,7 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg)
   // spills: three CTAs, 24 warps per SM.
   const int w = gm.np + std::max(gm.n_hoist, 1);
   // Paired gradient body of at most 25 parameters + hoisted values: two CTAs.
-  s += "#define GM_GRAD_CTAS " + std::to_string(pairg && w <= 25 ? 2 : 1) + "\n";
+  s += "#define GM_GRAD_CTAS 1\n";  // the gradient bodies keep up to 255 registers
   // Chain lanes: two CTAs while parameters + hoisted values stay within 80.
   s += "#define GM_VALUE_CTAS " +
        std::to_string(pair ? (G == 2 && G * w <= 40 ? 3 : 2) : (lanes && w <= 80 ? 2 : 1)) +
@@ -231,19 +227,19 @@ std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg)
 
 int jit_compile_check(const GenModel& gm, size_t* cubin_bytes, std::string* err) {
   int G = 1, GG = 1;
-  bool pair = false, pairg = false;
-  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair, &pairg);
+  bool pair = false;
+  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair);
   std::vector<char> cubin;
-  if (build_cubin(jit_source(gm, G, GG, pair, pairg), &cubin, err)) return 1;
+  if (build_cubin(jit_source(gm, G, GG, pair), &cubin, err)) return 1;
   if (cubin_bytes) *cubin_bytes = cubin.size();
   return 0;
 }
 
 int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   int G = 1, GG = 1;
-  bool pair = false, pairg = false;
-  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair, &pairg);
-  const std::string src = jit_source(gm, G, GG, pair, pairg);
+  bool pair = false;
+  jit_chains_per_thread(gm.np, gm.n_hoist, &G, &GG, &pair);
+  const std::string src = jit_source(gm, G, GG, pair);
   const size_t key = std::hash<std::string>()(src);
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = cache().find(key);
@@ -271,9 +267,8 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.G = G;
   e.model.GG = GG;
   e.model.pair = pair;
-  e.model.pairg = pairg;
   e.model.lanes = jit_value_lanes(gm, pair);
-  e.model.lanes_grad = jit_grad_lanes(gm, pairg);
+  e.model.lanes_grad = jit_grad_lanes(gm);
   e.model.n_mat = gm.n_mat;
   e.model.np = gm.np;
   e.model.compile_seconds =

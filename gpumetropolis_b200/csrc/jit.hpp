@@ -19,7 +19,6 @@ struct CompiledModel {
   int n_mat = 0;                    // materialized data-only operations
   int G = 1, GG = 1;                // chains per thread of each kernel
   bool pair = false;                // value kernel evaluates observation pairs
-  bool pairg = false;               // gradient kernel evaluates observation pairs
   bool lanes = false;               // value kernel: one chain per lane (G counts 32)
   bool lanes_grad = false;          // gradient kernel: one chain per lane
   int np = 0;
@@ -29,7 +28,7 @@ struct CompiledModel {
 // Chains per thread for the value and gradient kernels, and whether the
 // value kernel uses the paired-observation body, by parameter and hoisted
 // value counts.
-void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pairg);
+void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair);
 
 // Whether the value kernel maps chains to lanes (wide models: every lane
 // reads the same observation values, broadcast): models the paired body does
@@ -37,17 +36,17 @@ void jit_chains_per_thread(int np, int nh, int* G, int* GG, bool* pair, bool* pa
 // operations are materialized columns, so no lane repeats them).
 bool jit_value_lanes(const GenModel& gm, bool pair);
 
-// Whether the gradient kernel maps chains to lanes: models the paired
-// gradient body does not take, whose parameters + hoisted values (values and
-// adjoints in registers) stay within 100.
-bool jit_grad_lanes(const GenModel& gm, bool pairg);
+// Whether the gradient kernel maps chains to lanes: models whose parameters
+// + hoisted values (values and adjoints in registers) stay within 100; wider
+// ones take the scalar body (GG chains per thread, lanes over observations).
+bool jit_grad_lanes(const GenModel& gm);
 
 // Returns 0 and a loaded model, or 1 with a message (NVRTC missing, compile
 // error, load error).
 int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err);
 
 // The full NVRTC source a model compiles from (for tests and diagnostics).
-std::string jit_source(const GenModel& gm, int G, int GG, bool pair, bool pairg);
+std::string jit_source(const GenModel& gm, int G, int GG, bool pair);
 
 // Compile only (no GPU needed): returns 0 and the cubin size, or 1 + message.
 int jit_compile_check(const GenModel& gm, size_t* cubin_bytes, std::string* err);
