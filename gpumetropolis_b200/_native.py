@@ -278,6 +278,18 @@ def compile_check(code, consts, prior_code, prior_consts, n_params, n_cols) -> i
     return nbytes.value
 
 
+def _out_f32(out, n):
+    """A contiguous float32 array of at least max(n, 1) values: `out` itself
+    when given (checked), else a new one."""
+    if out is None:
+        return np.empty(max(n, 1), np.float32)
+    if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.ndim == 1
+            and out.flags.c_contiguous and out.size >= max(n, 1)):
+        raise ValueError(f"out_draws must be a contiguous 1-D float32 array of >= {max(n, 1)} "
+                         "values")
+    return out
+
+
 class Session:
     """A model + data resident on the GPU (``gpum_b200_session_*``)."""
 
@@ -327,11 +339,14 @@ class Session:
         return int(self._lib.gpum_b200_session_stream(self._h) or 0)
 
     def run(self, init, proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0,
-            de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
+            de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32, out_draws=None):
+        """One run of n_iter iterations.  `out_draws` (optional): a float32 array
+        of at least n_iter * n_chains * n_params values that receives the draws
+        (e.g. pinned memory allocated once)."""
         init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
         n_chains = self.n_chains = init.size // self.n_params
         L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
-        draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
+        draws = _out_f32(out_draws, n_iter * n_chains * self.n_params)
         acc = np.empty(n_chains, np.float32)
         last = np.empty(n_chains, np.float64)
         err = C.create_string_buffer(_ERRLEN)
@@ -426,13 +441,14 @@ class Session:
         return theta[: n.value], ll[: n.value]
 
     def run_da(self, surrogate, init, proposal_sd, temperatures, n_iter, seed, proposal_mode,
-               gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32):
+               gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32, out_draws=None):
         """Delayed-acceptance run with `surrogate` (a Surrogate) as stage 1.
-        Returns (draws, accept, last_logpost, exact_evals per chain)."""
+        Returns (draws, accept, last_logpost, exact_evals per chain); `out_draws`
+        as for run()."""
         init, sd, temps = _f64(init), _f64(proposal_sd), _f64(temperatures)
         n_chains = self.n_chains = init.size // self.n_params
         L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
-        draws = np.empty(max(n_iter * n_chains * self.n_params, 1), np.float32)
+        draws = _out_f32(out_draws, n_iter * n_chains * self.n_params)
         acc = np.empty(n_chains, np.float32)
         last = np.empty(n_chains, np.float64)
         exact = np.empty(n_chains, np.uint32)

@@ -167,7 +167,7 @@ class _Backend:
                      "holdout_resid_sd": float(np.std(resid))}
 
     def __call__(self, init, sd, n_iter, seed, temperatures=None, proposal_mode=0, gamma=0.0,
-                 de_noise=0.0, proposal_l=None):
+                 de_noise=0.0, proposal_l=None, out_draws=None):
         init = np.asarray(init, dtype=np.float64)
         C = init.shape[0]
         temps = np.ones(C) if temperatures is None else np.asarray(temperatures, np.float64)
@@ -182,13 +182,14 @@ class _Backend:
                     proposal_l = np.asarray(proposal_l, dtype=np.float64) * k
             d, acc, last, exact = self.session.run_da(
                 self.net, init, sd, temps, int(n_iter), int(seed) & 0xFFFFFFFF, proposal_mode,
-                gamma, de_noise, proposal_l, rng=self.rng)
+                gamma, de_noise, proposal_l, rng=self.rng, out_draws=out_draws)
             self.exact_evals += int(exact.sum())
             self.da_iters += int(n_iter) * C
         else:
             d, acc, last = self.session.run(init, sd, temps, int(n_iter),
                                             int(seed) & 0xFFFFFFFF, proposal_mode, gamma,
-                                            de_noise, proposal_l, rng=self.rng)
+                                            de_noise, proposal_l, rng=self.rng,
+                                            out_draws=out_draws)
         self.consumed += int(n_iter)
         return d.reshape((int(n_iter), C, self.np), order="F"), acc.astype(np.float64), last
 
