@@ -429,12 +429,16 @@ def run_b200(a):
     e2e = None
     if rank == 0 and not a.no_e2e:
         init2, sd2, temps2 = _init(w, C, seed=7)
+        # inputs and draws in pinned host memory, filled once before the timed calls
+        data_h = torch.empty(w.data.shape, dtype=torch.float64, pin_memory=True).numpy()
+        data_h[...] = w.data
+        draws_h = _pinned_f32(K * C * m.n_params)
 
         def e2e_call(n_iter, seed):
             t = time.perf_counter()
             _native.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
-                        m.n_params, w.data, m.n_cols, w.n_obs, init2, sd2, temps2, n_iter,
-                        seed, 0)
+                        m.n_params, data_h, m.n_cols, w.n_obs, init2, sd2, temps2, n_iter,
+                        seed, 0, out_draws=draws_h)
             return time.perf_counter() - t
 
         e2e_call(3, 2)  # untimed: first-call library and module set-up
@@ -445,9 +449,9 @@ def run_b200(a):
         d2h = K * C * m.n_params * 4 + C * 4 + C * 8
         e2e = {"value": K * C * N / dt, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                "d2h_bytes_per_step": d2h / K,
-               "note": "gpum_b200_run: one call of K iterations from host buffers (data "
-                       "upload + f64->f32 column layout + K iterations + draws back), wall "
-                       "clock, median of 3 calls after one untimed call"}
+               "note": "gpum_b200_run: one call of K iterations from pinned host buffers "
+                       "(data upload + f64->f32 column layout + K iterations + draws back), "
+                       "wall clock, median of 3 calls after one untimed call"}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:

@@ -188,17 +188,30 @@ def validate_program(code, n_consts, n_params, n_cols, allow_data=True) -> int:
     return depth.value
 
 
+def _out_f32(out, n):
+    """A contiguous float32 array of at least max(n, 1) values: `out` itself
+    when given (checked), else a new one."""
+    if out is None:
+        return np.empty(max(n, 1), np.float32)
+    if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.ndim == 1
+            and out.flags.c_contiguous and out.size >= max(n, 1)):
+        raise ValueError(f"out_draws must be a contiguous 1-D float32 array of >= {max(n, 1)} "
+                         "values")
+    return out
+
+
 def run(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
         proposal_sd, temperatures, n_iter, seed, proposal_mode, gamma=0.0, de_noise=0.0,
-        proposal_l=None):
-    """One-shot sampler (``gpum_b200_run``); host arrays in, host arrays out."""
+        proposal_l=None, out_draws=None):
+    """One-shot sampler (``gpum_b200_run``); host arrays in, host arrays out
+    (`out_draws`: optional float32 array receiving the draws)."""
     code, pcode = _u32(code), _u32(prior_code)
     consts, pconsts = _f64(consts), _f64(prior_consts)
     data, init = _f64(data), _f64(init)
     sd, temps = _f64(proposal_sd), _f64(temperatures)
     n_chains = init.size // n_params
     L = None if proposal_l is None or np.size(proposal_l) == 0 else _f64(proposal_l)
-    draws = np.empty(n_iter * n_chains * n_params, np.float32)
+    draws = _out_f32(out_draws, n_iter * n_chains * n_params)
     acc = np.empty(n_chains, np.float32)
     last = np.empty(n_chains, np.float64)
     err = C.create_string_buffer(_ERRLEN)
@@ -210,7 +223,7 @@ def run(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, i
         de_noise, _p(L, C.c_double), 0 if L is None else L.size, _p(draws, C.c_float),
         _p(acc, C.c_float), _p(last, C.c_double), err, _ERRLEN)
     _check(rc, err)
-    return draws, acc, last
+    return draws[: n_iter * n_chains * n_params], acc, last
 
 
 def run_de_sync(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
@@ -276,18 +289,6 @@ def compile_check(code, consts, prior_code, prior_consts, n_params, n_cols) -> i
         _p(pcode, C.c_uint32), pcode.size, _p(pconsts, C.c_double), pconsts.size, n_params,
         n_cols, C.byref(nbytes), err, 8192), err)
     return nbytes.value
-
-
-def _out_f32(out, n):
-    """A contiguous float32 array of at least max(n, 1) values: `out` itself
-    when given (checked), else a new one."""
-    if out is None:
-        return np.empty(max(n, 1), np.float32)
-    if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.ndim == 1
-            and out.flags.c_contiguous and out.size >= max(n, 1)):
-        raise ValueError(f"out_draws must be a contiguous 1-D float32 array of >= {max(n, 1)} "
-                         "values")
-    return out
 
 
 class Session:
