@@ -159,3 +159,27 @@ def test_philox_known_answers():
     for c, k, want in cases:
         assert philox4x32_10(c, *k) == want
     assert 0.0 < u53(0, 0) < 1e-15 and u53(0xFFFFFFFF, 0xFFFFFFFF) == 1.0
+
+
+def test_da_oracle_exchanges_permute_equal_temperature_ladders():
+    # with equal temperatures every attempted exchange is accepted: the
+    # oracle's draws show the pairs (0,1),(2,3) swapped after the first
+    # exchange and (1,2) after the second, in each ladder of four chains
+    from oracle import da_oracle
+    w = W.make("gaussian", n_obs=200)
+    m = w.model
+    C, K, every, n_iter = 8, 4, 3, 8
+    init = np.arange(1, C + 1, dtype=np.float64).reshape(C, 1)
+
+    def exact(th):
+        return O.loglik_batch(m.loglik.code, m.loglik.consts, 1, w.data, 1, w.n_obs,
+                              np.asarray(th, dtype=np.float64).reshape(-1, 1))
+
+    d, _, _, _, (att, ok) = da_oracle.run_da(
+        m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, 1, w.data, 1, w.n_obs,
+        init, np.full((C, 1), 1e-12), np.ones(C), n_iter, 5, exact, exchange=(K, every))
+    np.testing.assert_allclose(d[2, :, 0], init[:, 0], atol=1e-9)
+    np.testing.assert_allclose(d[3, :, 0], d[2, [1, 0, 3, 2, 5, 4, 7, 6], 0], atol=1e-9)
+    np.testing.assert_allclose(d[6, :, 0], d[5, [0, 2, 1, 3, 4, 6, 5, 7], 0], atol=1e-9)
+    np.testing.assert_array_equal(att, [1, 1, 1, 0, 1, 1, 1, 0])
+    np.testing.assert_array_equal(ok, att)
