@@ -218,3 +218,29 @@ def test_grad_batch_chain_lanes(gpu, n_pts):
                          w.n_obs, pts).reshape(n_pts, -1)
     err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
     assert err.max() < 2e-5, err.max()
+
+
+def test_wide_model_with_materialized_columns(gpu):
+    # 50 parameters (the chain-lane value and gradient bodies) whose 50
+    # data-only terms x_j^2 are materialized columns: values and gradients
+    # against the oracle
+    p = 50
+    rng = np.random.default_rng(8)
+    n = 2003
+    X = rng.normal(0.0, 1.0, (n, p))
+    beta = rng.normal(0.0, 0.1, p)
+    y = (X ** 2) @ beta + rng.normal(0.0, 1.0, n)
+    params = [f"b{j}" for j in range(1, p + 1)]
+    xs = [f"x{j}" for j in range(1, p + 1)]
+    m = gpum_model("~ -((y - (" + " + ".join(f"b{j} * x{j}^2" for j in range(1, p + 1))
+                   + "))^2) / 2", params, xs + ["y"])
+    data = np.column_stack([X, y])
+    pts = beta + rng.normal(0.0, 0.02, (40, p))
+    args = (m.loglik.code, m.loglik.consts, p, data, p + 1, n)
+    ref = O.loglik_batch(*args, pts)
+    ref_g = O.grad_batch(*args, pts).reshape(40, -1)
+    got = gpu.loglik_batch(*args, pts)
+    g = gpu.grad_batch(*args, pts).reshape(40, -1)
+    np.testing.assert_allclose(got, ref, rtol=1e-6)
+    err = np.linalg.norm(g - ref_g, axis=1) / np.linalg.norm(ref_g, axis=1)
+    assert err.max() < 2e-5, err.max()
