@@ -28,6 +28,11 @@ accept/propose step).
   of sampling, and the posterior means' agreement in MCSE units.
 
 ``--impl reference`` times that CPU implementation alone as the reference arm.
+``--configs`` instead times the Poisson (MALA), mixture (512 PT ladders with
+device exchanges), Student-t (DE) and Student-t (MALA) configurations at full
+size, one JSON line each (``--configs-obs-shift`` shrinks them for profiler
+captures); ``--pt-da`` measures exact vs surrogate delayed-acceptance ESS/s
+for PT on the mixture configuration.
 Multi-GPU (torchrun): one independent replica per GPU (the chains shard with
 no collective), weak scaling, max time over ranks.
 """
