@@ -77,3 +77,16 @@ def test_entry_points_reject_bad_input_before_cuda(native):
         with pytest.raises(native.GpumError) as e:
             native.loglik_batch([1, 0], [], 1, np.zeros(2), 1, 2, [0.0])
         assert e.value.code == native.ERR_NODEVICE
+
+
+def test_output_buffers_are_checked_before_any_call():
+    # caller-provided draws buffers (Session.run / run_da / run out_draws)
+    # must be contiguous 1-D float32 arrays of at least the draws' size
+    from gpumetropolis_b200._native import _out_f32
+    buf = np.zeros(12, np.float32)
+    assert _out_f32(buf, 12) is buf
+    assert _out_f32(None, 0).size == 1
+    for bad in (np.zeros(11, np.float32), np.zeros(12, np.float64),
+                np.zeros((3, 4), np.float32), np.zeros(24, np.float32)[::2]):
+        with pytest.raises(ValueError, match="out_draws"):
+            _out_f32(bad, 12)
