@@ -24,15 +24,23 @@ accept/propose step).
   adaptive warmup (exact, its second half recorded as training pairs), the
   surrogate trained on the GPU, then the same number of sampling iterations
   with plain exact MH and with surrogate delayed acceptance from the same
-  start; multi-chain ESS per parameter (min and mean over the 17) per second
-  of sampling, and the posterior means' agreement in MCSE units.
+  start (5,000 iterations each, the configuration's length); multi-chain ESS
+  per parameter (min and mean over the 17) per second of sampling, also
+  with the surrogate's training time added to the two-stage run, and the
+  posterior means' agreement in MCSE units.
+* ``logp_rel_err``: the log posterior the sampler holds for 32 chains'
+  final states against the f64 oracle at the same states (untimed).
+* ``configs``: the Poisson (MALA), mixture (512 PT ladders with device
+  exchanges), Student-t (DE) and Student-t (MALA) configurations at full
+  size: ms per iteration, chain-obs/s, FP32 and MUFU fractions, and each
+  one's ``logp_rel_err``.
+* ``pt_da``: exact vs surrogate delayed-acceptance ESS/s for PT on the
+  mixture configuration, with and without the training time.
 
 ``--impl reference`` times that CPU implementation alone as the reference arm.
-``--configs`` instead times the Poisson (MALA), mixture (512 PT ladders with
-device exchanges), Student-t (DE) and Student-t (MALA) configurations at full
-size, one JSON line each (``--configs-obs-shift`` shrinks them for profiler
-captures); ``--pt-da`` measures exact vs surrogate delayed-acceptance ESS/s
-for PT on the mixture configuration.
+``--configs`` prints only the configuration timings, one JSON line each
+(``--configs-obs-shift`` shrinks them for profiler captures); ``--pt-da``
+prints only the PT + delayed-acceptance leg.
 Multi-GPU (torchrun): one independent replica per GPU (the chains shard with
 no collective), weak scaling, max time over ranks.
 """
@@ -73,8 +81,15 @@ def _args():
     p.add_argument("--no-interp", action="store_true")
     p.add_argument("--engine", type=int, default=2, help="0 interpreter, 1 compiled, 2 auto")
     p.add_argument("--no-da", action="store_true")
+    p.add_argument("--no-logp", action="store_true")
+    p.add_argument("--no-configs", action="store_true",
+                   help="leave the Poisson / mixture / Student-t timings out of the line")
+    p.add_argument("--no-pt-da", action="store_true",
+                   help="leave the mixture PT + delayed-acceptance leg out of the line")
     p.add_argument("--da-warmup", type=int, default=1000)
-    p.add_argument("--da-iters", type=int, default=1000)
+    p.add_argument("--da-iters", type=int, default=5000,
+                   help="sampling iterations of each delayed-acceptance leg (the logistic "
+                        "configuration's 5,000)")
     p.add_argument("--configs", action="store_true",
                    help="instead of the headline line: time the Poisson (MALA), mixture (PT "
                         "ladders) and Student-t (DE) configurations at full size, one JSON "
@@ -83,7 +98,7 @@ def _args():
                    help="instead of the headline line: exact vs surrogate delayed-acceptance "
                         "ESS/s on the mixture configuration (512 ladders of 16 temperatures, "
                         "device exchanges), one JSON line")
-    p.add_argument("--pt-da-warmup", type=int, default=400)
+    p.add_argument("--pt-da-warmup", type=int, default=300)
     p.add_argument("--pt-da-iters", type=int, default=400)
     p.add_argument("--configs-obs-shift", type=int, default=0,
                    help="with --configs: divide each configuration's observation count by "
@@ -223,6 +238,54 @@ def _pinned_f32(n):
     return torch.empty(max(n, 1), dtype=torch.float32, pin_memory=True).numpy()
 
 
+def _acov_mean_gpu(xc):
+    """diagnostics.acov_chain_mean with the FFTs on the GPU (torch, f64):
+    thousands of chains x thousands of iterations per parameter."""
+    import torch
+    n = xc.shape[0]
+    L = 1 << int(np.ceil(np.log2(2 * n)))
+    t = torch.from_numpy(np.ascontiguousarray(xc)).cuda()
+    f = torch.fft.rfft(t, L, dim=0)
+    acov = torch.fft.irfft(f * f.conj(), L, dim=0)[:n] / n
+    out = acov.mean(dim=1).cpu().numpy()
+    del t, f, acov
+    return out
+
+
+def _ess_all(d):
+    """Multi-chain ESS per parameter of an (n_iter, C, np) array."""
+    from gpumetropolis_b200.diagnostics import ess_pooled
+    return np.array([ess_pooled(d[:, :, j], acov_mean_fn=_acov_mean_gpu)
+                     for j in range(d.shape[2])])
+
+
+def _oracle_logpost(w, states):
+    """The oracle's log posterior at each state: the data term through the
+    compiled f64 evaluator (bitwise the interpreter oracle's value) plus the
+    f64 prior, on all host cores."""
+    from oracle import cjit
+    from oracle import oracle as O
+    m = w.model
+    fn = cjit.compile_loglik(m.loglik.code, m.loglik.consts)
+    n = states.shape[0]
+    _, _, last = O.run(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
+                       m.n_params, w.data, m.n_cols, w.n_obs, states, np.ones_like(states),
+                       np.ones(n), 0, 1, 0, jit=fn, n_threads=_cpu_cores())
+    return last
+
+
+def logp_check(sess, w, n=32):
+    """Largest relative error, over the first `n` chains of the session's
+    last run, of the log posterior the sampler holds for its current state
+    (FP32 per-observation terms, FP64 sums, the value its accept decisions
+    used) against the f64 oracle at the same state.  Outside any timed
+    region."""
+    states = sess.state()[:n]
+    _, _, cur, _ = sess.fetch(want_draws=False)
+    ref = _oracle_logpost(w, states)
+    return float(np.max(np.abs(cur[:n] - ref) / np.abs(ref)))
+
+
 def da_measure(w, C, n_warm, n_samp, seed=11):
     """Exact MH vs surrogate delayed acceptance, ESS per second of sampling.
 
@@ -268,14 +331,17 @@ def da_measure(w, C, n_warm, n_samp, seed=11):
             am.final_init, am.final_proposal_sd, n_samp, seed + 2, None, mode, 0.0, 0.0, L,
             out_draws=buf_da))
         exact_frac = (call.exact_evals - e0) / (n_samp * C)
-        d_ex = d_ex.reshape((n_samp, C, npar), order="F").astype(np.float64)
-        d_da = np.asarray(d_da, dtype=np.float64)
-        e_ex = np.array([ess_pooled(d_ex[:, :, j]) for j in range(npar)])
-        e_da = np.array([ess_pooled(d_da[:, :, j]) for j in range(npar)])
-        mc_ex = d_ex.reshape(-1, npar).std(axis=0) / np.sqrt(e_ex)
-        mc_da = d_da.reshape(-1, npar).std(axis=0) / np.sqrt(e_da)
-        z = np.abs(d_ex.mean(axis=(0, 1)) - d_da.mean(axis=(0, 1))) / np.sqrt(mc_ex**2 + mc_da**2)
+        d_ex = d_ex.reshape((n_samp, C, npar), order="F")
+        d_da = np.asarray(d_da)
+        e_ex, e_da = _ess_all(d_ex), _ess_all(d_da)
+        sd_ex = np.array([d_ex[:, :, j].std(dtype=np.float64) for j in range(npar)])
+        sd_da = np.array([d_da[:, :, j].std(dtype=np.float64) for j in range(npar)])
+        mu_ex = np.array([d_ex[:, :, j].mean(dtype=np.float64) for j in range(npar)])
+        mu_da = np.array([d_da[:, :, j].mean(dtype=np.float64) for j in range(npar)])
+        mc_ex, mc_da = sd_ex / np.sqrt(e_ex), sd_da / np.sqrt(e_da)
+        z = np.abs(mu_ex - mu_da) / np.sqrt(mc_ex**2 + mc_da**2)
         r_ex, r_da = e_ex.min() / t_ex, e_da.min() / t_da
+        r_da_t = e_da.min() / (t_da + t_train)
         return {
             "used": True, "n_chains": C, "warmup_iters": n_warm, "sampling_iters": n_samp,
             "proposal": "cholesky rwm (adapted)" if L is not None else "diagonal rwm",
@@ -291,9 +357,16 @@ def da_measure(w, C, n_warm, n_samp, seed=11):
                    "ess_per_s_min": r_da, "ess_per_s_mean": float(e_da.mean() / t_da)},
             "gain_ess_per_s_min": r_da / r_ex,
             "gain_ess_per_s_mean": float((e_da.mean() / t_da) / (e_ex.mean() / t_ex)),
+            "gain_ess_per_s_min_with_training": r_da_t / r_ex,
+            "gain_ess_per_s_mean_with_training":
+                float((e_da.mean() / (t_da + t_train)) / (e_ex.mean() / t_ex)),
+            "gain_ess_per_exact_eval_min": float((e_da.min() / max(exact_frac, 1e-12))
+                                                 / e_ex.min()),
             "posterior_mean_max_z": float(z.max()),
             "ess": "multi-chain (chain-averaged autocovariance + between-chain variance, "
                    "Geyer initial monotone sequence) per parameter over all chains",
+            "with_training": "two-stage seconds + surrogate training seconds (train_s) "
+                             "against the exact sampler's seconds; warmup is common to both",
             "draws_buffers": "pinned host memory allocated before the timed calls",
             "timing": "wall seconds of each blocking sampling call (draws copied back in both, "
                       "into pinned buffers allocated before the calls)",
@@ -374,6 +447,9 @@ def run_b200(a):
         dev_ms = R.max_over_ranks(dev_ms, device=dev)
         dist.barrier()
     _, acc, _, _ = sess.fetch(want_draws=False)
+    # the precision clause of the metric, outside the timed region: the log
+    # posterior of 32 chains' final states against the f64 oracle
+    logp_err = logp_check(sess, w, n=32) if rank == 0 and not a.no_logp else None
     sess.close()
     value = R.whole_job_rate(K * C * N, world, dev_ms / 1e3)
     ms_step = dev_ms / K
@@ -394,6 +470,10 @@ def run_b200(a):
     roofline = {
         "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak, 3),
         "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4), "traffic": traffic,
+        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                          "kernel on this workload from the committed ncu capture "
+                          "(profiles/gm_iter_value_logistic_n2e20_c1024.md), not measured by "
+                          "this run",
         "peak_source": f"nominal {n_sm} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz "
                        "(median SM clock sampled in the timed region; "
                        "MEASURED_PEAKS.json has no FP32 figure)",
@@ -466,6 +546,15 @@ def run_b200(a):
     if rank == 0 and world == 1 and not a.no_da:
         da = da_measure(w, C, a.da_warmup, a.da_iters)
 
+    configs = None
+    if rank == 0 and world == 1 and not a.no_configs:
+        configs = configs_measure(a.configs_only.split(","), a.configs_obs_shift, n_warm=1,
+                                  n_timed=3)
+
+    pt_da = None
+    if rank == 0 and world == 1 and not a.no_pt_da:
+        pt_da = pt_da_measure(a.pt_da_warmup, a.pt_da_iters)
+
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -483,7 +572,10 @@ def run_b200(a):
                    "rng": "philox", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "engine": engine, "interpreter_engine": interp,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "delayed_acceptance": da,
+        "delayed_acceptance": da, "logp_rel_err": logp_err,
+        "logp_rel_err_note": "max over 32 chains of |sampler's log posterior of its final state "
+                             "- f64 oracle| / |oracle|",
+        "configs": configs, "pt_da": pt_da,
         "clocks": clocks, "wall_s_timed_region": wall,
         "accept_rate_mean": float(np.mean(acc)),
     }
@@ -538,26 +630,45 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
-def run_configs(a, n_warm=2, n_timed=6):
-    """Full-size timing of the other configurations: per configuration one
+# Essential work per chain-observation of each configuration's iteration
+# (FP32 flops, FMA = 2, after common subexpressions and parameter-only values
+# are hoisted; MUFU = exp/log/ex2/rcp-class operations), as the model is
+# written: the units behind each configuration's roofline fractions.
+CONFIG_WORK = {
+    "poisson": {"flop": 98.0, "mufu": 1.0,
+                "what": "forward 50 flop + 1 exp, adjoint of 24 parameters 48 flop (MALA)"},
+    "mixture": {"flop": 20.0, "mufu": 5.0,
+                "what": "two Gaussian kernels, their weights and the log (RWM)"},
+    "student_t": {"flop": 133.0, "mufu": 1.0,
+                  "what": "64-term linear predictor, scaled residual, log (DE)"},
+    "student_t_mala": {"flop": 263.0, "mufu": 1.0,
+                       "what": "forward 133 flop + adjoint of 65 parameters 130 flop (MALA)"},
+}
+MUFU_PER_SM_CLK = 16  # SFU lanes per SM per clock
+
+
+def configs_measure(configs, obs_shift=0, n_warm=2, n_timed=6, logp_points=16):
+    """Timing of the other configurations at full size: per configuration one
     session, `n_warm` untimed iterations, then `n_timed` single-iteration
     advances, each after an L2 flush and bracketed by CUDA events on the
-    session's stream."""
+    session's stream; then (untimed) the log posterior the sampler holds for
+    `logp_points` chains against the f64 oracle.  Returns one dict per
+    configuration."""
     import torch
 
     from gpumetropolis_b200 import _native
     from gpumetropolis_b200 import workloads as W
-    from gpumetropolis_b200.build import build
-    build()
-    if not _native.available():
-        raise SystemExit("gpum_b200: no usable sm_100 device")
     dev = torch.device("cuda", 0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
     import inspect
-    for label in a.configs_only.split(","):
+    out = []
+    for label in configs:
         name = label.replace("_mala", "")
         full = inspect.signature(W.ALL[name]).parameters["n_obs"].default
-        w = W.make(name, n_obs=max(1024, full >> max(a.configs_obs_shift, 0)))
+        t_gen = time.perf_counter()
+        w = W.make(name, n_obs=max(1024, full >> max(obs_shift, 0)))
+        t_gen = time.perf_counter() - t_gen
         m = w.model
         C, N, npar = w.n_chains, w.n_obs, m.n_params
         rng = np.random.default_rng(7)
@@ -585,36 +696,65 @@ def run_configs(a, n_warm=2, n_timed=6):
         sd = np.full((C, npar), step)
         sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
                                npar, w.data, m.n_cols, N)
-        if ladder:
-            sess.set_exchange(ladder, 10)
-        sess.prepare(init, sd, temps, n_warm + n_timed, 3, mode, gamma, 1e-3,
-                     rng=_native.RNG_PHILOX)
-        sess.advance(n_warm)
-        sess.sync()
-        stream = torch.cuda.ExternalStream(sess.stream, device=dev)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(n_timed)]
-        torch.cuda.synchronize()
-        with torch.cuda.stream(stream):
-            for s0, s1 in ev:
-                flush.zero_()
-                s0.record(stream)
-                sess.advance(1)
-                s1.record(stream)
-        torch.cuda.synchronize()
-        ms = float(np.mean([s0.elapsed_time(s1) for s0, s1 in ev]))
-        _, acc, last, _ = sess.fetch(want_draws=False)
-        sess.close()
-        print(json.dumps({
+        try:
+            if ladder:
+                sess.set_exchange(ladder, 10)
+            sess.prepare(init, sd, temps, n_warm + n_timed, 3, mode, gamma, 1e-3,
+                         rng=_native.RNG_PHILOX)
+            sess.advance(n_warm)
+            sess.sync()
+            stream = torch.cuda.ExternalStream(sess.stream, device=dev)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(n_timed)]
+            torch.cuda.synchronize()
+            with Clocks(0) as clk:
+                clk.mark_start()
+                with torch.cuda.stream(stream):
+                    for s0, s1 in ev:
+                        flush.zero_()
+                        s0.record(stream)
+                        sess.advance(1)
+                        s1.record(stream)
+                torch.cuda.synchronize()
+                clk.mark_end()
+            ms = float(np.mean([s0.elapsed_time(s1) for s0, s1 in ev]))
+            _, acc, last, _ = sess.fetch(want_draws=False)
+            logp = logp_check(sess, w, n=logp_points)
+        finally:
+            sess.close()
+        clocks = clk.summary()
+        mhz = clocks["sm_mhz"] or 1965.0
+        wk = CONFIG_WORK[label]
+        rate = C * N / (ms / 1e3)
+        fp32_peak = n_sm * 128 * 2 * mhz * 1e6
+        mufu_peak = n_sm * MUFU_PER_SM_CLK * mhz * 1e6
+        out.append({
             "config": label, "n_chains": C, "n_obs": N, "n_params": npar, "method": method,
-            "ms_per_iter": round(ms, 3), "chain_obs_per_s": C * N / (ms / 1e3),
+            "ms_per_iter": round(ms, 3), "chain_obs_per_s": rate,
+            "fp32_frac": round(rate * wk["flop"] / fp32_peak, 4),
+            "mufu_frac": round(rate * wk["mufu"] / mufu_peak, 4),
+            "work_per_chain_obs": f"{wk['flop']:.0f} flop + {wk['mufu']:.0f} MUFU: {wk['what']}",
+            "logp_rel_err": logp, "logp_points": logp_points,
             "all_finite": bool(np.all(np.isfinite(last))),
+            "sm_mhz": clocks["sm_mhz"], "clock_reasons": clocks["reasons"],
+            "data_gen_s": round(t_gen, 1),
             "timing": f"{n_timed} single-iteration advances after {n_warm} warm-up, L2 "
-                      "flushed before each, CUDA events on the session stream"}), flush=True)
+                      "flushed before each, CUDA events on the session stream"})
         del w
+    return out
 
 
-def run_pt_da(a, K=16, every=10, seed=21):
+def run_configs(a):
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    for r in configs_measure(a.configs_only.split(","), a.configs_obs_shift):
+        print(json.dumps(r), flush=True)
+
+
+def pt_da_measure(n_warm, n_samp, K=16, every=10, seed=21):
     """Mixture configuration, PT + surrogate delayed acceptance: 8192 chains
     as 512 ladders of K geometric temperatures 1..64 with device exchanges
     every `every` iterations; adaptive warmup (per-chain Robbins-Monro scales
@@ -623,17 +763,9 @@ def run_pt_da(a, K=16, every=10, seed=21):
     state, exact sampling and two-stage sampling of equal length, timed by
     the wall clock around each blocking run (draws copied back in both).
     ESS: multi-chain over the 512 temperature-1 chains, per parameter."""
-    import torch
-
     from gpumetropolis_b200 import _native, api
     from gpumetropolis_b200 import adaptive as AD
     from gpumetropolis_b200 import workloads as W
-    from gpumetropolis_b200.build import build
-    from gpumetropolis_b200.diagnostics import ess_pooled
-    build()
-    if not _native.available():
-        raise SystemExit("gpum_b200: no usable sm_100 device")
-    torch.cuda.set_device(0)
     w = W.make("mixture")
     m = w.model
     C, npar = w.n_chains, m.n_params
@@ -648,7 +780,6 @@ def run_pt_da(a, K=16, every=10, seed=21):
         centre = np.array([math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)])
         cur = centre + rng.normal(0.0, 0.01, (C, npar))
         sd = np.full((C, npar), 1e-3) * np.sqrt(temps)[:, None]
-        n_warm, n_samp = a.pt_da_warmup, a.pt_da_iters
         call.record_at = n_warm // 2
         nb = min(40, max(10, n_warm // 50), n_warm)
         sizes = np.full(nb, n_warm // nb, dtype=np.int64)
@@ -667,8 +798,7 @@ def run_pt_da(a, K=16, every=10, seed=21):
         call.start_da()
         t_train = time.perf_counter() - t
         if call.net is None:
-            print(json.dumps({"pt_da": {"used": False, "reason": call.info.get("reason")}}))
-            return
+            return {"used": False, "reason": call.info.get("reason")}
 
         def timed(f):
             s.sync()
@@ -687,8 +817,7 @@ def run_pt_da(a, K=16, every=10, seed=21):
         exact_frac = (call.exact_evals - e0) / (n_samp * C)
         d_ex = d_ex.reshape((n_samp, C, npar), order="F").astype(np.float64)[:, ::K, :]
         d_da = np.asarray(d_da, dtype=np.float64)[:, ::K, :]
-        e_ex = np.array([ess_pooled(d_ex[:, :, j]) for j in range(npar)])
-        e_da = np.array([ess_pooled(d_da[:, :, j]) for j in range(npar)])
+        e_ex, e_da = _ess_all(d_ex), _ess_all(d_da)
         mc_ex = d_ex.reshape(-1, npar).std(axis=0) / np.sqrt(e_ex)
         mc_da = d_da.reshape(-1, npar).std(axis=0) / np.sqrt(e_da)
         z = np.abs(d_ex.mean(axis=(0, 1)) - d_da.mean(axis=(0, 1))) / np.sqrt(mc_ex**2 + mc_da**2)
@@ -696,7 +825,9 @@ def run_pt_da(a, K=16, every=10, seed=21):
         with np.errstate(invalid="ignore", divide="ignore"):
             x_ex = float(np.nansum(ok_ex) / max(np.sum(att), 1))
             x_da = float(np.nansum(ok_da) / max(np.sum(att), 1))
-        print(json.dumps({"pt_da": {
+        r_da_t = e_da.min() / (t_da + t_train)
+        return {
+            "used": True,
             "config": "mixture N=2^22, 8192 chains = 512 ladders x 16 geometric temperatures "
                       "1..64, device exchanges every %d iterations, surrogate 5-%d-%d-1 on "
                       "<= 2^18 warmup pairs" % (every, cfg["hidden"], cfg["hidden"]),
@@ -711,11 +842,25 @@ def run_pt_da(a, K=16, every=10, seed=21):
                    "ess_per_s_min": r_da},
             "gain_ess_per_s_min": r_da / r_ex,
             "gain_ess_per_s_mean": float((e_da.mean() / t_da) / (e_ex.mean() / t_ex)),
+            "gain_ess_per_s_min_with_training": r_da_t / r_ex,
+            "gain_ess_per_s_mean_with_training":
+                float((e_da.mean() / (t_da + t_train)) / (e_ex.mean() / t_ex)),
             "posterior_mean_max_z": float(z.max()),
-            "ess": "multi-chain over the 512 temperature-1 chains, per parameter"}}),
-            flush=True)
+            "ess": "multi-chain over the 512 temperature-1 chains, per parameter"}
     finally:
         call.close()
+
+
+def run_pt_da(a):
+    import torch
+
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    torch.cuda.set_device(0)
+    print(json.dumps({"pt_da": pt_da_measure(a.pt_da_warmup, a.pt_da_iters)}), flush=True)
 
 
 def main():

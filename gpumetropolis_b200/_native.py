@@ -102,6 +102,7 @@ SIGNATURES = {
     "gpum_b200_session_fetch": (C.c_int, [C.c_void_p, _f32p, _f32p, _f64p,
                                           C.POINTER(C.c_uint32), _errp, _sz]),
     "gpum_b200_session_launches": (C.c_uint64, [C.c_void_p]),
+    "gpum_b200_session_selftest_wait": (C.c_int, [C.c_void_p, C.c_uint32, _errp, _sz]),
     "gpum_b200_session_stream": (C.c_void_p, [C.c_void_p]),
     "gpum_b200_session_destroy": (None, [C.c_void_p]),
     "gpum_b200_run_de_sync": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32, _f64p, C.c_uint32,
@@ -402,6 +403,12 @@ class Session:
             self._h, int(t0), int(n), _p(cm, C.c_double), _p(c2, C.c_double),
             _p(pm, C.c_double), _p(p2, C.c_double), err, _ERRLEN), err)
         return cm, c2, pm, p2
+
+    def selftest_wait(self, polls=1024):
+        """Run the bounded-wait self-test (a wait that must run out); raises
+        GpumError with code ERR_DEVICE, as a run whose device wait ran out."""
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_selftest_wait(self._h, int(polls), err, _ERRLEN), err)
 
     def state(self):
         """Current chain states (C, np)."""

@@ -59,19 +59,30 @@ def write_embedded() -> str:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel, then link the library."""
     if not force and not _stale():
         return LIB
     write_embedded()
-    tmp = LIB + f".{os.getpid()}.tmp"
-    cmd = [nvcc(), *host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
-           "--shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-           "-I", os.path.join(ROOT, "include"), "-o", tmp]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-lcudart", "-ldl"]
+    from concurrent.futures import ThreadPoolExecutor
+    import tempfile
+    common = [nvcc(), *host_compiler(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-I", os.path.join(ROOT, "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+    with tempfile.TemporaryDirectory(prefix="gpum_build_") as tmpdir:
+        def compile_one(f):
+            obj = os.path.join(tmpdir, f + ".o")
+            cmd = common + ["-c", os.path.join(CSRC, f), "-o", obj]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            return obj
+        with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            objs = list(ex.map(compile_one, SOURCES))
+        tmp = LIB + f".{os.getpid()}.tmp"
+        subprocess.run([nvcc(), *host_compiler(), *ARCH, "--shared", "-o", tmp, *objs,
+                        "-lcudart", "-ldl"], check=True)
     os.replace(tmp, LIB)
     return LIB
 

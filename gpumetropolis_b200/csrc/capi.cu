@@ -1319,6 +1319,18 @@ int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, double* o
   });
 }
 
+int gpum_b200_session_selftest_wait(gpum_b200_session* s, uint32_t polls, char* err,
+                                    size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr, "session is NULL");
+    require(polls >= 1 && polls <= (1u << 20), "polls must be in 1..2^20");
+    selftest_wait_kernel<<<1, 32, 0, s->stream>>>(s->d_err.p, polls, 50000000ull);
+    GPUM_CK(cudaGetLastError());
+    ++s->launches;
+    s->check_device_error();
+  });
+}
+
 int gpum_b200_session_run_da(gpum_b200_session* s, gpum_b200_mlp* surrogate, const double* init,
                              const double* sd, const double* temps, uint32_t n_chains,
                              uint32_t n_iter, uint32_t seed, uint32_t mode, double gamma,

@@ -478,7 +478,9 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
   for (int k = 0; k < nt; ++k) {
     const int st = k & 1;
     const float* tile = xs + st * stage_floats;
+    int gave_up = 0;
     if (staged && !mbar_wait_bounded(&bars[st], (uint32_t)((k >> 1) & 1))) {
+      gave_up = 1;
       if (lane == 0) atomicOr(E.err, DEV_ERR_TMA_TIMEOUT);
     }
     const int obs0 = (t0 + k) * T;
@@ -553,7 +555,19 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
         }
       }
     }
-    __syncthreads();  // every warp is done with this stage
+    // Every warp is done with this stage.  A wait that gave up anywhere in
+    // the CTA (the error bit is set) stops the tile loop for the whole CTA:
+    // no more loads are issued, thread 0 waits (bounded) for the loads still
+    // in flight into this CTA's stages, and the CTA goes on to the reduction
+    // and the ticket so the chain block's bookkeeping stays consistent.
+    if (__syncthreads_or(gave_up)) {
+      if (tid == 0 && staged) {
+        mbar_wait_bounded(&bars[st], (uint32_t)((k >> 1) & 1));
+        if (k + 1 < nt) mbar_wait_bounded(&bars[st ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+      }
+      __syncthreads();
+      break;
+    }
     if (tid == 0 && staged && k + 2 < nt) {
       mbar_expect_tx(&bars[st], tile_bytes);
       tma_load_2d(xs + st * stage_floats, tmap, &bars[st], (t0 + k + 2) * T, 0);

@@ -25,6 +25,8 @@ struct __align__(64) TmapDesc {
 // reads it after every run and turns it into a status code.
 enum DevErr : uint32_t {
   DEV_ERR_TMA_TIMEOUT = 1u << 0,   // a tile never arrived within the wait limit
+  // (1u << 1 is the tensor-core commit timeout of tc_gemm.cuh)
+  DEV_ERR_WAIT_SELFTEST = 1u << 2, // the self-test's wait ran out, as it must
 };
 
 // ------------------------------------------------------------- mbarrier/TMA
@@ -67,6 +69,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   for (uint32_t i = 0; i < kWaitLimit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+
+// Nanosecond clock of the GPU, for waits bounded in time as well as polls.
+__device__ __forceinline__ uint64_t gm_globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
 // 16-byte shared-memory load that the compiler may not merge with an earlier

@@ -56,6 +56,28 @@ iter_kernel(const __grid_constant__ EvalProg prog, const __grid_constant__ TmapD
   run_iteration<G, 1, InterpBody<G, D>, InterpPrior>(&tmap, E, A, phase, body);
 }
 
+// ------------------------------------------------------- failure self-test
+// The device-failure path end to end: an mbarrier that expects one arrival
+// and gets none, polled by every thread at most `polls` times and for at
+// most `max_ns` nanoseconds; the wait runs out, thread 0 sets the error word
+// the host reads after every run, and the kernel returns (no copy or MMA is
+// in flight, nothing hangs).
+static __global__ void selftest_wait_kernel(uint32_t* err, uint32_t polls, uint64_t max_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint64_t t0 = gm_globaltimer();
+  bool done = false;
+  for (uint32_t i = 0; i < polls && !done; ++i) {
+    done = mbar_try_wait(&bar, 0u);
+    if (gm_globaltimer() - t0 > max_ns) break;
+  }
+  if (__syncthreads_or(done ? 0 : 1) && threadIdx.x == 0) atomicOr(err, DEV_ERR_WAIT_SELFTEST);
+}
+
 // ------------------------------------------------------------- helpers
 // Row-major f64 rows [r0, r0+nr) -> column-major f32 [ncols][ld].
 static __global__ void convert_rows_kernel(const double* __restrict__ src, float* __restrict__ dst,

@@ -58,7 +58,12 @@ int scratch_for_device(void** out, char* err, size_t len) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
-      return fail(err, len, GPUM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+      if (err && len)
+        std::snprintf(err, len,
+                      "cudaGetSymbolAddress of the scratch array failed (%s); the 16 MiB "
+                      "array is placed when the library's device code first loads",
+                      cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? GPUM_ERR_NOMEM : GPUM_ERR_CUDA;
     }
     g_noalloc_ptr[dev] = p;
   }
@@ -127,6 +132,8 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
     return fail(err, err_len, GPUM_ERR_UNSUPPORTED, "more than 2^31 observations");
   if (n_points == 0) return GPUM_OK;
   if (!d_points || !d_out) return fail(err, err_len, GPUM_ERR_INVALID, "NULL points or out");
+  // A model with no data columns still adds its per-observation term once
+  // per observation (n_obs times); only then is no data pointer needed.
   const bool has_data = n_cols > 0 && n_obs > 0;
   if (has_data) {
     if (!d_data) return fail(err, err_len, GPUM_ERR_INVALID, "NULL data pointer");
@@ -147,7 +154,7 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
   cudaStream_t st = (cudaStream_t)stream;
   unsigned char* base = static_cast<unsigned char*>(scratch);
   uint32_t* d_err = reinterpret_cast<uint32_t*>(base);
-  if (prog.n_uops == 0 || !has_data) {
+  if (prog.n_uops == 0 || n_obs == 0) {
     // empty program or no observations: every sum is zero
     if (cudaMemsetAsync(d_out, 0, sizeof(double) * n_points, st) != cudaSuccess)
       return fail(err, err_len, GPUM_ERR_CUDA, "cudaMemsetAsync on the output failed");
@@ -159,7 +166,8 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
   const void* fn = depth <= 8 ? (const void*)iter_kernel<8, 8>
                               : (depth <= 16 ? (const void*)iter_kernel<4, 16>
                                              : (const void*)iter_kernel<2, 32>);
-  const int T = std::max(32, std::min(256, (int)((8192 / n_cols) / 32 * 32)));
+  const int T = n_cols > 0 ? std::max(32, std::min(256, (int)((8192 / n_cols) / 32 * 32)))
+                           : 256;
   const int n = (int)std::min<size_t>(n_points, 1u << 24);
   if ((size_t)n != n_points) return fail(err, err_len, GPUM_ERR_UNSUPPORTED, "too many points");
   const int groups = (n + G - 1) / G;
@@ -194,9 +202,10 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
   const int tiles_per_cta = (ntiles + nob - 1) / nob;
   nob = (ntiles + tiles_per_cta - 1) / tiles_per_cta;
 
+  // Without data columns the kernel stages no tiles and never reads the map.
   CUtensorMap tm;
   std::memset(&tm, 0, sizeof tm);
-  {
+  if (has_data) {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=

@@ -127,6 +127,7 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
   const uint32_t sa_addr = smem_addr(sa), sb_addr = smem_addr(sb);
   const uint32_t lbo_a = (kGemmBM / 8) * 128, lbo_b = (BN / 8) * 128;
   bool ok = true;
+  uint32_t fail_parity = 0;  // phase of the commit a wait gave up on
 
   // Staging: each thread owns kLA + kLB 16-byte chunks of a K slice.  All
   // global loads of a slice are issued back to back into registers, and the
@@ -179,12 +180,15 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
     }
     if (k0 + kGemmBK < kend) load_slice(k0 + kGemmBK);  // overlaps the MMAs
     __syncwarp();
-    if (!mbar_wait_bounded(bar, (uint32_t)(it & 1))) {
+    fail_parity = (uint32_t)(it & 1);
+    if (!mbar_wait_bounded(bar, fail_parity)) {
       ok = false;
       if (lane == 0) atomicOr(err, DEV_ERR_MMA_TIMEOUT);
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
+    // block-uniform: a wait that gave up in any thread ends the K loop and
+    // skips the epilogue in every thread
+    ok = __syncthreads_and(ok) != 0;
     if (!ok) break;
   }
 
@@ -224,6 +228,9 @@ tc_gemm_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restr
       }
     }
   }
+  // After a wait that gave up, give the MMAs in flight one more bounded wait
+  // before the tensor memory is released.
+  if (!ok && tid == 0) mbar_wait_bounded(bar, fail_parity);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kTmemCols);

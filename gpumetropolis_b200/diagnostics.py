@@ -63,8 +63,20 @@ def ess(draws, warmup: int | None = None) -> float:
     return float(sum(ess_chain(x[w:, c]) for c in range(x.shape[1])))
 
 
-def ess_pooled(draws) -> float:
-    """Multi-chain ESS of an ``(n_iter, n_chains)`` array (all draws kept)."""
+def acov_chain_mean(xc: np.ndarray) -> np.ndarray:
+    """Autocovariance (divisor n) at lags 0..n-1 of each column of the
+    centred ``(n, m)`` array, averaged over the m columns."""
+    n = xc.shape[0]
+    L = 1 << int(np.ceil(np.log2(2 * n)))
+    f = np.fft.rfft(xc, L, axis=0)
+    acov = np.fft.irfft(f * np.conj(f), L, axis=0)[:n] / n       # (n, m), divisor n
+    return acov.mean(axis=1)
+
+
+def ess_pooled(draws, acov_mean_fn=None) -> float:
+    """Multi-chain ESS of an ``(n_iter, n_chains)`` array (all draws kept).
+    ``acov_mean_fn`` replaces :func:`acov_chain_mean` (e.g. the same FFTs
+    on a GPU for thousands of chains)."""
     x = np.asarray(draws, dtype=np.float64)
     if x.ndim == 1:
         x = x[:, None]
@@ -72,10 +84,7 @@ def ess_pooled(draws) -> float:
     if n < 4:
         return float(n * m)
     xc = x - x.mean(axis=0)
-    L = 1 << int(np.ceil(np.log2(2 * n)))
-    f = np.fft.rfft(xc, L, axis=0)
-    acov = np.fft.irfft(f * np.conj(f), L, axis=0)[:n] / n       # (n, m), divisor n
-    acov_mean = acov.mean(axis=1)
+    acov_mean = (acov_mean_fn or acov_chain_mean)(xc)
     W = acov_mean[0] * n / (n - 1)
     B_over_n = x.mean(axis=0).var(ddof=1) if m > 1 else 0.0
     var_plus = W * (n - 1) / n + B_over_n

@@ -101,12 +101,17 @@ def mixture(n_obs: int = 1 << 22, seed: int = 4) -> Workload:
 
 def student_t(n_obs: int = 1 << 24, seed: int = 5, p: int = 64) -> Workload:
     rng = np.random.Generator(np.random.PCG64(seed))
-    X = np.empty((n_obs, p), np.float32)
-    X[:, 0] = rng.standard_normal(n_obs, dtype=np.float32)
+    # Covariates generated column by column (contiguous rows of XT, so the
+    # AR(1) recursion streams memory), then written into the row-major data.
+    XT = np.empty((p, n_obs), np.float32)
+    XT[0] = rng.standard_normal(n_obs, dtype=np.float32)
     for j in range(1, p):
-        X[:, j] = 0.6 * X[:, j - 1] + 0.8 * rng.standard_normal(n_obs, dtype=np.float32)
+        XT[j] = 0.6 * XT[j - 1] + 0.8 * rng.standard_normal(n_obs, dtype=np.float32)
     beta = rng.normal(0.0, 0.3, p)
-    y = X.astype(np.float64) @ beta + 1.5 * rng.standard_t(4.0, n_obs)
+    y = np.zeros(n_obs)
+    for j in range(p):
+        y += beta[j] * XT[j].astype(np.float64)
+    y += 1.5 * rng.standard_t(4.0, n_obs)
     y = y.astype(np.float32).astype(np.float64)
     params = [f"b{j}" for j in range(1, p + 1)] + ["ls"]
     xs = [f"x{j}" for j in range(1, p + 1)]
@@ -114,7 +119,12 @@ def student_t(n_obs: int = 1 << 24, seed: int = 5, p: int = 64) -> Workload:
     ll = (f"~ lgamma(2.5) - lgamma(2) - 0.5 * log(4 * 3.141592653589793) - ls"
           f" - 2.5 * log(1 + ((y - ({lp})) / exp(ls))^2 / 4)")
     m = gpum_model(ll, params=params, data=xs + ["y"], prior=_prior(params, 10.0))
-    data = np.concatenate([X.astype(np.float64), y[:, None]], axis=1)
+    data = np.empty((n_obs, p + 1))
+    step = 1 << 16
+    for r0 in range(0, n_obs, step):
+        data[r0:r0 + step, :p] = XT[:, r0:r0 + step].T
+    data[:, p] = y
+    del XT
     return Workload("student_t", m, data, {"beta": beta, "sigma": 1.5}, 8192, 2000, "de")
 
 

@@ -126,9 +126,13 @@ GPUM_API int gpum_b200_loglik_pointwise(const uint32_t* code, size_t n_code, con
  * the caller's DEVICE buffers -- data column-major f32 d_data[j*ld + i]
  * (ld >= n_obs, ld % 4 == 0, 16-byte aligned), points f64 n_points x
  * n_params, out f64 n_points -- and the scratch is a fixed 16 MiB
- * __device__ array per GPU, held from library load to process exit; inputs
- * needing more (n_params x points beyond it) are rejected with
- * GPUM_ERR_UNSUPPORTED.  Work is enqueued on `stream` (a cudaStream_t, NULL
+ * __device__ array per GPU, held until process exit from the moment the
+ * library's device code is loaded on that GPU (at the first call that uses
+ * it under CUDA's default lazy loading, at library load with
+ * CUDA_MODULE_LOADING=EAGER; a GPU without 16 MiB free fails that first
+ * call with GPUM_ERR_NOMEM); inputs needing more (n_params x points beyond
+ * it) are rejected with GPUM_ERR_UNSUPPORTED.  With n_cols == 0 (a
+ * per-observation term that reads no data) d_data may be NULL.  Work is enqueued on `stream` (a cudaStream_t, NULL
  * for the legacy stream) and the call waits for it.  Calls share the scratch:
  * calls that overlap on the GPU race.  The first call on a device sets up
  * the scratch address; make it before any stream capture.  The program is
@@ -255,6 +259,16 @@ GPUM_API int gpum_b200_session_draw_moments(gpum_b200_session* s, uint32_t t0, u
 /* The current chain states (n_chains x n_params, f64). */
 GPUM_API int gpum_b200_session_state(gpum_b200_session* s, double* out_state, char* err,
                                      size_t err_len);
+
+/* The device-failure path, exercised without a fault: a one-warp kernel on
+ * the session's stream waits on an mbarrier that nothing arrives on, gives
+ * up after `polls` polls (1..2^20) or 50 ms, sets the session's device error
+ * word and returns; the call then reports GPUM_ERR_DEVICE exactly as a run
+ * whose bounded TMA or tensor-core wait ran out does, clears the word, and
+ * the session stays usable.  No counterpart in the reference (its kernels
+ * have no bounded waits); for tests of failure detection. */
+GPUM_API int gpum_b200_session_selftest_wait(gpum_b200_session* s, uint32_t polls, char* err,
+                                             size_t err_len);
 
 /* The session's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events with the session's launches. */

@@ -1,4 +1,4 @@
-"""Bytecode -> C -> gcc -> dlopen: the CPU compiled log-likelihood -- TEST/BASELINE ONLY.
+"""Bytecode -> C -> gcc -> dlopen: the CPU compiled log-likelihood -- TEST AND CPU-BASELINE ONLY.
 
 Restates the reference's Cranelift JIT (``src/rust/src/jit.rs:441-631``): the
 per-observation program becomes straight-line f64 code inside the loop over
@@ -38,8 +38,11 @@ def _c_double(v: float) -> str:
     return repr(float(v))
 
 
-def emit_c(code, consts) -> str:
-    """C source of ``double gpum_jit_loglik(params, data, n_obs, n_cols)``."""
+def emit_c(code, consts, absolute=False) -> str:
+    """C source of ``double gpum_jit_loglik(params, data, n_obs, n_cols)``;
+    with ``absolute`` it returns the sum of the per-observation values'
+    absolute values instead (the scale of the sum's rounding error when the
+    terms cancel)."""
     code = np.asarray(code, dtype=np.uint32).reshape(-1)
     n = code.size // 2
     lines = [
@@ -73,15 +76,17 @@ def emit_c(code, consts) -> str:
                     6: f"{l} / {r}"}.get(op, f"pow({l}, {r})")
             lines.append(f"    const double {v} = {expr};")
         stack.append(v)
-    lines.append(f"    acc += {stack[0] if n else '0.0'};")
+    term = stack[0] if n else "0.0"
+    lines.append(f"    acc += fabs({term});" if absolute else f"    acc += {term};")
     lines += ["  }", "  return acc;", "}"]
     return "\n".join(lines) + "\n"
 
 
-def compile_loglik(code, consts):
+def compile_loglik(code, consts, absolute=False):
     """Compile and load; returns a ctypes function pointer usable by
-    :func:`oracle.oracle.run` (``jit=``)."""
-    src = emit_c(code, consts)
+    :func:`oracle.oracle.run` (``jit=``) and :func:`oracle.oracle.jit_batch`
+    (``absolute``: the sum of absolute per-observation values)."""
+    src = emit_c(code, consts, absolute)
     key = hashlib.sha1(src.encode()).hexdigest()[:16]
     if key in _keep:
         return _keep[key][1]

@@ -273,6 +273,76 @@ void gpo_loglik_pointwise(const uint32_t *code, size_t n_instr, const double *co
 typedef double (*gpo_loglik_fn)(const double *params, const double *data,
                                 int64_t n_obs, int64_t n_cols);
 
+/* Checker at full configuration sizes (not a reference function): the
+ * compiled evaluator `fn` at each point, parallel over points.  With the
+ * evaluator cjit emits, the result is gpo_loglik_batch's value (same f64
+ * operations in the same order). */
+void gpo_jit_batch(gpo_loglik_fn fn, size_t n_params, const double *data, size_t n_cols,
+                   size_t n_obs, const double *points, size_t n_points, double *out,
+                   int n_threads) {
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic) num_threads(n_threads)
+    for (long p = 0; p < (long)n_points; ++p)
+        out[p] = fn(points + p * n_params, data, (int64_t)n_obs, (int64_t)n_cols);
+}
+
+/* Checker at full configuration sizes (not a reference function): the
+ * data-term gradient of cpu_native.rs:306-329 at each point, and per
+ * component the sum over observations of the per-observation gradient's
+ * absolute value (the scale a cancelling sum's rounding error is bounded
+ * by).  Parallel over (point, block of `block` observations); the blocks of
+ * a point are added in block order.  out_grad, out_abs: point-major. */
+int gpo_grad_abs_batch(const uint32_t *code, size_t n_instr, const double *consts,
+                       size_t n_params, const double *data, size_t n_cols, size_t n_obs,
+                       const double *points, size_t n_points, size_t block,
+                       double *out_grad, double *out_abs, int n_threads) {
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+    if (block < 1) block = 1;
+    const size_t nb = n_obs ? (n_obs + block - 1) / block : 1;
+    double *part = (double *)calloc(n_points * nb * 2 * (n_params ? n_params : 1),
+                                    sizeof(double));
+    if (!part) return -1;
+    int err = 0;
+#pragma omp parallel num_threads(n_threads) reduction(| : err)
+    {
+        gpo_tape w;
+        double *g1 = (double *)malloc((n_params ? n_params : 1) * sizeof(double));
+        const int ok = gpo_tape_alloc(&w, n_instr) == 0 && g1 != NULL;
+        if (!ok) err = 1;
+        /* every thread reaches the worksharing loop; one without scratch skips */
+#pragma omp for schedule(dynamic)
+            for (long t = 0; t < (long)(n_points * nb); ++t) {
+                if (!ok) continue;
+                const size_t p = (size_t)t / nb, b = (size_t)t % nb;
+                double *pg = part + (size_t)t * 2 * n_params, *pa = pg + n_params;
+                const size_t i1 = (b + 1) * block < n_obs ? (b + 1) * block : n_obs;
+                for (size_t i = b * block; i < i1; ++i) {
+                    for (size_t j = 0; j < n_params; ++j) g1[j] = 0.0;
+                    gpo_eval_grad(code, n_instr, consts, points + p * n_params,
+                                  data + i * n_cols, &w, g1);
+                    for (size_t j = 0; j < n_params; ++j) {
+                        pg[j] += g1[j];
+                        pa[j] += fabs(g1[j]);
+                    }
+                }
+            }
+        gpo_tape_free(&w);
+        free(g1);
+    }
+    for (size_t p = 0; p < n_points; ++p)
+        for (size_t j = 0; j < n_params; ++j) {
+            double sg = 0.0, sa = 0.0;
+            for (size_t b = 0; b < nb; ++b) {
+                sg += part[((p * nb + b) * 2) * n_params + j];
+                sa += part[((p * nb + b) * 2 + 1) * n_params + j];
+            }
+            out_grad[p * n_params + j] = sg;
+            out_abs[p * n_params + j] = sa;
+        }
+    free(part);
+    return err ? -1 : 0;
+}
+
 typedef struct {
     const uint32_t *code; size_t n_instr; const double *consts;
     const uint32_t *prior_code; size_t n_prior; const double *prior_consts;

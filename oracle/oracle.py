@@ -58,6 +58,11 @@ def lib():
                               _f64p, _f64p, _f64p, sz, sz, C.c_uint32, C.c_uint32,
                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int,
                               _f32p, _f32p, _f64p]
+        L.gpo_jit_batch.restype = None
+        L.gpo_jit_batch.argtypes = [C.c_void_p, sz, _f64p, sz, sz, _f64p, sz, _f64p, C.c_int]
+        L.gpo_grad_abs_batch.restype = C.c_int
+        L.gpo_grad_abs_batch.argtypes = [_u32p, sz, _f64p, sz, _f64p, sz, sz, _f64p, sz, sz,
+                                         _f64p, _f64p, C.c_int]
         L.gpo_run_de_sync.restype = C.c_int
         L.gpo_run_de_sync.argtypes = [_u32p, sz, _f64p, _u32p, sz, _f64p, sz, _f64p, sz,
                                       sz, _f64p, _f64p, sz, sz, C.c_uint32, C.c_double,
@@ -128,6 +133,42 @@ def loglik_pointwise(code, consts, n_params, data, n_cols, n_obs, points):
     """``out[p * n_obs + i]`` per-observation log-likelihood (``:371-391``)."""
     return _batch("gpo_loglik_pointwise", code, consts, n_params, data, n_cols, n_obs,
                   points, n_obs)
+
+
+def jit_batch(fn, n_params, data, n_cols, n_obs, points, n_threads=0):
+    """A compiled evaluator (:func:`oracle.cjit.compile_loglik`) at each point,
+    parallel over points: ``loglik_batch``'s value at full configuration
+    sizes (the compiled code performs the interpreter's f64 operations in the
+    same order).  Checker only; no reference counterpart."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1)
+    n_points = pts.size // n_params
+    out = np.zeros(max(n_points, 1))
+    lib().gpo_jit_batch(C.cast(fn, C.c_void_p), n_params, _data(data, n_cols, n_obs), n_cols,
+                        n_obs, pts if pts.size else np.zeros(1), n_points, out, n_threads)
+    return out[:n_points]
+
+
+def grad_abs_batch(code, consts, n_params, data, n_cols, n_obs, points, block=4096,
+                   n_threads=0):
+    """``grad_batch``'s gradient (``cpu_native.rs:306-329``) at each point and,
+    per component, the sum over observations of the per-observation
+    gradient's absolute value (the scale that bounds the rounding error of a
+    sum that cancels).  Parallel over (point, block of observations), blocks
+    added in order.  Returns ``(grad, abs_sum)``, both ``(n_points,
+    n_params)``.  Checker only; no reference counterpart."""
+    code, consts = _prog(code, consts)
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1)
+    n_points = pts.size // n_params
+    g = np.zeros(max(n_points * n_params, 1))
+    a = np.zeros(max(n_points * n_params, 1))
+    rc = lib().gpo_grad_abs_batch(code, code.size // 2, consts, n_params,
+                                  _data(data, n_cols, n_obs), n_cols, n_obs,
+                                  pts if pts.size else np.zeros(1), n_points, block, g, a,
+                                  n_threads)
+    if rc != 0:
+        raise MemoryError("oracle grad_abs_batch failed to allocate")
+    return (g[:n_points * n_params].reshape(n_points, n_params),
+            a[:n_points * n_params].reshape(n_points, n_params))
 
 
 def run(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,

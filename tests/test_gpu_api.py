@@ -19,7 +19,7 @@ def _mcse(d):
 
 
 def test_config1_adaptive_rwm_recovers_closed_form(gpu):
-    # y ~ N(3.4, 2^2), N = 20,000; rwm, 8 chains x 3,000
+    # the Gaussian-mean configuration: y ~ N(3.4, 2^2), N = 20,000; rwm, 8 chains x 3,000
     # iterations, adaptive warmup, proposal_sd 0.5; posterior N(mean y, 4/N)
     w = W.make("gaussian")
     fit = gpu_metropolis(w.model, data={"y": w.data[:, 0]}, proposal_sd=0.5, n_iter=3000,

@@ -138,7 +138,7 @@ def test_reproducible_from_the_seed(gpu):
 
 @pytest.mark.parametrize("rng_kind", [0, 1])
 def test_gaussian_posterior_recovered(gpu, rng_kind):
-    # BASELINE config 1 data: y ~ N(3.4, 2^2), N = 20,000; closed form N(mean y, 4/N)
+    # the Gaussian-mean configuration: y ~ N(3.4, 2^2), N = 20,000; closed form N(mean y, 4/N)
     w = W.make("gaussian")
     C, n_iter = 8, 3000
     init = np.linspace(2.5, 4.5, C).reshape(C, 1)

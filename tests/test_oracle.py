@@ -85,6 +85,33 @@ def test_jit_matches_interpreter_bitwise():
     assert np.all(np.isfinite(ref))
 
 
+@pytest.mark.parametrize("name", ["logistic", "poisson", "mixture", "student_t"])
+def test_full_size_checkers_agree_with_the_oracle(name):
+    # The checkers used at the configurations' full sizes: the compiled
+    # evaluator per point equals loglik_batch bitwise, its absolute-value
+    # variant bounds |loglik|, and the blocked parallel gradient equals
+    # grad_batch up to the f64 reordering of the sum.
+    w = W.make(name, n_obs=3001)
+    m = w.model
+    pts = np.random.default_rng(1).normal(0, 0.2, (5, m.n_params))
+    if name == "student_t":
+        pts[:, -1] += np.log(1.5)
+    ref = O.loglik_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
+                         w.n_obs, pts)
+    fn = cjit.compile_loglik(m.loglik.code, m.loglik.consts)
+    got = O.jit_batch(fn, m.n_params, w.data, m.n_cols, w.n_obs, pts)
+    assert np.array_equal(got, ref)
+    fa = cjit.compile_loglik(m.loglik.code, m.loglik.consts, absolute=True)
+    ab = O.jit_batch(fa, m.n_params, w.data, m.n_cols, w.n_obs, pts)
+    assert np.all(ab >= np.abs(ref))
+    gref = O.grad_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols, w.n_obs,
+                        pts).reshape(5, -1)
+    g, ga = O.grad_abs_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols,
+                             w.n_obs, pts, block=257)
+    np.testing.assert_allclose(g, gref, rtol=1e-12, atol=1e-12 * np.abs(ga).max())
+    assert np.all(ga >= np.abs(g))
+
+
 def _draws(d, n_iter, C, np_):
     return d.reshape((n_iter, C, np_), order="F")
 
