@@ -79,6 +79,8 @@ SIGNATURES = {
     "gpum_b200_mlp_train": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, C.c_uint32, C.c_double,
                                       _f32p, _errp, _sz]),
     "gpum_b200_mlp_predict": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
+    "gpum_b200_mlp_predict_grad": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _f64p, _errp,
+                                             _sz]),
     "gpum_b200_mlp_gradients": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, _f32p, _f32p, _errp,
                                           _sz]),
     "gpum_b200_mlp_get_params": (C.c_int, [C.c_void_p, _f32p, _errp, _sz]),
@@ -629,6 +631,20 @@ class Surrogate:
         _check(self._lib.gpum_b200_mlp_predict(self._h, _p(th, C.c_double), n,
                                                _p(out, C.c_double), err, _ERRLEN), err)
         return out[:n]
+
+    def predict_grad(self, theta):
+        """(log-likelihood (n,), gradient with respect to the parameters
+        (n, d)) at n points: the drift of the Langevin delayed-acceptance
+        proposal."""
+        th = _f64(theta)
+        n = th.size // self.d
+        out = np.empty(max(n, 1))
+        grad = np.empty(max(n * self.d, 1))
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_predict_grad(self._h, _p(th, C.c_double), n,
+                                                    _p(out, C.c_double), _p(grad, C.c_double),
+                                                    err, _ERRLEN), err)
+        return out[:n], grad[:n * self.d].reshape(n, self.d)
 
     def gradients(self, theta, ll):
         th, y = _f64(theta), _f64(ll)

@@ -174,7 +174,7 @@ class _Backend:
         if self.da_at is not None and self.consumed >= self.da_at:
             self.start_da()
         self._maybe_record(C, n_iter)
-        if self.net is not None and proposal_mode != _native.MODE_MALA:
+        if self.net is not None:
             k = float(self.cfg["step_scale"])
             if proposal_mode in (_native.MODE_RWM, _native.MODE_CHOL) and k != 1.0:
                 sd = np.asarray(sd, dtype=np.float64) * k
@@ -234,7 +234,9 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
 
     ``surrogate``: None/False (exact Metropolis, the reference's behaviour),
     True, or a dict overriding ``SURROGATE_DEFAULTS`` -- delayed acceptance
-    in the sampling phase (rwm, pt, de; needs warmup > 0).
+    in the sampling phase (rwm, pt, de, mala; needs warmup > 0).  With mala
+    the two-stage phase proposes Langevin moves whose drift is the
+    surrogate's log-posterior gradient, so it evaluates no exact gradient.
 
     ``swap_on_device`` (pt): exchanges run on the GPU after every
     ``swap_every`` iterations inside one run instead of between host batches;
@@ -316,9 +318,6 @@ def gpu_metropolis(model: GpumModel, data=None, init=None, proposal_sd=0.1, n_it
 
     scfg = None
     if surrogate is not None and surrogate is not False:
-        if method == "mala":
-            raise GpumInputError("`surrogate` (delayed acceptance) needs a symmetric proposal: "
-                                 'method "rwm", "pt" or "de", not "mala".')
         if warmup <= 0:
             raise GpumInputError("`surrogate` needs warmup > 0: its training pairs come from "
                                  "the warmup's exact evaluations.")

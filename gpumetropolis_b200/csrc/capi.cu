@@ -40,6 +40,9 @@ namespace gpum {
 int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, cudaStream_t st,
               std::string* err);
 int mlp_infer_launches(const gpum_b200_mlp* m, int n);
+int mlp_infer_grad(gpum_b200_mlp* m, const double* theta, int n, int d, double* out_val,
+                   double* out_grad, cudaStream_t st, std::string* err);
+int mlp_infer_grad_launches(const gpum_b200_mlp* m, int n);
 }  // namespace gpum
 
 static_assert(sizeof(CUtensorMap) == sizeof(TmapDesc), "tensor map size");
@@ -220,8 +223,8 @@ struct gpum_b200_session {
   DBuf<double> rec_ll;
   uint64_t rec_cap = 0, rec_count = 0;
   // Delayed acceptance.
-  DBuf<double> sll_x, sll_y, prior_x, prior_y, da_partials;
-  DBuf<uint32_t> da_flag, da_slot, da_active, da_iter, da_stage1;
+  DBuf<double> sll_x, sll_y, prior_x, prior_y, da_partials, da_gs, da_tvals, da_tadj;
+  DBuf<uint32_t> da_flag, da_slot, da_active, da_iter, da_stage1, da_tlhs, da_trhs;
   DBuf<float> da_params;
   Geometry geo_da{};
   EvalArgs E_da{};
@@ -805,7 +808,10 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
 void da_step(gpum_b200_session* s) {
   const int C = s->n_chains, np = (int)s->np;
   std::string e;
-  const int rc = mlp_infer(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->stream, &e);
+  const int rc = s->A.mode == MODE_MALA
+                     ? mlp_infer_grad(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->D.gs,
+                                      s->stream, &e)
+                     : mlp_infer(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->stream, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
   cudaStream_t st = s->stream;
   // 64-thread blocks spread the per-chain f64 work (prior, proposal) over
@@ -837,13 +843,19 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
             float* out_accept, double* out_last, uint32_t* out_exact) {
   require(s != nullptr, "session is NULL");
   require(mlp != nullptr, "surrogate is NULL");
-  require(mode <= 2, "delayed acceptance needs a symmetric proposal: mode 0 (rwm), 1 (de) or 2 "
-                     "(cholesky)");
+  require(mode <= 3, "delayed acceptance takes proposal mode 0 (rwm), 1 (de), 2 (cholesky) or "
+                     "3 (mala: a Langevin move driven by the surrogate's gradient)");
   require(s->n_beta == 0, "delayed acceptance does not support likelihood powers");
+  // The Langevin proposal's drift is the surrogate log-posterior gradient, so
+  // the exact start evaluates values only (as the random walk with the same
+  // preconditioner), and the chains draw their first proposals again below.
+  const bool lang = mode == 3;
+  const bool lang_L = lang && L != nullptr && n_l > 0;
   const uint64_t keep_cap = s->rec_cap;
   s->rec_cap = 0;  // stage-1 rejections leave no exact pair to record
   try {
-    prepare(s, init, sd, temps, C, n_iter, seed, mode, gamma, de_noise, L, n_l, rng);
+    prepare(s, init, sd, temps, C, n_iter, seed, lang ? (lang_L ? 2u : 0u) : mode, gamma,
+            de_noise, L, n_l, rng);
   } catch (...) {
     s->rec_cap = keep_cap;
     throw;
@@ -852,6 +864,20 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   const int np = (int)s->np;
   cudaStream_t st = s->stream;
   const Geometry& g = s->geo;
+  if (lang) {
+    for (auto* b : {&s->gx, &s->gy, &s->mx, &s->my, &s->vbuf, &s->da_gs}) b->ensure((size_t)C * np);
+    const size_t nt = (size_t)C * std::max<size_t>(s->prior_code.size() / 2, 1);
+    s->da_tvals.ensure(nt);
+    s->da_tadj.ensure(nt);
+    s->da_tlhs.ensure(nt);
+    s->da_trhs.ensure(nt);
+    s->A.mode = MODE_MALA;
+    s->A.gx = s->gx.p;
+    s->A.gy = s->gy.p;
+    s->A.mx = s->mx.p;
+    s->A.my = s->my.p;
+    s->A.vbuf = s->vbuf.p;
+  }
   s->sll_x.ensure(C);
   s->sll_y.ensure(C);
   s->prior_x.ensure(C);
@@ -893,12 +919,19 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   D.params = s->da_params.p;
   D.full = s->params.p;
   D.C_pad = g.C_pad;
+  D.gs = lang ? s->da_gs.p : nullptr;
+  D.tvals = lang ? s->da_tvals.p : nullptr;
+  D.tadj = lang ? s->da_tadj.p : nullptr;
+  D.tlhs = lang ? s->da_tlhs.p : nullptr;
+  D.trhs = lang ? s->da_trhs.p : nullptr;
   s->da_mlp = mlp;
   s->da_mlp_launches = 0;
   std::string e;
-  int rc = mlp_infer(mlp, s->state.p, (int)C, np, s->sll_x.p, st, &e);
+  int rc = lang ? mlp_infer_grad(mlp, s->state.p, (int)C, np, s->sll_x.p, D.gs, st, &e)
+                : mlp_infer(mlp, s->state.p, (int)C, np, s->sll_x.p, st, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
-  s->da_mlp_launches = mlp_infer_launches(mlp, (int)C);
+  s->da_mlp_launches = lang ? mlp_infer_grad_launches(mlp, (int)C)
+                            : mlp_infer_launches(mlp, (int)C);
   s->launches += (uint64_t)s->da_mlp_launches;
   da_setup_kernel<<<(C + 255) / 256, 256, 0, st>>>(s->A, D);
   GPUM_CK(cudaGetLastError());

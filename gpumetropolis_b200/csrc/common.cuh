@@ -138,6 +138,82 @@ __device__ inline double prior_interp(const uint32_t* __restrict__ code, int n,
   return st[0];
 }
 
+// Value and gradient of the f64 prior by a reverse-mode tape over its
+// bytecode (the reference's tape AD, cpu_native.rs:148-279, for a program
+// that reads no data): forward pass recording each instruction's value and
+// operands, then adjoints in reverse order with the reference's local
+// derivatives (POW's exponent term only where the base is positive; LGAMMA's
+// derivative the digamma).  The gradient is added into g.  vals/adj/lhs/rhs
+// are this chain's scratch of n entries each.  Used by delayed acceptance
+// with the Langevin proposal, whose drift needs the prior's gradient in
+// either evaluation engine.
+__device__ inline double prior_value_grad_tape(const uint32_t* __restrict__ code, int n,
+                                               const double* __restrict__ cst,
+                                               const double* __restrict__ p, double* g,
+                                               double* vals, double* adj, uint32_t* lhs,
+                                               uint32_t* rhs) {
+  if (n == 0) return 0.0;
+  uint32_t ist[kMaxStackF64];
+  int sp = 0;
+  for (int pc = 0; pc < n; ++pc) {
+    const uint32_t op = code[2 * pc], a = code[2 * pc + 1];
+    if (op <= 2) {
+      vals[pc] = op == 0 ? cst[a] : (op == 1 ? p[a] : 0.0);
+      lhs[pc] = 0xFFFFFFFFu;
+      ist[sp++] = (uint32_t)pc;
+    } else if ((op >= 7 && op <= 10) || op == 12) {
+      const uint32_t l = ist[sp - 1];
+      const double x = vals[l];
+      vals[pc] = op == 7 ? -x : op == 8 ? exp(x) : op == 9 ? log(x) : op == 10 ? sqrt(x)
+                                                                                  : lgamma(x);
+      lhs[pc] = l;
+      rhs[pc] = 0xFFFFFFFFu;
+      ist[sp - 1] = (uint32_t)pc;
+    } else {
+      const uint32_t r = ist[sp - 1], l = ist[sp - 2];
+      const double a0 = vals[l], b0 = vals[r];
+      vals[pc] = op == 3 ? a0 + b0 : op == 4 ? a0 - b0 : op == 5 ? a0 * b0 : op == 6 ? a0 / b0
+                                                      : (b0 == 2.0 ? a0 * a0 : pow(a0, b0));
+      lhs[pc] = l;
+      rhs[pc] = r;
+      ist[sp - 2] = (uint32_t)pc;
+      --sp;
+    }
+  }
+  const int root = n - 1;
+  for (int i = 0; i < n; ++i) adj[i] = 0.0;
+  adj[root] = 1.0;
+  for (int k = n - 1; k >= 0; --k) {
+    const double gk = adj[k];
+    if (gk == 0.0) continue;
+    const uint32_t op = code[2 * k], arg = code[2 * k + 1];
+    const uint32_t l = lhs[k], r = rhs[k];
+    switch (op) {
+      case 0: case 2: break;
+      case 1: g[arg] += gk; break;
+      case 3: adj[l] += gk; adj[r] += gk; break;
+      case 4: adj[l] += gk; adj[r] -= gk; break;
+      case 5: adj[l] += gk * vals[r]; adj[r] += gk * vals[l]; break;
+      case 6:
+        adj[l] += gk / vals[r];
+        adj[r] -= gk * vals[k] / vals[r];
+        break;
+      case 7: adj[l] -= gk; break;
+      case 8: adj[l] += gk * vals[k]; break;
+      case 9: adj[l] += gk / vals[l]; break;
+      case 10: adj[l] += gk * 0.5 / vals[k]; break;
+      case 12: adj[l] += gk * gm_digamma(vals[l]); break;
+      default: {
+        const double a0 = vals[l], b0 = vals[r];
+        adj[l] += gk * b0 * pow(a0, b0 - 1.0);
+        if (a0 > 0.0) adj[r] += gk * vals[k] * log(a0);
+        break;
+      }
+    }
+  }
+  return vals[ist[0]];  // stack slot 0, as the value interpreter returns
+}
+
 // ------------------------------------------------------- uniform streams
 struct Stream {
   int kind;

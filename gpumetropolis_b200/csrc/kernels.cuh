@@ -122,11 +122,15 @@ static __global__ void draws_layout_kernel(const float* __restrict__ in, float* 
 // ===================================================== delayed acceptance
 // Two-stage Metropolis-Hastings (Christen & Fox 2005) with the surrogate
 // log-likelihood s() as stage 1 and the exact log-likelihood l() as stage 2:
-//   stage 1: accept y with min(1, exp([s(y)+p(y) - s(x)-p(x)] / T))
+//   stage 1: accept y with min(1, exp([s(y)+p(y) - s(x)-p(x)] / T) q(x|y)/q(y|x))
 //   stage 2: accept with min(1, exp([(l(y)-l(x)) - (s(y)-s(x))] / T))
-// (p = prior, which cancels in stage 2).  The product of the two acceptance
-// probabilities satisfies detailed balance for the exact tempered posterior,
-// so the target is unchanged; only stage-1 survivors are evaluated exactly.
+// (p = prior, which cancels in stage 2, as does the proposal ratio: the
+// stage-1 acceptance of the reverse move carries its inverse).  The product
+// of the two acceptance probabilities satisfies detailed balance for the
+// exact tempered posterior, so the target is unchanged; only stage-1
+// survivors are evaluated exactly.  The proposal is the random walk, DE, or
+// a Langevin move whose drift is the surrogate log-posterior gradient (so no
+// exact gradient is ever needed).
 namespace gpum {
 
 // ------------------------------------------------- draw moments (adaptation)
@@ -305,7 +309,26 @@ struct DaArgs {
   float* params;     // [np][C_pad] compacted evaluation points
   float* full;       // [np][C_pad] scratch for propose()
   int C_pad;
+  // Langevin proposal (MALA): the surrogate's data-term gradient at the
+  // proposals (at the states during set-up), and the prior tape's scratch
+  double* gs;        // [C][np]
+  double* tvals;     // [C][n_prior]
+  double* tadj;      // [C][n_prior]
+  uint32_t* tlhs;    // [C][n_prior]
+  uint32_t* trhs;    // [C][n_prior]
 };
+
+// Surrogate log-posterior gradient at theta: the surrogate's data-term
+// gradient gs plus the f64 prior's gradient (tape); returns the prior.
+__device__ __forceinline__ double da_post_grad(const ChainArgs& A, const DaArgs& D, int c,
+                                               const double* theta, const double* gs,
+                                               double* g) {
+  const int np = A.np, n = A.n_prior;
+  for (int j = 0; j < np; ++j) g[j] = gs[j];
+  const size_t o = (size_t)c * (size_t)(n > 0 ? n : 1);
+  return prior_value_grad_tape(A.prior_code, n, A.prior_consts, theta, g, D.tvals + o,
+                               D.tadj + o, D.tlhs + o, D.trhs + o);
+}
 
 __device__ __forceinline__ double da_uniform(Stream& rs, uint32_t t, uint32_t k) {
   if (rs.kind == RNG_TRIPLE32) return rs.next();
@@ -315,25 +338,62 @@ __device__ __forceinline__ double da_uniform(Stream& rs, uint32_t t, uint32_t k)
 }
 
 // After the exact start (PH_INIT): the prior at each state, zero counters.
+// With the Langevin proposal (A.mode == MODE_MALA; the start ran with a
+// symmetric mode) also the surrogate log-posterior gradient at each state
+// (D.gs holds the surrogate's data-term gradient there), and every chain
+// draws its first proposal again, now with that drift.
 static __global__ void da_setup_kernel(ChainArgs A, DaArgs D) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c == 0) D.iter[0] = 0;
   if (c >= A.n_chains) return;
-  D.prior_x[c] = InterpPrior::value(A, A.state + (size_t)c * A.np);
+  const double* x = A.state + (size_t)c * A.np;
+  if (A.mode == MODE_MALA) {
+    D.prior_x[c] = da_post_grad(A, D, c, x, D.gs + (size_t)c * A.np, A.gx + (size_t)c * A.np);
+    if (A.n_iter > 0) {
+      Stream rs = make_stream(A, c);
+      rs.it = 0;
+      rs.k = 0x20000000u;  // counters apart from the start's own proposal
+      propose(A, c, rs, D.full, D.C_pad);
+      A.ctr[c] = rs.ctr;
+    }
+  } else {
+    D.prior_x[c] = InterpPrior::value(A, x);
+  }
   D.stage1[c] = 0;
 }
 
+// Stage 1 on the surrogate.  With the Langevin proposal the ratio carries
+// q(x | y) / q(y | x) of the surrogate-driven drift (the reverse drift from
+// the surrogate log-posterior gradient at y, capped as the forward one;
+// cpu_native.rs:704-710 for the exact-gradient form), and the surrogate
+// log posterior at y must be finite (cpu_native.rs:713-714).
 static __global__ void da_stage1_kernel(ChainArgs A, DaArgs D) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= A.n_chains) return;
   const uint32_t t = D.iter[0];
-  const double* y = A.prop + (size_t)c * A.np;
-  const double py = InterpPrior::value(A, y);
+  const int np = A.np;
+  const double* y = A.prop + (size_t)c * np;
+  double py, lqd = 0.0;
+  if (A.mode == MODE_MALA) {
+    double* gy = A.gy + (size_t)c * np;
+    py = da_post_grad(A, D, c, y, D.gs + (size_t)c * np, gy);
+    const double* sd = A.sd + (size_t)c * np;
+    const double* L = A.L ? A.L + (size_t)c * np * np : nullptr;
+    double* my = A.my + (size_t)c * np;
+    double* tmp = A.vbuf + (size_t)c * np;
+    half_m_times(np, sd, L, gy, my, tmp);
+    for (int j = 0; j < np; ++j) my[j] += y[j];
+    lqd = log_q(np, sd, L, A.state + (size_t)c * np, my, tmp) -
+          log_q(np, sd, L, y, A.mx + (size_t)c * np, tmp);
+  } else {
+    py = InterpPrior::value(A, y);
+  }
   D.prior_y[c] = py;
   Stream rs = make_stream(A, c);
   const double u = da_uniform(rs, t, 0xFFFF0001u);
-  const double a1 = ((D.sll_y[c] + py) - (D.sll_x[c] + D.prior_x[c])) / A.temp[c];
-  D.flag[c] = log(u) < a1 ? 1u : 0u;
+  const double a1 = ((D.sll_y[c] + py) - (D.sll_x[c] + D.prior_x[c])) / A.temp[c] + lqd;
+  const bool finite = A.mode != MODE_MALA || isfinite(D.sll_y[c] + py);
+  D.flag[c] = (finite && log(u) < a1) ? 1u : 0u;
   A.ctr[c] = rs.ctr;
 }
 
@@ -417,6 +477,11 @@ static __global__ void da_finalize_kernel(ChainArgs A, DaArgs D, const double* _
     const double a2 = ((ll - llx) - (D.sll_y[c] - D.sll_x[c])) / A.temp[c];
     if (log(u) < a2) {
       for (int j = 0; j < np; ++j) x[j] = y[j];
+      if (A.mode == MODE_MALA) {  // the drift of the new state
+        double* gx = A.gx + (size_t)c * np;
+        const double* gy = A.gy + (size_t)c * np;
+        for (int j = 0; j < np; ++j) gx[j] = gy[j];
+      }
       A.cur[c] = plp;
       D.sll_x[c] = D.sll_y[c];
       D.prior_x[c] = D.prior_y[c];

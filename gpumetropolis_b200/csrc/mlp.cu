@@ -2,22 +2,28 @@
 // trained and evaluated on the GPU with the tcgen05 GEMM (tc_gemm.cuh).
 // No reference counterpart: the surrogate and delayed acceptance are new.
 //
-// Inputs are standardised parameters (per-coordinate mean and sd of the
-// training pairs), the target is the standardised exact log-likelihood, the
-// loss is the mean squared error.  Weights live in f32 (master) with Adam
-// moments; BF16 copies feed the tensor cores.  All reductions are fixed-order
-// (no atomics), so training is bitwise repeatable for a given seed.
+// Inputs are standardised (or whitened) parameters, the target is the
+// standardised exact log-likelihood, the loss is the mean squared error.
+// Weights live in f32 (master) with Adam moments, all in one flat vector
+// [W1 | b1 | W2 | b2 | w3 | b3]; BF16 copies feed the tensor cores.  All
+// reductions are fixed-order (no atomics on values), so training is bitwise
+// repeatable for a given seed.
 //
-// Per training step, for a batch of B rows (B, H multiples of 128; the input
-// width is padded to dp, a multiple of 64):
-//   Z1 = X W1^T + b1, A1 = silu(Z1)          tcgen05 GEMM, fused epilogue
-//   Z2 = A1 W2^T + b2, A2 = silu(Z2)         tcgen05 GEMM, fused epilogue
-//   yhat = A2 w3 + b3; r = yhat - t          row kernel (warp per row)
-//   dZ2 = (2r/B) w3 * silu'(Z2)              row kernel
-//   dW2 = dZ2^T A1                           tcgen05 GEMM (K = B)
-//   dA1 = dZ2 W2                             tcgen05 GEMM (K = H)
-//   dZ1 = dA1 * silu'(Z1); dW1 = dZ1^T X     elementwise + tcgen05 GEMM
-//   biases / w3: fixed-order column sums; Adam on every parameter.
+// One training step on a batch of B rows (B, H multiples of 128, H <= 512;
+// the input width padded to dp, a multiple of 64) is seven kernels, captured
+// once per train() call as a CUDA graph and replayed:
+//   gather   X (bf16, row-major and transposed), targets t
+//   GEMM1    Z1 = X W1^T + b1; A1 = silu(Z1) (row-major and transposed)
+//   GEMM2    Z2 = A1 W2^T + b2 with the head fused into its epilogue (one
+//            CTA holds whole rows): y = silu(Z2) w3 + b3, r = y - t, dy =
+//            2r/B, dZ2 = dy w3 silu'(Z2) (both layouts); per-CTA column sums
+//            for w3's and b2's gradients, row sums for b3's and the loss
+//   GEMM3    dW2 = dZ2^T A1, split K into fixed partials
+//   GEMM4    dZ1 = (dZ2 W2) * silu'(Z1) (transposed); per-CTA sums for b1's
+//   GEMM5    dW1 = dZ1^T X, split K into fixed partials
+//   adam     every gradient from its partials in a fixed order, then Adam
+//            (Kingma & Ba, bias-corrected) and the BF16 copies; the last
+//            block advances the device step counter the gather reads.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -66,28 +72,25 @@ struct Buf {
 };
 
 // ----------------------------------------------------------------- kernels
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) {
-  const float s = sigmoidf_(z);
-  return s * (1.0f + z * (1.0f - s));
-}
-
 // Deterministic uniform index for (seed, step, row): Philox counter.
 __device__ __forceinline__ uint32_t pick(uint32_t seed, uint32_t step, uint32_t row, uint32_t n) {
   const U4 r = philox4x32_10(U4{row, step, 0x4D4C5031u, 0u}, seed, 0x2545F491u);
   return (uint32_t)(((uint64_t)r.x * n) >> 32);
 }
 
-// Input transform of one row into Xh (bf16, zero padded to dp):
+// Input transform of one row into out (bf16, zero padded to dp):
 //   per coordinate  v_j = (theta_j - xmean_j) * xinv_j            (xw == nullptr)
 //   whitening       v_j = sum_k xw[j][k] (theta_k - xmean_k)      (xw: d x d)
-// `cen` is block-shared scratch of d floats.  Called by every thread.
+// and, when outT is set, the same values into column `row` of the
+// transposed copy outT[j * ldT + row].  `cen` is block-shared scratch of d
+// floats.  Called by every thread.
 template <class Src>
 __device__ __forceinline__ void mlp_input_row(Src theta_at, bool live, int d, int dp,
                                               const float* __restrict__ xmean,
                                               const float* __restrict__ xinv,
                                               const float* __restrict__ xw, float* cen,
-                                              bf16* __restrict__ out) {
+                                              bf16* __restrict__ out, bf16* __restrict__ outT,
+                                              int row, int ldT) {
   if (xw) {
     for (int k = threadIdx.x; k < d; k += blockDim.x) cen[k] = live ? theta_at(k) - xmean[k] : 0.0f;
     __syncthreads();
@@ -102,161 +105,146 @@ __device__ __forceinline__ void mlp_input_row(Src theta_at, bool live, int d, in
         v = (theta_at(j) - xmean[j]) * xinv[j];
       }
     }
-    out[j] = __float2bfloat16(v);
+    const bf16 h = __float2bfloat16(v);
+    out[j] = h;
+    if (outT) outT[(size_t)j * ldT + row] = h;
   }
 }
 
-// Batch rows: transformed inputs (bf16, padded with zeros) and targets.
+// Batch rows: transformed inputs (bf16, padded with zeros; row-major and
+// transposed) and standardised targets, one warp per row, kGatherRows rows
+// per block.
 // idx_mode 0: rows 0..n-1 in order (inference / gradient check);
-//          1: Philox-random rows of the training set.
+//          1: Philox-random rows of the training set at step ctr[0].
+constexpr int kGatherRows = 8;
+
 __global__ void mlp_gather(const float* __restrict__ theta, const double* __restrict__ ll,
                            size_t n, int d, int dp, int B, int idx_mode, uint32_t seed,
-                           uint32_t step, const float* __restrict__ xmean,
+                           const uint32_t* __restrict__ ctr, const float* __restrict__ xmean,
                            const float* __restrict__ xinv, const float* __restrict__ xw,
                            float ymean, float yinv, bf16* __restrict__ Xh,
-                           float* __restrict__ t) {
-  __shared__ float cen[256];
-  const int row = blockIdx.x;
-  if (row >= B) return;
-  size_t src = idx_mode ? pick(seed, step, (uint32_t)row, (uint32_t)n) : (size_t)row;
+                           bf16* __restrict__ XTh, float* __restrict__ t) {
+  __shared__ float cen[kGatherRows][256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * kGatherRows + warp;
+  if (row >= B) return;  // whole warps leave; no block-wide barrier follows
+  size_t src = idx_mode ? pick(seed, ctr[0], (uint32_t)row, (uint32_t)n) : (size_t)row;
   const bool live = src < n;
   if (!live) src = 0;
   const float* th = theta + src * d;
-  mlp_input_row([&](int k) { return th[k]; }, live, d, dp, xmean, xinv, xw, cen,
-                Xh + (size_t)row * dp);
-  if (threadIdx.x == 0 && t) t[row] = live && ll ? (float)((ll[src] - ymean) * yinv) : 0.0f;
+  if (xw) {
+    for (int k = lane; k < d; k += 32) cen[warp][k] = live ? th[k] - xmean[k] : 0.0f;
+    __syncwarp();
+  }
+  for (int j = lane; j < dp; j += 32) {
+    float v = 0.0f;
+    if (live && j < d) {
+      if (xw) {
+        const float* wr = xw + (size_t)j * d;
+        for (int k = 0; k < d; ++k) v = fmaf(wr[k], cen[warp][k], v);
+      } else {
+        v = (th[j] - xmean[j]) * xinv[j];
+      }
+    }
+    const bf16 h = __float2bfloat16(v);
+    Xh[(size_t)row * dp + j] = h;
+    XTh[(size_t)j * B + row] = h;
+  }
+  if (lane == 0 && t) t[row] = live && ll ? (float)((ll[src] - ymean) * yinv) : 0.0f;
 }
 
-// Output layer, loss and dZ2 for one row per warp (fixed lane-order sums).
-//   yhat = silu(Z2) . w3 + b3; r = yhat - t; loss row = r^2
-//   dZ2 = (2 r / B) w3 * silu'(Z2)  (f32 and bf16, and bf16 transposed)
-__global__ void mlp_head(const float* __restrict__ Z2, const float* __restrict__ w3,
-                         const float* __restrict__ b3, const float* __restrict__ t, int B,
-                         int H, int n_live, float* __restrict__ yhat, float* __restrict__ rsq,
-                         float* __restrict__ dyhat, bf16* __restrict__ dZ2h,
-                         bf16* __restrict__ dZ2Th, int backward) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= B) return;
-  const float* z = Z2 + (size_t)warp * H;
-  float acc = 0.0f;
-  for (int j = lane; j < H; j += 32) acc += silu(z[j]) * w3[j];
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-  const float y = acc + b3[0];
-  if (lane == 0 && yhat) yhat[warp] = y;
-  if (!backward) return;
-  const bool live = warp < n_live;
-  const float r = live ? y - t[warp] : 0.0f;
-  if (lane == 0) {
-    rsq[warp] = r * r;
-    dyhat[warp] = 2.0f * r / (float)n_live;
-  }
-  const float g = 2.0f * r / (float)n_live;
-  for (int j = lane; j < H; j += 32) {
-    const float dz = g * w3[j] * dsilu(z[j]);
-    dZ2h[(size_t)warp * H + j] = __float2bfloat16(dz);
-    dZ2Th[(size_t)j * B + warp] = __float2bfloat16(dz);
-  }
-}
+// Offsets of the flat parameter vector [W1 | b1 | W2 | b2 | w3 | b3].
+struct MlpLayout {
+  size_t oW1, ob1, oW2, ob2, ow3, ob3, n;
+  int H, dp;
+};
 
-// dZ1 = dA1 * silu'(Z1) -> bf16 transposed [H][B] and f32 [B][H] for db1.
-__global__ void mlp_dz1(const float* __restrict__ dA1, const float* __restrict__ Z1, int B, int H,
-                        float* __restrict__ dZ1, bf16* __restrict__ dZ1Th) {
+// Sources of one step's gradients: split-K partials of the two weight
+// gradients, per-CTA column partials of the bias / head gradients, per-CTA
+// row partials of b3's gradient and of the loss.
+struct GradParts {
+  const float* pW1;      // [S1][H][dp]
+  int S1;
+  const float* pW2;      // [S2][H][H]
+  int S2;
+  const float* colhead;  // [2][nct][H]: w3's, then b2's
+  const float* colb1;    // [nct][H]
+  const float* rowpart;  // [2][nct]: b3's, then sum r^2
+  int nct;
+};
+
+// Every gradient from its partials (fixed order) into G; with `apply`, Adam
+// at step ctr[0] + 1 on the master weights and their BF16 copies (W1h, W2h
+// and the transposed W1Th, W2Th), the loss of the step into
+// loss_hist[ctr[0] - loss_base], and the last block advances ctr[0].
+__global__ void mlp_reduce_adam(MlpLayout L, GradParts Gp, float* __restrict__ P,
+                                float* __restrict__ Mm, float* __restrict__ V,
+                                float* __restrict__ G, bf16* __restrict__ W1h,
+                                bf16* __restrict__ W1Th, bf16* __restrict__ W2h,
+                                bf16* __restrict__ W2Th, float lr,
+                                int apply, uint32_t* __restrict__ ctr, float* __restrict__ loss,
+                                uint32_t loss_base, uint32_t loss_cap) {
+  const uint32_t step = *reinterpret_cast<volatile const uint32_t*>(ctr);
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)B * H) return;
-  const size_t b = i / H, j = i % H;
-  const float v = dA1[i] * dsilu(Z1[i]);
-  dZ1[i] = v;
-  dZ1Th[j * B + b] = __float2bfloat16(v);
-}
-
-// bf16 [R][Cc] -> [Cc][R]
-__global__ void mlp_transpose(const bf16* __restrict__ in, bf16* __restrict__ out, int R, int Cc) {
-  __shared__ bf16 tile[32][34];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
-    const int r = r0 + y, c = c0 + threadIdx.x;
-    if (r < R && c < Cc) tile[y][threadIdx.x] = in[(size_t)r * Cc + c];
-  }
-  __syncthreads();
-  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
-    const int c = c0 + y, r = r0 + threadIdx.x;
-    if (r < R && c < Cc) out[(size_t)c * R + r] = tile[threadIdx.x][y];
-  }
-}
-
-// Column sums out[j] = scale_j * sum_b f(M[b][j]) * (s ? s[b] : 1) with
-// f = identity, silu or silu' (mode 0/1/2), in two fixed-order passes: blocks
-// of 32 columns x kColRows rows (8 warps, each a fixed row stride, then the
-// warps in order) write partials[chunk][j]; the second pass adds the chunks
-// in order.  Deterministic, and parallel over rows.
-constexpr int kColRows = 128;
-
-__global__ void mlp_colsum_part(const float* __restrict__ M, const float* __restrict__ s, int B,
-                                int H, int mode, float* __restrict__ part) {
-  __shared__ float red[8][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int j = blockIdx.x * 32 + lane;
-  const int b0 = blockIdx.y * kColRows, b1 = min(b0 + kColRows, B);
-  float acc = 0.0f;
-  if (j < H) {
-    for (int b = b0 + w; b < b1; b += 8) {
-      float v = M[(size_t)b * H + j];
-      v = mode == 1 ? silu(v) : (mode == 2 ? dsilu(v) : v);
-      acc += s ? v * s[b] : v;
+  const int H = L.H, dp = L.dp;
+  if (i < L.n) {
+    float g = 0.0f;
+    if (i < L.ob1) {
+      for (int z = 0; z < Gp.S1; ++z) g += Gp.pW1[(size_t)z * H * dp + i];
+    } else if (i < L.oW2) {
+      const size_t j = i - L.ob1;
+      for (int c = 0; c < Gp.nct; ++c) g += Gp.colb1[(size_t)c * H + j];
+    } else if (i < L.ob2) {
+      const size_t k = i - L.oW2;
+      for (int z = 0; z < Gp.S2; ++z) g += Gp.pW2[(size_t)z * H * H + k];
+    } else if (i < L.ow3) {
+      const size_t j = i - L.ob2;
+      for (int c = 0; c < Gp.nct; ++c) g += Gp.colhead[((size_t)Gp.nct + c) * H + j];
+    } else if (i < L.ob3) {
+      const size_t j = i - L.ow3;
+      for (int c = 0; c < Gp.nct; ++c) g += Gp.colhead[(size_t)c * H + j];
+    } else {
+      for (int c = 0; c < Gp.nct; ++c) g += Gp.rowpart[c];
+    }
+    G[i] = g;
+    if (apply) {
+      const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+      const float t = (float)(step + 1);
+      const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
+      const float mi = b1 * Mm[i] + (1.0f - b1) * g;
+      const float vi = b2 * V[i] + (1.0f - b2) * g * g;
+      Mm[i] = mi;
+      V[i] = vi;
+      const float wi = P[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+      P[i] = wi;
+      if (i < L.ob1) {
+        W1h[i] = __float2bfloat16(wi);
+        W1Th[(i % dp) * H + i / dp] = __float2bfloat16(wi);
+      } else if (i >= L.oW2 && i < L.ob2) {
+        const size_t k = i - L.oW2;
+        W2h[k] = __float2bfloat16(wi);
+        W2Th[(k % H) * H + k / H] = __float2bfloat16(wi);
+      }
     }
   }
-  red[w][lane] = acc;
-  __syncthreads();
-  if (w == 0 && j < H) {
-    float t = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) t += red[k][lane];
-    part[(size_t)blockIdx.y * H + j] = t;
+  if (i == 0 && loss) {
+    float s = 0.0f;
+    for (int c = 0; c < Gp.nct; ++c) s += Gp.rowpart[Gp.nct + c];
+    const uint32_t slot = step - loss_base;
+    if (slot < loss_cap) loss[slot] = s;
   }
-}
-
-__global__ void mlp_colsum_fin(const float* __restrict__ part, int nchunk, int H,
-                               const float* __restrict__ scale, float* __restrict__ out) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= H) return;
-  float t = 0.0f;
-  for (int c = 0; c < nchunk; ++c) t += part[(size_t)c * H + j];
-  out[j] = scale ? t * scale[j] : t;
-}
-
-// out[0] = sum of v[0..n), fixed order: 256 strided per-thread sums, then a
-// fixed shared-memory tree.  One block of 256 threads.
-__global__ void mlp_sum(const float* __restrict__ v, int n, float* __restrict__ out) {
-  __shared__ float red[256];
-  float t = 0.0f;
-  for (int i = threadIdx.x; i < n; i += 256) t += v[i];
-  red[threadIdx.x] = t;
+  // Every block has read ctr[0]; the last one advances it (training steps)
+  // and re-arms the ticket.
   __syncthreads();
-  for (int off = 128; off > 0; off >>= 1) {
-    if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
-    __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t ticket = atomicAdd(&ctr[1], 1u);
+    if (ticket == gridDim.x - 1) {
+      if (apply) ctr[0] = step + 1;
+      ctr[1] = 0;
+      __threadfence();
+    }
   }
-  if (threadIdx.x == 0) out[0] = red[0];
-}
-
-// Adam (Kingma & Ba) with bias correction; also refreshes the bf16 copy and,
-// when `wt` is set, the transposed bf16 copy of an R x Cc weight.
-__global__ void mlp_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
-                         const float* __restrict__ g, size_t n, float lr, float b1, float b2,
-                         float c1, float c2, float eps, bf16* __restrict__ wh,
-                         bf16* __restrict__ wt, int R, int Cc) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float gi = g[i];
-  const float mi = b1 * m[i] + (1.0f - b1) * gi;
-  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-  m[i] = mi;
-  v[i] = vi;
-  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-  w[i] = wi;
-  if (wh) wh[i] = __float2bfloat16(wi);
-  if (wt) wt[(i % Cc) * R + i / Cc] = __float2bfloat16(wi);
 }
 
 __global__ void mlp_init_weights(float* __restrict__ w, size_t n, int fan_in, int cols_live,
@@ -290,13 +278,35 @@ __global__ void mlp_gather64(const double* __restrict__ theta, int n, int d, int
   const bool live = row < n;
   const double* th = theta + (size_t)(live ? row : 0) * d;
   mlp_input_row([&](int k) { return (float)th[k]; }, live, d, dp, xmean, xinv, xw, cen,
-                Xh + (size_t)row * dp);
+                Xh + (size_t)row * dp, nullptr, row, B);
 }
 
 __global__ void mlp_unscale(const float* __restrict__ y, int n, float ysd, float ymean,
                             double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (double)y[i] * ysd + ymean;
+}
+
+// Gradient of the surrogate log-likelihood with respect to the parameters,
+// from dX = dy/dx (rows x dp, f32) of the network input x: through the input
+// transform (whitening x = xw (theta - xmean), or per coordinate x_j =
+// (theta_j - xmean_j) xinv_j) and the target's scale ysd.  One warp per row.
+__global__ void mlp_input_grad(const float* __restrict__ dX, int n, int d, int dp,
+                               const float* __restrict__ xinv, const float* __restrict__ xw,
+                               float ysd, double* __restrict__ out) {
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const float* g = dX + (size_t)row * dp;
+  for (int j = lane; j < d; j += 32) {
+    float v;
+    if (xw) {
+      v = 0.0f;
+      for (int k = 0; k < d; ++k) v = fmaf(g[k], xw[(size_t)k * d + j], v);
+    } else {
+      v = g[j] * xinv[j];
+    }
+    out[(size_t)row * d + j] = (double)v * ysd;
+  }
 }
 
 // Fused inference for 128 rows per CTA, for d <= 64 (dp = 64) and H in
@@ -498,124 +508,163 @@ mlp_infer_fused(const double* __restrict__ theta, int n, int d, int H,
 struct gpum_b200_mlp {
   int d = 0, dp = 0, H = 0, B = 0;
   uint32_t seed = 0;
-  uint32_t step = 0;
+  uint32_t steps_done = 0;  // host mirror of the device step counter
   cudaStream_t st = nullptr;
-  // parameters (f32 master), Adam moments, gradients
-  Buf<float> W1, b1, W2, b2, w3, b3;
-  Buf<float> mW1, mb1, mW2, mb2, mw3, mb3, vW1, vb1, vW2, vb2, vw3, vb3;
-  Buf<float> gW1, gb1, gW2, gb2, gw3, gb3;
-  Buf<bf16> W1h, W2h, W2Th;
-  // activations and work buffers (batch rows)
-  Buf<bf16> Xh, XTh, A1h, A1Th, A2h, dZ2h, dZ2Th, dZ1Th;
-  Buf<float> Z1, Z2, t, yhat, rsq, dyhat, dA1, dZ1, loss, scratch;
-  Buf<float> colpart;  // [B / kColRows][H] column-sum partials
-  Buf<float> splitk;   // split-K GEMM partials
+  // second stream and events: the dW2 GEMM runs beside the dZ1 -> dW1 chain
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  MlpLayout L{};
+  // parameters (f32 master), Adam moments, gradients: flat [W1|b1|W2|b2|w3|b3]
+  Buf<float> P, Mm, V, G;
+  Buf<bf16> W1h, W1Th, W2h, W2Th;
+  // batch work buffers
+  Buf<bf16> Xh, XTh, A1h, A1Th, dZ2h, dZ2Th, dZ1Th;
+  Buf<float> Z1, t, yhat, dX;
+  // gradient partials: split K (weights), per-CTA columns / rows (biases, head, loss)
+  Buf<float> pW1, pW2, colhead, colb1, rowpart;
+  int S1 = 1, S2 = 1;
+  Buf<uint32_t> ctr;   // [step, ticket]
+  Buf<float> losses;   // per-step sums of squared residuals of one train() call
   // normaliser
   Buf<float> xmean, xinv, xw;  // xw: d x d whitening, used when `whiten`
   bool whiten = false;
   const float* xw_or_null() const { return whiten ? xw.p : nullptr; }
   float ymean = 0.0f, yinv = 1.0f, ysd = 1.0f;
   Buf<uint32_t> err;
-  int adam_t = 0;
-  bool smem_set[2] = {false, false};
   bool infer_smem_set = false;
+  bool gemm_smem_set[16] = {};  // per (BN, epilogue) instantiation
+
+  float* W1p() const { return P.p + L.oW1; }
+  float* b1p() const { return P.p + L.ob1; }
+  float* W2p() const { return P.p + L.oW2; }
+  float* b2p() const { return P.p + L.ob2; }
+  float* w3p() const { return P.p + L.ow3; }
+  float* b3p() const { return P.p + L.ob3; }
 
   // The fused inference kernel covers d <= 64 and H in {128, 256}.
   bool fused_inference() const { return dp == 64 && (H == 128 || H == 256); }
 
   ~gpum_b200_mlp() {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
     if (st) cudaStreamDestroy(st);
   }
 
-  template <int BN>
-  void gemm(const bf16* A, const bf16* Bm, float* C, const float* bias, bf16* act, int M, int N,
-            int K) {
+  template <int BN, int EPI>
+  void gemm(const GemmArgs& a, int S) {
     const size_t smem = tc_gemm_smem<BN>();
-    // Set once, so later launches (possibly under stream capture) make no
-    // non-stream API calls.
-    if (!smem_set[BN == 128]) {
-      MLP_CK(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-      smem_set[BN == 128] = true;
+    // Set once per instantiation, so later launches (possibly under stream
+    // capture) make no non-stream API calls.
+    constexpr int slot = (BN == 64 ? 0 : BN == 128 ? 1 : BN == 256 ? 2 : 3) * 4 + EPI;
+    if (!gemm_smem_set[slot]) {
+      MLP_CK(cudaFuncSetAttribute(tc_gemm_kernel<BN, EPI>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      gemm_smem_set[slot] = true;
     }
-    // Long-K products with few output tiles (the weight gradients, K = batch)
-    // split K across CTAs so the GPU is not left with a handful of CTAs.
-    int S = 1;
-    if (!bias && !act) {
-      const int tiles = (N / BN) * (M / kGemmBM);
-      while (S < 32 && tiles * S < 128 && K % (2 * S * kGemmBK) == 0 &&
-             (size_t)2 * S * M * N <= splitk.n)
-        S *= 2;
+    dim3 grid(a.N / BN, a.M / kGemmBM, S);
+    tc_gemm_kernel<BN, EPI><<<grid, kGemmThreads, smem, st>>>(a);
+    MLP_CK(cudaGetLastError());
+  }
+
+  GemmArgs args(const bf16* A, const bf16* Bm, int M, int N, int K) const {
+    GemmArgs a{};
+    a.A = A;
+    a.B = Bm;
+    a.M = M;
+    a.N = N;
+    a.K = K;
+    a.kz = K;
+    a.err = err.p;
+    return a;
+  }
+
+  // Layer 1 (SiLU epilogue) and layer 2 with the head, for `rows` rows in Xh;
+  // targets in t for the first n_live rows (nullptr: inference, r = 0).
+  void forward(int rows, int n_live, const float* targets, int unit_dy = 0) {
+    GemmArgs a1 = args(Xh.p, W1h.p, rows, H, dp);
+    a1.C = Z1.p;
+    a1.bias = b1p();
+    a1.act = A1h.p;
+    a1.actT = targets ? A1Th.p : nullptr;
+    gemm<128, EPI_SILU>(a1, 1);
+    GemmArgs a2 = args(A1h.p, W2h.p, rows, H, H);
+    a2.bias = b2p();
+    a2.w3 = w3p();
+    a2.b3 = b3p();
+    a2.t = targets;
+    a2.n_live = n_live;
+    a2.dzh = dZ2h.p;
+    a2.colpart = targets ? colhead.p : nullptr;
+    a2.rowpart = targets ? rowpart.p : nullptr;
+    a2.actT = targets ? dZ2Th.p : nullptr;
+    a2.unit_dy = unit_dy;
+    a2.yhat = yhat.p;
+    if (H == 128) gemm<128, EPI_HEAD>(a2, 1);
+    else if (H == 256) gemm<256, EPI_HEAD>(a2, 1);
+    else gemm<512, EPI_HEAD>(a2, 1);
+  }
+
+  // Weight gradients and b1's (after forward() with targets), then the
+  // reduction of every gradient into G, with Adam when `apply`.
+  void backward_and_update(float lr, int apply, float* loss_hist, uint32_t loss_base,
+                           uint32_t loss_cap) {
+    GemmArgs g3 = args(dZ2Th.p, A1Th.p, H, H, B);  // dW2 = dZ2^T A1
+    g3.C = pW2.p;
+    g3.kz = B / S2;
+    // dW2 on the second stream, concurrent with dZ1 and dW1 (both only read
+    // dZ2); the reduction waits for both.  Under stream capture the fork and
+    // join become graph edges.
+    const bool fork = st2 != nullptr;
+    if (fork) {
+      MLP_CK(cudaEventRecord(ev_fork, st));
+      MLP_CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+      cudaStream_t keep = st;
+      st = st2;
+      try {
+        gemm<64, EPI_STORE>(g3, S2);
+      } catch (...) {
+        st = keep;
+        throw;
+      }
+      st = keep;
+      MLP_CK(cudaEventRecord(ev_join, st2));
+    } else {
+      gemm<64, EPI_STORE>(g3, S2);
     }
-    dim3 grid(N / BN, M / kGemmBM, S);
-    tc_gemm_kernel<BN><<<grid, kGemmThreads, smem, st>>>(A, Bm, S > 1 ? splitk.p : C, bias, act,
-                                                         M, N, K, K / S, err.p);
-    if (S > 1)
-      tc_splitk_sum<<<blocks((size_t)M * N), 256, 0, st>>>(splitk.p, S, (size_t)M * N, C);
+    GemmArgs g4 = args(dZ2h.p, W2Th.p, B, H, H);   // dZ1 = (dZ2 W2) * silu'(Z1)
+    g4.Zprev = Z1.p;
+    g4.actT = dZ1Th.p;
+    g4.colpart = colb1.p;
+    gemm<128, EPI_DSILU>(g4, 1);
+    GemmArgs g5 = args(dZ1Th.p, XTh.p, H, dp, B);  // dW1 = dZ1^T X
+    g5.C = pW1.p;
+    g5.kz = B / S1;
+    gemm<64, EPI_STORE>(g5, S1);
+    if (fork) MLP_CK(cudaStreamWaitEvent(st, ev_join, 0));
+    GradParts gp{pW1.p, S1, pW2.p, S2, colhead.p, colb1.p, rowpart.p, B / kGemmBM};
+    mlp_reduce_adam<<<blocks(L.n), 256, 0, st>>>(L, gp, P.p, Mm.p, V.p, G.p, W1h.p, W1Th.p,
+                                                  W2h.p, W2Th.p, lr, apply, ctr.p, loss_hist,
+                                                  loss_base, loss_cap);
     MLP_CK(cudaGetLastError());
   }
 
-  void gemm_any(const bf16* A, const bf16* Bm, float* C, const float* bias, bf16* act, int M,
-                int N, int K) {
-    if (N % 128 == 0) gemm<128>(A, Bm, C, bias, act, M, N, K);
-    else gemm<64>(A, Bm, C, bias, act, M, N, K);
-  }
-
-  // Forward of the first `rows` rows already gathered into Xh.
-  void forward(int rows) {
-    gemm_any(Xh.p, W1h.p, Z1.p, b1.p, A1h.p, rows, H, dp);
-    gemm_any(A1h.p, W2h.p, Z2.p, b2.p, A2h.p, rows, H, H);
-  }
-
-  // Gradients for the gathered batch (n_live real rows of B).
-  void backward(int n_live) {
-    mlp_head<<<blocks((size_t)B * 32), 256, 0, st>>>(Z2.p, w3.p, b3.p, t.p, B, H, n_live, yhat.p,
-                                                     rsq.p, dyhat.p, dZ2h.p, dZ2Th.p, 1);
-    MLP_CK(cudaGetLastError());
-    // w3 and b3: dw3[j] = sum_b dyhat[b] silu(Z2[b][j]); db3 = sum dyhat
-    colsum(Z2.p, dyhat.p, 1, nullptr, gw3.p);
-    mlp_sum<<<1, 256, 0, st>>>(dyhat.p, B, gb3.p);
-    mlp_sum<<<1, 256, 0, st>>>(rsq.p, B, loss.p);
-    // db2 = column sums of dZ2 (from its bf16 transpose would lose bits: use
-    // the f32 row kernel output through dA1's buffer as scratch)
-    mlp_transpose<<<dim3(H / 32, B / 32), dim3(32, 8), 0, st>>>(A1h.p, A1Th.p, B, H);
-    gemm_any(dZ2Th.p, A1Th.p, gW2.p, nullptr, nullptr, H, H, B);  // dW2 = dZ2^T A1
-    gemm_any(dZ2h.p, W2Th.p, dA1.p, nullptr, nullptr, B, H, H);   // dA1 = dZ2 W2
-    // db2 = sum_b dZ2[b][j]: recompute in f32 from Z2 and dyhat
-    db2_from_head();
-    mlp_dz1<<<blocks((size_t)B * H), 256, 0, st>>>(dA1.p, Z1.p, B, H, dZ1.p, dZ1Th.p);
-    colsum(dZ1.p, nullptr, 0, nullptr, gb1.p);
-    mlp_transpose<<<dim3(dp / 32, B / 32), dim3(32, 8), 0, st>>>(Xh.p, XTh.p, B, dp);
-    gemm_any(dZ1Th.p, XTh.p, gW1.p, nullptr, nullptr, H, dp, B);  // dW1 = dZ1^T X
-    MLP_CK(cudaGetLastError());
-  }
-
-  // db2[j] = w3[j] sum_b dyhat[b] silu'(Z2[b][j]), fixed order over b.
-  void db2_from_head() { colsum(Z2.p, dyhat.p, 2, w3.p, gb2.p); }
-
-  // Column sums of a B x H row-major matrix (mlp_colsum_part / _fin).
-  void colsum(const float* M, const float* sc, int mode, const float* scale, float* out) {
-    const int nchunk = (B + kColRows - 1) / kColRows;
-    mlp_colsum_part<<<dim3((H + 31) / 32, nchunk), 256, 0, st>>>(M, sc, B, H, mode, colpart.p);
-    mlp_colsum_fin<<<blocks(H), 256, 0, st>>>(colpart.p, nchunk, H, scale, out);
-    MLP_CK(cudaGetLastError());
-  }
-
-  void adam(float lr) {
-    ++adam_t;
-    const float bb1 = 0.9f, bb2 = 0.999f, eps = 1e-8f;
-    const float c1 = 1.0f - std::pow(bb1, (float)adam_t), c2 = 1.0f - std::pow(bb2, (float)adam_t);
-    auto go = [&](Buf<float>& w, Buf<float>& m, Buf<float>& v, Buf<float>& g, bf16* wh, bf16* wt,
-                  int R, int Cc) {
-      mlp_adam<<<blocks(w.n), 256, 0, st>>>(w.p, m.p, v.p, g.p, w.n, lr, bb1, bb2, c1, c2, eps,
-                                            wh, wt, R, Cc);
-    };
-    go(W1, mW1, vW1, gW1, W1h.p, nullptr, H, dp);
-    go(b1, mb1, vb1, gb1, nullptr, nullptr, 1, H);
-    go(W2, mW2, vW2, gW2, W2h.p, W2Th.p, H, H);
-    go(b2, mb2, vb2, gb2, nullptr, nullptr, 1, H);
-    go(w3, mw3, vw3, gw3, nullptr, nullptr, 1, H);
-    go(b3, mb3, vb3, gb3, nullptr, nullptr, 1, 1);
+  // Value and parameter gradient of the surrogate log-likelihood for `rows`
+  // rows in Xh (after the gather): layer 1, layer 2 with the head at dy = 1,
+  // then back through both layers to the input (dZ1 row-major in A1Th's
+  // space, dX = dZ1 W1), and through the input transform.
+  void value_grad(int rows, int n, int d_in, double* out_val, double* out_grad) {
+    forward(rows, rows, nullptr, /*unit_dy=*/1);
+    mlp_unscale<<<blocks(n), 256, 0, st>>>(yhat.p, n, ysd, ymean, out_val);
+    GemmArgs g4 = args(dZ2h.p, W2Th.p, rows, H, H);  // dZ1 = (dZ2 W2) * silu'(Z1)
+    g4.Zprev = Z1.p;
+    g4.act = A1Th.p;
+    gemm<128, EPI_DSILU>(g4, 1);
+    GemmArgs g5 = args(A1Th.p, W1Th.p, rows, dp, H);  // dX = dZ1 W1
+    g5.C = dX.p;
+    gemm<64, EPI_STORE>(g5, 1);
+    mlp_input_grad<<<blocks((size_t)n * 32), 256, 0, st>>>(dX.p, n, d_in, dp, xinv.p,
+                                                           xw_or_null(), ysd, out_grad);
     MLP_CK(cudaGetLastError());
   }
 
@@ -653,10 +702,6 @@ void need(bool ok, const char* msg, int code = GPUM_ERR_INVALID) {
   if (!ok) throw MlpFail{code, msg};
 }
 
-}  // namespace
-
-namespace {
-
 // Upload host pairs (theta f64 -> f32, ll f64) into device buffers.
 void upload_pairs(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n,
                   Buf<float>& dth, Buf<double>& dll) {
@@ -672,13 +717,25 @@ void upload_pairs(gpum_b200_mlp* m, const double* theta, const double* ll, size_
   MLP_CK(cudaStreamSynchronize(m->st));
 }
 
+// Split-K factor of a B-deep weight-gradient GEMM with `tiles` output tiles:
+// the largest power of two up to `cap` that keeps at least one 64-wide K
+// slice per CTA and at most about two waves of CTAs (each split is one
+// partial of the weight's size that the reduction reads back).
+int split_k(int B, int tiles, int sms, int cap) {
+  int S = 1;
+  while (S < cap && (B / (2 * S)) % kGemmBK == 0 && B / (2 * S) >= kGemmBK &&
+         tiles * 2 * S <= 2 * sms)
+    S *= 2;
+  return S;
+}
+
 }  // namespace
 
 namespace gpum {
 
 // Kernel launches one mlp_infer call of n rows makes.
 int mlp_infer_launches(const gpum_b200_mlp* m, int n) {
-  return m->fused_inference() ? 1 : 5 * ((n + m->B - 1) / m->B);
+  return m->fused_inference() ? 1 : 4 * ((n + m->B - 1) / m->B);
 }
 
 // Surrogate log-likelihood of n f64 parameter vectors (device, chain-major)
@@ -702,8 +759,8 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
       }
       if (n > 0) {
         mlp_infer_fused<<<(unsigned)((n + kInfRows - 1) / kInfRows), kInfThreads, smem, st>>>(
-            theta, n, d, m->H, m->xmean.p, m->xinv.p, m->xw_or_null(), m->W1h.p, m->b1.p,
-            m->W2h.p, m->b2.p, m->w3.p, m->b3.p, m->ysd, m->ymean, out, m->err.p);
+            theta, n, d, m->H, m->xmean.p, m->xinv.p, m->xw_or_null(), m->W1h.p, m->b1p(),
+            m->W2h.p, m->b2p(), m->w3p(), m->b3p(), m->ysd, m->ymean, out, m->err.p);
         MLP_CK(cudaGetLastError());
       }
       m->st = keep;
@@ -714,10 +771,7 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
       const int Mi = (rows + kGemmBM - 1) / kGemmBM * kGemmBM;  // rows padded to the tile
       mlp_gather64<<<Mi, 128, 0, st>>>(theta + (size_t)r0 * d, rows, d, m->dp, Mi, m->xmean.p,
                                        m->xinv.p, m->xw_or_null(), m->Xh.p);
-      m->forward(Mi);
-      mlp_head<<<blocks((size_t)Mi * 32), 256, 0, st>>>(m->Z2.p, m->w3.p, m->b3.p, nullptr, Mi,
-                                                       m->H, Mi, m->yhat.p, nullptr, nullptr,
-                                                       nullptr, nullptr, 0);
+      m->forward(Mi, Mi, nullptr);
       mlp_unscale<<<blocks(rows), 256, 0, st>>>(m->yhat.p, rows, m->ysd, m->ymean, out + r0);
       MLP_CK(cudaGetLastError());
     }
@@ -727,6 +781,41 @@ int mlp_infer(gpum_b200_mlp* m, const double* theta, int n, int d, double* out, 
   }
   m->st = keep;
   return rc;
+}
+
+// Surrogate log-likelihood and its gradient with respect to the parameters
+// at n f64 parameter vectors (device, chain-major), into out_val[n] and
+// out_grad[n][d] (device), enqueued on `st`: the drift of the
+// delayed-acceptance Langevin proposal.
+int mlp_infer_grad(gpum_b200_mlp* m, const double* theta, int n, int d, double* out_val,
+                   double* out_grad, cudaStream_t st, std::string* err) {
+  if (!m || d != m->d) {
+    *err = "surrogate input width does not match the model's parameter count";
+    return GPUM_ERR_INVALID;
+  }
+  cudaStream_t keep = m->st;
+  m->st = st;
+  int rc = GPUM_OK;
+  try {
+    for (int r0 = 0; r0 < n; r0 += m->B) {
+      const int rows = std::min(m->B, n - r0);
+      const int Mi = (rows + kGemmBM - 1) / kGemmBM * kGemmBM;
+      mlp_gather64<<<Mi, 128, 0, st>>>(theta + (size_t)r0 * d, rows, d, m->dp, Mi, m->xmean.p,
+                                       m->xinv.p, m->xw_or_null(), m->Xh.p);
+      MLP_CK(cudaGetLastError());
+      m->value_grad(Mi, rows, d, out_val + r0, out_grad + (size_t)r0 * d);
+    }
+  } catch (const MlpFail& f) {
+    *err = f.msg;
+    rc = f.code;
+  }
+  m->st = keep;
+  return rc;
+}
+
+// Kernel launches one mlp_infer_grad call of n rows makes.
+int mlp_infer_grad_launches(const gpum_b200_mlp* m, int n) {
+  return 7 * ((n + m->B - 1) / m->B);
 }
 
 }  // namespace gpum
@@ -739,8 +828,7 @@ int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t s
     need(out != nullptr, "output pointer is NULL");
     *out = nullptr;
     need(d >= 1 && d <= 256, "input width must be in 1..256");
-    need(hidden >= 128 && hidden <= 1024 && hidden % 128 == 0,
-         "hidden width must be a multiple of 128 in 128..1024");
+    need(hidden == 128 || hidden == 256 || hidden == 512, "hidden width must be 128, 256 or 512");
     need(batch >= 128 && batch <= 65536 && batch % 128 == 0,
          "batch must be a multiple of 128 in 128..65536");
     int n = 0;
@@ -748,6 +836,9 @@ int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t s
       cudaGetLastError();
       throw MlpFail{GPUM_ERR_NODEVICE, "no CUDA device is visible"};
     }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     std::unique_ptr<gpum_b200_mlp> m(new gpum_b200_mlp());
     m->d = (int)d;
     m->dp = (int)((d + 63) / 64 * 64);
@@ -755,42 +846,59 @@ int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t s
     m->B = (int)batch;
     m->seed = seed;
     MLP_CK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
+    MLP_CK(cudaStreamCreateWithFlags(&m->st2, cudaStreamNonBlocking));
+    MLP_CK(cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming));
+    MLP_CK(cudaEventCreateWithFlags(&m->ev_join, cudaEventDisableTiming));
     const int H = m->H, dp = m->dp, B = m->B;
-    for (auto* b : {&m->W1, &m->mW1, &m->vW1, &m->gW1}) b->alloc((size_t)H * dp);
-    for (auto* b : {&m->W2, &m->mW2, &m->vW2, &m->gW2}) b->alloc((size_t)H * H);
-    for (auto* b : {&m->b1, &m->mb1, &m->vb1, &m->gb1, &m->b2, &m->mb2, &m->vb2, &m->gb2, &m->w3,
-                    &m->mw3, &m->vw3, &m->gw3})
-      b->alloc(H);
-    for (auto* b : {&m->b3, &m->mb3, &m->vb3, &m->gb3}) b->alloc(1);
+    MlpLayout& L = m->L;
+    L.H = H;
+    L.dp = dp;
+    L.oW1 = 0;
+    L.ob1 = L.oW1 + (size_t)H * dp;
+    L.oW2 = L.ob1 + H;
+    L.ob2 = L.oW2 + (size_t)H * H;
+    L.ow3 = L.ob2 + H;
+    L.ob3 = L.ow3 + H;
+    L.n = L.ob3 + 1;
+    for (auto* b : {&m->P, &m->Mm, &m->V, &m->G}) b->alloc(L.n);
     m->W1h.alloc((size_t)H * dp);
+    m->W1Th.alloc((size_t)dp * H);
     m->W2h.alloc((size_t)H * H);
     m->W2Th.alloc((size_t)H * H);
     m->Xh.alloc((size_t)B * dp);
     m->XTh.alloc((size_t)dp * B);
-    for (auto* b : {&m->A1h, &m->A2h, &m->dZ2h}) b->alloc((size_t)B * H);
+    for (auto* b : {&m->A1h, &m->dZ2h}) b->alloc((size_t)B * H);
     for (auto* b : {&m->A1Th, &m->dZ2Th, &m->dZ1Th}) b->alloc((size_t)H * B);
-    for (auto* b : {&m->Z1, &m->Z2, &m->dA1, &m->dZ1}) b->alloc((size_t)B * H);
-    for (auto* b : {&m->t, &m->yhat, &m->rsq, &m->dyhat}) b->alloc(B);
-    m->loss.alloc(1);
-    m->colpart.alloc((size_t)((B + kColRows - 1) / kColRows) * H);
-    m->splitk.alloc((size_t)32 * H * std::max(H, dp));
+    m->Z1.alloc((size_t)B * H);
+    m->t.alloc(B);
+    m->yhat.alloc(B);
+    m->dX.alloc((size_t)B * dp);
+    m->S2 = split_k(B, (H / 128) * (H / 64), sms, 16);
+    m->S1 = split_k(B, (H / 128) * (dp / 64), sms, 64);
+    m->pW2.alloc((size_t)m->S2 * H * H);
+    m->pW1.alloc((size_t)m->S1 * H * dp);
+    const int nct = B / kGemmBM;
+    m->colhead.alloc((size_t)2 * nct * H);
+    m->colb1.alloc((size_t)nct * H);
+    m->rowpart.alloc((size_t)2 * nct);
+    m->ctr.alloc(2);
     m->xmean.alloc(d);
     m->xinv.alloc(d);
     m->xw.alloc((size_t)d * d);
     m->err.alloc(1);
     MLP_CK(cudaMemsetAsync(m->err.p, 0, sizeof(uint32_t), m->st));
-    // zero moments and padded rows
-    for (auto* b : {&m->mW1, &m->vW1, &m->mW2, &m->vW2, &m->mb1, &m->vb1, &m->mb2, &m->vb2,
-                    &m->mw3, &m->vw3, &m->mb3, &m->vb3, &m->b1, &m->b2, &m->b3})
+    MLP_CK(cudaMemsetAsync(m->ctr.p, 0, 2 * sizeof(uint32_t), m->st));
+    // zero moments, biases and the (padded) batch buffers
+    for (auto* b : {&m->P, &m->Mm, &m->V, &m->G})
       MLP_CK(cudaMemsetAsync(b->p, 0, b->n * sizeof(float), m->st));
-    mlp_init_weights<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1.p, (size_t)H * dp, (int)d,
+    mlp_init_weights<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1p(), (size_t)H * dp, (int)d,
                                                                 (int)d, dp, seed, 1);
-    mlp_init_weights<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2.p, (size_t)H * H, H, H, H,
+    mlp_init_weights<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2p(), (size_t)H * H, H, H, H,
                                                                seed, 2);
-    mlp_init_weights<<<blocks(H), 256, 0, m->st>>>(m->w3.p, H, H, H, H, seed, 3);
-    mlp_to_bf16<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1.p, m->W1h.p, nullptr,
+    mlp_init_weights<<<blocks(H), 256, 0, m->st>>>(m->w3p(), H, H, H, H, seed, 3);
+    mlp_to_bf16<<<blocks((size_t)H * dp), 256, 0, m->st>>>(m->W1p(), m->W1h.p, m->W1Th.p,
                                                            (size_t)H * dp, H, dp);
-    mlp_to_bf16<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2.p, m->W2h.p, m->W2Th.p,
+    mlp_to_bf16<<<blocks((size_t)H * H), 256, 0, m->st>>>(m->W2p(), m->W2h.p, m->W2Th.p,
                                                           (size_t)H * H, H, H);
     MLP_CK(cudaGetLastError());
     std::vector<float> ones(d, 1.0f);
@@ -863,22 +971,52 @@ int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll,
   return mlp_guard(err, err_len, [&] {
     need(m && theta && ll, "NULL argument");
     need(n_pairs >= 1 && n_pairs <= (1u << 28), "n_pairs must be in 1..2^28");
+    if (steps == 0) return;
     Buf<float> dth;
     Buf<double> dll;
     upload_pairs(m, theta, ll, n_pairs, dth, dll);
-    std::vector<float> losses(steps);
-    for (uint32_t s = 0; s < steps; ++s) {
-      mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed,
-                                          m->step++, m->xmean.p, m->xinv.p, m->xw_or_null(),
-                                          m->ymean, m->yinv,
-                                          m->Xh.p, m->t.p);
-      m->forward(m->B);
-      m->backward(m->B);
-      m->adam((float)lr);
-      if (out_loss)
-        MLP_CK(cudaMemcpyAsync(&losses[s], m->loss.p, sizeof(float), cudaMemcpyDeviceToHost,
-                               m->st));
+    m->losses.alloc(steps);
+    const uint32_t base = m->steps_done;
+    // One step as a CUDA graph (its kernels read the step from the device
+    // counter the reduction advances), replayed `steps` times.
+    auto one_step = [&] {
+      mlp_gather<<<m->B / kGatherRows, 32 * kGatherRows, 0, m->st>>>(
+          dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed,
+                                          m->ctr.p, m->xmean.p, m->xinv.p, m->xw_or_null(),
+                                          m->ymean, m->yinv, m->Xh.p, m->XTh.p, m->t.p);
+      MLP_CK(cudaGetLastError());
+      m->forward(m->B, m->B, m->t.p);
+      m->backward_and_update((float)lr, 1, m->losses.p, base, steps);
+    };
+    one_step();  // first step eagerly: sets every kernel attribute outside capture
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (steps > 1) {
+      MLP_CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+      try {
+        one_step();
+      } catch (...) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(m->st, &g2);
+        if (g2) cudaGraphDestroy(g2);
+        throw;
+      }
+      MLP_CK(cudaStreamEndCapture(m->st, &graph));
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        MLP_CK(ie);
+      }
+      cudaError_t le = cudaSuccess;
+      for (uint32_t s = 1; s < steps && le == cudaSuccess; ++s) le = cudaGraphLaunch(exec, m->st);
+      cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      MLP_CK(le);
     }
+    m->steps_done += steps;
+    std::vector<float> losses(steps);
+    MLP_CK(cudaMemcpyAsync(losses.data(), m->losses.p, steps * sizeof(float),
+                           cudaMemcpyDeviceToHost, m->st));
     m->check_err();
     if (out_loss)
       for (uint32_t s = 0; s < steps; ++s) out_loss[s] = losses[s] / (float)m->B;
@@ -906,6 +1044,30 @@ int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, doubl
   });
 }
 
+int gpum_b200_mlp_predict_grad(gpum_b200_mlp* m, const double* theta, size_t n, double* out,
+                               double* out_grad, char* err, size_t err_len) {
+  return mlp_guard(err, err_len, [&] {
+    need(m && theta && out && out_grad, "NULL argument");
+    need(n <= (1u << 24), "more than 2^24 points");
+    if (n == 0) return;
+    // The same device path as the delayed-acceptance Langevin loop.
+    Buf<double> dth, dout, dgrad;
+    dth.alloc(n * m->d);
+    dout.alloc(n);
+    dgrad.alloc(n * m->d);
+    MLP_CK(cudaMemcpyAsync(dth.p, theta, n * m->d * sizeof(double), cudaMemcpyHostToDevice,
+                           m->st));
+    std::string e;
+    const int rc = gpum::mlp_infer_grad(m, dth.p, (int)n, m->d, dout.p, dgrad.p, m->st, &e);
+    if (rc != GPUM_OK) throw MlpFail{rc, e};
+    MLP_CK(cudaMemcpyAsync(out, dout.p, n * sizeof(double), cudaMemcpyDeviceToHost, m->st));
+    MLP_CK(cudaMemcpyAsync(out_grad, dgrad.p, n * m->d * sizeof(double), cudaMemcpyDeviceToHost,
+                           m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
+    m->check_err();
+  });
+}
+
 int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n,
                             float* out_grads, float* out_loss, char* err, size_t err_len) {
   return mlp_guard(err, err_len, [&] {
@@ -914,26 +1076,23 @@ int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double*
     Buf<float> dth;
     Buf<double> dll;
     upload_pairs(m, theta, ll, n, dth, dll);
-    mlp_gather<<<m->B, 128, 0, m->st>>>(dth.p, dll.p, n, m->d, m->dp, m->B, 0, 0, 0, m->xmean.p,
-                                        m->xinv.p, m->xw_or_null(), m->ymean, m->yinv, m->Xh.p,
-                                        m->t.p);
-    m->forward(m->B);
-    m->backward((int)n);
-    const int H = m->H, dp = m->dp;
-    size_t off = 0;
-    auto cp = [&](const float* src, size_t cnt) {
-      MLP_CK(cudaMemcpyAsync(out_grads + off, src, cnt * sizeof(float), cudaMemcpyDeviceToHost,
-                             m->st));
-      off += cnt;
-    };
-    cp(m->gW1.p, (size_t)H * dp);
-    cp(m->gb1.p, H);
-    cp(m->gW2.p, (size_t)H * H);
-    cp(m->gb2.p, H);
-    cp(m->gw3.p, H);
-    cp(m->gb3.p, 1);
+    Buf<float> loss1;
+    loss1.alloc(1);
+    mlp_gather<<<m->B / kGatherRows, 32 * kGatherRows, 0, m->st>>>(
+        dth.p, dll.p, n, m->d, m->dp, m->B, 0, 0, m->ctr.p,
+                                        m->xmean.p, m->xinv.p, m->xw_or_null(), m->ymean,
+                                        m->yinv, m->Xh.p, m->XTh.p, m->t.p);
+    MLP_CK(cudaGetLastError());
+    m->forward(m->B, (int)n, m->t.p);
+    // loss slot: the device step counter is not advanced without `apply`
+    uint32_t step = 0;
+    MLP_CK(cudaMemcpyAsync(&step, m->ctr.p, sizeof step, cudaMemcpyDeviceToHost, m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));
+    m->backward_and_update(0.0f, 0, loss1.p, step, 1);
+    MLP_CK(cudaMemcpyAsync(out_grads, m->G.p, m->L.n * sizeof(float), cudaMemcpyDeviceToHost,
+                           m->st));
     float l = 0.0f;
-    MLP_CK(cudaMemcpyAsync(&l, m->loss.p, sizeof l, cudaMemcpyDeviceToHost, m->st));
+    MLP_CK(cudaMemcpyAsync(&l, loss1.p, sizeof l, cudaMemcpyDeviceToHost, m->st));
     m->check_err();
     if (out_loss) *out_loss = l / (float)n;
   });
@@ -942,18 +1101,7 @@ int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double*
 int gpum_b200_mlp_get_params(gpum_b200_mlp* m, float* out, char* err, size_t err_len) {
   return mlp_guard(err, err_len, [&] {
     need(m && out, "NULL argument");
-    const int H = m->H, dp = m->dp;
-    size_t off = 0;
-    auto cp = [&](const float* src, size_t cnt) {
-      MLP_CK(cudaMemcpyAsync(out + off, src, cnt * sizeof(float), cudaMemcpyDeviceToHost, m->st));
-      off += cnt;
-    };
-    cp(m->W1.p, (size_t)H * dp);
-    cp(m->b1.p, H);
-    cp(m->W2.p, (size_t)H * H);
-    cp(m->b2.p, H);
-    cp(m->w3.p, H);
-    cp(m->b3.p, 1);
+    MLP_CK(cudaMemcpyAsync(out, m->P.p, m->L.n * sizeof(float), cudaMemcpyDeviceToHost, m->st));
     MLP_CK(cudaStreamSynchronize(m->st));
   });
 }
@@ -962,7 +1110,7 @@ int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
                              float* C, char* err, size_t err_len) {
   return mlp_guard(err, err_len, [&] {
     need(A && B && C, "NULL argument");
-    need(M % 128 == 0 && K % 64 == 0 && (N % 128 == 0 || N % 64 == 0) && M && N && K,
+    need(M % 128 == 0 && K % 64 == 0 && N % 64 == 0 && M && N && K,
          "M, N, K must be multiples of 128, 64 and 64");
     std::vector<bf16> ah((size_t)M * K), bh((size_t)N * K);
     for (size_t i = 0; i < ah.size(); ++i) ah[i] = __float2bfloat16(A[i]);
@@ -975,11 +1123,15 @@ int gpum_b200_mlp_gemm_check(uint32_t M, uint32_t N, uint32_t K, const float* A,
     db.alloc(bh.size());
     dc.alloc((size_t)M * N);
     tmp.err.alloc(1);
-    tmp.splitk.alloc(std::min<size_t>((size_t)32 * M * N, (size_t)1 << 26));
     MLP_CK(cudaMemsetAsync(tmp.err.p, 0, sizeof(uint32_t), tmp.st));
     MLP_CK(cudaMemcpyAsync(da.p, ah.data(), ah.size() * 2, cudaMemcpyHostToDevice, tmp.st));
     MLP_CK(cudaMemcpyAsync(db.p, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice, tmp.st));
-    tmp.gemm_any(da.p, db.p, dc.p, nullptr, nullptr, (int)M, (int)N, (int)K);
+    GemmArgs a = tmp.args(da.p, db.p, (int)M, (int)N, (int)K);
+    a.C = dc.p;
+    if (N % 512 == 0) tmp.gemm<512, EPI_STORE>(a, 1);
+    else if (N % 256 == 0) tmp.gemm<256, EPI_STORE>(a, 1);
+    else if (N % 128 == 0) tmp.gemm<128, EPI_STORE>(a, 1);
+    else tmp.gemm<64, EPI_STORE>(a, 1);
     MLP_CK(cudaMemcpyAsync(C, dc.p, (size_t)M * N * 4, cudaMemcpyDeviceToHost, tmp.st));
     tmp.check_err();
   });

@@ -285,7 +285,10 @@ GPUM_API void gpum_b200_session_destroy(gpum_b200_session* s);
  * parameters, trained and evaluated on the GPU with BF16 tcgen05 tensor-core
  * GEMMs (f32 accumulation in tensor memory), f32 master weights and Adam.
  * No counterpart in the reference: it is the first stage of delayed
- * acceptance.  hidden and batch are multiples of 128; d <= 256. */
+ * acceptance.  hidden is 128, 256 or 512; batch a multiple of 128; d <= 256.
+ * A training step is seven kernels (input gather, two forward GEMMs with
+ * the head fused into the second one's epilogue, three gradient GEMMs, one
+ * fixed-order gradient reduction with Adam), replayed as a CUDA graph. */
 typedef struct gpum_b200_mlp gpum_b200_mlp;
 
 GPUM_API int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t seed,
@@ -309,6 +312,12 @@ GPUM_API int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const do
 /* Predicted log-likelihood at n points (host arrays). */
 GPUM_API int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, double* out,
                                    char* err, size_t err_len);
+/* Predicted log-likelihood and its gradient with respect to the parameters
+ * (out_grad n x d, row-major) at n points (host arrays): the drift of the
+ * Langevin proposal in session_run_da, through the same device path. */
+GPUM_API int gpum_b200_mlp_predict_grad(gpum_b200_mlp* m, const double* theta, size_t n,
+                                        double* out, double* out_grad, char* err,
+                                        size_t err_len);
 /* Gradients of the batch loss at the first n <= batch pairs, without an
  * update: out = [dW1 (H x dp) | db1 (H) | dW2 (H x H) | db2 (H) | dw3 (H) |
  * db3 (1)], dp = d rounded up to 64; *out_loss = mean squared error. */
@@ -348,10 +357,14 @@ GPUM_API int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, 
 /* Two-stage Metropolis-Hastings (Christen & Fox): the surrogate screens each
  * proposal (stage 1) and only survivors are evaluated exactly (stage 2), so
  * the chains target the exact tempered posterior.  Same arguments and
- * outputs as session_run for proposal modes 0, 1 and 2 (MALA is refused);
- * out_exact (may be NULL) receives per chain the number of exact
- * evaluations (stage-1 acceptances).  The surrogate must have d = n_params.
- * Device exchanges (session_set_exchange) run as in session_run. */
+ * outputs as session_run for proposal modes 0, 1 and 2; mode 3 is a
+ * Langevin proposal whose drift is the surrogate log-posterior gradient
+ * (the surrogate's input gradient plus the f64 prior's), preconditioned and
+ * capped as MALA (cpu_native.rs:617-651), with q(x|y)/q(y|x) in stage 1 --
+ * no exact gradient is evaluated, so it runs on either engine.  out_exact
+ * (may be NULL) receives per chain the number of exact evaluations (stage-1
+ * acceptances).  The surrogate must have d = n_params.  Device exchanges
+ * (session_set_exchange) run as in session_run. */
 GPUM_API int gpum_b200_session_run_da(gpum_b200_session* s, gpum_b200_mlp* surrogate,
                                       const double* init, const double* proposal_sd,
                                       const double* temperatures, uint32_t n_chains,

@@ -15,6 +15,16 @@ then per iteration the stage-1 uniform, the stage-2 uniform (only when stage 1
 accepted), and the next proposal's normals.  The surrogate is a callable, so
 the test can hand in the very network the GPU uses.  Used by tests only.
 
+With ``proposal="mala"`` the proposal is the reference's Langevin move
+(``cpu_native.rs:617-703``: drift (1/2) f M g with M = L L' or diag sd^2, the
+whitened drift capped at 2 sqrt(d), then y = mean + L z or mean + sd z) whose
+gradient g is the surrogate log posterior's (the surrogate's gradient plus
+the prior's, by the oracle's tape), and stage 1 carries q(x|y) / q(y|x)
+(``cpu_native.rs:704-714``); the surrogate callable then returns (values,
+gradients).  The stream starts with the np normals of the random-walk start
+proposal that the device draws and discards before its first Langevin
+proposal.
+
 With ``exchange=(ladder_len, every)`` it adds the device replica exchange:
 after every ``every``-th iteration the adjacent pairs of one parity within
 each ladder of ``ladder_len`` consecutive chains (pairs 0-1, 2-3, ... at odd
@@ -87,8 +97,70 @@ def exchange_uniform(seed, exchange, pair):
     return u53(r[0], r[1])
 
 
+def _half_m_times(sd, L, g):
+    """(1/2) f M g with the MALTA cap (``cpu_native.rs:617-651``)."""
+    n = g.size
+    dmax = 2.0 * math.sqrt(n)
+    tmp = np.empty(n)
+    if L is None:
+        for j in range(n):
+            tmp[j] = 0.5 * sd[j] * g[j]
+    else:
+        for j in range(n):
+            acc = 0.0
+            for k in range(j, n):
+                acc += L[k, j] * g[k]
+            tmp[j] = 0.5 * acc
+    ss = 0.0
+    for j in range(n):
+        ss += tmp[j] * tmp[j]
+    norm = math.sqrt(ss)
+    f = dmax / norm if norm > dmax else 1.0
+    out = np.empty(n)
+    if L is None:
+        for j in range(n):
+            out[j] = f * sd[j] * tmp[j]
+    else:
+        for k in range(n):
+            acc = 0.0
+            for j in range(k + 1):
+                acc += L[k, j] * tmp[j]
+            out[k] = f * acc
+    return out
+
+
+def _log_q(sd, L, v, m):
+    """-1/2 |Ls^-1 (v - m)|^2 (``cpu_native.rs:655-673``)."""
+    n = v.size
+    q = 0.0
+    if L is None:
+        for j in range(n):
+            r = (v[j] - m[j]) / sd[j]
+            q -= 0.5 * r * r
+        return q
+    tmp = np.empty(n)
+    for k in range(n):
+        acc = v[k] - m[k]
+        for j in range(k):
+            acc -= L[k, j] * tmp[j]
+        tmp[k] = acc / L[k, k]
+        q -= 0.5 * tmp[k] * tmp[k]
+    return q
+
+
+def _prior_grad(pcode, pconsts, n_params, theta):
+    """Gradient of the prior at theta by the oracle's tape (a program that
+    reads no data, evaluated once)."""
+    pcode = np.ascontiguousarray(pcode, dtype=np.uint32).reshape(-1)
+    if pcode.size == 0:
+        return np.zeros(n_params)
+    return O.grad_batch(pcode, pconsts, n_params, np.zeros(1), 0, 1,
+                        np.asarray(theta, dtype=np.float64).reshape(1, n_params))
+
+
 def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs, init,
-           proposal_sd, temperatures, n_iter, seed, surrogate, tie=1e-4, exchange=None):
+           proposal_sd, temperatures, n_iter, seed, surrogate, tie=1e-4, exchange=None,
+           proposal="rwm", proposal_l=None):
     """Random-walk delayed acceptance for every chain.
 
     ``surrogate(theta (n x np)) -> (n,)``.  Returns ``(draws (n_iter, C, np),
@@ -110,17 +182,47 @@ def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs
     streams = [_Stream(seed, c) for c in range(C)]
     llx = exact(x)
     px = np.array([_prior(prior_code, prior_consts, x[c]) for c in range(C)])
-    sx = np.asarray(surrogate(x), dtype=np.float64)
+    mala = proposal == "mala"
+    Ls = None
+    if proposal_l is not None:
+        Ls = np.asarray(proposal_l, dtype=np.float64).reshape(C, n_params, n_params)
+    if mala:
+        sx, gsx = surrogate(x)
+        sx = np.asarray(sx, dtype=np.float64)
+        gx = np.asarray(gsx, dtype=np.float64).reshape(C, n_params).copy()
+        for c in range(C):
+            gx[c] += _prior_grad(prior_code, prior_consts, n_params, x[c])
+            for _ in range(2 * n_params):  # the discarded random-walk start proposal
+                streams[c].next()
+        mx = np.zeros_like(x)
+    else:
+        sx = np.asarray(surrogate(x), dtype=np.float64)
     draws = np.zeros((n_iter, C, n_params))
     accepts = np.zeros(C, dtype=np.int64)
     exact_n = np.zeros(C, dtype=np.int64)
     tie_at = np.full(C, n_iter, dtype=np.int64)
 
+    def propose_one(c, y):
+        if not mala:
+            for j in range(n_params):
+                y[c, j] = x[c, j] + sd[c, j] * streams[c].normal()
+            return
+        L = None if Ls is None else Ls[c]
+        mx[c] = _half_m_times(sd[c], L, gx[c]) + x[c]
+        z = np.array([streams[c].normal() for _ in range(n_params)])
+        if L is None:
+            y[c] = mx[c] + sd[c] * z
+        else:
+            for k in range(n_params):
+                acc = mx[c, k]
+                for j in range(k + 1):
+                    acc += L[k, j] * z[j]
+                y[c, k] = acc
+
     def propose():
         y = np.empty_like(x)
         for c in range(C):
-            for j in range(n_params):
-                y[c, j] = x[c, j] + sd[c, j] * streams[c].normal()
+            propose_one(c, y)
         return y
 
     att = np.zeros(C, dtype=np.int64)
@@ -144,22 +246,33 @@ def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs
             if not (math.isfinite(delta) and lu < delta):
                 continue
             ok[i] += 1
-            for arr in (x, llx, px, sx):
+            for arr in (x, llx, px, sx) + ((gx,) if mala else ()):
                 arr[[i, i + 1]] = arr[[i + 1, i]]
             for c in (i, i + 1):
-                for j in range(n_params):
-                    y[c, j] = x[c, j] + sd[c, j] * streams[c].normal()
+                propose_one(c, y)
 
     y = propose()
     for t in range(n_iter):
-        sy = np.asarray(surrogate(y), dtype=np.float64)
+        if mala:
+            sy, gsy = surrogate(y)
+            sy = np.asarray(sy, dtype=np.float64)
+            gsy = np.asarray(gsy, dtype=np.float64).reshape(C, n_params)
+        else:
+            sy = np.asarray(surrogate(y), dtype=np.float64)
         for c in range(C):
             py = _prior(prior_code, prior_consts, y[c])
+            lqd, finite = 0.0, True
+            if mala:
+                L = None if Ls is None else Ls[c]
+                gy = gsy[c] + _prior_grad(prior_code, prior_consts, n_params, y[c])
+                my = _half_m_times(sd[c], L, gy) + y[c]
+                lqd = _log_q(sd[c], L, x[c], my) - _log_q(sd[c], L, y[c], mx[c])
+                finite = math.isfinite(sy[c] + py)
             u1 = streams[c].next()
-            a1 = ((sy[c] + py) - (sx[c] + px[c])) / temps[c]
+            a1 = ((sy[c] + py) - (sx[c] + px[c])) / temps[c] + lqd
             if abs(math.log(u1) - a1) < tie and tie_at[c] == n_iter:
                 tie_at[c] = t
-            if math.log(u1) < a1:
+            if finite and math.log(u1) < a1:
                 exact_n[c] += 1
                 lly = float(exact(y[c])[0])
                 u2 = streams[c].next()
@@ -169,6 +282,8 @@ def run_da(code, consts, prior_code, prior_consts, n_params, data, n_cols, n_obs
                 if math.log(u2) < a2:
                     x[c] = y[c]
                     llx[c], px[c], sx[c] = lly, py, sy[c]
+                    if mala:
+                        gx[c] = gy
                     accepts[c] += 1
         draws[t] = x
         if t + 1 < n_iter:

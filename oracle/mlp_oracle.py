@@ -79,3 +79,21 @@ def predict(params, d, H, X):
     Z1 = f32(bf16(Xp) @ bf16(W1).T + b1)
     Z2 = f32(bf16(silu(Z1)) @ bf16(W2).T + b2)
     return silu(Z2) @ w3 + b3[0]
+
+
+def input_grad(params, d, H, X):
+    """Gradient of the network output with respect to its (standardised or
+    whitened) input X (n x d), through the same BF16 roundings as the GPU's
+    backward pass: dZ2 = w3 silu'(Z2), dZ1 = bf16(dZ2) bf16(W2) * silu'(Z1),
+    dX = bf16(dZ1) bf16(W1).  Returns (y (n,), dX (n x d))."""
+    W1, b1, W2, b2, w3, b3, dp = unpack(params, d, H)
+    Xp = np.zeros((X.shape[0], dp))
+    Xp[:, :d] = X
+    Z1 = f32(bf16(Xp) @ bf16(W1).T + b1)
+    Z2 = f32(bf16(silu(Z1)) @ bf16(W2).T + b2)
+    y = silu(Z2) @ w3 + b3[0]
+    dZ2 = f32(w3[None, :] * dsilu(Z2))
+    dZ1 = f32(f32(bf16(dZ2) @ bf16(W2)) * dsilu(Z1))
+    dX = bf16(dZ1) @ bf16(W1)
+    return y, dX[:, :d]
+

@@ -91,16 +91,109 @@ def test_two_stage_trajectories_match_oracle(gpu, temps_kind):
     assert exact.sum() < C * n_iter
 
 
-def test_run_da_refuses_mala(gpu):
+def test_run_da_refuses_de_sync(gpu):
     w = W.make("gaussian", n_obs=500)
     C = 4
     with _session(gpu, w) as s:
         net = gpu.Surrogate(1, hidden=128, batch=128)
         try:
-            with pytest.raises(gpu.GpumError, match="symmetric proposal"):
-                s.run_da(net, np.zeros((C, 1)), np.full((C, 1), 0.1), np.ones(C), 10, 1, 3)
+            with pytest.raises(gpu.GpumError, match="proposal mode"):
+                s.run_da(net, np.zeros((C, 1)), np.full((C, 1), 0.1), np.ones(C), 10, 1, 4)
         finally:
             net.close()
+
+
+@pytest.mark.parametrize("whiten", [False, True])
+def test_surrogate_input_gradient_matches_cpu_oracle(gpu, whiten):
+    # the drift of the Langevin proposal: d(surrogate)/d(theta) through the
+    # network's backward pass and the input transform, against the numpy
+    # restatement with the same BF16 roundings
+    from oracle import mlp_oracle as MO
+    rng = np.random.default_rng(7)
+    d, H = 6, 256
+    theta = rng.normal(0, 1, (4000, d)) @ rng.normal(0, 0.5, (d, d)) + 1.0
+    ll = -0.5 * np.sum((theta - 1.0) ** 2, axis=1) * 50.0 - 1e3
+    net = gpu.Surrogate(d, hidden=H, batch=1024, seed=2)
+    try:
+        net.fit_normalizer(theta, ll, whiten=whiten)
+        net.train(theta, ll, 200, lr=2e-3)
+        pts = theta[:300]
+        val, grad = net.predict_grad(pts)
+        # the fused inference kernel sums the head in another order
+        np.testing.assert_allclose(val, net.predict(pts), rtol=1e-6)
+        mu = theta.mean(axis=0)
+        th = pts.astype(np.float32)
+        if whiten:
+            cov = np.cov(theta, rowvar=False)
+            cov = cov + np.eye(d) * 1e-10 * float(np.mean(np.diag(cov)))
+            T = np.linalg.inv(np.linalg.cholesky(cov)).astype(np.float32).astype(np.float64)
+            X = MO.f32((th - mu.astype(np.float32)) @ T.T.astype(np.float32))
+        else:
+            inv = (1.0 / theta.std(axis=0)).astype(np.float32).astype(np.float64)
+            T = np.diag(inv)
+            X = MO.f32((th - mu.astype(np.float32)) * inv.astype(np.float32))
+        _, dX = MO.input_grad(net.params(), d, H, X)
+        ref = dX @ T * np.float32(np.std(ll))
+        err = np.linalg.norm(grad - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        assert np.median(err) < 2e-3 and err.max() < 2e-2, (np.median(err), err.max())
+    finally:
+        net.close()
+
+
+@pytest.mark.parametrize("with_L", [False, True])
+def test_langevin_two_stage_trajectories_match_oracle(gpu, with_L):
+    # delayed acceptance with the Langevin proposal driven by the surrogate
+    # gradient: same draws, decisions and exact-evaluation counts as the
+    # oracle (outside the tie band), with the very network the GPU uses
+    w = W.make("logistic", n_obs=2048, p=4)
+    m = w.model
+    rng = np.random.default_rng(8)
+    C, n_iter, seed = 12, 30, 41
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.03)
+    L = None
+    if with_L:
+        A = rng.normal(0, 1, (m.n_params, m.n_params))
+        Lc = np.linalg.cholesky(A @ A.T / m.n_params + np.eye(m.n_params)) * 0.03
+        L = np.broadcast_to(Lc, (C, m.n_params, m.n_params)).copy()
+    temps = np.ones(C)
+    with _session(gpu, w) as s:
+        big = w.truth["beta"] + rng.normal(0, 0.05, (256, m.n_params))
+        net = _trained(gpu, s, w, big, np.full((256, m.n_params), 0.04))
+        try:
+            d, acc, last, exact = s.run_da(net, init, sd, temps, n_iter, seed, 3, proposal_l=L)
+            d = d.reshape((n_iter, C, m.n_params), order="F")
+            od, oacc, oexact, tie_at = da_oracle.run_da(
+                m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                w.data, m.n_cols, w.n_obs, init, sd, temps, n_iter, seed, net.predict_grad,
+                proposal="mala", proposal_l=L)
+        finally:
+            net.close()
+    clean = tie_at == n_iter
+    assert clean.sum() >= C // 2
+    for c in range(C):
+        t = tie_at[c]
+        np.testing.assert_allclose(d[:t, c], od[:t, c], rtol=1e-5, atol=1e-6)
+    np.testing.assert_array_equal(exact[clean], oexact[clean])
+    np.testing.assert_allclose(acc[clean], oacc[clean] / n_iter, atol=1e-6)
+    assert 0 < exact.sum() < C * n_iter
+    assert acc.mean() > 0.05
+
+
+def test_surrogate_mode_mala_recovers_closed_form(gpu):
+    w = W.make("gaussian", n_obs=20000)
+    fit = api.gpu_metropolis(w.model, {"y": w.data[:, 0]}, init=np.full((128, 1), 3.0),
+                             proposal_sd=0.02, n_iter=3000, warmup=1500, seed=4, method="mala",
+                             surrogate={"hidden": 128, "batch": 2048, "steps": 800})
+    info = fit.extra["surrogate"]
+    assert info["used"], info
+    assert 0.0 < info["exact_fraction"] < 1.0
+    d = fit.draws[:, :, 0]
+    n_eff = d.size / 20.0
+    mcse = d.std() / np.sqrt(n_eff)
+    assert abs(d.mean() - w.truth["post_mean"]) < 5 * mcse
+    assert abs(d.std() - w.truth["post_sd"]) < 0.1 * w.truth["post_sd"]
+    assert rhat(d, warmup=0) < 1.01
 
 
 def test_surrogate_mode_recovers_closed_form(gpu):
@@ -198,3 +291,51 @@ def test_surrogate_mode_pt_with_device_exchanges(gpu):
     assert np.any(cold > 1.5) and np.any(cold < -1.5)
     assert abs(cold[cold > 0].mean() - 3) < 0.4 and abs(cold[cold < 0].mean() + 3) < 0.4
     assert np.nanmax(fit.extra["exchange_rate"]) > 0.2
+
+
+def test_trained_surrogate_gains_ess_per_exact_evaluation(gpu):
+    # What the trained network gains over the method without it, counted
+    # rather than timed: logistic regression (4096 observations, 5
+    # parameters), 256 chains, adaptive exact warmup whose second half is
+    # recorded, the surrogate trained on those pairs, then exact MH and
+    # two-stage sampling of equal length from the same state.  The two-stage
+    # run must reach at least twice the exact sampler's ESS per exact
+    # log-likelihood evaluation, with the same posterior means within MCSE.
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200 import adaptive as AD
+    from gpumetropolis_b200.diagnostics import ess_pooled
+    w = W.make("logistic", n_obs=4096, p=4)
+    m = w.model
+    npar, C, n_warm, n_samp, seed = m.n_params, 256, 800, 1500, 13
+    cfg = dict(api.SURROGATE_DEFAULTS)
+    cfg.update({"hidden": 128, "batch": 2048, "steps": 600, "min_pairs": 1024})
+    call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, cfg)
+    try:
+        call.record_at = n_warm // 2
+        rng = np.random.default_rng(seed)
+        init = w.truth["beta"] + rng.normal(0, 0.05, (C, npar))
+        am = AD.am_orchestrate_warmup(call, npar, C, init, np.full((C, npar), 0.02), n_warm,
+                                      seed)
+        call.start_da()
+        assert call.net is not None, call.info
+        L = am.final_L
+        mode = _native.MODE_CHOL if L is not None else _native.MODE_RWM
+        d_ex, _, _ = call.session.run(am.final_init, am.final_proposal_sd, np.ones(C), n_samp,
+                                      seed + 1, mode, 0.0, 0.0, L, rng=_native.RNG_PHILOX)
+        d_ex = d_ex.reshape((n_samp, C, npar), order="F").astype(np.float64)
+        e0 = call.exact_evals
+        d_da, _, _ = call(am.final_init, am.final_proposal_sd, n_samp, seed + 2, None, mode,
+                          0.0, 0.0, L)
+        n_exact_da = call.exact_evals - e0
+    finally:
+        call.close()
+    d_da = np.asarray(d_da, dtype=np.float64)
+    e_ex = np.array([ess_pooled(d_ex[:, :, j]) for j in range(npar)])
+    e_da = np.array([ess_pooled(d_da[:, :, j]) for j in range(npar)])
+    per_eval_ex = e_ex / (n_samp * C)
+    per_eval_da = e_da / max(n_exact_da, 1)
+    assert np.all(per_eval_da >= 2.0 * per_eval_ex), per_eval_da / per_eval_ex
+    mc = np.sqrt(d_ex.reshape(-1, npar).var(axis=0) / e_ex +
+                 d_da.reshape(-1, npar).var(axis=0) / e_da)
+    z = np.abs(d_ex.mean(axis=(0, 1)) - d_da.mean(axis=(0, 1))) / mc
+    assert z.max() < 4.0, z
