@@ -99,6 +99,12 @@ def _args():
                         "ESS/s on the mixture configuration (512 ladders of 16 temperatures, "
                         "device exchanges), one JSON line")
     p.add_argument("--pt-da-warmup", type=int, default=300)
+    p.add_argument("--c5-da", action="store_true",
+                   help="instead of the headline line: exact vs delayed-acceptance ESS/s for "
+                        "DE and the Langevin move on the Student-t configuration at full size "
+                        "with the 65-512-512-1 surrogate (minutes), one JSON line")
+    p.add_argument("--c5-warmup", type=int, default=128)
+    p.add_argument("--c5-iters", type=int, default=40)
     p.add_argument("--pt-da-iters", type=int, default=400)
     p.add_argument("--configs-obs-shift", type=int, default=0,
                    help="with --configs: divide each configuration's observation count by "
@@ -771,7 +777,7 @@ def pt_da_measure(n_warm, n_samp, K=16, every=10, seed=21):
     C, npar = w.n_chains, m.n_params
     temps = np.tile(np.geomspace(1.0, 64.0, K), C // K)
     cfg = dict(api.SURROGATE_DEFAULTS)
-    cfg["max_pairs"] = 1 << 18
+    cfg.update({"max_pairs": 1 << 18, "hidden": 256})  # the configuration's 5-256-256-1
     call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, cfg)
     try:
         s = call.session
@@ -863,10 +869,103 @@ def run_pt_da(a):
     print(json.dumps({"pt_da": pt_da_measure(a.pt_da_warmup, a.pt_da_iters)}), flush=True)
 
 
+def c5_da_measure(n_warm, n_samp, seed=31, modes=("de", "mala")):
+    """Student-t regression at full size (N = 2^24, 65 parameters, 8192
+    chains) with the 65-512-512-1 surrogate: adaptive exact warmup (random
+    walk with the pooled Cholesky factor) whose draws' proposals are all
+    recorded (n_warm x 8192 pairs, 2^20 at n_warm = 128), the surrogate
+    trained on them, then for each method exact and two-stage sampling of
+    equal length from the warmup's last state: DE (snapshot differences,
+    gamma 2.38 / sqrt(2 d)) and the Langevin move (exact MALA with the
+    adjoint kernel against delayed acceptance whose drift is the surrogate's
+    gradient).  Seconds are wall seconds of each blocking call (draws back);
+    ESS multi-chain per parameter."""
+    from gpumetropolis_b200 import _native, api
+    from gpumetropolis_b200 import adaptive as AD
+    from gpumetropolis_b200 import workloads as W
+    t = time.perf_counter()
+    w = W.make("student_t")
+    t_gen = time.perf_counter() - t
+    m = w.model
+    C, npar = w.n_chains, m.n_params
+    cfg = dict(api.SURROGATE_DEFAULTS)
+    cfg.update({"hidden": 512, "max_pairs": 1 << 20})
+    call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, cfg)
+    out = {"config": "student-t regression N=2^24, 65 params, 8192 chains; surrogate 65-512-512-1",
+           "data_gen_s": round(t_gen, 1), "warmup_iters": n_warm, "sampling_iters": n_samp}
+    try:
+        call.record_at = 0
+        rng = np.random.default_rng(seed)
+        centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
+        init = centre + rng.normal(0.0, 1e-3, (C, npar))
+        t = time.perf_counter()
+        am = AD.am_orchestrate_warmup(call, npar, C, init, np.full((C, npar), 2e-4), n_warm,
+                                      seed)
+        out["warmup_s"] = round(time.perf_counter() - t, 2)
+        t = time.perf_counter()
+        call.start_da()
+        out["train_s"] = round(time.perf_counter() - t, 3)
+        out["surrogate"] = call.da_summary()
+        if call.net is None:
+            return out
+        x0, sd0, L0 = am.final_init, am.final_proposal_sd, am.final_L
+        ones = np.ones(C)
+        s = call.session
+        buf = _pinned_f32(n_samp * C * npar)
+
+        def timed(f):
+            s.sync()
+            t0 = time.perf_counter()
+            r = f()
+            return r, time.perf_counter() - t0
+
+        for meth in modes:
+            if meth == "de":
+                mode, g, dn, L = _native.MODE_DE, 2.38 / math.sqrt(2 * npar), 1e-3, None
+            else:
+                mode, g, dn, L = _native.MODE_MALA, 0.0, 0.0, L0
+            (d_ex, acc_ex, _), t_ex = timed(lambda: s.run(
+                x0, sd0, ones, n_samp, seed + 7, mode, g, dn, L, rng=_native.RNG_PHILOX,
+                out_draws=buf))
+            e_ex = _ess_all(d_ex.reshape((n_samp, C, npar), order="F"))
+            e0 = call.exact_evals
+            (d_da, acc_da, _), t_da = timed(lambda: call(x0, sd0, n_samp, seed + 8, None, mode,
+                                                         g, dn, L, out_draws=buf))
+            frac = (call.exact_evals - e0) / (n_samp * C)
+            e_da = _ess_all(np.asarray(d_da))
+            r_ex, r_da = e_ex.min() / t_ex, e_da.min() / t_da
+            out[meth] = {
+                "exact": {"seconds": round(t_ex, 2), "accept": float(np.mean(acc_ex)),
+                          "ess_min": float(e_ex.min()), "ess_per_s_min": r_ex},
+                "da": {"seconds": round(t_da, 2), "accept": float(np.mean(acc_da)),
+                       "exact_fraction": frac, "ess_min": float(e_da.min()),
+                       "ess_per_s_min": r_da},
+                "gain_ess_per_s_min": r_da / r_ex,
+                "gain_ess_per_s_min_with_training":
+                    e_da.min() / (t_da + out["train_s"]) / r_ex}
+    finally:
+        call.close()
+    return out
+
+
+def run_c5_da(a):
+    import torch
+
+    from gpumetropolis_b200 import _native
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    torch.cuda.set_device(0)
+    print(json.dumps({"c5_da": c5_da_measure(a.c5_warmup, a.c5_iters)}), flush=True)
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.c5_da:
+        run_c5_da(a)
     elif a.pt_da:
         run_pt_da(a)
     elif a.configs:

@@ -78,6 +78,8 @@ SIGNATURES = {
                                               C.c_double, _errp, _sz]),
     "gpum_b200_mlp_train": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, C.c_uint32, C.c_double,
                                       _f32p, _errp, _sz]),
+    "gpum_b200_mlp_train_stages": (C.c_int, [C.c_void_p, _f64p, _f64p, _sz, C.c_uint32,
+                                             _u32p, _f64p, _f32p, _errp, _sz]),
     "gpum_b200_mlp_predict": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
     "gpum_b200_mlp_predict_grad": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _f64p, _errp,
                                              _sz]),
@@ -622,6 +624,21 @@ class Surrogate:
                                              y.size, steps, lr, _p(losses, C.c_float), err,
                                              _ERRLEN), err)
         return losses[:steps]
+
+    def train_stages(self, theta, ll, stages):
+        """Adam on the pairs with a learning-rate schedule, ``stages`` a list of
+        (steps, lr); the pairs are uploaded once.  Returns every step's loss."""
+        th, y = _f64(theta), _f64(ll)
+        steps = np.ascontiguousarray([int(s) for s, _ in stages], dtype=np.uint32)
+        lrs = np.ascontiguousarray([float(r) for _, r in stages], dtype=np.float64)
+        total = int(steps.sum())
+        losses = np.empty(max(total, 1), np.float32)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_mlp_train_stages(
+            self._h, _p(th, C.c_double), _p(y, C.c_double), y.size, steps.size,
+            _p(steps, C.c_uint32), _p(lrs, C.c_double), _p(losses, C.c_float), err, _ERRLEN),
+            err)
+        return losses[:total]
 
     def predict(self, theta):
         th = _f64(theta)

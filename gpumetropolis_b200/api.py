@@ -93,12 +93,12 @@ def _data_matrix(model: GpumModel, data):
     return np.ascontiguousarray(np.stack(cols, axis=1)), n
 
 
-# hidden/batch: network width and training batch (multiples of 128); steps/lr:
+# hidden: network width (128, 256 or 512); batch: training batch (a multiple of 128); steps/lr:
 # Adam steps at lr, then steps at lr/3 and lr/10; step_scale multiplies the
 # adapted random-walk proposal in the two-stage phase (screening makes
 # rejections cheap, so longer steps pay: Sherlock, Thiery & Golightly 2021);
 # whiten: inputs whitened by the pairs' covariance.
-SURROGATE_DEFAULTS = {"hidden": 256, "batch": 4096, "steps": 2000, "lr": 2e-3,
+SURROGATE_DEFAULTS = {"hidden": 128, "batch": 4096, "steps": 1200, "lr": 3e-3,
                       "max_pairs": 1 << 20, "min_pairs": 2048, "seed": 1,
                       "step_scale": 1.6, "whiten": True}
 
@@ -158,8 +158,8 @@ class _Backend:
                                 batch=int(self.cfg["batch"]), seed=int(self.cfg["seed"]))
         net.fit_normalizer(theta[train], ll[train], whiten=bool(self.cfg["whiten"]))
         steps, lr = int(self.cfg["steps"]), float(self.cfg["lr"])
-        for f in (1.0, 1.0 / 3.0, 0.1):
-            loss = net.train(theta[train], ll[train], steps, lr=lr * f)
+        loss = net.train_stages(theta[train], ll[train],
+                                [(steps, lr), (steps, lr / 3.0), (steps, lr / 10.0)])
         resid = net.predict(theta[hold]) - ll[hold]
         self.net = net
         self.info = {"used": True, "pairs": int(theta.shape[0]),

@@ -805,6 +805,18 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
 // survivors -> exact evaluation of the compacted prefix only (CTAs of dead
 // chain blocks exit at once) -> stage-2 decision, draw, next proposal.
 // The loop is captured in a CUDA graph of kDaGraphLen iterations.
+// The compiled engine's f64 prior at the chains' points (state or proposal)
+// into out; with the Langevin proposal its gradient is added into D.gs (the
+// surrogate's data-term gradient there).
+void launch_prior(gpum_b200_session* s, double* pts, double* out) {
+  int n = s->n_chains;
+  double* grad = s->A.mode == MODE_MALA ? s->D.gs : nullptr;
+  void* args[] = {(void*)&pts, (void*)&n, (void*)&out, (void*)&grad};
+  GPUM_CK(cudaLaunchKernel((const void*)s->cm.k_prior, dim3((unsigned)((n + 127) / 128)),
+                           dim3(128), args, 0, s->stream));
+  ++s->launches;
+}
+
 void da_step(gpum_b200_session* s) {
   const int C = s->n_chains, np = (int)s->np;
   std::string e;
@@ -814,6 +826,7 @@ void da_step(gpum_b200_session* s) {
                      : mlp_infer(s->da_mlp, s->prop.p, C, np, s->sll_y.p, s->stream, &e);
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
   cudaStream_t st = s->stream;
+  if (s->D.prior_ready) launch_prior(s, s->prop.p, s->prior_y.p);
   // 64-thread blocks spread the per-chain f64 work (prior, proposal) over
   // more SMs; finalize runs one warp per chain.
   const unsigned cb = (unsigned)((C + 63) / 64);
@@ -822,12 +835,12 @@ void da_step(gpum_b200_session* s) {
   da_pack_kernel<<<(unsigned)(((size_t)C * np + 255) / 256), 256, 0, st>>>(s->A, s->D);
   GPUM_CK(cudaGetLastError());
   s->launch_with(s->geo_da, s->E_da, PH_EVAL);
-  da_finalize_kernel<<<(unsigned)((C + 7) / 8), 256, 0, st>>>(
+  da_finalize_kernel<<<(unsigned)((C + 7) / 8), 256, (size_t)8 * 2 * np * sizeof(double), st>>>(
       s->A, s->D, s->da_partials.p, s->geo_da.CG, s->geo_da.NCB * s->geo_da.NOB,
       s->geo_da.ntiles, s->geo_da.C_pad);
   da_tick_kernel<<<1, 32, 0, st>>>(s->D);
   GPUM_CK(cudaGetLastError());
-  s->launches += 5 + (uint64_t)s->da_mlp_launches;
+  s->launches += 5 + (uint64_t)s->da_mlp_launches;  // launch_prior counts itself
   if (s->pt_K > 0) {  // exchanges on the exact log posteriors, caches swapped along
     PtArgs P{s->pt_K,   s->pt_every,  s->D.iter, s->D.sll_x, s->D.prior_x,
              s->pt_n.p, s->pt_att.p, s->pt_acc.p, s->D.full,  s->D.C_pad};
@@ -888,7 +901,7 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   s->da_active.ensure(1);
   s->da_iter.ensure(1);
   s->da_params.ensure((size_t)np * g.C_pad);
-  // The exact evaluation runs a fixed 1-D grid of 4 CTAs per resident slot
+  // The exact evaluation runs a fixed 1-D grid of one CTA per resident slot
   // (at least one per chain block); the kernel splits it into (live chain
   // blocks x observation blocks) from the stage-1 survivor count on the
   // device (da_obs_blocks).
@@ -896,7 +909,9 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   {
     int occ = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kc.fn, kThreads, g.smem);
-    s->geo_da.NCB = std::max(4 * num_sms() * std::max(occ, 1), g.NCB);
+    // one wave of resident CTAs: with few survivors each CTA then takes many
+    // tiles, so the per-CTA set-up is paid once per SM slot
+    s->geo_da.NCB = std::max(num_sms() * std::max(occ, 1), g.NCB);
     s->geo_da.NOB = 1;
   }
   const int max_nob = std::max(1, std::min(s->geo_da.NCB, std::max(g.ntiles, 1)));
@@ -932,6 +947,10 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   if (rc != GPUM_OK) throw Failure{rc, "surrogate: " + e};
   s->da_mlp_launches = lang ? mlp_infer_grad_launches(mlp, (int)C)
                             : mlp_infer_launches(mlp, (int)C);
+  // With the compiled engine the prior is its generated f64 code, one kernel
+  // over all chains, instead of an interpreted prior per chain thread.
+  D.prior_ready = s->kc.compiled && s->cm.k_prior ? 1 : 0;
+  if (D.prior_ready) launch_prior(s, s->state.p, s->prior_x.p);
   s->launches += (uint64_t)s->da_mlp_launches;
   da_setup_kernel<<<(C + 255) / 256, 256, 0, st>>>(s->A, D);
   GPUM_CK(cudaGetLastError());

@@ -372,6 +372,17 @@ extern "C" __global__ void gm_materialize(float* __restrict__ cols, long long n_
   for (int k = 0; k < GM_NMAT; ++k) cols[(size_t)(GM_NCOLS + k) * ld + o] = m[k];
 }
 
+// The generated f64 prior at n points x[n][GM_NP], one thread per point;
+// with grad != nullptr its gradient is added into grad[n][GM_NP].  Delayed
+// acceptance reads these instead of interpreting the prior per chain.
+extern "C" __global__ void gm_prior_batch(const double* __restrict__ x, int n,
+                                          double* __restrict__ out, double* __restrict__ grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* p = x + (size_t)i * GM_NP;
+  out[i] = grad ? gpum::gm_prior_grad(p, grad + (size_t)i * GM_NP) : gpum::gm_prior(p);
+}
+
 // Value-only kernel: PH_EVAL / PH_POINTWISE / RWM, DE and Cholesky steps.
 // CTAs per SM the registers must allow (GM_VALUE_CTAS from the host: three
 // for narrow paired models, 80 registers; two for the other paired ones).

@@ -259,7 +259,8 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   }
   if (cudaLibraryGetKernel(&e.model.k_value, e.lib, "gm_iter_value") != cudaSuccess ||
       cudaLibraryGetKernel(&e.model.k_grad, e.lib, "gm_iter_grad") != cudaSuccess ||
-      cudaLibraryGetKernel(&e.model.k_mat, e.lib, "gm_materialize") != cudaSuccess) {
+      cudaLibraryGetKernel(&e.model.k_mat, e.lib, "gm_materialize") != cudaSuccess ||
+      cudaLibraryGetKernel(&e.model.k_prior, e.lib, "gm_prior_batch") != cudaSuccess) {
     *err = "compiled model is missing its kernels";
     cudaLibraryUnload(e.lib);
     return 1;

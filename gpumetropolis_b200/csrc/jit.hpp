@@ -16,6 +16,7 @@ struct CompiledModel {
   cudaKernel_t k_value = nullptr;   // gm_iter_value
   cudaKernel_t k_grad = nullptr;    // gm_iter_grad
   cudaKernel_t k_mat = nullptr;     // gm_materialize (extra data columns)
+  cudaKernel_t k_prior = nullptr;   // gm_prior_batch (f64 prior, optional gradient)
   int n_mat = 0;                    // materialized data-only operations
   int G = 1, GG = 1;                // chains per thread of each kernel
   bool pair = false;                // value kernel evaluates observation pairs

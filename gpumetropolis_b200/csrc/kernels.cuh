@@ -316,6 +316,10 @@ struct DaArgs {
   double* tadj;      // [C][n_prior]
   uint32_t* tlhs;    // [C][n_prior]
   uint32_t* trhs;    // [C][n_prior]
+  // 1: the compiled engine's prior kernel has already written prior_x (set-up)
+  // or prior_y (each iteration) and, with the Langevin proposal, added the
+  // prior's gradient into gs; 0: the kernels interpret the prior themselves
+  int prior_ready;
 };
 
 // Surrogate log-posterior gradient at theta: the surrogate's data-term
@@ -348,7 +352,12 @@ static __global__ void da_setup_kernel(ChainArgs A, DaArgs D) {
   if (c >= A.n_chains) return;
   const double* x = A.state + (size_t)c * A.np;
   if (A.mode == MODE_MALA) {
-    D.prior_x[c] = da_post_grad(A, D, c, x, D.gs + (size_t)c * A.np, A.gx + (size_t)c * A.np);
+    if (D.prior_ready) {
+      for (int j = 0; j < A.np; ++j) A.gx[(size_t)c * A.np + j] = D.gs[(size_t)c * A.np + j];
+    } else {
+      D.prior_x[c] =
+          da_post_grad(A, D, c, x, D.gs + (size_t)c * A.np, A.gx + (size_t)c * A.np);
+    }
     if (A.n_iter > 0) {
       Stream rs = make_stream(A, c);
       rs.it = 0;
@@ -356,7 +365,7 @@ static __global__ void da_setup_kernel(ChainArgs A, DaArgs D) {
       propose(A, c, rs, D.full, D.C_pad);
       A.ctr[c] = rs.ctr;
     }
-  } else {
+  } else if (!D.prior_ready) {
     D.prior_x[c] = InterpPrior::value(A, x);
   }
   D.stage1[c] = 0;
@@ -376,7 +385,12 @@ static __global__ void da_stage1_kernel(ChainArgs A, DaArgs D) {
   double py, lqd = 0.0;
   if (A.mode == MODE_MALA) {
     double* gy = A.gy + (size_t)c * np;
-    py = da_post_grad(A, D, c, y, D.gs + (size_t)c * np, gy);
+    if (D.prior_ready) {
+      py = D.prior_y[c];
+      for (int j = 0; j < np; ++j) gy[j] = D.gs[(size_t)c * np + j];
+    } else {
+      py = da_post_grad(A, D, c, y, D.gs + (size_t)c * np, gy);
+    }
     const double* sd = A.sd + (size_t)c * np;
     const double* L = A.L ? A.L + (size_t)c * np * np : nullptr;
     double* my = A.my + (size_t)c * np;
@@ -386,7 +400,7 @@ static __global__ void da_stage1_kernel(ChainArgs A, DaArgs D) {
     lqd = log_q(np, sd, L, A.state + (size_t)c * np, my, tmp) -
           log_q(np, sd, L, y, A.mx + (size_t)c * np, tmp);
   } else {
-    py = InterpPrior::value(A, y);
+    py = D.prior_ready ? D.prior_y[c] : InterpPrior::value(A, y);
   }
   D.prior_y[c] = py;
   Stream rs = make_stream(A, c);
@@ -444,10 +458,117 @@ static __global__ void da_pack_kernel(ChainArgs A, DaArgs D) {
   D.params[(size_t)j * D.C_pad + D.slot[c]] = (float)A.prop[i];
 }
 
+// The i-th uniform (i >= 1) a chain's stream `rs` would return from its
+// current position, without advancing it: both streams are counter-based, so
+// the lanes of a warp can draw a chain's normals in parallel.
+__device__ __forceinline__ double stream_at(const Stream& rs, uint32_t i) {
+  if (rs.kind == RNG_TRIPLE32) return t32_uniform(rs.seedmix, rs.ctr + i);
+  const U4 r = philox4x32_10(U4{rs.k + i - 1u, rs.it, rs.chain, 0xB2000001u}, rs.seed,
+                             0x6A09E667u);
+  return u53(r.x, r.y);
+}
+__device__ __forceinline__ double stream_normal_at(const Stream& rs, uint32_t i0, int j) {
+  const double u1 = stream_at(rs, i0 + 2u * (uint32_t)j + 1u);
+  const double u2 = stream_at(rs, i0 + 2u * (uint32_t)j + 2u);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+// propose() for chain c by the 32 lanes of a warp: the same draws, the same
+// arithmetic per coordinate (each lane runs one coordinate's loops in the
+// serial order; the drift norm is summed by lane 0 in coordinate order), so
+// the proposal equals the serial one bit for bit.  `sm` is this warp's
+// scratch of 2 np doubles.  Returns the stream advanced past the draws.
+__device__ inline Stream propose_warp(const ChainArgs& A, int c, Stream rs, float* params,
+                                      int C_pad, int lane, double* sm) {
+  const int np = A.np;
+  const double* x = A.state + (size_t)c * np;
+  double* y = A.prop + (size_t)c * np;
+  const double* sd = A.sd + (size_t)c * np;
+  const double* L = A.L ? A.L + (size_t)c * np * np : nullptr;
+  uint32_t used = 2u * (uint32_t)np;
+  if (A.mode == MODE_RWM) {
+    for (int j = lane; j < np; j += 32) y[j] = x[j] + sd[j] * stream_normal_at(rs, 0, j);
+  } else if (A.mode == MODE_CHOL || A.mode == MODE_MALA) {
+    double* z = sm;
+    double* base = sm + np;
+    if (A.mode == MODE_MALA) {
+      // mean = x + f (1/2) M g (half_m_times, cpu_native.rs:617-651)
+      const double* gx = A.gx + (size_t)c * np;
+      double* tmp = z;  // reused for z below, after the mean is built
+      for (int j = lane; j < np; j += 32) {
+        double acc = 0.0;
+        if (!L) {
+          tmp[j] = 0.5 * sd[j] * gx[j];
+        } else {
+          for (int k = j; k < np; ++k) acc += L[(size_t)k * np + j] * gx[k];
+          tmp[j] = 0.5 * acc;
+        }
+      }
+      __syncwarp();
+      double f = 1.0;
+      if (lane == 0) {
+        double ss = 0.0;
+        for (int j = 0; j < np; ++j) ss += tmp[j] * tmp[j];
+        const double norm = sqrt(ss), dmax = 2.0 * sqrt((double)np);
+        f = norm > dmax ? dmax / norm : 1.0;
+      }
+      f = __shfl_sync(0xffffffffu, f, 0);
+      double* mx = A.mx + (size_t)c * np;
+      for (int k = lane; k < np; k += 32) {
+        double out;
+        if (!L) {
+          out = f * sd[k] * tmp[k];
+        } else {
+          double acc = 0.0;
+          for (int j = 0; j <= k; ++j) acc += L[(size_t)k * np + j] * tmp[j];
+          out = f * acc;
+        }
+        mx[k] = out + x[k];
+        base[k] = mx[k];
+      }
+    } else {
+      for (int k = lane; k < np; k += 32) base[k] = x[k];
+    }
+    __syncwarp();
+    for (int j = lane; j < np; j += 32) z[j] = stream_normal_at(rs, 0, j);
+    __syncwarp();
+    for (int k = lane; k < np; k += 32) {
+      if (L) {
+        double acc = base[k];
+        for (int j = 0; j <= k; ++j) acc += L[(size_t)k * np + j] * z[j];
+        y[k] = acc;
+      } else {
+        y[k] = base[k] + sd[k] * z[k];
+      }
+    }
+  } else {  // DE on the snapshot
+    const int n = A.n_chains;
+    int a = (int)(stream_at(rs, 1) * (double)n);
+    if (a >= n) a = n - 1;
+    int b = (int)(stream_at(rs, 2) * (double)n);
+    if (b >= n) b = n - 1;
+    if (b == a) b = (b + 1) % n;
+    const double g = stream_at(rs, 3) < 0.1 ? 1.0 : A.gamma;
+    const double* pa = A.snap + (size_t)a * np;
+    const double* pb = A.snap + (size_t)b * np;
+    for (int j = lane; j < np; j += 32) {
+      const double zj = stream_normal_at(rs, 3, j);
+      const double diff = pa[j] - pb[j];
+      y[j] = x[j] + g * diff + A.de_noise * sd[j] * zj;
+    }
+    used += 3u;
+  }
+  for (int j = lane; j < np; j += 32) params[(size_t)j * C_pad + c] = (float)y[j];
+  __syncwarp();
+  if (rs.kind == RNG_TRIPLE32) rs.ctr += used;
+  else rs.k += used;
+  return rs;
+}
+
 // Stage 2 for the survivors, the draw for every chain, the next proposal.
 // One warp per chain: the lanes add the chain's observation-block partials in
 // a fixed lane-strided order and a fixed shuffle tree (deterministic), lane 0
-// does the rest.
+// takes the decision, and the lanes copy, record and propose in parallel.
 static __global__ void da_finalize_kernel(ChainArgs A, DaArgs D, const double* __restrict__ partials,
                                           int CG, int total, int ntiles, int C_pad_eval) {
   const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -463,40 +584,51 @@ static __global__ void da_finalize_kernel(ChainArgs A, DaArgs D, const double* _
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(0xffffffffu, ll, off);
   }
-  if (lane != 0) return;
+  extern __shared__ double fin_sm[];  // [warps per block][2 np]
   const int np = A.np;
   const uint32_t t = D.iter[0];
   double* x = A.state + (size_t)c * np;
   const double* y = A.prop + (size_t)c * np;
   Stream rs = make_stream(A, c);
+  int take = 0;
   if (live) {
-    const double plp = ll + D.prior_y[c];
-    A.last_eval[c] = plp;
-    const double u = da_uniform(rs, t, 0xFFFF0002u);
-    const double llx = A.cur[c] - D.prior_x[c];
-    const double a2 = ((ll - llx) - (D.sll_y[c] - D.sll_x[c])) / A.temp[c];
-    if (log(u) < a2) {
-      for (int j = 0; j < np; ++j) x[j] = y[j];
+    if (lane == 0) {
+      const double plp = ll + D.prior_y[c];
+      A.last_eval[c] = plp;
+      const double u = da_uniform(rs, t, 0xFFFF0002u);
+      const double llx = A.cur[c] - D.prior_x[c];
+      const double a2 = ((ll - llx) - (D.sll_y[c] - D.sll_x[c])) / A.temp[c];
+      take = log(u) < a2 ? 1 : 0;
+      if (take) {
+        A.cur[c] = plp;
+        D.sll_x[c] = D.sll_y[c];
+        D.prior_x[c] = D.prior_y[c];
+        A.accepts[c] += 1;
+      }
+      D.stage1[c] += 1;
+    } else if (rs.kind == RNG_TRIPLE32) {
+      rs.ctr += 1;  // the stage-2 uniform lane 0 drew
+    }
+    take = __shfl_sync(0xffffffffu, take, 0);
+    if (take) {
+      for (int j = lane; j < np; j += 32) x[j] = y[j];
       if (A.mode == MODE_MALA) {  // the drift of the new state
         double* gx = A.gx + (size_t)c * np;
         const double* gy = A.gy + (size_t)c * np;
-        for (int j = 0; j < np; ++j) gx[j] = gy[j];
+        for (int j = lane; j < np; j += 32) gx[j] = gy[j];
       }
-      A.cur[c] = plp;
-      D.sll_x[c] = D.sll_y[c];
-      D.prior_x[c] = D.prior_y[c];
-      A.accepts[c] += 1;
     }
-    D.stage1[c] += 1;
+    __syncwarp();
   }
   if (t < A.n_iter)
-    for (int j = 0; j < np; ++j) A.draws[((size_t)t * np + j) * D.C_pad + c] = (float)x[j];
+    for (int j = lane; j < np; j += 32) A.draws[((size_t)t * np + j) * D.C_pad + c] = (float)x[j];
+  __syncwarp();
   if (t + 1 < A.n_iter) {
     rs.it = t + 1;
     rs.k = 0;
-    propose(A, c, rs, D.full, D.C_pad);
+    rs = propose_warp(A, c, rs, D.full, D.C_pad, lane, fin_sm + (size_t)(threadIdx.x >> 5) * 2 * np);
   }
-  A.ctr[c] = rs.ctr;
+  if (lane == 0) A.ctr[c] = rs.ctr;
 }
 
 static __global__ void da_tick_kernel(DaArgs D) {

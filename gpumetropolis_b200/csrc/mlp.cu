@@ -174,14 +174,15 @@ struct GradParts {
 };
 
 // Every gradient from its partials (fixed order) into G; with `apply`, Adam
-// at step ctr[0] + 1 on the master weights and their BF16 copies (W1h, W2h
+// (learning rate *lr_p, device memory, so a captured step serves every stage
+// of a schedule) at step ctr[0] + 1 on the master weights and their BF16 copies (W1h, W2h
 // and the transposed W1Th, W2Th), the loss of the step into
-// loss_hist[ctr[0] - loss_base], and the last block advances ctr[0].
+// loss_hist[ctr[0] - loss_base]; mlp_step_done then advances ctr[0].
 __global__ void mlp_reduce_adam(MlpLayout L, GradParts Gp, float* __restrict__ P,
                                 float* __restrict__ Mm, float* __restrict__ V,
                                 float* __restrict__ G, bf16* __restrict__ W1h,
                                 bf16* __restrict__ W1Th, bf16* __restrict__ W2h,
-                                bf16* __restrict__ W2Th, float lr,
+                                bf16* __restrict__ W2Th, const float* __restrict__ lr_p,
                                 int apply, uint32_t* __restrict__ ctr, float* __restrict__ loss,
                                 uint32_t loss_base, uint32_t loss_cap) {
   const uint32_t step = *reinterpret_cast<volatile const uint32_t*>(ctr);
@@ -208,6 +209,7 @@ __global__ void mlp_reduce_adam(MlpLayout L, GradParts Gp, float* __restrict__ P
     }
     G[i] = g;
     if (apply) {
+      const float lr = *lr_p;
       const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
       const float t = (float)(step + 1);
       const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
@@ -233,18 +235,12 @@ __global__ void mlp_reduce_adam(MlpLayout L, GradParts Gp, float* __restrict__ P
     const uint32_t slot = step - loss_base;
     if (slot < loss_cap) loss[slot] = s;
   }
-  // Every block has read ctr[0]; the last one advances it (training steps)
-  // and re-arms the ticket.
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const uint32_t ticket = atomicAdd(&ctr[1], 1u);
-    if (ticket == gridDim.x - 1) {
-      if (apply) ctr[0] = step + 1;
-      ctr[1] = 0;
-      __threadfence();
-    }
-  }
+}
+
+// The step counter advances after the reduction (a kernel of its own: every
+// block of the reduction has read the counter by then).
+__global__ void mlp_step_done(uint32_t* __restrict__ ctr) {
+  if (threadIdx.x == 0) ctr[0] += 1;
 }
 
 __global__ void mlp_init_weights(float* __restrict__ w, size_t n, int fan_in, int cols_live,
@@ -523,7 +519,8 @@ struct gpum_b200_mlp {
   // gradient partials: split K (weights), per-CTA columns / rows (biases, head, loss)
   Buf<float> pW1, pW2, colhead, colb1, rowpart;
   int S1 = 1, S2 = 1;
-  Buf<uint32_t> ctr;   // [step, ticket]
+  Buf<uint32_t> ctr;   // [step, unused]
+  Buf<float> lr;       // [1] the current learning rate
   Buf<float> losses;   // per-step sums of squared residuals of one train() call
   // normaliser
   Buf<float> xmean, xinv, xw;  // xw: d x d whitening, used when `whiten`
@@ -607,7 +604,7 @@ struct gpum_b200_mlp {
 
   // Weight gradients and b1's (after forward() with targets), then the
   // reduction of every gradient into G, with Adam when `apply`.
-  void backward_and_update(float lr, int apply, float* loss_hist, uint32_t loss_base,
+  void backward_and_update(int apply, float* loss_hist, uint32_t loss_base,
                            uint32_t loss_cap) {
     GemmArgs g3 = args(dZ2Th.p, A1Th.p, H, H, B);  // dW2 = dZ2^T A1
     g3.C = pW2.p;
@@ -644,8 +641,9 @@ struct gpum_b200_mlp {
     if (fork) MLP_CK(cudaStreamWaitEvent(st, ev_join, 0));
     GradParts gp{pW1.p, S1, pW2.p, S2, colhead.p, colb1.p, rowpart.p, B / kGemmBM};
     mlp_reduce_adam<<<blocks(L.n), 256, 0, st>>>(L, gp, P.p, Mm.p, V.p, G.p, W1h.p, W1Th.p,
-                                                  W2h.p, W2Th.p, lr, apply, ctr.p, loss_hist,
+                                                  W2h.p, W2Th.p, lr.p, apply, ctr.p, loss_hist,
                                                   loss_base, loss_cap);
+    if (apply) mlp_step_done<<<1, 32, 0, st>>>(ctr.p);
     MLP_CK(cudaGetLastError());
   }
 
@@ -882,6 +880,7 @@ int gpum_b200_mlp_create(uint32_t d, uint32_t hidden, uint32_t batch, uint32_t s
     m->colb1.alloc((size_t)nct * H);
     m->rowpart.alloc((size_t)2 * nct);
     m->ctr.alloc(2);
+    m->lr.alloc(1);
     m->xmean.alloc(d);
     m->xinv.alloc(d);
     m->xw.alloc((size_t)d * d);
@@ -966,61 +965,87 @@ int gpum_b200_mlp_set_whitening(gpum_b200_mlp* m, const double* xmean, const dou
   });
 }
 
-int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n_pairs,
-                        uint32_t steps, double lr, float* out_loss, char* err, size_t err_len) {
+int gpum_b200_mlp_train_stages(gpum_b200_mlp* m, const double* theta, const double* ll,
+                               size_t n_pairs, uint32_t n_stages, const uint32_t* steps,
+                               const double* lrs, float* out_loss, char* err, size_t err_len) {
   return mlp_guard(err, err_len, [&] {
-    need(m && theta && ll, "NULL argument");
+    need(m && theta && ll && (n_stages == 0 || (steps && lrs)), "NULL argument");
     need(n_pairs >= 1 && n_pairs <= (1u << 28), "n_pairs must be in 1..2^28");
-    if (steps == 0) return;
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n_stages; ++k) {
+      need(std::isfinite(lrs[k]) && lrs[k] >= 0.0, "learning rates must be finite and >= 0");
+      total += steps[k];
+    }
+    need(total <= (1u << 24), "more than 2^24 steps");
+    if (total == 0) return;
+    // The pairs are uploaded once for every stage.
     Buf<float> dth;
     Buf<double> dll;
     upload_pairs(m, theta, ll, n_pairs, dth, dll);
-    m->losses.alloc(steps);
+    m->losses.alloc(total);
     const uint32_t base = m->steps_done;
-    // One step as a CUDA graph (its kernels read the step from the device
-    // counter the reduction advances), replayed `steps` times.
+    // One step: its kernels read the step from the device counter the
+    // reduction advances and the learning rate from device memory, so one
+    // captured CUDA graph serves all steps of all stages.
     auto one_step = [&] {
       mlp_gather<<<m->B / kGatherRows, 32 * kGatherRows, 0, m->st>>>(
-          dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed,
-                                          m->ctr.p, m->xmean.p, m->xinv.p, m->xw_or_null(),
-                                          m->ymean, m->yinv, m->Xh.p, m->XTh.p, m->t.p);
+          dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed, m->ctr.p, m->xmean.p,
+          m->xinv.p, m->xw_or_null(), m->ymean, m->yinv, m->Xh.p, m->XTh.p, m->t.p);
       MLP_CK(cudaGetLastError());
       m->forward(m->B, m->B, m->t.p);
-      m->backward_and_update((float)lr, 1, m->losses.p, base, steps);
+      m->backward_and_update(1, m->losses.p, base, (uint32_t)total);
     };
-    one_step();  // first step eagerly: sets every kernel attribute outside capture
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    if (steps > 1) {
-      MLP_CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-      try {
-        one_step();
-      } catch (...) {
-        cudaGraph_t g2 = nullptr;
-        cudaStreamEndCapture(m->st, &g2);
-        if (g2) cudaGraphDestroy(g2);
-        throw;
+    bool first = true;
+    cudaError_t le = cudaSuccess;
+    for (uint32_t k = 0; k < n_stages && le == cudaSuccess; ++k) {
+      if (steps[k] == 0) continue;
+      const float lr_f = (float)lrs[k];
+      MLP_CK(cudaMemcpyAsync(m->lr.p, &lr_f, sizeof lr_f, cudaMemcpyHostToDevice, m->st));
+      MLP_CK(cudaStreamSynchronize(m->st));  // lr_f is a stack value
+      uint32_t left = steps[k];
+      if (first) {
+        one_step();  // eagerly: sets every kernel attribute outside capture
+        first = false;
+        --left;
       }
-      MLP_CK(cudaStreamEndCapture(m->st, &graph));
-      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-      if (ie != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        MLP_CK(ie);
+      if (left > 0 && !exec) {
+        MLP_CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+        try {
+          one_step();
+        } catch (...) {
+          cudaGraph_t g2 = nullptr;
+          cudaStreamEndCapture(m->st, &g2);
+          if (g2) cudaGraphDestroy(g2);
+          throw;
+        }
+        MLP_CK(cudaStreamEndCapture(m->st, &graph));
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        if (ie != cudaSuccess) {
+          cudaGraphDestroy(graph);
+          MLP_CK(ie);
+        }
       }
-      cudaError_t le = cudaSuccess;
-      for (uint32_t s = 1; s < steps && le == cudaSuccess; ++s) le = cudaGraphLaunch(exec, m->st);
-      cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
-      MLP_CK(le);
+      for (; left > 0 && le == cudaSuccess; --left) le = cudaGraphLaunch(exec, m->st);
     }
-    m->steps_done += steps;
-    std::vector<float> losses(steps);
-    MLP_CK(cudaMemcpyAsync(losses.data(), m->losses.p, steps * sizeof(float),
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    MLP_CK(le);
+    m->steps_done += (uint32_t)total;
+    std::vector<float> losses(total);
+    MLP_CK(cudaMemcpyAsync(losses.data(), m->losses.p, total * sizeof(float),
                            cudaMemcpyDeviceToHost, m->st));
     m->check_err();
     if (out_loss)
-      for (uint32_t s = 0; s < steps; ++s) out_loss[s] = losses[s] / (float)m->B;
+      for (uint64_t s = 0; s < total; ++s) out_loss[s] = losses[s] / (float)m->B;
   });
+}
+
+int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll, size_t n_pairs,
+                        uint32_t steps, double lr, float* out_loss, char* err, size_t err_len) {
+  return gpum_b200_mlp_train_stages(m, theta, ll, n_pairs, 1, &steps, &lr, out_loss, err,
+                                    err_len);
 }
 
 int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, double* out, char* err,
@@ -1088,7 +1113,7 @@ int gpum_b200_mlp_gradients(gpum_b200_mlp* m, const double* theta, const double*
     uint32_t step = 0;
     MLP_CK(cudaMemcpyAsync(&step, m->ctr.p, sizeof step, cudaMemcpyDeviceToHost, m->st));
     MLP_CK(cudaStreamSynchronize(m->st));
-    m->backward_and_update(0.0f, 0, loss1.p, step, 1);
+    m->backward_and_update(0, loss1.p, step, 1);
     MLP_CK(cudaMemcpyAsync(out_grads, m->G.p, m->L.n * sizeof(float), cudaMemcpyDeviceToHost,
                            m->st));
     float l = 0.0f;

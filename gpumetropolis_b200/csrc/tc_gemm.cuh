@@ -193,9 +193,9 @@ struct GemmArgs {
 template <int BN>
 constexpr size_t tc_gemm_smem() {
   // A slice | B slice | column-sum scratch [2][4 lane quarters][BN] | row
-  // partials [2 halves][128] | barrier, slot
+  // partials [2 halves][128] | bias, w3 [2][BN] | barrier, slot
   return (size_t)kGemmBM * kGemmBK * 2 + (size_t)BN * kGemmBK * 2 + (size_t)2 * 4 * BN * 4 +
-         2 * 128 * 4 + 16 + 16 + 1024;
+         2 * 128 * 4 + (size_t)2 * BN * 4 + 16 + 16 + 1024;
 }
 
 // Stores 16 bf16 values of one row (32 bytes).
@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const GemmArgs
   unsigned char* sb = gsm + kGemmBM * kGemmBK * 2;          // BN x 64 bf16
   float* red = reinterpret_cast<float*>(sb + BN * kGemmBK * 2);  // [2][4][BN]
   float* ypart = red + 2 * 4 * BN;                                // [2][128]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ypart + 2 * 128);
+  float* s_bias = ypart + 2 * 128;                                 // [BN]
+  float* s_w3 = s_bias + BN;                                       // [BN]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(s_w3 + BN);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int M = g.M, N = g.N, K = g.K;
@@ -236,6 +238,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const GemmArgs
   if (tid == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
+  }
+  // the epilogue's per-column operands, read by every row: staged once
+  for (int i = tid; i < BN; i += kGemmThreads) {
+    s_bias[i] = g.bias ? g.bias[n0 + i] : 0.0f;
+    s_w3[i] = g.w3 ? g.w3[n0 + i] : 0.0f;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -332,7 +339,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const GemmArgs
         tmem_ld16(trow + (uint32_t)c, v);
         if (g.bias) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] += g.bias[n0 + c + j];
+          for (int j = 0; j < 16; ++j) v[j] += s_bias[c + j];
         }
         float4* c4 = reinterpret_cast<float4*>(C + (size_t)row * N + n0 + c);
 #pragma unroll
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const GemmArgs
         float v[16];
         tmem_ld16(trow + (uint32_t)c, v);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) yp = fmaf(silu(v[j] + g.bias[c + j]), g.w3[c + j], yp);
+        for (int j = 0; j < 16; ++j) yp = fmaf(silu(v[j] + s_bias[c + j]), s_w3[c + j], yp);
       }
       ypart[half * 128 + quarter * 32 + lane] = yp;
       __syncthreads();
@@ -374,10 +381,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1) tc_gemm_kernel(const GemmArgs
         tmem_ld16(trow + (uint32_t)c, v);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const float z = v[j] + g.bias[c + j];
+          const float z = v[j] + s_bias[c + j];
           const float s = sigmoidf_(z);
           wa[j] = dy * (z * s);
-          dz[j] = dy * g.w3[c + j] * (s * (1.0f + z * (1.0f - s)));
+          dz[j] = dy * s_w3[c + j] * (s * (1.0f + z * (1.0f - s)));
         }
         store_bf16x16(g.dzh + (size_t)row * N + c, dz);
         if (g.actT) {

@@ -309,6 +309,13 @@ GPUM_API int gpum_b200_mlp_set_whitening(gpum_b200_mlp* m, const double* xmean, 
 GPUM_API int gpum_b200_mlp_train(gpum_b200_mlp* m, const double* theta, const double* ll,
                                  size_t n_pairs, uint32_t steps, double lr, float* out_loss,
                                  char* err, size_t err_len);
+/* A learning-rate schedule in one call: steps[k] Adam steps at lrs[k] for
+ * k < n_stages, the pairs uploaded once; out_loss (may be NULL) receives
+ * sum(steps) losses. */
+GPUM_API int gpum_b200_mlp_train_stages(gpum_b200_mlp* m, const double* theta, const double* ll,
+                                        size_t n_pairs, uint32_t n_stages,
+                                        const uint32_t* steps, const double* lrs,
+                                        float* out_loss, char* err, size_t err_len);
 /* Predicted log-likelihood at n points (host arrays). */
 GPUM_API int gpum_b200_mlp_predict(gpum_b200_mlp* m, const double* theta, size_t n, double* out,
                                    char* err, size_t err_len);

@@ -102,13 +102,15 @@ def test_noalloc_deep_programs_and_shapes_in_a_row(gpu):
     stream = torch.cuda.current_stream().cuda_stream
     rng = np.random.default_rng(3)
     n_obs = 3001
-    y = rng.normal(0.0, 1.0, n_obs)
+    # positive data and parameters: every term positive, so the sums do not
+    # cancel and the relative bound applies as stated
+    y = rng.uniform(0.5, 1.5, n_obs)
     cols, ld = _device_layout(torch, y.reshape(-1, 1), n_obs, 1)
     for depth, n_points in ((12, 50), (24, 7), (3, 129), (24, 400)):
         f = "~ " + "(y * a + " * (depth - 1) + "b" + ")" * (depth - 1)
         m = gpum_model(f, ["a", "b"], "y")
         assert gpu.validate_program(m.loglik.code, m.loglik.consts.size, 2, 1) >= depth
-        pts = rng.normal(0.0, 0.3, (n_points, 2))
+        pts = rng.uniform(0.1, 0.5, (n_points, 2))
         _check(gpu, torch, m.loglik.code, m.loglik.consts, 2, y.reshape(-1, 1), 1, n_obs,
                cols, ld, pts, stream)
     w = W.make("logistic", n_obs=2048)
