@@ -128,6 +128,34 @@ void launch_interp(int v, dim3 grid, size_t smem, cudaStream_t st, const EvalPro
   GPUM_CK(cudaGetLastError());
 }
 
+// Interpreter gradient kernels by width (1 + parameters, rounded up).
+int grad_width(uint32_t np) {
+  const int w = 1 + (int)np;
+  return w <= 9 ? 9 : (w <= 17 ? 17 : (w <= 33 ? 33 : (w <= 65 ? 65 : 129)));
+}
+
+const void* interp_grad_kernel(int W) {
+  switch (W) {
+    case 9: return (const void*)iter_kernel_grad<9>;
+    case 17: return (const void*)iter_kernel_grad<17>;
+    case 33: return (const void*)iter_kernel_grad<33>;
+    case 65: return (const void*)iter_kernel_grad<65>;
+    default: return (const void*)iter_kernel_grad<129>;
+  }
+}
+
+void launch_interp_grad(int W, dim3 grid, size_t smem, cudaStream_t st, const GradProg& prog,
+                        const TmapDesc& tmap, const EvalArgs& E, const ChainArgs& A, int phase) {
+  switch (W) {
+    case 9: iter_kernel_grad<9><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    case 17: iter_kernel_grad<17><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    case 33: iter_kernel_grad<33><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    case 65: iter_kernel_grad<65><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+    default: iter_kernel_grad<129><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
+  }
+  GPUM_CK(cudaGetLastError());
+}
+
 int num_sms() {
   static int n = 0;
   if (!n) {
@@ -146,6 +174,7 @@ struct KernelChoice {
   int G = 8;                 // chains per thread (per warp for a chain-lane body)
   int W = 1;                 // values per chain (1, or 1 + np with the gradient)
   bool lanes = false;        // chain-lane body: G = 32 chains per warp group
+  bool grad_interp = false;  // the interpreter engine's gradient (tape) kernel
 };
 
 struct Geometry {
@@ -177,6 +206,9 @@ struct gpum_b200_session {
   cudaStream_t stream = nullptr;
   UProg ll;
   std::unique_ptr<EvalProg> prog;
+  // the interpreter engine's gradient program (or why there is none)
+  std::unique_ptr<GradProg> gprog;
+  std::string gprog_err;
   GenModel gm;
   CompiledModel cm;
   bool cm_ready = false;
@@ -210,7 +242,8 @@ struct gpum_b200_session {
   DBuf<double> state, prop, cur, last_eval, sd, temp, L, snap, zbuf, partials, pointwise,
       points, out64, gx, gy, mx, my, vbuf;
   DBuf<float> params, draws, draws_out;
-  DBuf<uint32_t> ctr, accepts, iter, tickets;
+  DBuf<uint32_t> ctr, accepts, iter, tickets, ptape_i;
+  DBuf<double> ptape;
   EvalArgs E{};
   ChainArgs A{};
   cudaGraph_t graph = nullptr;
@@ -287,6 +320,21 @@ struct gpum_b200_session {
 
   KernelChoice choose(bool need_grad) {
     KernelChoice k;
+    // Gradients: the compiled engine's adjoint unless the interpreter engine
+    // was chosen or NVRTC cannot build the model; then the interpreted tape.
+    if (need_grad && (engine == GPUM_ENGINE_INTERP ||
+                      (engine == GPUM_ENGINE_AUTO && !compiled_available()))) {
+      if (!gprog)
+        throw Failure{GPUM_ERR_UNSUPPORTED,
+                      "the interpreter engine's gradient is unavailable (" + gprog_err +
+                          ")" + (cm_error.empty() ? "" : "; compiled engine: " + cm_error)};
+      k.compiled = false;
+      k.grad_interp = true;
+      k.W = grad_width(np);
+      k.fn = interp_grad_kernel(k.W);
+      k.G = 1;
+      return k;
+    }
     const bool want_compiled =
         need_grad || engine == GPUM_ENGINE_COMPILED ||
         (engine == GPUM_ENGINE_AUTO && compiled_available());
@@ -410,6 +458,8 @@ struct gpum_b200_session {
     if (kc.compiled) {
       void* args[] = {(void*)(ext(kc) ? &tmap_c : &tmap), (void*)&e, (void*)&A, (void*)&phase};
       GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, g.smem, stream));
+    } else if (kc.grad_interp) {
+      launch_interp_grad(kc.W, grid, g.smem, stream, *gprog, tmap, e, A, phase);
     } else {
       launch_interp(variant, grid, g.smem, stream, *prog, tmap, e, A, phase);
     }
@@ -502,7 +552,26 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
   std::memset(s->prog.get(), 0, sizeof(EvalProg));
   s->prog->n_uops = (uint32_t)s->ll.uops.size();
   std::copy(s->ll.uops.begin(), s->ll.uops.end(), s->prog->uop);
+  std::copy(s->ll.terms.begin(), s->ll.terms.end(), s->prog->term);
   std::copy(s->ll.consts.begin(), s->ll.consts.end(), s->prog->cst);
+  {
+    UGradProg gp;
+    std::string ge;
+    if (compile_grad_program(code, n_code, n_params, &gp, &ge) == 0) {
+      s->gprog.reset(new GradProg());
+      std::memset(s->gprog.get(), 0, sizeof(GradProg));
+      s->gprog->n_nodes = (uint32_t)gp.nodes.size();
+      s->gprog->root = gp.root;
+      s->gprog->has_root = gp.has_root ? 1u : 0u;
+      s->gprog->np = n_params;
+      std::copy(gp.nodes.begin(), gp.nodes.end(), s->gprog->node);
+      std::copy(s->ll.consts.begin(),
+                s->ll.consts.begin() + std::min<size_t>(n_consts, (size_t)kMaxConsts),
+                s->gprog->cst);
+    } else {
+      s->gprog_err = ge;
+    }
+  }
   s->prior_code.assign(prior_code, prior_code + n_prior);
   s->prior_consts.assign(prior_consts, prior_consts + n_prior_consts);
 
@@ -596,6 +665,11 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
     s->mx.ensure(C * np);
     s->my.ensure(C * np);
     s->vbuf.ensure(C * np);
+    if (!s->kc.compiled) {  // the interpreted prior's gradient tape
+      const size_t npr = std::max<size_t>(s->prior_code.size() / 2, 1);
+      s->ptape.ensure((size_t)C * 2 * npr);
+      s->ptape_i.ensure((size_t)C * 2 * npr);
+    }
   }
   cudaStream_t st = s->stream;
   GPUM_CK(cudaMemcpyAsync(s->state.p, init, sizeof(double) * C * np, cudaMemcpyHostToDevice, st));
@@ -650,6 +724,10 @@ void prepare(gpum_b200_session* s, const double* init, const double* sd, const d
     A.mx = s->mx.p;
     A.my = s->my.p;
     A.vbuf = s->vbuf.p;
+    if (!s->kc.compiled) {
+      A.ptape = s->ptape.p;
+      A.ptape_i = s->ptape_i.p;
+    }
   }
   if (s->n_beta > 0) {
     require(s->n_beta == C, "likelihood powers were set for " + std::to_string(s->n_beta) +

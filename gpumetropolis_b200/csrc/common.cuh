@@ -65,6 +65,10 @@ struct ChainArgs {
   // Power posteriors (thermodynamic integration): chain c targets
   // beta[c] * loglik + prior; nullptr means beta = 1.
   const double* beta;
+  // The interpreted prior's gradient (MALA on the interpreter engine): per
+  // chain a tape of n_prior values, adjoints and operand indices.
+  double* ptape;        // [C][2][n_prior]
+  uint32_t* ptape_i;    // [C][2][n_prior]
 };
 
 struct EvalArgs {
@@ -376,8 +380,8 @@ __device__ inline void propose_desync(const ChainArgs& A, int c, Stream& rs, flo
 
 // Accept/reject + record + propose for chain c.  `ll` is the data-term sum;
 // with MALA the data-term gradient has been summed into A.gy (STEP) or A.gx
-// (INIT).  Prior::value(A, p) and Prior::value_grad(A, p, g) give the f64
-// prior (value_grad accumulates into g).
+// (INIT).  Prior::value(A, c, p) and Prior::value_grad(A, c, p, g) give the
+// f64 prior of chain c's point p (value_grad accumulates into g).
 template <class Prior>
 __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double ll, int phase,
                                       float* params, int C_pad) {
@@ -388,8 +392,8 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
   double* x = A.state + (size_t)c * np;
   const double bl = A.beta ? A.beta[c] * ll : ll;  // likelihood power
   if (phase == PH_INIT) {
-    const double lp = bl + (mala ? Prior::value_grad(A, x, A.gx + (size_t)c * np)
-                                 : Prior::value(A, x));
+    const double lp = bl + (mala ? Prior::value_grad(A, c, x, A.gx + (size_t)c * np)
+                                 : Prior::value(A, c, x));
     A.cur[c] = lp;
     A.last_eval[c] = lp;
     if (A.n_iter > 0 && A.mode != MODE_DESYNC) {  // path B proposes in its own kernel
@@ -398,8 +402,8 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
     }
   } else {
     const double* y = A.prop + (size_t)c * np;
-    const double plp = bl + (mala ? Prior::value_grad(A, y, A.gy + (size_t)c * np)
-                                  : Prior::value(A, y));
+    const double plp = bl + (mala ? Prior::value_grad(A, c, y, A.gy + (size_t)c * np)
+                                  : Prior::value(A, c, y));
     A.last_eval[c] = plp;
     if (A.rec_ll) {
       const uint64_t slot = A.rec_base + (uint64_t)t * A.n_chains + c;

@@ -351,8 +351,8 @@ constexpr int kGradG = GM_GG;
 
 // The generated f64 prior (value and reverse-mode gradient).
 struct JitPrior {
-  __device__ static double value(const ChainArgs&, const double* p) { return gm_prior(p); }
-  __device__ static double value_grad(const ChainArgs&, const double* p, double* g) {
+  __device__ static double value(const ChainArgs&, int, const double* p) { return gm_prior(p); }
+  __device__ static double value_grad(const ChainArgs&, int, const double* p, double* g) {
     return gm_prior_grad(p, g);
   }
 };

@@ -23,6 +23,7 @@ struct __align__(16) EvalProg {
   uint32_t n_uops;
   uint32_t pad_[3];
   uint32_t uop[kMaxUops];
+  uint32_t term[kMaxTerms];  // K_DOT terms: param | column << 11
   float cst[kMaxConsts];
 };
 
@@ -246,6 +247,17 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
       float pv[G];                                                                     \
       load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_DOT:                                                              \
+    if constexpr (S < D) {                                                             \
+      for (uint32_t k = 0; k < a1; ++k) {                                              \
+        const uint32_t tw = pg.term[a0 + k];                                           \
+        const float v = GPUM_XD(tw >> 11);                                             \
+        float pv[G];                                                                   \
+        load_params<G>(pc0 + (size_t)(tw & 0x7FFu) * CG, pv);                          \
+        _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
+      }                                                                                \
     }                                                                                  \
     break;
 

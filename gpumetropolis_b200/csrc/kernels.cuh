@@ -37,19 +37,26 @@ struct InterpBody {
   __device__ __forceinline__ double total(int g, int) const { return acc[g].total(); }
 };
 
-// f64 prior interpreted from the source bytecode; the interpreter engine has
-// no gradient (MALA runs on the compiled engine).
+// f64 prior interpreted from the source bytecode; its gradient (MALA on the
+// interpreter engine) by the reverse-mode tape over chain c's scratch.
 struct InterpPrior {
-  __device__ static double value(const ChainArgs& A, const double* p) {
+  __device__ static double value(const ChainArgs& A, int, const double* p) {
     return prior_interp(A.prior_code, A.n_prior, A.prior_consts, p);
   }
-  __device__ static double value_grad(const ChainArgs& A, const double* p, double*) {
-    return prior_interp(A.prior_code, A.n_prior, A.prior_consts, p);
+  __device__ static double value_grad(const ChainArgs& A, int c, const double* p, double* g) {
+    const size_t n = (size_t)(A.n_prior > 0 ? A.n_prior : 1);
+    double* tv = A.ptape + (size_t)c * 2 * n;
+    uint32_t* ti = A.ptape_i + (size_t)c * 2 * n;
+    return prior_value_grad_tape(A.prior_code, A.n_prior, A.prior_consts, p, g, tv, tv + n, ti,
+                                 ti + n);
   }
 };
 
+// The widest variant (eight chains per thread, an eight-deep stack: 64
+// stack registers) keeps its stack in registers at one CTA per SM; the others
+// fit two.
 template <int G, int D>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, (G == 8 ? 1 : 2))
 iter_kernel(const __grid_constant__ EvalProg prog, const __grid_constant__ TmapDesc tmap,
             EvalArgs E, ChainArgs A, int phase) {
   InterpBody<G, D> body(prog);
@@ -76,6 +83,164 @@ static __global__ void selftest_wait_kernel(uint32_t* err, uint32_t polls, uint6
     if (gm_globaltimer() - t0 > max_ns) break;
   }
   if (__syncthreads_or(done ? 0 : 1) && threadIdx.x == 0) atomicOr(err, DEV_ERR_WAIT_SELFTEST);
+}
+
+// ------------------------------------------ gradient in the interpreter engine
+// The node program of compile_grad_program (program.hpp) in the constant bank.
+struct __align__(16) GradProg {
+  uint32_t n_nodes, root, has_root, np;
+  uint32_t node[kMaxGradNodes];
+  float cst[kMaxConsts];
+};
+
+// Value and parameter gradient per observation by a reverse sweep over a tape
+// of the observation's node values (cpu_native.rs:148-279 in FP32, with the
+// compiled engine's local derivatives: POW's exponent term only where the
+// base is positive, LGAMMA's the digamma, an exponent of constant 2 as a
+// square).  One chain per thread, lanes over observations (G = 1); the tape
+// and the adjoints live in the thread's local memory.  W = 1 + the largest
+// parameter count the instantiation serves; entries past np stay 0.
+template <int W>
+struct InterpGradBody {
+  static constexpr bool kChainLanes = false;
+  static constexpr int kObsPerEval = 1;
+  static constexpr int kNp = W - 1;
+  const GradProg& pg;
+  const float* pc0;
+  int CG;
+  float vals[kMaxGradNodes];
+  float adj[kMaxGradNodes];
+  float gp[kNp];
+  double gpd[kNp];
+  double s;
+  float part, lastv;
+  int cnt;
+  __device__ explicit InterpGradBody(const GradProg& p) : pg(p), pc0(nullptr), CG(0) {}
+
+  __device__ __forceinline__ void begin(const float* p0, int cg) {
+    pc0 = p0;
+    CG = cg;
+    for (int j = 0; j < kNp; ++j) {
+      gp[j] = 0.0f;
+      gpd[j] = 0.0;
+    }
+    s = 0.0;
+    part = 0.0f;
+    lastv = 0.0f;
+    cnt = 0;
+  }
+  __device__ __forceinline__ float fetch(uint32_t r, const float* xo, int T) const {
+    const uint32_t t = r & 3u, i = r >> 2;
+    return t == GREF_NODE ? vals[i]
+         : t == GREF_CONST ? pg.cst[i]
+         : t == GREF_PARAM ? pc0[(size_t)i * CG]
+                           : xo[(size_t)i * T];
+  }
+  __device__ __forceinline__ void sink(uint32_t r, float x) {
+    const uint32_t t = r & 3u, i = r >> 2;
+    if (t == GREF_NODE) adj[i] += x;
+    else if (t == GREF_PARAM) gp[i] += x;
+  }
+  __device__ __forceinline__ void flush() {
+    s += (double)part;
+    part = 0.0f;
+    for (uint32_t j = 0; j < pg.np; ++j) {
+      gpd[j] += (double)gp[j];
+      gp[j] = 0.0f;
+    }
+    cnt = 0;
+  }
+  __device__ void eval(const float* xo, int T, bool valid) {
+    if (!valid) {  // padding rows add neither value nor gradient
+      lastv = 0.0f;
+      return;
+    }
+    const uint32_t n = pg.n_nodes;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t w = pg.node[i], op = w & 15u;
+      const uint32_t ra = (w >> 4) & 0x3FFFu, rb = w >> 18;
+      const float a = fetch(ra, xo, T);
+      float v;
+      if (op == 7) v = -a;
+      else if (op == 8) v = expf(a);
+      else if (op == 9) v = logf(a);
+      else if (op == 10) v = sqrtf(a);
+      else if (op == 12) v = lgammaf(a);
+      else {
+        const float b = fetch(rb, xo, T);
+        if (op == 3) v = a + b;
+        else if (op == 4) v = a - b;
+        else if (op == 5) v = a * b;
+        else if (op == 6) v = a / b;
+        else v = ((rb & 3u) == GREF_CONST && b == 2.0f) ? a * a : powf(a, b);
+      }
+      vals[i] = v;
+    }
+    const float val = pg.has_root ? fetch(pg.root, xo, T) : 0.0f;
+    lastv = val;
+    part += val;
+    if (pg.has_root) {
+      if ((pg.root & 3u) == GREF_NODE) {
+        for (uint32_t i = 0; i < n; ++i) adj[i] = 0.0f;
+        adj[pg.root >> 2] = 1.0f;
+        for (int i = (int)n - 1; i >= 0; --i) {
+          const float g = adj[i];
+          if (g == 0.0f) continue;
+          const uint32_t w = pg.node[i], op = w & 15u;
+          const uint32_t ra = (w >> 4) & 0x3FFFu, rb = w >> 18;
+          const float a = fetch(ra, xo, T), v = vals[i];
+          switch (op) {
+            case 3: sink(ra, g); sink(rb, g); break;
+            case 4: sink(ra, g); sink(rb, -g); break;
+            case 5: {
+              const float b = fetch(rb, xo, T);
+              sink(ra, g * b);
+              sink(rb, g * a);
+              break;
+            }
+            case 6: {
+              const float b = fetch(rb, xo, T);
+              sink(ra, g / b);
+              sink(rb, -g * v / b);
+              break;
+            }
+            case 7: sink(ra, -g); break;
+            case 8: sink(ra, g * v); break;
+            case 9: sink(ra, g / a); break;
+            case 10: sink(ra, g * 0.5f / v); break;
+            case 12: sink(ra, g * gm_digammaf(a)); break;
+            default: {
+              const float b = fetch(rb, xo, T);
+              if ((rb & 3u) == GREF_CONST && b == 2.0f) {
+                sink(ra, g * 2.0f * a);
+              } else {
+                sink(ra, g * b * powf(a, b - 1.0f));
+                sink(rb, a > 0.0f ? g * v * logf(a) : 0.0f);
+              }
+              break;
+            }
+          }
+        }
+      } else if ((pg.root & 3u) == GREF_PARAM) {
+        gp[pg.root >> 2] += 1.0f;
+      }
+    }
+    if (++cnt == 8) flush();
+  }
+  __device__ __forceinline__ float last(int) const { return lastv; }
+  __device__ __forceinline__ void end() { flush(); }
+  __device__ __forceinline__ double total(int, int w) const {
+    if (w == 0) return s + (double)part;
+    return w - 1 < (int)pg.np ? gpd[w - 1] : 0.0;
+  }
+};
+
+template <int W>
+__global__ void __launch_bounds__(kThreads, 1)
+iter_kernel_grad(const __grid_constant__ GradProg prog, const __grid_constant__ TmapDesc tmap,
+                 EvalArgs E, ChainArgs A, int phase) {
+  InterpGradBody<W> body(prog);
+  run_iteration<1, W, InterpGradBody<W>, InterpPrior>(&tmap, E, A, phase, body);
 }
 
 // ------------------------------------------------------------- helpers
@@ -366,7 +531,7 @@ static __global__ void da_setup_kernel(ChainArgs A, DaArgs D) {
       A.ctr[c] = rs.ctr;
     }
   } else if (!D.prior_ready) {
-    D.prior_x[c] = InterpPrior::value(A, x);
+    D.prior_x[c] = InterpPrior::value(A, c, x);
   }
   D.stage1[c] = 0;
 }
@@ -400,7 +565,7 @@ static __global__ void da_stage1_kernel(ChainArgs A, DaArgs D) {
     lqd = log_q(np, sd, L, A.state + (size_t)c * np, my, tmp) -
           log_q(np, sd, L, y, A.mx + (size_t)c * np, tmp);
   } else {
-    py = D.prior_ready ? D.prior_y[c] : InterpPrior::value(A, y);
+    py = D.prior_ready ? D.prior_y[c] : InterpPrior::value(A, c, y);
   }
   D.prior_y[c] = py;
   Stream rs = make_stream(A, c);

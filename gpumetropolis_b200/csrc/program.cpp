@@ -184,6 +184,33 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
     }
     ++pc;
   }
+  // Runs of multiply-adds into one slot become one K_DOT over a term table
+  // (the same fmaf sequence in the same order, so the value is unchanged).
+  {
+    std::vector<uint32_t> merged;
+    merged.reserve(out->uops.size());
+    size_t i = 0;
+    while (i < out->uops.size()) {
+      const uint32_t w = out->uops[i];
+      const uint32_t id = w & 1023u, kind = id % NKIND, slot = id / NKIND;
+      size_t j = i + 1;
+      if (kind == K_FMA_PD)
+        while (j < out->uops.size() && (out->uops[j] & 1023u) == id) ++j;
+      if (kind == K_FMA_PD && j - i >= 2 &&
+          out->terms.size() + (j - i) <= (size_t)kMaxTerms) {
+        const uint32_t t0 = (uint32_t)out->terms.size();
+        for (size_t k = i; k < j; ++k)
+          out->terms.push_back(((out->uops[k] >> 10) & 0x7FFu) |
+                               (((out->uops[k] >> 21) & 0x7FFu) << 11));
+        merged.push_back(uop_word(K_DOT, slot, t0, (uint32_t)(j - i)));
+        i = j;
+      } else {
+        merged.push_back(w);
+        ++i;
+      }
+    }
+    out->uops.swap(merged);
+  }
   if ((int)out->uops.size() > kMaxUops) {
     *err = fmt("program compiles to %ld micro-ops, limit %ld", (long)out->uops.size(),
                kMaxUops);
@@ -197,4 +224,54 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
   return 0;
 }
 
+int compile_grad_program(const uint32_t* code, size_t n_code, uint32_t n_params,
+                         UGradProg* out, std::string* err) {
+  *out = UGradProg();
+  if (n_params > (uint32_t)kMaxGradParams) {
+    *err = fmt("the interpreter's gradient takes at most %ld parameters (%ld here); the "
+               "compiled engine has no such limit",
+               kMaxGradParams, (long)n_params);
+    return 1;
+  }
+  const size_t n = n_code / 2;
+  std::vector<uint32_t> st;  // refs on the stack
+  auto ref = [](uint32_t type, uint32_t idx) { return type | (idx << 2); };
+  for (size_t pc = 0; pc < n; ++pc) {
+    const uint32_t op = norm_op(code[2 * pc]), arg = code[2 * pc + 1];
+    if (is_push(op)) {
+      if (arg >= 4096) {
+        *err = "operand index beyond the interpreter's gradient (4096)";
+        return 1;
+      }
+      st.push_back(ref(op == OP_CONST ? GREF_CONST : op == OP_PARAM ? GREF_PARAM : GREF_DATA,
+                       arg));
+      continue;
+    }
+    if ((int)out->nodes.size() >= kMaxGradNodes) {
+      *err = fmt("the interpreter's gradient takes at most %ld operations (more here); the "
+                 "compiled engine has no such limit",
+                 kMaxGradNodes);
+      return 1;
+    }
+    uint32_t a = 0, b = 0;
+    if (is_unary(op)) {
+      a = st.back();
+      st.pop_back();
+    } else {
+      b = st.back();
+      st.pop_back();
+      a = st.back();
+      st.pop_back();
+    }
+    out->nodes.push_back(op | (a << 4) | (b << 18));
+    st.push_back(ref(GREF_NODE, (uint32_t)out->nodes.size() - 1));
+  }
+  if (!st.empty()) {
+    out->root = st.front();
+    out->has_root = true;
+  }
+  return 0;
+}
+
 }  // namespace gpum
+

@@ -17,7 +17,9 @@
 //   bits 10..20  a0 (const / param / column index)
 //   bits 21..31  a1 (second index for two-operand fused forms)
 // plus an f32 constant pool.  Peephole fusion folds a push into the binary op
-// that consumes it, and `p*x + acc` patterns into one multiply-add.
+// that consumes it, `p*x + acc` patterns into one multiply-add, and a run of
+// such multiply-adds into the same slot (a linear predictor) into one K_DOT
+// micro-op over a term table, so the dispatch is paid once per run.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -34,6 +36,8 @@ enum Kind : uint32_t {
   K_NEG, K_EXP, K_LOG, K_SQRT, K_LGAMMA,        // s[t] = f(s[t])
   K_SQR,                                        // s[t] = s[t]*s[t]  (x^2)
   K_FMA_PD,                                     // s[t] += param[a0]*data[a1]
+  K_DOT,                                        // s[t] += sum over terms[a0 .. a0+a1)
+                                                //   of param[p_k]*data[x_k], in order
   NKIND
 };
 
@@ -42,9 +46,11 @@ constexpr int kMaxUops = 1024;     // micro-ops per program (constant bank)
 constexpr int kMaxConsts = 512;    // f32 constants per program
 constexpr int kMaxIndex = 2047;    // 11-bit operand fields
 constexpr int kMaxSlots = 32;      // deepest interpreter variant
+constexpr int kMaxTerms = 1024;    // (param, column) terms of K_DOT micro-ops
 
 struct UProg {
   std::vector<uint32_t> uops;
+  std::vector<uint32_t> terms;  // K_DOT terms: param | column << 11
   std::vector<float> consts;
   int depth = 0;          // peak stack depth of the source program
   int n_src = 0;          // source instructions
@@ -55,6 +61,30 @@ struct UProg {
 inline uint32_t uop_word(uint32_t kind, uint32_t slot, uint32_t a0, uint32_t a1) {
   return (slot * NKIND + kind) | (a0 << 10) | (a1 << 21);
 }
+
+// The interpreter engine's gradient program: the source bytecode as a list
+// of its non-push instructions ("nodes"), each naming its operands directly
+// -- another node, a constant, a parameter or a data column -- so a thread
+// can keep one observation's forward values in a tape of nodes and sweep it
+// backwards (the reference's tape AD, cpu_native.rs:148-279).
+//   node word: op (4 bits: 3..12, unknown opcodes as POW 11) | refA << 4 |
+//              refB << 18;  ref = type (2 bits) | index << 2, type 0 node,
+//              1 constant, 2 parameter, 3 data column (index < 4096)
+//   root: the ref of the program's result (slot 0)
+enum GradRef : uint32_t { GREF_NODE = 0, GREF_CONST = 1, GREF_PARAM = 2, GREF_DATA = 3 };
+constexpr int kMaxGradNodes = 512;   // tape entries per observation
+constexpr int kMaxGradParams = 128;  // parameters of the interpreted gradient
+
+struct UGradProg {
+  std::vector<uint32_t> nodes;
+  uint32_t root = 0;   // a ref; meaningful when has_root
+  bool has_root = false;
+};
+
+// Builds the gradient program; 1 with *err when the program is beyond the
+// interpreted gradient's limits (the compiled engine has none of them).
+int compile_grad_program(const uint32_t* code, size_t n_code, uint32_t n_params,
+                         UGradProg* out, std::string* err);
 
 // Validates and compiles.  Returns 0 or an error message in *err.
 int compile_program(const uint32_t* code, size_t n_code, const double* consts,

@@ -98,7 +98,10 @@ GPUM_API int gpum_b200_loglik_batch(const uint32_t* code, size_t n_code, const d
 
 /* Gradient of the summed log-likelihood (data term) at each point,
  * point-major out[p*n_params + j] f64, by the compiled engine's reverse-mode
- * adjoint (rust_grad_batch, lib.rs:158-179; cpu_native.rs:306-329). */
+ * adjoint, or, on the interpreter engine (chosen, or when NVRTC cannot build
+ * the model), by a reverse sweep over a per-observation tape of the
+ * interpreted program (at most 128 parameters and 512 operations)
+ * (rust_grad_batch, lib.rs:158-179; cpu_native.rs:306-329). */
 GPUM_API int gpum_b200_grad_batch(const uint32_t* code, size_t n_code, const double* consts,
                          size_t n_consts, uint32_t n_params, const double* data,
                          uint32_t n_cols, uint64_t n_obs, const double* points,
@@ -191,7 +194,9 @@ GPUM_API int gpum_b200_session_run_de_sync(gpum_b200_session* s, const double* i
                                            char* err, size_t err_len);
 
 /* Select the evaluation engine (GPUM_ENGINE_*); the default is AUTO.
- * Gradients (MALA, grad_batch) always use the compiled engine. */
+ * Gradients (MALA, grad_batch) use the engine too: the compiled engine's
+ * generated adjoint, or the interpreter's tape (up to 128 parameters and 512
+ * operations; AUTO falls back to it when NVRTC cannot build the model). */
 GPUM_API int gpum_b200_session_set_engine(gpum_b200_session* s, int engine, char* err,
                                           size_t err_len);
 /* The engine plain evaluations use (GPUM_ENGINE_INTERP or _COMPILED). */

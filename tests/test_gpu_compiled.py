@@ -244,3 +244,57 @@ def test_wide_model_with_materialized_columns(gpu):
     np.testing.assert_allclose(got, ref, rtol=1e-6)
     err = np.linalg.norm(g - ref_g, axis=1) / np.linalg.norm(ref_g, axis=1)
     assert err.max() < 2e-5, err.max()
+
+
+@pytest.mark.parametrize("name,n_obs", [("logistic", 3001), ("poisson", 2049),
+                                         ("mixture", 4001), ("student_t", 1003)])
+def test_interpreter_grad_batch_matches_oracle(gpu, name, n_obs):
+    # the interpreter engine's gradient (a reverse sweep over each
+    # observation's tape of the interpreted program) without NVRTC's code:
+    # against the oracle, at the compiled engine's tolerance
+    w = W.make(name, n_obs=n_obs)
+    m = w.model
+    rng = np.random.default_rng(1)
+    base = np.zeros(m.n_params)
+    if name in ("logistic", "poisson"):
+        base[:] = w.truth["beta"]
+    elif name == "student_t":
+        base[:-1] = w.truth["beta"]
+        base[-1] = math.log(1.5)
+    else:
+        base[:] = [math.log(0.3 / 0.7), -2.0, 3.0, 0.0, math.log(1.5)]
+    pts = base + rng.normal(0, 0.1, (7, m.n_params))
+    ref = O.grad_batch(m.loglik.code, m.loglik.consts, m.n_params, w.data, m.n_cols, w.n_obs,
+                       pts).reshape(7, -1)
+    with gpu.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts, m.n_params,
+                     w.data, m.n_cols, w.n_obs, engine=0) as s:
+        got = s.grad_batch(pts).reshape(7, -1)
+    err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err.max() < 2e-5, err
+
+
+@pytest.mark.parametrize("with_L", [False, True])
+def test_mala_on_the_interpreter_engine_follows_the_oracle(gpu, with_L):
+    # MALA with the interpreter engine's gradient and the interpreted prior's
+    # tape gradient: the oracle's trajectories, as on the compiled engine
+    w = W.make("poisson", n_obs=1000, p=6)
+    m = w.model
+    C, n_iter, seed = 16, 60, 4
+    rng = np.random.default_rng(5)
+    init = w.truth["beta"] + rng.normal(0, 0.03, (C, m.n_params))
+    sd = np.full((C, m.n_params), 0.02)
+    L = None
+    if with_L:
+        A = rng.normal(0, 1, (m.n_params, m.n_params))
+        Lc = np.linalg.cholesky(A @ A.T / m.n_params + np.eye(m.n_params)) * 0.02
+        L = np.broadcast_to(Lc, (C, m.n_params, m.n_params)).copy()
+    temps = np.ones(C)
+    with gpu.Session(*_args(w), engine=0) as s:
+        d_g, a_g, l_g = s.run(init, sd, temps, n_iter, seed, 3, proposal_l=L)
+    d_o, a_o, l_o = O.run(*_args(w), init, sd, temps, n_iter, seed, 3, proposal_l=L)
+    same = a_g == a_o
+    assert same.mean() >= 0.75, (a_g, a_o)
+    assert 0.3 < a_g.mean() < 0.99
+    dg = d_g.reshape((n_iter, C, m.n_params), order="F")
+    do = d_o.reshape((n_iter, C, m.n_params), order="F")
+    np.testing.assert_allclose(dg[:, same], do[:, same], rtol=1e-4, atol=1e-5)
