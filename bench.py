@@ -103,6 +103,10 @@ def _args():
                    help="instead of the headline line: exact vs delayed-acceptance ESS/s for "
                         "DE and the Langevin move on the Student-t configuration at full size "
                         "with the 65-512-512-1 surrogate (minutes), one JSON line")
+    p.add_argument("--profile-da", action="store_true",
+                   help="profiler target: a short warmup, surrogate training inside the "
+                        "NVTX range 'training' and 48 two-stage iterations inside "
+                        "'da_sampling' (logistic configuration)")
     p.add_argument("--c5-warmup", type=int, default=128)
     p.add_argument("--c5-iters", type=int, default=40)
     p.add_argument("--pt-da-iters", type=int, default=400)
@@ -960,10 +964,57 @@ def run_c5_da(a):
     print(json.dumps({"c5_da": c5_da_measure(a.c5_warmup, a.c5_iters)}), flush=True)
 
 
+def run_profile_da(a, n_warm=200, n_samp=48, seed=11):
+    """A small, self-contained target for profiler captures of the surrogate's
+    training and of the two-stage loop on the logistic configuration (1024
+    chains, N = 2^20): a short adaptive exact warmup whose second half is
+    recorded, the surrogate trained inside an NVTX range "training", then
+    n_samp two-stage iterations inside an NVTX range "da_sampling" (select
+    them with ncu --nvtx --nvtx-include)."""
+    import torch
+
+    from gpumetropolis_b200 import _native, api
+    from gpumetropolis_b200 import adaptive as AD
+    from gpumetropolis_b200.build import build
+    build()
+    if not _native.available():
+        raise SystemExit("gpum_b200: no usable sm_100 device")
+    w = _workload(a.n_obs)
+    m = w.model
+    C, npar = a.chains, m.n_params
+    call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, dict(api.SURROGATE_DEFAULTS))
+    try:
+        call.record_at = n_warm // 2
+        rng = np.random.default_rng(seed)
+        init = w.truth["beta"] + rng.normal(0, 0.05, (C, npar))
+        am = AD.am_orchestrate_warmup(call, npar, C, init, np.full((C, npar), 0.01), n_warm,
+                                      seed)
+        call.session.sync()
+        torch.cuda.nvtx.range_push("training")
+        t = time.perf_counter()
+        call.start_da()
+        t_train = time.perf_counter() - t
+        torch.cuda.nvtx.range_pop()
+        call.session.sync()
+        torch.cuda.nvtx.range_push("da_sampling")
+        t = time.perf_counter()
+        call(am.final_init, am.final_proposal_sd, n_samp, seed + 2, None, _native.MODE_CHOL,
+             0.0, 0.0, am.final_L)
+        t_da = time.perf_counter() - t
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"profile_da": {"train_s": round(t_train, 4),
+                                         "da_us_per_iter": round(1e6 * t_da / n_samp, 1),
+                                         "surrogate": call.da_summary()}}), flush=True)
+    finally:
+        call.close()
+
+
 def main():
     a = _args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.profile_da:
+        run_profile_da(a)
     elif a.c5_da:
         run_c5_da(a)
     elif a.pt_da:

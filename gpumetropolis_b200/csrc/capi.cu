@@ -105,13 +105,25 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+// Static shared memory of a kernel (the interpreter's operand scratch): with
+// it, a dynamic request below 48 KB can still need the opt-in attribute.
+size_t static_smem(const void* fn) {
+  cudaFuncAttributes fa{};
+  return cudaFuncGetAttributes(&fa, fn) == cudaSuccess ? fa.sharedSizeBytes : 0;
+}
+
 // Interpreter variants by peak stack depth: registers go to depth or to
 // chains per thread.
-enum Variant { V8x8 = 0, V4x16 = 1, V2x32 = 2 };
-int variant_G(int v) { return v == V8x8 ? 8 : (v == V4x16 ? 4 : 2); }
+enum Variant { V8x8 = 0, V4x16 = 1, V2x32 = 2, V16x6 = 3 };
+int variant_G(int v) { return v == V16x6 ? 16 : v == V8x8 ? 8 : (v == V4x16 ? 4 : 2); }
+int choose_variant(const UProg& p) {
+  if (p.depth <= 6 && p.n_saves <= 1) return V16x6;
+  return p.depth <= 8 ? V8x8 : (p.depth <= 16 ? V4x16 : V2x32);
+}
 
 const void* interp_kernel(int v) {
   switch (v) {
+    case V16x6: return (const void*)iter_kernel<16, 6>;
     case V8x8: return (const void*)iter_kernel<8, 8>;
     case V4x16: return (const void*)iter_kernel<4, 16>;
     default: return (const void*)iter_kernel<2, 32>;
@@ -121,6 +133,7 @@ const void* interp_kernel(int v) {
 void launch_interp(int v, dim3 grid, size_t smem, cudaStream_t st, const EvalProg& prog,
                    const TmapDesc& tmap, const EvalArgs& E, const ChainArgs& A, int phase) {
   switch (v) {
+    case V16x6: iter_kernel<16, 6><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
     case V8x8: iter_kernel<8, 8><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
     case V4x16: iter_kernel<4, 16><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
     default: iter_kernel<2, 32><<<grid, kThreads, smem, st>>>(prog, tmap, E, A, phase); break;
@@ -396,7 +409,7 @@ struct gpum_b200_session {
   void setup_eval(int n, bool need_grad) {
     kc = choose(need_grad);
     geo = geometry(n, kc);
-    if (geo.smem > 48 * 1024)
+    if (geo.smem + static_smem(kc.fn) > 48 * 1024)
       GPUM_CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)geo.smem));
     params.ensure((size_t)np * geo.C_pad);
@@ -547,7 +560,7 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
   s->np = n_params;
   s->ncols = n_cols;
   s->n_obs = n_obs;
-  s->variant = s->ll.depth <= 8 ? V8x8 : (s->ll.depth <= 16 ? V4x16 : V2x32);
+  s->variant = choose_variant(s->ll);
   s->prog.reset(new EvalProg());
   std::memset(s->prog.get(), 0, sizeof(EvalProg));
   s->prog->n_uops = (uint32_t)s->ll.uops.size();

@@ -19,6 +19,8 @@
 
 namespace gpum {
 
+constexpr int kInterpThreads = 256;  // threads per interpreter CTA
+
 struct __align__(16) EvalProg {
   uint32_t n_uops;
   uint32_t pad_[3];
@@ -55,20 +57,30 @@ __device__ __forceinline__ void load_params(const float* __restrict__ p, float (
 //   xo : this lane's observation inside the tile; column j is at xo[j*T]
 //   pc0: this thread's first chain in the param tile; param p, chain g at
 //        pc0[p*CG + g]  (16-byte aligned; G is a multiple of 2)
+//   hsm: this thread's operand scratch for the shared expensive ops, 2*G
+//        floats at a stride of kInterpThreads (the block's thread count)
 template <int G, int D>
 __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
                                            const float* __restrict__ xo, int T,
-                                           const float* __restrict__ pc0, int CG) {
+                                           const float* __restrict__ pc0, int CG,
+                                           float* __restrict__ hsm) {
   const uint32_t n = pg.n_uops;
+  // Saved subtrees (K_SAVEk / K_LOADk): registers, since every case names
+  // its save index at compile time.  The sixteen-chain variant keeps one, the
+  // deep-stack variants none (the compiler saves nothing for stacks deeper
+  // than kMaxSavedDepth).
+  constexpr int NS = D > kMaxSavedDepth ? 0 : (G >= 16 ? 1 : kMaxSaves);
+  float sv[NS > 0 ? NS : 1][G];
   for (uint32_t pc = 0; pc < n; ++pc) {
     const uint32_t w = pg.uop[pc];
-    const uint32_t a0 = (w >> 10) & 0x7FFu;
-    const uint32_t a1 = w >> 21;
+    const uint32_t a0 = (w >> kCaseBits) & 0x7FFu;
+    const uint32_t a1 = w >> 22;
     int hk = H_NONE, hs = 0;
-    float ta[G], tb[G];
 
 #define GPUM_PL(g) pv[g]
 #define GPUM_XD(a) xo[(size_t)(a) * T]
+#define GPUM_HA(g) hsm[(g) * kInterpThreads]
+#define GPUM_HB(g) hsm[(G + (g)) * kInterpThreads]
 #define GPUM_SLOT(S)                                                                   \
   case S * NKIND + K_PUSH_C:                                                           \
     if constexpr (S < D) {                                                             \
@@ -108,10 +120,10 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
   case S * NKIND + K_POW:                                                              \
     if constexpr (S + 1 < D) {                                                         \
       _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        ta[g] = s[S][g];                                                               \
-        tb[g] = s[S + 1][g];                                                           \
+        GPUM_HA(g) = s[S][g];                                                          \
+        GPUM_HB(g) = s[S + 1][g];                                                      \
       }                                                                                \
-      hk = ((w & 1023u) == S * NKIND + K_DIV) ? H_DIV : H_POW;                         \
+      hk = ((w & kCaseMask) == S * NKIND + K_DIV) ? H_DIV : H_POW;                         \
       hs = S;                                                                          \
     }                                                                                  \
     break;                                                                             \
@@ -138,10 +150,10 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     if constexpr (S < D) {                                                             \
       const float v = pg.cst[a0];                                                      \
       _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        ta[g] = s[S][g];                                                               \
-        tb[g] = v;                                                                     \
+        GPUM_HA(g) = s[S][g];                                                          \
+        GPUM_HB(g) = v;                                                                \
       }                                                                                \
-      hk = ((w & 1023u) == S * NKIND + K_DIV_C) ? H_DIV : H_POW;                       \
+      hk = ((w & kCaseMask) == S * NKIND + K_DIV_C) ? H_DIV : H_POW;                       \
       hs = S;                                                                          \
     }                                                                                  \
     break;                                                                             \
@@ -172,10 +184,10 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
       float pv[G];                                                                     \
       load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
       _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        ta[g] = s[S][g];                                                               \
-        tb[g] = GPUM_PL(g);                                                            \
+        GPUM_HA(g) = s[S][g];                                                          \
+        GPUM_HB(g) = GPUM_PL(g);                                                       \
       }                                                                                \
-      hk = ((w & 1023u) == S * NKIND + K_DIV_P) ? H_DIV : H_POW;                       \
+      hk = ((w & kCaseMask) == S * NKIND + K_DIV_P) ? H_DIV : H_POW;                       \
       hs = S;                                                                          \
     }                                                                                  \
     break;                                                                             \
@@ -202,10 +214,10 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     if constexpr (S < D) {                                                             \
       const float v = GPUM_XD(a0);                                                     \
       _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        ta[g] = s[S][g];                                                               \
-        tb[g] = v;                                                                     \
+        GPUM_HA(g) = s[S][g];                                                          \
+        GPUM_HB(g) = v;                                                                \
       }                                                                                \
-      hk = ((w & 1023u) == S * NKIND + K_DIV_D) ? H_DIV : H_POW;                       \
+      hk = ((w & kCaseMask) == S * NKIND + K_DIV_D) ? H_DIV : H_POW;                       \
       hs = S;                                                                          \
     }                                                                                  \
     break;                                                                             \
@@ -231,7 +243,7 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
     break;                                                                             \
   case S * NKIND + K_LGAMMA:                                                           \
     if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) ta[g] = s[S][g];                   \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) GPUM_HA(g) = s[S][g];              \
       hk = H_LGAMMA;                                                                   \
       hs = S;                                                                          \
     }                                                                                  \
@@ -259,6 +271,36 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
         _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
       }                                                                                \
     }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SAVE0:                                                            \
+    if constexpr (S < D && NS > 0) {                                                   \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) sv[0][g] = s[S][g];                \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_LOAD0:                                                            \
+    if constexpr (S < D && NS > 0) {                                                   \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sv[0][g];                \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SAVE1:                                                            \
+    if constexpr (S < D && NS > 1) {                                                   \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) sv[NS - 1][g] = s[S][g];           \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_LOAD1:                                                            \
+    if constexpr (S < D && NS > 1) {                                                   \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sv[NS - 1][g];           \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SOFTPLUS:                                                         \
+    if constexpr (S < D) {                                                             \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = gm_softplus(s[S][g]);    \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SOFTPLUS1:                                                        \
+    if constexpr (S + 1 < D) {                                                         \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = gm_softplus(s[S + 1][g]); \
+    }                                                                                  \
     break;
 
     // Only the labels a variant can reach (slot < D) are emitted, so each
@@ -272,17 +314,17 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
   GPUM_SLOT(25) GPUM_SLOT(26) GPUM_SLOT(27) GPUM_SLOT(28) GPUM_SLOT(29) GPUM_SLOT(30) \
   GPUM_SLOT(31)
     if constexpr (D <= 8) {
-      switch (w & 1023u) {
+      switch (w & kCaseMask) {
         GPUM_SLOTS_8
         default: break;
       }
     } else if constexpr (D <= 16) {
-      switch (w & 1023u) {
+      switch (w & kCaseMask) {
         GPUM_SLOTS_16
         default: break;
       }
     } else {
-      switch (w & 1023u) {
+      switch (w & kCaseMask) {
         GPUM_SLOTS_32
         default: break;
       }
@@ -295,21 +337,19 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
 #undef GPUM_XD
 
     if (hk != H_NONE) {  // warp-uniform
-      if (hk == H_DIV) {
-#pragma unroll
-        for (int g = 0; g < G; ++g) ta[g] = ta[g] / tb[g];
-      } else if (hk == H_POW) {
-#pragma unroll
-        for (int g = 0; g < G; ++g) ta[g] = powf(ta[g], tb[g]);
-      } else {
-#pragma unroll
-        for (int g = 0; g < G; ++g) ta[g] = lgammaf(ta[g]);
+      // One copy of the expensive function for every slot and chain: the
+      // operands went through shared memory, so this loop stays rolled.
+#pragma unroll 1
+      for (int g = 0; g < G; ++g) {
+        const float x = GPUM_HA(g);
+        GPUM_HA(g) = hk == H_DIV ? x / GPUM_HB(g)
+                                 : (hk == H_POW ? powf(x, GPUM_HB(g)) : lgammaf(x));
       }
       // Write back to the slot named by the case (a second uniform switch).
 #define GPUM_WB(S)                                                        \
   case S:                                                                 \
     if constexpr (S < D) {                                                \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = ta[g];      \
+      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = GPUM_HA(g); \
     }                                                                     \
     break;
       switch (hs) {
@@ -322,6 +362,8 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
       }
 #undef GPUM_WB
     }
+#undef GPUM_HA
+#undef GPUM_HB
   }
 }
 

@@ -16,9 +16,10 @@ struct InterpBody {
   const EvalProg& pg;
   const float* pc0;
   int CG;
+  float* hsm;
   float s[D][G];
   Comp acc[G];
-  __device__ explicit InterpBody(const EvalProg& p) : pg(p), pc0(nullptr), CG(0) {}
+  __device__ InterpBody(const EvalProg& p, float* h) : pg(p), pc0(nullptr), CG(0), hsm(h) {}
   __device__ __forceinline__ void begin(const float* p0, int cg) {
     pc0 = p0;
     CG = cg;
@@ -26,7 +27,7 @@ struct InterpBody {
     for (int g = 0; g < G; ++g) acc[g].init();
   }
   __device__ __forceinline__ void eval(const float* xo, int T, bool valid) {
-    interp_run<G, D>(pg, s, xo, T, pc0, CG);
+    interp_run<G, D>(pg, s, xo, T, pc0, CG, hsm);
     if (valid) {
 #pragma unroll
       for (int g = 0; g < G; ++g) acc[g].add(s[0][g]);
@@ -52,14 +53,16 @@ struct InterpPrior {
   }
 };
 
-// The widest variant (eight chains per thread, an eight-deep stack: 64
-// stack registers) keeps its stack in registers at one CTA per SM; the others
-// fit two.
+// The widest variants (sixteen chains per thread over a six-deep stack, eight
+// over eight: 96 and 64 stack registers) keep their stacks in registers at one
+// CTA per SM; the others fit two.
 template <int G, int D>
-__global__ void __launch_bounds__(kThreads, (G == 8 ? 1 : 2))
+__global__ void __launch_bounds__(kThreads, (G >= 8 ? 1 : 2))
 iter_kernel(const __grid_constant__ EvalProg prog, const __grid_constant__ TmapDesc tmap,
             EvalArgs E, ChainArgs A, int phase) {
-  InterpBody<G, D> body(prog);
+  static_assert(kThreads == kInterpThreads, "the operand scratch is laid out per thread");
+  __shared__ float hsm[2 * G * kInterpThreads];
+  InterpBody<G, D> body(prog, hsm + threadIdx.x);
   run_iteration<G, 1, InterpBody<G, D>, InterpPrior>(&tmap, E, A, phase, body);
 }
 

@@ -179,7 +179,10 @@ extern "C" int gpum_b200_loglik_batch_noalloc(
   int occ = 1, sms = 148, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (smem > 48 * 1024 &&
+  cudaFuncAttributes fa{};  // the interpreter's static operand scratch counts too
+  if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess)
+    return fail(err, err_len, GPUM_ERR_CUDA, "cudaFuncGetAttributes failed");
+  if (smem + fa.sharedSizeBytes > 48 * 1024 &&
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess)
     return fail(err, err_len, GPUM_ERR_UNSUPPORTED, "shared memory request refused");

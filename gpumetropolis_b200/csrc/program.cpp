@@ -1,6 +1,7 @@
 // program.cpp -- bytecode validation and micro-op compilation (see program.hpp).
 #include "program.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -127,6 +128,94 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
     if (op[pc] == OP_DATA) out->uses_data = true;
   }
 
+  // Repeated subtrees.  In postfix order a subtree is the contiguous range
+  // [start[pc], pc] that ends at its root; two subtrees compute the same value
+  // when their instruction ranges match (constants compared by value).
+  std::vector<size_t> start(n, 0);
+  {
+    std::vector<size_t> st;
+    for (size_t pc = 0; pc < n; ++pc) {
+      if (is_push(op[pc])) {
+        start[pc] = pc;
+      } else if (is_unary(op[pc])) {
+        start[pc] = st.back();
+        st.pop_back();
+      } else {
+        st.pop_back();
+        start[pc] = st.back();
+        st.pop_back();
+      }
+      st.push_back(start[pc]);
+    }
+  }
+  auto same_range = [&](size_t a, size_t b, size_t len) {
+    for (size_t k = 0; k < len; ++k) {
+      if (op[a + k] != op[b + k]) return false;
+      if (op[a + k] == OP_CONST) {
+        if (consts[arg[a + k]] != consts[arg[b + k]]) return false;
+      } else if (is_push(op[a + k]) && arg[a + k] != arg[b + k]) {
+        return false;
+      }
+    }
+    return true;
+  };
+  // LOG(1 + EXP(a)) and LOG(EXP(a) + 1): the instructions other than `a` are
+  // not emitted (omit), and the LOG emits the softplus of `a` into the slot
+  // of the LOG's result -- in place when `a` sits there (EXP first), from the
+  // slot above when the constant 1 was pushed first.
+  std::vector<char> omit(n, 0);
+  std::vector<int> softplus_kind(n, 0);
+  auto is_one = [&](size_t i) { return op[i] == OP_CONST && consts[arg[i]] == 1.0; };
+  for (size_t pc = 2; pc < n; ++pc) {
+    if (op[pc] != OP_LOG || op[pc - 1] != OP_ADD) continue;
+    const size_t r = pc - 2;            // the ADD's right operand root
+    if (start[r] == 0) continue;
+    const size_t l = start[r] - 1;      // its left operand root
+    if (start[l] == l && is_one(l) && op[r] == OP_EXP && r >= 1) {
+      omit[l] = omit[r] = omit[pc - 1] = 1;
+      softplus_kind[pc] = K_SOFTPLUS1;
+    } else if (start[r] == r && is_one(r) && op[l] == OP_EXP) {
+      omit[l] = omit[r] = omit[pc - 1] = 1;
+      softplus_kind[pc] = K_SOFTPLUS;
+    }
+  }
+  // save_end[pc] = k + 1 when the first copy of saved subtree k ends at pc;
+  // load_at[pc] = k + 1 when a later copy of it starts at pc (skipped).
+  std::vector<int> save_end(n, 0), load_at(n, 0);
+  std::vector<size_t> load_root(n, 0);
+  std::vector<char> skipped(n, 0);
+  {
+    std::vector<size_t> roots;
+    for (size_t pc = 0; pc < n && depth <= kMaxSavedDepth; ++pc)
+      if (!is_push(op[pc]) && !omit[pc] && pc - start[pc] + 1 >= (size_t)kMinSaved)
+        roots.push_back(pc);
+    // Largest subtrees first: a smaller one inside a skipped copy is gone.
+    std::stable_sort(roots.begin(), roots.end(), [&](size_t a, size_t b) {
+      return a - start[a] > b - start[b];
+    });
+    std::vector<char> used(n, 0);
+    for (size_t ri = 0; ri < roots.size() && out->n_saves < kMaxSaves; ++ri) {
+      const size_t r = roots[ri], len = r - start[r] + 1;
+      if (used[r] || skipped[r]) continue;
+      std::vector<size_t> occ;
+      for (size_t rj = ri; rj < roots.size(); ++rj) {
+        const size_t q = roots[rj];
+        if (q - start[q] + 1 != len || used[q] || skipped[q]) continue;
+        if (same_range(start[r], start[q], len)) occ.push_back(q);
+      }
+      for (size_t q : occ) used[q] = 1;
+      if (occ.size() < 2) continue;
+      std::sort(occ.begin(), occ.end());
+      const int k = out->n_saves++;
+      save_end[occ[0]] = k + 1;
+      for (size_t o = 1; o < occ.size(); ++o) {
+        load_at[start[occ[o]]] = k + 1;
+        load_root[start[occ[o]]] = occ[o];
+        for (size_t i = start[occ[o]]; i <= occ[o]; ++i) skipped[i] = 1;
+      }
+    }
+  }
+
   auto add_const = [&](float v) -> int {
     out->consts.push_back(v);
     return (int)out->consts.size() - 1;
@@ -140,16 +229,40 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
   };
 
   size_t pc = 0;
+  // After each emitted group (fused groups never straddle the end of a saved
+  // subtree, whose root is an operation that ends its group): keep the value.
+  auto after = [&](size_t next) {
+    const int k = save_end[next - 1];
+    if (k) emit(k == 1 ? K_SAVE0 : K_SAVE1, before[start[next - 1]], 0, 0);
+  };
   while (pc < n) {
     const uint32_t o = op[pc];
+    if (load_at[pc]) {  // a later copy of a saved subtree
+      const int k = load_at[pc];
+      emit(k == 1 ? K_LOAD0 : K_LOAD1, before[pc], 0, 0);
+      pc = load_root[pc] + 1;
+      after(pc);
+      continue;
+    }
+    if (omit[pc]) {  // the 1, EXP and ADD of a softplus
+      ++pc;
+      continue;
+    }
+    if (softplus_kind[pc]) {
+      emit((uint32_t)softplus_kind[pc], before[pc] - 1, 0, 0);
+      ++pc;
+      after(pc);
+      continue;
+    }
     // acc + p*x  or  acc + x*p  -> one multiply-add into the accumulator slot.
     if (pc + 3 < n && before[pc] >= 1 && op[pc + 2] == OP_MUL && op[pc + 3] == OP_ADD &&
-        ((o == OP_PARAM && op[pc + 1] == OP_DATA) ||
-         (o == OP_DATA && op[pc + 1] == OP_PARAM))) {
+        ((o == OP_PARAM && op[pc + 1] == OP_DATA && arg[pc + 1] <= (uint32_t)kMaxA1) ||
+         (o == OP_DATA && op[pc + 1] == OP_PARAM && arg[pc] <= (uint32_t)kMaxA1))) {
       const uint32_t p = o == OP_PARAM ? arg[pc] : arg[pc + 1];
       const uint32_t x = o == OP_PARAM ? arg[pc + 1] : arg[pc];
       emit(K_FMA_PD, before[pc] - 1, p, x);
       pc += 4;
+      after(pc);
       continue;
     }
     // push followed by the binary op that consumes it: fold the operand.
@@ -169,6 +282,7 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
         emit(base + (uint32_t)bin_index(b), slot, arg[pc], 0);
       }
       pc += 2;
+      after(pc);
       continue;
     }
     switch (o) {
@@ -183,6 +297,7 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
       default: emit(kBin[bin_index(o)], before[pc] - 2, 0, 0); break;
     }
     ++pc;
+    after(pc);
   }
   // Runs of multiply-adds into one slot become one K_DOT over a term table
   // (the same fmaf sequence in the same order, so the value is unchanged).
@@ -192,16 +307,18 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
     size_t i = 0;
     while (i < out->uops.size()) {
       const uint32_t w = out->uops[i];
-      const uint32_t id = w & 1023u, kind = id % NKIND, slot = id / NKIND;
+      const uint32_t id = w & kCaseMask, kind = id % NKIND, slot = id / NKIND;
       size_t j = i + 1;
       if (kind == K_FMA_PD)
-        while (j < out->uops.size() && (out->uops[j] & 1023u) == id) ++j;
+        while (j < out->uops.size() && (out->uops[j] & kCaseMask) == id &&
+               j - i < (size_t)kMaxA1)
+          ++j;
       if (kind == K_FMA_PD && j - i >= 2 &&
           out->terms.size() + (j - i) <= (size_t)kMaxTerms) {
         const uint32_t t0 = (uint32_t)out->terms.size();
         for (size_t k = i; k < j; ++k)
-          out->terms.push_back(((out->uops[k] >> 10) & 0x7FFu) |
-                               (((out->uops[k] >> 21) & 0x7FFu) << 11));
+          out->terms.push_back(((out->uops[k] >> kCaseBits) & 0x7FFu) |
+                               ((out->uops[k] >> 22) << 11));
         merged.push_back(uop_word(K_DOT, slot, t0, (uint32_t)(j - i)));
         i = j;
       } else {

@@ -12,14 +12,21 @@
 // error before anything reaches the GPU.
 //
 // Output: one 32-bit word per micro-op,
-//   bits  0..9   case id = slot * NKIND + kind   (slot = stack index of the
+//   bits  0..10  case id = slot * NKIND + kind   (slot = stack index of the
 //                 result, a compile-time register index in the kernel)
-//   bits 10..20  a0 (const / param / column index)
-//   bits 21..31  a1 (second index for two-operand fused forms)
+//   bits 11..21  a0 (const / param / column index)
+//   bits 22..31  a1 (second index for two-operand fused forms, < 1024)
 // plus an f32 constant pool.  Peephole fusion folds a push into the binary op
 // that consumes it, `p*x + acc` patterns into one multiply-add, and a run of
 // such multiply-adds into the same slot (a linear predictor) into one K_DOT
-// micro-op over a term table, so the dispatch is paid once per run.
+// micro-op over a term table, so the dispatch is paid once per run.  A
+// subtree of at least kMinSaved instructions that the program computes again
+// later (the logistic and Poisson likelihoods write their linear predictor
+// twice) is kept after its first evaluation (K_SAVEk) and every later copy
+// becomes one K_LOADk: the same FP32 value, computed once.  LOG(1 + EXP(a))
+// (either operand order of the ADD) becomes one K_SOFTPLUS of a, evaluated
+// as max(a, 0) + log1p(e^-|a|): more accurate than the two calls in FP32
+// (no rounding of 1 + e^a to 1 where e^a < 2^-24) and about half the work.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -38,13 +45,23 @@ enum Kind : uint32_t {
   K_FMA_PD,                                     // s[t] += param[a0]*data[a1]
   K_DOT,                                        // s[t] += sum over terms[a0 .. a0+a1)
                                                 //   of param[p_k]*data[x_k], in order
+  K_SAVE0, K_SAVE1,                             // saved[k] = s[t]
+  K_LOAD0, K_LOAD1,                             // s[t] = saved[k]
+  K_SOFTPLUS,                                   // s[t] = log(1 + exp(s[t]))
+  K_SOFTPLUS1,                                  // s[t] = log(1 + exp(s[t+1]))
   NKIND
 };
+constexpr int kMaxSaves = 2;       // saved subtrees per program
+constexpr int kMinSaved = 8;       // smallest subtree worth saving (instructions)
+constexpr int kMaxSavedDepth = 8;  // programs with deeper stacks save nothing
+constexpr int kCaseBits = 11;
+constexpr uint32_t kCaseMask = (1u << kCaseBits) - 1u;
 
 constexpr int kMaxStack = 32;      // reference limit (R/dsl.R:20)
 constexpr int kMaxUops = 1024;     // micro-ops per program (constant bank)
 constexpr int kMaxConsts = 512;    // f32 constants per program
-constexpr int kMaxIndex = 2047;    // 11-bit operand fields
+constexpr int kMaxIndex = 2047;    // 11-bit a0 field
+constexpr int kMaxA1 = 1023;       // 10-bit a1 field
 constexpr int kMaxSlots = 32;      // deepest interpreter variant
 constexpr int kMaxTerms = 1024;    // (param, column) terms of K_DOT micro-ops
 
@@ -53,14 +70,16 @@ struct UProg {
   std::vector<uint32_t> terms;  // K_DOT terms: param | column << 11
   std::vector<float> consts;
   int depth = 0;          // peak stack depth of the source program
+  int n_saves = 0;        // saved subtrees (K_SAVEk / K_LOADk pairs)
   int n_src = 0;          // source instructions
   bool uses_data = false;
   bool empty() const { return n_src == 0; }
 };
 
 inline uint32_t uop_word(uint32_t kind, uint32_t slot, uint32_t a0, uint32_t a1) {
-  return (slot * NKIND + kind) | (a0 << 10) | (a1 << 21);
+  return (slot * NKIND + kind) | (a0 << kCaseBits) | (a1 << 22);
 }
+static_assert(kMaxSlots * NKIND <= (1 << kCaseBits), "case ids must fit their field");
 
 // The interpreter engine's gradient program: the source bytecode as a list
 // of its non-push instructions ("nodes"), each naming its operands directly

@@ -99,6 +99,38 @@ def test_interpreter_variants_by_depth(gpu, depth):
     assert np.all(np.abs(got_i - ref) <= 1e-6 * scale)
 
 
+# Programs that compute a subtree again (the interpreter evaluates it once and
+# reuses the value): one repeated linear predictor at a shallow stack, two
+# different repeated subtrees, three copies of one, a repeated subtree inside a
+# repeated subtree, and a repeat at a stack deeper than the reuse limit.
+_LP = "(a + b * x + c * z)"
+_LQ = "(d * x + e * z + a)"
+_REPEATS = [
+    f"~ y * {_LP} - log(1 + exp({_LP}))",
+    f"~ y * {_LP} - exp({_LQ}) + {_LQ} / (1 + {_LP}^2)",
+    f"~ {_LP} * {_LP} - {_LP} / (2 + exp(-{_LP}))",
+    f"~ exp(-({_LP} + {_LQ})^2 / 8) + log(1 + ({_LP} + {_LQ})^2) - {_LP}",
+    "~ " + "(y * a + " * 9 + f"log(1 + exp({_LP})) - {_LP}" + ")" * 9,
+]
+
+
+@pytest.mark.parametrize("k", range(len(_REPEATS)))
+def test_interpreter_reuses_repeated_subtrees(gpu, k):
+    m = gpum_model(_REPEATS[k], ["a", "b", "c", "d", "e"], ["y", "x", "z"])
+    rng = np.random.default_rng(10 + k)
+    n = 1537
+    data = np.column_stack([rng.uniform(0, 1, n) < 0.5, rng.normal(size=n),
+                            rng.normal(size=n)]).astype(np.float64)
+    pts = rng.normal(0, 0.3, (19, 5))
+    ref = O.loglik_pointwise(m.loglik.code, m.loglik.consts, 5, data, 3, n, pts)
+    with gpu.Session(m.loglik.code, m.loglik.consts, [], [], 5, data, 3, n, engine=0) as s:
+        got = s.loglik_pointwise(pts)
+        tot = s.loglik_batch(pts)
+    np.testing.assert_allclose(got, ref, rtol=2e-5, atol=2e-5)
+    pw = ref.reshape(pts.shape[0], -1)
+    assert np.all(np.abs(tot - pw.sum(axis=1)) <= 1e-6 * np.abs(pw).sum(axis=1))
+
+
 def test_every_opcode_and_edge_sizes(gpu, golden):
     c = golden["gamma"]
     m = gpum_model(c["formula"], c["params"], c["data"])
