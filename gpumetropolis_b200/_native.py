@@ -128,6 +128,9 @@ SIGNATURES = {
     "gpum_b200_session_record": (C.c_int, [C.c_void_p, C.c_uint64, _errp, _sz]),
     "gpum_b200_session_recorded": (C.c_int, [C.c_void_p, _f32p, _f64p, C.c_uint64,
                                              C.POINTER(C.c_uint64), _errp, _sz]),
+    "gpum_b200_session_train_surrogate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32,
+                                                    C.c_int, C.c_uint32, _u32p, _f64p, _f32p,
+                                                    _f64p, _errp, _sz]),
     "gpum_b200_session_run_da": (C.c_int, [C.c_void_p, C.c_void_p, _f64p, _f64p, _f64p,
                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                            C.c_double, C.c_double, _f64p, _sz, C.c_int, _f32p,
@@ -451,6 +454,36 @@ class Session:
             self._h, _p(theta, C.c_float), _p(ll, C.c_double), n.value, C.byref(n), err,
             _ERRLEN), err)
         return theta[: n.value], ll[: n.value]
+
+    def recorded_count(self) -> int:
+        """Pairs recorded so far."""
+        n = C.c_uint64(0)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_recorded(self._h, None, None, 0, C.byref(n), err,
+                                                    _ERRLEN), err)
+        return int(n.value)
+
+    def train_surrogate(self, surrogate, stages, holdout_every=10, whiten=True):
+        """Fit `surrogate` (a Surrogate with d = n_params) to the recorded
+        pairs on the device: every `holdout_every`-th pair held out, the
+        normaliser from the training pairs' moments (whitened inputs with
+        `whiten`), Adam over `stages` [(steps, lr), ...].  Returns (losses,
+        info) with info = {pairs, train_pairs, holdout_pairs,
+        holdout_resid_sd, whitened}."""
+        steps = np.ascontiguousarray([int(k) for k, _ in stages], dtype=np.uint32)
+        lrs = np.ascontiguousarray([float(r) for _, r in stages], dtype=np.float64)
+        total = int(steps.sum())
+        losses = np.empty(max(total, 1), np.float32)
+        info = np.full(5, np.nan)
+        err = C.create_string_buffer(_ERRLEN)
+        _check(self._lib.gpum_b200_session_train_surrogate(
+            self._h, surrogate._h, int(holdout_every), int(bool(whiten)), steps.size,
+            _p(steps, C.c_uint32), _p(lrs, C.c_double), _p(losses, C.c_float),
+            _p(info, C.c_double), err, _ERRLEN), err)
+        return losses[:total], {"pairs": int(info[0]), "train_pairs": int(info[1]),
+                                "holdout_pairs": int(info[2]),
+                                "holdout_resid_sd": float(info[3]),
+                                "whitened": bool(info[4])}
 
     def run_da(self, surrogate, init, proposal_sd, temperatures, n_iter, seed, proposal_mode,
                gamma=0.0, de_noise=0.0, proposal_l=None, rng=RNG_TRIPLE32, out_draws=None):

@@ -142,29 +142,33 @@ class _Backend:
         if not self.recording:
             self.info = {"used": False, "reason": "no exact pairs were recorded"}
             return
-        theta, ll = self.session.recorded()
-        self.session.record(0)
-        self.recording = False
-        ok = np.isfinite(ll) & np.all(np.isfinite(theta), axis=1)
-        theta, ll = theta[ok].astype(np.float64), ll[ok]
-        if theta.shape[0] < int(self.cfg["min_pairs"]):
-            self.info = {"used": False, "reason": f"only {theta.shape[0]} finite pairs"}
+        n_rec = self.session.recorded_count()
+        if n_rec < int(self.cfg["min_pairs"]):
+            self.session.record(0)
+            self.recording = False
+            self.info = {"used": False, "reason": f"only {n_rec} recorded pairs"}
             return
-        g = np.random.Generator(np.random.PCG64(int(self.cfg["seed"])))
-        idx = g.permutation(theta.shape[0])
-        n_hold = max(1, theta.shape[0] // 10)
-        hold, train = idx[:n_hold], idx[n_hold:]
+        # The pairs stay on the device: split (every tenth held out), moments
+        # for the normaliser, training and the held-out check in one call.
         net = _native.Surrogate(self.np, hidden=int(self.cfg["hidden"]),
                                 batch=int(self.cfg["batch"]), seed=int(self.cfg["seed"]))
-        net.fit_normalizer(theta[train], ll[train], whiten=bool(self.cfg["whiten"]))
         steps, lr = int(self.cfg["steps"]), float(self.cfg["lr"])
-        loss = net.train_stages(theta[train], ll[train],
-                                [(steps, lr), (steps, lr / 3.0), (steps, lr / 10.0)])
-        resid = net.predict(theta[hold]) - ll[hold]
+        try:
+            loss, fit = self.session.train_surrogate(
+                net, [(steps, lr), (steps, lr / 3.0), (steps, lr / 10.0)], holdout_every=10,
+                whiten=bool(self.cfg["whiten"]))
+        except _native.GpumError as e:
+            net.close()
+            self.session.record(0)
+            self.recording = False
+            self.info = {"used": False, "reason": str(e)}
+            return
+        self.session.record(0)
+        self.recording = False
         self.net = net
-        self.info = {"used": True, "pairs": int(theta.shape[0]),
+        self.info = {"used": True, "pairs": fit["train_pairs"] + fit["holdout_pairs"],
                      "final_loss": float(np.mean(loss[-50:])),
-                     "holdout_resid_sd": float(np.std(resid))}
+                     "holdout_resid_sd": fit["holdout_resid_sd"]}
 
     def __call__(self, init, sd, n_iter, seed, temperatures=None, proposal_mode=0, gamma=0.0,
                  de_noise=0.0, proposal_l=None, out_draws=None):

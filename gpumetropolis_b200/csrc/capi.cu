@@ -43,6 +43,10 @@ int mlp_infer_launches(const gpum_b200_mlp* m, int n);
 int mlp_infer_grad(gpum_b200_mlp* m, const double* theta, int n, int d, double* out_val,
                    double* out_grad, cudaStream_t st, std::string* err);
 int mlp_infer_grad_launches(const gpum_b200_mlp* m, int n);
+int mlp_train_device(gpum_b200_mlp* m, const float* dth, const double* dll, size_t n_pairs,
+                     uint32_t n_stages, const uint32_t* steps, const double* lrs,
+                     float* out_loss, std::string* err);
+int mlp_input_width(const gpum_b200_mlp* m);
 }  // namespace gpum
 
 static_assert(sizeof(CUtensorMap) == sizeof(TmapDesc), "tensor map size");
@@ -1441,6 +1445,315 @@ int gpum_b200_session_record(gpum_b200_session* s, uint64_t capacity, char* err,
     }
     s->rec_theta.ensure((size_t)capacity * s->np);
     s->rec_ll.ensure((size_t)capacity);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// ----------------------------------------- surrogate fit from device pairs
+// Pair i of the recording is held out when holdout_every > 0 and
+// i % holdout_every == 0; a pair with a non-finite log-likelihood or
+// parameter is dropped.  One CTA scans the flags in pair order, so the
+// positions (and the training set's order) are deterministic:
+//   pos[i] = training position | kHeldOut for a held-out position |
+//            kDropped.
+constexpr int kSplitThreads = 1024;
+constexpr uint32_t kHeldOut = 0x80000000u, kDropped = 0xFFFFFFFFu;
+
+__global__ void __launch_bounds__(kSplitThreads)
+pairs_split_kernel(const float* __restrict__ th, const double* __restrict__ ll, uint32_t n,
+                   int np, uint32_t every, uint32_t* __restrict__ pos,
+                   uint32_t* __restrict__ counts) {
+  __shared__ uint32_t wsum[2][32], tot[2], base[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) base[0] = base[1] = 0;
+  __syncthreads();
+  for (uint32_t i0 = 0; i0 < n; i0 += kSplitThreads) {
+    const uint32_t i = i0 + tid;
+    bool ok = false, hold = false;
+    if (i < n) {
+      ok = isfinite(ll[i]);
+      for (int j = 0; j < np && ok; ++j) ok = isfinite(th[(size_t)i * np + j]);
+      hold = every > 0 && i % every == 0;
+    }
+    const bool ft = ok && !hold, fh = ok && hold;
+    const uint32_t bt = __ballot_sync(0xffffffffu, ft), bh = __ballot_sync(0xffffffffu, fh);
+    const uint32_t below = (1u << lane) - 1u;
+    if (lane == 0) {
+      wsum[0][warp] = __popc(bt);
+      wsum[1][warp] = __popc(bh);
+    }
+    __syncthreads();
+    if (warp == 0) {  // exclusive prefix over the warps, and the totals
+      const uint32_t a0 = wsum[0][lane], b0 = wsum[1][lane];
+      uint32_t a = a0, b = b0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, a, o);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, b, o);
+        if (lane >= o) {
+          a += x;
+          b += y;
+        }
+      }
+      wsum[0][lane] = a - a0;
+      wsum[1][lane] = b - b0;
+      if (lane == 31) {
+        tot[0] = a;
+        tot[1] = b;
+      }
+    }
+    __syncthreads();
+    if (i < n)
+      pos[i] = ft   ? base[0] + wsum[0][warp] + __popc(bt & below)
+               : fh ? kHeldOut | (base[1] + wsum[1][warp] + __popc(bh & below))
+                    : kDropped;
+    __syncthreads();
+    if (tid == 0) {
+      base[0] += tot[0];
+      base[1] += tot[1];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    counts[0] = base[0];
+    counts[1] = base[1];
+  }
+}
+
+// Training pairs keep the f32 parameters the gather reads; held-out pairs
+// become the f64 rows the inference path takes.
+__global__ void pairs_scatter_kernel(const float* __restrict__ th, const double* __restrict__ ll,
+                                     uint32_t n, int np, const uint32_t* __restrict__ pos,
+                                     float* __restrict__ tr_th, double* __restrict__ tr_ll,
+                                     double* __restrict__ ho_th, double* __restrict__ ho_ll) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = pos[i];
+  if (p == kDropped) return;
+  const float* src = th + (size_t)i * np;
+  if (p & kHeldOut) {
+    const uint32_t q = p & ~kHeldOut;
+    for (int j = 0; j < np; ++j) ho_th[(size_t)q * np + j] = (double)src[j];
+    ho_ll[q] = ll[i];
+  } else {
+    for (int j = 0; j < np; ++j) tr_th[(size_t)p * np + j] = src[j];
+    tr_ll[p] = ll[i];
+  }
+}
+
+// Shifted f64 sums over the training pairs (shift: the first pair, so the
+// sums of squares do not cancel): accumulator a < d is sum x_j, d <= a <
+// d + d(d+1)/2 is sum x_j x_k over the row-major upper triangle (j <= k),
+// then sum y and sum y^2.  Block (c, g) sums rows of chunk c into
+// accumulator g * blockDim.x + threadIdx.x, in row order.
+constexpr int kMomRows = 32;
+__global__ void pairs_moments_kernel(const float* __restrict__ th, const double* __restrict__ ll,
+                                     uint32_t n, int d, uint32_t chunk,
+                                     double* __restrict__ part) {
+  extern __shared__ double xs[];  // [kMomRows][d + 1]
+  const int NA = d + d * (d + 1) / 2 + 2;
+  const int a = blockIdx.y * blockDim.x + threadIdx.x;
+  int kind = 3, j = 0, k = 0;
+  if (a < d) {
+    kind = 0;
+    j = a;
+  } else if (a < NA - 2) {
+    int p = a - d;
+    while (p >= d - j) {
+      p -= d - j;
+      ++j;
+    }
+    k = j + p;
+    kind = 1;
+  } else if (a == NA - 2) {
+    kind = 2;
+  }
+  const uint32_t r0 = blockIdx.x * chunk, r1 = min(n, r0 + chunk);
+  double acc = 0.0;
+  for (uint32_t rb = r0; rb < r1; rb += kMomRows) {
+    const int rows = (int)min((uint32_t)kMomRows, r1 - rb);
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * (d + 1); e += blockDim.x) {
+      const int r = e / (d + 1), c = e % (d + 1);
+      xs[e] = c < d ? (double)th[(size_t)(rb + r) * d + c] - (double)th[c]
+                    : ll[rb + r] - ll[0];
+    }
+    __syncthreads();
+    if (a < NA) {
+      for (int r = 0; r < rows; ++r) {
+        const double* x = xs + r * (d + 1);
+        acc += kind == 0 ? x[j] : kind == 1 ? x[j] * x[k] : kind == 2 ? x[d] : x[d] * x[d];
+      }
+    }
+  }
+  if (a < NA) part[(size_t)blockIdx.x * NA + a] = acc;
+}
+
+// Lower Cholesky factor of the d x d matrix A (row-major) and its inverse;
+// false when a pivot is not positive.
+bool cholesky_inverse(int d, const std::vector<double>& A, std::vector<double>* Linv) {
+  std::vector<double> L((size_t)d * d, 0.0);
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double v = A[(size_t)i * d + j];
+      for (int k = 0; k < j; ++k) v -= L[(size_t)i * d + k] * L[(size_t)j * d + k];
+      if (i == j) {
+        if (!(v > 0.0) || !std::isfinite(v)) return false;
+        L[(size_t)i * d + i] = std::sqrt(v);
+      } else {
+        L[(size_t)i * d + j] = v / L[(size_t)j * d + j];
+      }
+    }
+  Linv->assign((size_t)d * d, 0.0);
+  for (int c = 0; c < d; ++c)  // forward substitution, column c of the inverse
+    for (int i = c; i < d; ++i) {
+      double v = i == c ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) v -= L[(size_t)i * d + k] * (*Linv)[(size_t)k * d + c];
+      (*Linv)[(size_t)i * d + c] = v / L[(size_t)i * d + i];
+    }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpum_b200_session_train_surrogate(gpum_b200_session* s, gpum_b200_mlp* m,
+                                      uint32_t holdout_every, int whiten, uint32_t n_stages,
+                                      const uint32_t* steps, const double* lrs,
+                                      float* out_loss, double* out_info, char* err,
+                                      size_t err_len) {
+  return guard(err, err_len, [&] {
+    require(s != nullptr && m != nullptr, "session or surrogate is NULL");
+    require(mlp_input_width(m) == (int)s->np,
+            "surrogate input width does not match the model's parameter count");
+    require(holdout_every != 1, "holdout_every = 1 would hold out every pair");
+    s->settle_recording();
+    const uint64_t n64 = s->rec_count;
+    require(n64 >= 2 && s->rec_ll.p, "fewer than two recorded pairs");
+    require(n64 < kHeldOut, "too many recorded pairs", GPUM_ERR_UNSUPPORTED);
+    const uint32_t n = (uint32_t)n64;
+    const int d = (int)s->np;
+    s->check_device_error();
+    cudaStream_t st = s->stream;
+    DBuf<uint32_t> pos, counts;
+    pos.ensure(n);
+    counts.ensure(2);
+    pairs_split_kernel<<<1, kSplitThreads, 0, st>>>(s->rec_theta.p, s->rec_ll.p, n, d,
+                                                    holdout_every, pos.p, counts.p);
+    GPUM_CK(cudaGetLastError());
+    uint32_t cnt[2] = {0, 0};
+    GPUM_CK(cudaMemcpyAsync(cnt, counts.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaStreamSynchronize(st));
+    const uint32_t n_tr = cnt[0], n_ho = cnt[1];
+    require(n_tr >= 2, "fewer than two finite training pairs");
+    DBuf<float> tr_th;
+    DBuf<double> tr_ll, ho_th, ho_ll;
+    tr_th.ensure((size_t)n_tr * d);
+    tr_ll.ensure(n_tr);
+    ho_th.ensure((size_t)std::max<uint32_t>(n_ho, 1) * d);
+    ho_ll.ensure(std::max<uint32_t>(n_ho, 1));
+    pairs_scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->rec_theta.p, s->rec_ll.p, n, d,
+                                                           pos.p, tr_th.p, tr_ll.p, ho_th.p,
+                                                           ho_ll.p);
+    GPUM_CK(cudaGetLastError());
+
+    // Moments of the training pairs (f64, fixed order) -> the normaliser.
+    const int NA = d + d * (d + 1) / 2 + 2;
+    const uint32_t nchunk = std::max<uint32_t>(1, std::min<uint32_t>(64, n_tr / 2048));
+    const uint32_t chunk = (n_tr + nchunk - 1) / nchunk;
+    const size_t msmem = (size_t)kMomRows * (d + 1) * sizeof(double);
+    if (msmem > 48 * 1024)
+      GPUM_CK(cudaFuncSetAttribute(pairs_moments_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
+    DBuf<double> part;
+    part.ensure((size_t)nchunk * NA);
+    pairs_moments_kernel<<<dim3(nchunk, (NA + 255) / 256), 256, msmem, st>>>(
+        tr_th.p, tr_ll.p, n_tr, d, chunk, part.p);
+    GPUM_CK(cudaGetLastError());
+    std::vector<double> hp((size_t)nchunk * NA);
+    std::vector<float> x0(d);
+    double y0 = 0.0;
+    GPUM_CK(cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaMemcpyAsync(x0.data(), tr_th.p, d * sizeof(float), cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaMemcpyAsync(&y0, tr_ll.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GPUM_CK(cudaStreamSynchronize(st));
+    std::vector<double> S(NA, 0.0);
+    for (uint32_t c = 0; c < nchunk; ++c)
+      for (int a = 0; a < NA; ++a) S[a] += hp[(size_t)c * NA + a];
+    const double N = (double)n_tr;
+    std::vector<double> mean(d), cov((size_t)d * d);
+    for (int j = 0; j < d; ++j) mean[j] = (double)x0[j] + S[j] / N;
+    for (int j = 0, a = d; j < d; ++j)
+      for (int k = j; k < d; ++k, ++a) {
+        const double c = (S[a] - S[j] * S[k] / N) / (N - 1.0);
+        cov[(size_t)j * d + k] = cov[(size_t)k * d + j] = c;
+      }
+    const double sy = S[NA - 2], syy = S[NA - 1];
+    const double ymean = y0 + sy / N;
+    const double yvar = (syy - sy * sy / N) / N;
+    const double ysd = yvar > 0.0 && std::isfinite(yvar) ? std::sqrt(yvar) : 1.0;
+    char merr[512];
+    bool whitened = false;
+    if (whiten && d > 1) {
+      double md = 0.0;
+      for (int j = 0; j < d; ++j) md += cov[(size_t)j * d + j];
+      md = std::max(md / d, 1e-300);
+      std::vector<double> cj = cov, Linv;
+      for (int j = 0; j < d; ++j) cj[(size_t)j * d + j] += 1e-10 * md;
+      if (cholesky_inverse(d, cj, &Linv)) {
+        const int rc = gpum_b200_mlp_set_whitening(m, mean.data(), Linv.data(), ymean, ysd,
+                                                   merr, sizeof merr);
+        if (rc != GPUM_OK) throw Failure{rc, merr};
+        whitened = true;
+      }
+    }
+    if (!whitened) {
+      std::vector<double> sd(d);
+      for (int j = 0; j < d; ++j) {
+        const double v = cov[(size_t)j * d + j] * (N - 1.0) / N;
+        sd[j] = v > 0.0 && std::isfinite(v) ? std::sqrt(v) : 1.0;
+      }
+      const int rc = gpum_b200_mlp_set_normalizer(m, mean.data(), sd.data(), ymean, ysd, merr,
+                                                  sizeof merr);
+      if (rc != GPUM_OK) throw Failure{rc, merr};
+    }
+
+    std::string e;
+    int rc = mlp_train_device(m, tr_th.p, tr_ll.p, n_tr, n_stages, steps, lrs, out_loss, &e);
+    if (rc != GPUM_OK) throw Failure{rc, e};
+
+    double resid_sd = std::nan("");
+    if (n_ho > 0) {  // residual spread of the trained network on the held-out pairs
+      DBuf<double> pred;
+      pred.ensure(n_ho);
+      rc = mlp_infer(m, ho_th.p, (int)n_ho, d, pred.p, st, &e);
+      if (rc != GPUM_OK) throw Failure{rc, e};
+      std::vector<double> hpred(n_ho), hll(n_ho);
+      GPUM_CK(cudaMemcpyAsync(hpred.data(), pred.p, n_ho * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+      GPUM_CK(cudaMemcpyAsync(hll.data(), ho_ll.p, n_ho * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+      GPUM_CK(cudaStreamSynchronize(st));
+      double mr = 0.0, m2 = 0.0;
+      for (uint32_t i = 0; i < n_ho; ++i) mr += hpred[i] - hll[i];
+      mr /= n_ho;
+      for (uint32_t i = 0; i < n_ho; ++i) {
+        const double r = hpred[i] - hll[i] - mr;
+        m2 += r * r;
+      }
+      resid_sd = std::sqrt(m2 / n_ho);
+    }
+    if (out_info) {
+      out_info[0] = (double)n;
+      out_info[1] = (double)n_tr;
+      out_info[2] = (double)n_ho;
+      out_info[3] = resid_sd;
+      out_info[4] = whitened ? 1.0 : 0.0;
+    }
   });
 }
 

@@ -965,80 +965,123 @@ int gpum_b200_mlp_set_whitening(gpum_b200_mlp* m, const double* xmean, const dou
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// Checks a learning-rate schedule; returns its total step count.
+uint64_t schedule_steps(uint32_t n_stages, const uint32_t* steps, const double* lrs) {
+  need(n_stages == 0 || (steps && lrs), "NULL argument");
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n_stages; ++k) {
+    need(std::isfinite(lrs[k]) && lrs[k] >= 0.0, "learning rates must be finite and >= 0");
+    total += steps[k];
+  }
+  need(total <= (1u << 24), "more than 2^24 steps");
+  return total;
+}
+
+// Adam on n_pairs device-resident pairs (theta f32 [n][d], ll f64 [n]) with
+// a learning-rate schedule of `total` steps; out_loss (may be NULL) receives
+// every step's mean squared error.
+void train_on_device(gpum_b200_mlp* m, const float* dth, const double* dll, size_t n_pairs,
+                     uint32_t n_stages, const uint32_t* steps, const double* lrs, uint64_t total,
+                     float* out_loss) {
+  m->losses.alloc(total);
+  const uint32_t base = m->steps_done;
+  // One step: its kernels read the step from the device counter the
+  // reduction advances and the learning rate from device memory, so one
+  // captured CUDA graph serves all steps of all stages.
+  auto one_step = [&] {
+    mlp_gather<<<m->B / kGatherRows, 32 * kGatherRows, 0, m->st>>>(
+        dth, dll, n_pairs, m->d, m->dp, m->B, 1, m->seed, m->ctr.p, m->xmean.p,
+        m->xinv.p, m->xw_or_null(), m->ymean, m->yinv, m->Xh.p, m->XTh.p, m->t.p);
+    MLP_CK(cudaGetLastError());
+    m->forward(m->B, m->B, m->t.p);
+    m->backward_and_update(1, m->losses.p, base, (uint32_t)total);
+  };
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool first = true;
+  cudaError_t le = cudaSuccess;
+  for (uint32_t k = 0; k < n_stages && le == cudaSuccess; ++k) {
+    if (steps[k] == 0) continue;
+    const float lr_f = (float)lrs[k];
+    MLP_CK(cudaMemcpyAsync(m->lr.p, &lr_f, sizeof lr_f, cudaMemcpyHostToDevice, m->st));
+    MLP_CK(cudaStreamSynchronize(m->st));  // lr_f is a stack value
+    uint32_t left = steps[k];
+    if (first) {
+      one_step();  // eagerly: sets every kernel attribute outside capture
+      first = false;
+      --left;
+    }
+    if (left > 0 && !exec) {
+      MLP_CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
+      try {
+        one_step();
+      } catch (...) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(m->st, &g2);
+        if (g2) cudaGraphDestroy(g2);
+        throw;
+      }
+      MLP_CK(cudaStreamEndCapture(m->st, &graph));
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        MLP_CK(ie);
+      }
+    }
+    for (; left > 0 && le == cudaSuccess; --left) le = cudaGraphLaunch(exec, m->st);
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  MLP_CK(le);
+  m->steps_done += (uint32_t)total;
+  std::vector<float> losses(total);
+  MLP_CK(cudaMemcpyAsync(losses.data(), m->losses.p, total * sizeof(float),
+                         cudaMemcpyDeviceToHost, m->st));
+  m->check_err();
+  if (out_loss)
+    for (uint64_t s = 0; s < total; ++s) out_loss[s] = losses[s] / (float)m->B;
+}
+
+}  // namespace
+
+namespace gpum {
+int mlp_input_width(const gpum_b200_mlp* m) { return m ? m->d : 0; }
+
+// Training from pairs already on the device (the session's recorded pairs).
+int mlp_train_device(gpum_b200_mlp* m, const float* dth, const double* dll, size_t n_pairs,
+                     uint32_t n_stages, const uint32_t* steps, const double* lrs,
+                     float* out_loss, std::string* err) {
+  char buf[512];
+  const int rc = mlp_guard(buf, sizeof buf, [&] {
+    need(m && dth && dll, "NULL argument");
+    need(n_pairs >= 1 && n_pairs <= (1u << 28), "n_pairs must be in 1..2^28");
+    const uint64_t total = schedule_steps(n_stages, steps, lrs);
+    if (total > 0) train_on_device(m, dth, dll, n_pairs, n_stages, steps, lrs, total, out_loss);
+  });
+  if (rc != GPUM_OK && err) *err = buf;
+  return rc;
+}
+}  // namespace gpum
+
+extern "C" {
+
 int gpum_b200_mlp_train_stages(gpum_b200_mlp* m, const double* theta, const double* ll,
                                size_t n_pairs, uint32_t n_stages, const uint32_t* steps,
                                const double* lrs, float* out_loss, char* err, size_t err_len) {
   return mlp_guard(err, err_len, [&] {
-    need(m && theta && ll && (n_stages == 0 || (steps && lrs)), "NULL argument");
+    need(m && theta && ll, "NULL argument");
     need(n_pairs >= 1 && n_pairs <= (1u << 28), "n_pairs must be in 1..2^28");
-    uint64_t total = 0;
-    for (uint32_t k = 0; k < n_stages; ++k) {
-      need(std::isfinite(lrs[k]) && lrs[k] >= 0.0, "learning rates must be finite and >= 0");
-      total += steps[k];
-    }
-    need(total <= (1u << 24), "more than 2^24 steps");
+    const uint64_t total = schedule_steps(n_stages, steps, lrs);
     if (total == 0) return;
     // The pairs are uploaded once for every stage.
     Buf<float> dth;
     Buf<double> dll;
     upload_pairs(m, theta, ll, n_pairs, dth, dll);
-    m->losses.alloc(total);
-    const uint32_t base = m->steps_done;
-    // One step: its kernels read the step from the device counter the
-    // reduction advances and the learning rate from device memory, so one
-    // captured CUDA graph serves all steps of all stages.
-    auto one_step = [&] {
-      mlp_gather<<<m->B / kGatherRows, 32 * kGatherRows, 0, m->st>>>(
-          dth.p, dll.p, n_pairs, m->d, m->dp, m->B, 1, m->seed, m->ctr.p, m->xmean.p,
-          m->xinv.p, m->xw_or_null(), m->ymean, m->yinv, m->Xh.p, m->XTh.p, m->t.p);
-      MLP_CK(cudaGetLastError());
-      m->forward(m->B, m->B, m->t.p);
-      m->backward_and_update(1, m->losses.p, base, (uint32_t)total);
-    };
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    bool first = true;
-    cudaError_t le = cudaSuccess;
-    for (uint32_t k = 0; k < n_stages && le == cudaSuccess; ++k) {
-      if (steps[k] == 0) continue;
-      const float lr_f = (float)lrs[k];
-      MLP_CK(cudaMemcpyAsync(m->lr.p, &lr_f, sizeof lr_f, cudaMemcpyHostToDevice, m->st));
-      MLP_CK(cudaStreamSynchronize(m->st));  // lr_f is a stack value
-      uint32_t left = steps[k];
-      if (first) {
-        one_step();  // eagerly: sets every kernel attribute outside capture
-        first = false;
-        --left;
-      }
-      if (left > 0 && !exec) {
-        MLP_CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeThreadLocal));
-        try {
-          one_step();
-        } catch (...) {
-          cudaGraph_t g2 = nullptr;
-          cudaStreamEndCapture(m->st, &g2);
-          if (g2) cudaGraphDestroy(g2);
-          throw;
-        }
-        MLP_CK(cudaStreamEndCapture(m->st, &graph));
-        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-        if (ie != cudaSuccess) {
-          cudaGraphDestroy(graph);
-          MLP_CK(ie);
-        }
-      }
-      for (; left > 0 && le == cudaSuccess; --left) le = cudaGraphLaunch(exec, m->st);
-    }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    MLP_CK(le);
-    m->steps_done += (uint32_t)total;
-    std::vector<float> losses(total);
-    MLP_CK(cudaMemcpyAsync(losses.data(), m->losses.p, total * sizeof(float),
-                           cudaMemcpyDeviceToHost, m->st));
-    m->check_err();
-    if (out_loss)
-      for (uint64_t s = 0; s < total; ++s) out_loss[s] = losses[s] / (float)m->B;
+    train_on_device(m, dth.p, dll.p, n_pairs, n_stages, steps, lrs, total, out_loss);
   });
 }
 

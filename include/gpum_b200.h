@@ -366,6 +366,23 @@ GPUM_API int gpum_b200_session_record(gpum_b200_session* s, uint64_t capacity, c
 GPUM_API int gpum_b200_session_recorded(gpum_b200_session* s, float* out_theta, double* out_ll,
                                         uint64_t max_pairs, uint64_t* n_pairs, char* err,
                                         size_t err_len);
+/* Fits the surrogate to the pairs this session recorded without copying them
+ * to the host.  Pair i is held out when holdout_every > 0 and i %
+ * holdout_every == 0 (holdout_every = 1 is refused); pairs with a non-finite
+ * value are dropped.  The normaliser comes from the training pairs' f64
+ * moments: with `whiten` (and n_params > 1) inputs are whitened by the
+ * inverse Cholesky factor of their covariance (ddof 1, diagonal jitter
+ * 1e-10 x its mean), else standardised per coordinate; the target is
+ * standardised (ddof 0).  Then Adam with the learning-rate schedule of
+ * mlp_train_stages.  out_loss (may be NULL) receives sum(steps) losses;
+ * out_info (may be NULL) receives 5 values: pairs recorded, training pairs,
+ * held-out pairs, the held-out residual standard deviation of the trained
+ * network (NaN without held-out pairs), 1 if the inputs were whitened. */
+GPUM_API int gpum_b200_session_train_surrogate(gpum_b200_session* s, gpum_b200_mlp* m,
+                                               uint32_t holdout_every, int whiten,
+                                               uint32_t n_stages, const uint32_t* steps,
+                                               const double* lrs, float* out_loss,
+                                               double* out_info, char* err, size_t err_len);
 /* Two-stage Metropolis-Hastings (Christen & Fox): the surrogate screens each
  * proposal (stage 1) and only survivors are evaluated exactly (stage 2), so
  * the chains target the exact tempered posterior.  Same arguments and

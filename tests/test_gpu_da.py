@@ -60,6 +60,66 @@ def test_recording_stores_every_exact_proposal(gpu):
         assert s.recorded()[0].shape[0] == 0
 
 
+@pytest.mark.parametrize("whiten", [True, False])
+def test_surrogate_fit_on_device_matches_the_host_path(gpu, whiten):
+    # The device path (split, moments, normaliser, training, held-out check)
+    # against the same steps done from host copies of the pairs: every tenth
+    # pair held out, the normaliser from numpy, train_stages on the rest.
+    w = W.make("logistic", n_obs=3000, p=6)
+    m = w.model
+    d = m.n_params
+    C, n = 64, 40
+    rng = np.random.default_rng(4)
+    init = w.truth["beta"] + rng.normal(0, 0.05, (C, d))
+    sd = np.full((C, d), 0.02)
+    stages = [(60, 2e-3), (30, 5e-4)]
+    with _session(gpu, w) as s:
+        s.record(n * C)
+        s.run(init, sd, np.ones(C), n, 5, 0)
+        theta, ll = s.recorded()
+        net = gpu.Surrogate(d, hidden=128, batch=1024, seed=3)
+        loss, info = s.train_surrogate(net, stages, holdout_every=10, whiten=whiten)
+    idx = np.arange(theta.shape[0])
+    tr, ho = idx % 10 != 0, idx % 10 == 0
+    assert info["pairs"] == n * C
+    assert info["train_pairs"] == tr.sum() and info["holdout_pairs"] == ho.sum()
+    assert info["whitened"] == whiten
+    assert loss.shape == (90,) and np.all(np.isfinite(loss))
+    th64 = theta.astype(np.float64)
+    ref = gpu.Surrogate(d, hidden=128, batch=1024, seed=3)
+    ref.fit_normalizer(th64[tr], ll[tr], whiten=whiten)
+    ref_loss = ref.train_stages(th64[tr], ll[tr], stages)
+    pd, pr = net.predict(th64[ho]), ref.predict(th64[ho])
+    # the normalisers agree to f64 rounding, so the two trainings follow each
+    # other to within f32 noise
+    scale = np.std(ll)
+    assert np.max(np.abs(pd - pr)) <= 1e-3 * scale, np.max(np.abs(pd - pr)) / scale
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-3, atol=1e-6)
+    r = pd - ll[ho]
+    assert info["holdout_resid_sd"] == pytest.approx(np.std(r), rel=1e-9)
+    net.close()
+    ref.close()
+
+
+def test_surrogate_fit_on_device_refuses_bad_arguments(gpu):
+    w = W.make("logistic", n_obs=500, p=3)
+    m = w.model
+    d = m.n_params
+    with _session(gpu, w) as s:
+        net = gpu.Surrogate(d + 1, hidden=128, batch=128, seed=1)
+        with pytest.raises(gpu.GpumError, match="input width"):
+            s.train_surrogate(net, [(5, 1e-3)])
+        net.close()
+        net = gpu.Surrogate(d, hidden=128, batch=128, seed=1)
+        with pytest.raises(gpu.GpumError, match="fewer than two"):
+            s.train_surrogate(net, [(5, 1e-3)])
+        s.record(100)
+        s.run(np.tile(w.truth["beta"], (4, 1)), np.full((4, d), 0.01), np.ones(4), 3, 1, 0)
+        with pytest.raises(gpu.GpumError, match="holdout_every"):
+            s.train_surrogate(net, [(5, 1e-3)], holdout_every=1)
+        net.close()
+
+
 @pytest.mark.parametrize("temps_kind", ["cold", "tempered"])
 def test_two_stage_trajectories_match_oracle(gpu, temps_kind):
     w = W.make("logistic", n_obs=2048, p=4)
