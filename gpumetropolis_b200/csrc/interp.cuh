@@ -7,7 +7,8 @@
 //     kernel parameter), read at a warp-uniform pc, so the dispatch is a
 //     uniform indirect branch with no divergence;
 //   * every case names its stack slot at compile time, so the operand stack
-//     `s[D][G]` is an array of registers (never local memory);
+//     `s[D][G/2]` (chain pairs) is an array of registers (never local
+//     memory), and the arithmetic runs on two-wide FP32 instructions;
 //   * each thread carries G chains through the same instruction, amortising
 //     one dispatch over G chain-observations; the 32 lanes of a warp take 32
 //     consecutive observations of the shared-memory tile;
@@ -31,275 +32,196 @@ struct __align__(16) EvalProg {
 
 enum HeavyKind : int { H_NONE = -1, H_DIV = 0, H_POW = 1, H_LGAMMA = 2 };
 
-// The G parameters of this thread's chains for one parameter index: one
-// broadcast 16- or 8-byte shared load per 4 or 2 chains.
+// The G parameters of this thread's chains for one parameter index, as G/2
+// pairs: one broadcast 16- or 8-byte shared load per 4 or 2 chains.
 template <int G>
-__device__ __forceinline__ void load_params(const float* __restrict__ p, float (&v)[G]) {
+__device__ __forceinline__ void load_params2(const float* __restrict__ p,
+                                             float2 (&v)[G / 2]) {
   if constexpr (G % 4 == 0) {
 #pragma unroll
     for (int g = 0; g < G; g += 4) {
       const float4 q = *reinterpret_cast<const float4*>(p + g);
-      v[g] = q.x; v[g + 1] = q.y; v[g + 2] = q.z; v[g + 3] = q.w;
-    }
-  } else if constexpr (G % 2 == 0) {
-#pragma unroll
-    for (int g = 0; g < G; g += 2) {
-      const float2 q = *reinterpret_cast<const float2*>(p + g);
-      v[g] = q.x; v[g + 1] = q.y;
+      v[g / 2] = make_float2(q.x, q.y);
+      v[g / 2 + 1] = make_float2(q.z, q.w);
     }
   } else {
 #pragma unroll
-    for (int g = 0; g < G; ++g) v[g] = p[g];
+    for (int g = 0; g < G; g += 2) v[g / 2] = *reinterpret_cast<const float2*>(p + g);
   }
 }
 
-// Interpret the program once for G chains at one observation.
+// Interpret the program once for G chains at one observation.  The stack
+// holds the chains as pairs, so the arithmetic runs on sm_100's two-wide
+// FP32 instructions (FADD2, FMUL2, FFMA2; subtraction and negation as exact
+// FFMA2 / FMUL2 by -1), which round each half exactly like the scalar
+// instruction: the values are those of one chain per instruction.
+//   s  : slot S, chains 2h and 2h+1 in s[S][h]
 //   xo : this lane's observation inside the tile; column j is at xo[j*T]
 //   pc0: this thread's first chain in the param tile; param p, chain g at
 //        pc0[p*CG + g]  (16-byte aligned; G is a multiple of 2)
 //   hsm: this thread's operand scratch for the shared expensive ops, 2*G
 //        floats at a stride of kInterpThreads (the block's thread count)
 template <int G, int D>
-__device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
+__device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G / 2],
                                            const float* __restrict__ xo, int T,
                                            const float* __restrict__ pc0, int CG,
                                            float* __restrict__ hsm) {
+  static_assert(G % 2 == 0, "chains are processed in pairs");
+  constexpr int H = G / 2;
   const uint32_t n = pg.n_uops;
   // Saved subtrees (K_SAVEk / K_LOADk): registers, since every case names
   // its save index at compile time.  The sixteen-chain variant keeps one, the
   // deep-stack variants none (the compiler saves nothing for stacks deeper
   // than kMaxSavedDepth).
   constexpr int NS = D > kMaxSavedDepth ? 0 : (G >= 16 ? 1 : kMaxSaves);
-  float sv[NS > 0 ? NS : 1][G];
+  float2 sv[NS > 0 ? NS : 1][H];
   for (uint32_t pc = 0; pc < n; ++pc) {
     const uint32_t w = pg.uop[pc];
     const uint32_t a0 = (w >> kCaseBits) & 0x7FFu;
     const uint32_t a1 = w >> 22;
     int hk = H_NONE, hs = 0;
 
-#define GPUM_PL(g) pv[g]
 #define GPUM_XD(a) xo[(size_t)(a) * T]
 #define GPUM_HA(g) hsm[(g) * kInterpThreads]
 #define GPUM_HB(g) hsm[(G + (g)) * kInterpThreads]
+#define GPUM_UN(S, EXPR)                                                               \
+  if constexpr (S < D) {                                                               \
+    _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = EXPR;                      \
+  }                                                                                    \
+  break;
+#define GPUM_HEAVY2(S, KIND, BX, BY)                                                   \
+  if constexpr (S < D) {                                                               \
+    _Pragma("unroll") for (int h = 0; h < H; ++h) {                                    \
+      GPUM_HA(2 * h) = s[S][h].x;                                                      \
+      GPUM_HA(2 * h + 1) = s[S][h].y;                                                  \
+      GPUM_HB(2 * h) = BX;                                                             \
+      GPUM_HB(2 * h + 1) = BY;                                                         \
+    }                                                                                  \
+    hk = KIND;                                                                         \
+    hs = S;                                                                            \
+  }                                                                                    \
+  break;
 #define GPUM_SLOT(S)                                                                   \
-  case S * NKIND + K_PUSH_C:                                                           \
-    if constexpr (S < D) {                                                             \
-      const float v = pg.cst[a0];                                                      \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = v;                       \
-    }                                                                                  \
-    break;                                                                             \
+  case S * NKIND + K_PUSH_C: GPUM_UN(S, gm2(pg.cst[a0]))                               \
   case S * NKIND + K_PUSH_P:                                                           \
-    if constexpr (S < D) {                                                             \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = GPUM_PL(g);              \
-    }                                                                                  \
+    if constexpr (S < D) load_params2<G>(pc0 + (size_t)a0 * CG, s[S]);                 \
     break;                                                                             \
-  case S * NKIND + K_PUSH_D:                                                           \
-    if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a0);                                                     \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = v;                       \
-    }                                                                                  \
-    break;                                                                             \
+  case S * NKIND + K_PUSH_D: GPUM_UN(S, gm2(GPUM_XD(a0)))                              \
   case S * NKIND + K_ADD:                                                              \
     if constexpr (S + 1 < D) {                                                         \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + s[S + 1][g];   \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_add(s[S][h], s[S + 1][h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SUB:                                                              \
     if constexpr (S + 1 < D) {                                                         \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - s[S + 1][g];   \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_sub(s[S][h], s[S + 1][h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_MUL:                                                              \
     if constexpr (S + 1 < D) {                                                         \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * s[S + 1][g];   \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_mul(s[S][h], s[S + 1][h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_DIV:                                                              \
+    if constexpr (S + 1 < D) { GPUM_HEAVY2(S, H_DIV, s[S + 1][h].x, s[S + 1][h].y) }   \
+    break;                                                                             \
   case S * NKIND + K_POW:                                                              \
-    if constexpr (S + 1 < D) {                                                         \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        GPUM_HA(g) = s[S][g];                                                          \
-        GPUM_HB(g) = s[S + 1][g];                                                      \
-      }                                                                                \
-      hk = ((w & kCaseMask) == S * NKIND + K_DIV) ? H_DIV : H_POW;                         \
-      hs = S;                                                                          \
-    }                                                                                  \
+    if constexpr (S + 1 < D) { GPUM_HEAVY2(S, H_POW, s[S + 1][h].x, s[S + 1][h].y) }   \
     break;                                                                             \
-  case S * NKIND + K_ADD_C:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = pg.cst[a0];                                                      \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_SUB_C:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = pg.cst[a0];                                                      \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_MUL_C:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = pg.cst[a0];                                                      \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_DIV_C:                                                            \
-  case S * NKIND + K_POW_C:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = pg.cst[a0];                                                      \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        GPUM_HA(g) = s[S][g];                                                          \
-        GPUM_HB(g) = v;                                                                \
-      }                                                                                \
-      hk = ((w & kCaseMask) == S * NKIND + K_DIV_C) ? H_DIV : H_POW;                       \
-      hs = S;                                                                          \
-    }                                                                                  \
-    break;                                                                             \
+  case S * NKIND + K_ADD_C: GPUM_UN(S, gm2_add(s[S][h], gm2(pg.cst[a0])))              \
+  case S * NKIND + K_SUB_C: GPUM_UN(S, gm2_sub(s[S][h], gm2(pg.cst[a0])))              \
+  case S * NKIND + K_MUL_C: GPUM_UN(S, gm2_mul(s[S][h], gm2(pg.cst[a0])))              \
+  case S * NKIND + K_DIV_C: GPUM_HEAVY2(S, H_DIV, pg.cst[a0], pg.cst[a0])              \
+  case S * NKIND + K_POW_C: GPUM_HEAVY2(S, H_POW, pg.cst[a0], pg.cst[a0])              \
   case S * NKIND + K_ADD_P:                                                            \
     if constexpr (S < D) {                                                             \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + GPUM_PL(g);    \
+      float2 pv[H];                                                                    \
+      load_params2<G>(pc0 + (size_t)a0 * CG, pv);                                      \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_add(s[S][h], pv[h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SUB_P:                                                            \
     if constexpr (S < D) {                                                             \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - GPUM_PL(g);    \
+      float2 pv[H];                                                                    \
+      load_params2<G>(pc0 + (size_t)a0 * CG, pv);                                      \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_sub(s[S][h], pv[h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_MUL_P:                                                            \
     if constexpr (S < D) {                                                             \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * GPUM_PL(g);    \
+      float2 pv[H];                                                                    \
+      load_params2<G>(pc0 + (size_t)a0 * CG, pv);                                      \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_mul(s[S][h], pv[h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_DIV_P:                                                            \
   case S * NKIND + K_POW_P:                                                            \
     if constexpr (S < D) {                                                             \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        GPUM_HA(g) = s[S][g];                                                          \
-        GPUM_HB(g) = GPUM_PL(g);                                                       \
+      const float* pp = pc0 + (size_t)a0 * CG;                                         \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) {                                  \
+        GPUM_HA(2 * h) = s[S][h].x;                                                    \
+        GPUM_HA(2 * h + 1) = s[S][h].y;                                                \
+        GPUM_HB(2 * h) = pp[2 * h];                                                    \
+        GPUM_HB(2 * h + 1) = pp[2 * h + 1];                                            \
       }                                                                                \
-      hk = ((w & kCaseMask) == S * NKIND + K_DIV_P) ? H_DIV : H_POW;                       \
+      hk = ((w & kCaseMask) == S * NKIND + K_DIV_P) ? H_DIV : H_POW;                   \
       hs = S;                                                                          \
     }                                                                                  \
     break;                                                                             \
-  case S * NKIND + K_ADD_D:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a0);                                                     \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] + v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_SUB_D:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a0);                                                     \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] - v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_MUL_D:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a0);                                                     \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * v;             \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_DIV_D:                                                            \
-  case S * NKIND + K_POW_D:                                                            \
-    if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a0);                                                     \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) {                                  \
-        GPUM_HA(g) = s[S][g];                                                          \
-        GPUM_HB(g) = v;                                                                \
-      }                                                                                \
-      hk = ((w & kCaseMask) == S * NKIND + K_DIV_D) ? H_DIV : H_POW;                       \
-      hs = S;                                                                          \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_NEG:                                                              \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = -s[S][g];                \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_EXP:                                                              \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = expf(s[S][g]);           \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_LOG:                                                              \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = logf(s[S][g]);           \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_SQRT:                                                             \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sqrtf(s[S][g]);          \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_LGAMMA:                                                           \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) GPUM_HA(g) = s[S][g];              \
-      hk = H_LGAMMA;                                                                   \
-      hs = S;                                                                          \
-    }                                                                                  \
-    break;                                                                             \
-  case S * NKIND + K_SQR:                                                              \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = s[S][g] * s[S][g];       \
-    }                                                                                  \
-    break;                                                                             \
+  case S * NKIND + K_ADD_D: GPUM_UN(S, gm2_add(s[S][h], gm2(GPUM_XD(a0))))             \
+  case S * NKIND + K_SUB_D: GPUM_UN(S, gm2_sub(s[S][h], gm2(GPUM_XD(a0))))             \
+  case S * NKIND + K_MUL_D: GPUM_UN(S, gm2_mul(s[S][h], gm2(GPUM_XD(a0))))             \
+  case S * NKIND + K_DIV_D: GPUM_HEAVY2(S, H_DIV, GPUM_XD(a0), GPUM_XD(a0))            \
+  case S * NKIND + K_POW_D: GPUM_HEAVY2(S, H_POW, GPUM_XD(a0), GPUM_XD(a0))            \
+  case S * NKIND + K_NEG: GPUM_UN(S, gm2_neg(s[S][h]))                                 \
+  case S * NKIND + K_EXP: GPUM_UN(S, gm2_exp(s[S][h]))                                 \
+  case S * NKIND + K_LOG: GPUM_UN(S, gm2_log(s[S][h]))                                 \
+  case S * NKIND + K_SQRT: GPUM_UN(S, gm2_sqrt(s[S][h]))                               \
+  case S * NKIND + K_LGAMMA: GPUM_HEAVY2(S, H_LGAMMA, 0.0f, 0.0f)                      \
+  case S * NKIND + K_SQR: GPUM_UN(S, gm2_mul(s[S][h], s[S][h]))                        \
   case S * NKIND + K_FMA_PD:                                                           \
     if constexpr (S < D) {                                                             \
-      const float v = GPUM_XD(a1);                                                     \
-      float pv[G];                                                                     \
-      load_params<G>(pc0 + (size_t)a0 * CG, pv);                                       \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
+      const float2 v = gm2(GPUM_XD(a1));                                               \
+      float2 pv[H];                                                                    \
+      load_params2<G>(pc0 + (size_t)a0 * CG, pv);                                      \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_fma(pv[h], v, s[S][h]); \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_DOT:                                                              \
     if constexpr (S < D) {                                                             \
       for (uint32_t k = 0; k < a1; ++k) {                                              \
         const uint32_t tw = pg.term[a0 + k];                                           \
-        const float v = GPUM_XD(tw >> 11);                                             \
-        float pv[G];                                                                   \
-        load_params<G>(pc0 + (size_t)(tw & 0x7FFu) * CG, pv);                          \
-        _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = fmaf(GPUM_PL(g), v, s[S][g]); \
+        const float2 v = gm2(GPUM_XD(tw >> 11));                                       \
+        float2 pv[H];                                                                  \
+        load_params2<G>(pc0 + (size_t)(tw & 0x7FFu) * CG, pv);                         \
+        _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_fma(pv[h], v, s[S][h]); \
       }                                                                                \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SAVE0:                                                            \
     if constexpr (S < D && NS > 0) {                                                   \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) sv[0][g] = s[S][g];                \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) sv[0][h] = s[S][h];                \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_LOAD0:                                                            \
     if constexpr (S < D && NS > 0) {                                                   \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sv[0][g];                \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = sv[0][h];                \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SAVE1:                                                            \
     if constexpr (S < D && NS > 1) {                                                   \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) sv[NS - 1][g] = s[S][g];           \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) sv[NS - 1][h] = s[S][h];           \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_LOAD1:                                                            \
     if constexpr (S < D && NS > 1) {                                                   \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = sv[NS - 1][g];           \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = sv[NS - 1][h];           \
     }                                                                                  \
     break;                                                                             \
-  case S * NKIND + K_SOFTPLUS:                                                         \
-    if constexpr (S < D) {                                                             \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = gm_softplus(s[S][g]);    \
-    }                                                                                  \
-    break;                                                                             \
+  case S * NKIND + K_SOFTPLUS: GPUM_UN(S, gm2_softplus(s[S][h]))                       \
   case S * NKIND + K_SOFTPLUS1:                                                        \
     if constexpr (S + 1 < D) {                                                         \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = gm_softplus(s[S + 1][g]); \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_softplus(s[S + 1][h]); \
     }                                                                                  \
     break;
 
@@ -333,7 +255,8 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
 #undef GPUM_SLOTS_16
 #undef GPUM_SLOTS_32
 #undef GPUM_SLOT
-#undef GPUM_PL
+#undef GPUM_UN
+#undef GPUM_HEAVY2
 #undef GPUM_XD
 
     if (hk != H_NONE) {  // warp-uniform
@@ -346,11 +269,12 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float (&s)[D][G],
                                  : (hk == H_POW ? powf(x, GPUM_HB(g)) : lgammaf(x));
       }
       // Write back to the slot named by the case (a second uniform switch).
-#define GPUM_WB(S)                                                        \
-  case S:                                                                 \
-    if constexpr (S < D) {                                                \
-      _Pragma("unroll") for (int g = 0; g < G; ++g) s[S][g] = GPUM_HA(g); \
-    }                                                                     \
+#define GPUM_WB(S)                                                              \
+  case S:                                                                       \
+    if constexpr (S < D) {                                                      \
+      _Pragma("unroll") for (int h = 0; h < H; ++h)                             \
+        s[S][h] = make_float2(GPUM_HA(2 * h), GPUM_HA(2 * h + 1));              \
+    }                                                                           \
     break;
       switch (hs) {
         GPUM_WB(0) GPUM_WB(1) GPUM_WB(2) GPUM_WB(3) GPUM_WB(4) GPUM_WB(5) GPUM_WB(6)

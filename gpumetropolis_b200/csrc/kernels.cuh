@@ -17,7 +17,7 @@ struct InterpBody {
   const float* pc0;
   int CG;
   float* hsm;
-  float s[D][G];
+  float2 s[D][G / 2];  // chain pairs
   Comp acc[G];
   __device__ InterpBody(const EvalProg& p, float* h) : pg(p), pc0(nullptr), CG(0), hsm(h) {}
   __device__ __forceinline__ void begin(const float* p0, int cg) {
@@ -30,10 +30,15 @@ struct InterpBody {
     interp_run<G, D>(pg, s, xo, T, pc0, CG, hsm);
     if (valid) {
 #pragma unroll
-      for (int g = 0; g < G; ++g) acc[g].add(s[0][g]);
+      for (int h = 0; h < G / 2; ++h) {
+        acc[2 * h].add(s[0][h].x);
+        acc[2 * h + 1].add(s[0][h].y);
+      }
     }
   }
-  __device__ __forceinline__ float last(int g) const { return s[0][g]; }
+  __device__ __forceinline__ float last(int g) const {
+    return (g & 1) ? s[0][g >> 1].y : s[0][g >> 1].x;
+  }
   __device__ __forceinline__ void end() {}
   __device__ __forceinline__ double total(int g, int) const { return acc[g].total(); }
 };
