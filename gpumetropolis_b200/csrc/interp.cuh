@@ -50,6 +50,38 @@ __device__ __forceinline__ void load_params2(const float* __restrict__ p,
   }
 }
 
+// acc += sum over n terms of param[p_k] * x[col_k] for the G chains, in term
+// order (one FFMA2 per chain pair and term).  The narrower variants load two
+// terms ahead of their multiply-adds to overlap the loads' latency.
+template <int G>
+__device__ __forceinline__ void gpum_dot(float2 (&acc)[G / 2], const uint32_t* __restrict__ tm,
+                                         uint32_t n, const float* __restrict__ xo, int T,
+                                         const float* __restrict__ pc0, int CG) {
+  constexpr int H = G / 2;
+  uint32_t k = 0;
+  if constexpr (H <= 4) {
+    for (; k + 2 <= n; k += 2) {
+      const uint32_t ta = tm[k], tb = tm[k + 1];
+      const float2 va = gm2(xo[(size_t)(ta >> 11) * T]), vb = gm2(xo[(size_t)(tb >> 11) * T]);
+      float2 pa[H], pb[H];
+      load_params2<G>(pc0 + (size_t)(ta & 0x7FFu) * CG, pa);
+      load_params2<G>(pc0 + (size_t)(tb & 0x7FFu) * CG, pb);
+#pragma unroll
+      for (int h = 0; h < H; ++h) acc[h] = gm2_fma(pa[h], va, acc[h]);
+#pragma unroll
+      for (int h = 0; h < H; ++h) acc[h] = gm2_fma(pb[h], vb, acc[h]);
+    }
+  }
+  for (; k < n; ++k) {
+    const uint32_t tw = tm[k];
+    const float2 v = gm2(xo[(size_t)(tw >> 11) * T]);
+    float2 pv[H];
+    load_params2<G>(pc0 + (size_t)(tw & 0x7FFu) * CG, pv);
+#pragma unroll
+    for (int h = 0; h < H; ++h) acc[h] = gm2_fma(pv[h], v, acc[h]);
+  }
+}
+
 // Interpret the program once for G chains at one observation.  The stack
 // holds the chains as pairs, so the arithmetic runs on sm_100's two-wide
 // FP32 instructions (FADD2, FMUL2, FFMA2; subtraction and negation as exact
@@ -75,8 +107,10 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G 
   // than kMaxSavedDepth).
   constexpr int NS = D > kMaxSavedDepth ? 0 : (G >= 16 ? 1 : kMaxSaves);
   float2 sv[NS > 0 ? NS : 1][H];
+  uint32_t wnext = n > 0 ? pg.uop[0] : 0u;
   for (uint32_t pc = 0; pc < n; ++pc) {
-    const uint32_t w = pg.uop[pc];
+    const uint32_t w = wnext;
+    wnext = pc + 1 < n ? pg.uop[pc + 1] : 0u;  // in flight while this one runs
     const uint32_t a0 = (w >> kCaseBits) & 0x7FFu;
     const uint32_t a1 = w >> 22;
     int hk = H_NONE, hs = 0;
@@ -187,15 +221,28 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G 
       _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_fma(pv[h], v, s[S][h]); \
     }                                                                                  \
     break;                                                                             \
+  case S * NKIND + K_DOTP:                                                             \
+    if constexpr (S < D) load_params2<G>(pc0 + (size_t)(pg.term[a0] & 0x7FFu) * CG, s[S]); \
+    [[fallthrough]];                                                                   \
   case S * NKIND + K_DOT:                                                              \
     if constexpr (S < D) {                                                             \
-      for (uint32_t k = 0; k < a1; ++k) {                                              \
-        const uint32_t tw = pg.term[a0 + k];                                           \
-        const float2 v = gm2(GPUM_XD(tw >> 11));                                       \
-        float2 pv[H];                                                                  \
-        load_params2<G>(pc0 + (size_t)(tw & 0x7FFu) * CG, pv);                         \
-        _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_fma(pv[h], v, s[S][h]); \
+      const uint32_t t0 = a0 + ((w & kCaseMask) == S * NKIND + K_DOTP ? 1u : 0u);      \
+      gpum_dot<G>(s[S], pg.term + t0, a1 & kDotCount, xo, T, pc0, CG);                 \
+      if (a1 & kDotSave) {                                                             \
+        if constexpr (NS > 0) {                                                        \
+          _Pragma("unroll") for (int h = 0; h < H; ++h) sv[0][h] = s[S][h];            \
+        }                                                                              \
       }                                                                                \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_SOFTPLUS_SV:                                                      \
+    if constexpr (S < D && NS > 0) {                                                   \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_softplus(sv[0][h]);  \
+    }                                                                                  \
+    break;                                                                             \
+  case S * NKIND + K_EXP_SV:                                                           \
+    if constexpr (S < D && NS > 0) {                                                   \
+      _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_exp(sv[0][h]);       \
     }                                                                                  \
     break;                                                                             \
   case S * NKIND + K_SAVE0:                                                            \

@@ -311,16 +311,38 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
       size_t j = i + 1;
       if (kind == K_FMA_PD)
         while (j < out->uops.size() && (out->uops[j] & kCaseMask) == id &&
-               j - i < (size_t)kMaxA1)
+               j - i < (size_t)kDotCount)
           ++j;
       if (kind == K_FMA_PD && j - i >= 2 &&
-          out->terms.size() + (j - i) <= (size_t)kMaxTerms) {
+          out->terms.size() + (j - i) + 1 <= (size_t)kMaxTerms) {
+        // A parameter pushed into the same slot just before starts the sum.
+        const bool from_param = !merged.empty() &&
+                                (merged.back() & kCaseMask) == slot * NKIND + K_PUSH_P;
         const uint32_t t0 = (uint32_t)out->terms.size();
+        if (from_param) {
+          out->terms.push_back((merged.back() >> kCaseBits) & 0x7FFu);
+          merged.pop_back();
+        }
         for (size_t k = i; k < j; ++k)
           out->terms.push_back(((out->uops[k] >> kCaseBits) & 0x7FFu) |
                                ((out->uops[k] >> 22) << 11));
-        merged.push_back(uop_word(K_DOT, slot, t0, (uint32_t)(j - i)));
+        uint32_t a1 = (uint32_t)(j - i);
+        // A K_SAVE0 of the sum right after it becomes the K_DOT's save flag.
+        if (j < out->uops.size() && (out->uops[j] & kCaseMask) == slot * NKIND + K_SAVE0) {
+          a1 |= kDotSave;
+          ++j;
+        }
+        merged.push_back(uop_word(from_param ? K_DOTP : K_DOT, slot, t0, a1));
         i = j;
+      } else if (kind == K_LOAD0 && j < out->uops.size() &&
+                 ((out->uops[j] & kCaseMask) == (slot - 1) * NKIND + K_SOFTPLUS1 ||
+                  (out->uops[j] & kCaseMask) == slot * NKIND + K_SOFTPLUS ||
+                  (out->uops[j] & kCaseMask) == slot * NKIND + K_EXP)) {
+        // The loaded value feeds only this operation: read it from the save.
+        const uint32_t nid = out->uops[j] & kCaseMask;
+        const uint32_t nk = nid % NKIND, ns = nid / NKIND;
+        merged.push_back(uop_word(nk == K_EXP ? K_EXP_SV : K_SOFTPLUS_SV, ns, 0, 0));
+        i = j + 1;
       } else {
         merged.push_back(w);
         ++i;

@@ -23,7 +23,11 @@
 // subtree of at least kMinSaved instructions that the program computes again
 // later (the logistic and Poisson likelihoods write their linear predictor
 // twice) is kept after its first evaluation (K_SAVEk) and every later copy
-// becomes one K_LOADk: the same FP32 value, computed once.  LOG(1 + EXP(a))
+// becomes one K_LOADk: the same FP32 value, computed once.  A last pass
+// folds micro-op pairs that always meet into one dispatch: a parameter push
+// that starts a K_DOT (K_DOTP), a K_SAVE0 of a K_DOT's result (a flag of the
+// K_DOT), and a K_LOAD0 whose value only feeds a softplus or an exponential
+// (K_SOFTPLUS_SV, K_EXP_SV).  LOG(1 + EXP(a))
 // (either operand order of the ADD) becomes one K_SOFTPLUS of a, evaluated
 // as max(a, 0) + log1p(e^-|a|): more accurate than the two calls in FP32
 // (no rounding of 1 + e^a to 1 where e^a < 2^-24) and about half the work.
@@ -49,9 +53,15 @@ enum Kind : uint32_t {
   K_LOAD0, K_LOAD1,                             // s[t] = saved[k]
   K_SOFTPLUS,                                   // s[t] = log(1 + exp(s[t]))
   K_SOFTPLUS1,                                  // s[t] = log(1 + exp(s[t+1]))
+  K_DOTP,                                       // s[t] = param[terms[a0]], then
+                                                //   the terms a0+1 .. a0+count as K_DOT
+  K_SOFTPLUS_SV,                                // s[t] = log(1 + exp(saved[0]))
+  K_EXP_SV,                                     // s[t] = exp(saved[0])
   NKIND
 };
 constexpr int kMaxSaves = 2;       // saved subtrees per program
+constexpr uint32_t kDotCount = 0x1FFu;  // K_DOT / K_DOTP a1: term count (bits 0-8)
+constexpr uint32_t kDotSave = 0x200u;   //   and bit 9: also keep the result as saved[0]
 constexpr int kMinSaved = 8;       // smallest subtree worth saving (instructions)
 constexpr int kMaxSavedDepth = 8;  // programs with deeper stacks save nothing
 constexpr int kCaseBits = 11;
