@@ -123,6 +123,11 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G 
     _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = EXPR;                      \
   }                                                                                    \
   break;
+#define GPUM_UN1(S, EXPR)                                                              \
+  if constexpr (S + 1 < D) {                                                           \
+    _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = EXPR;                      \
+  }                                                                                    \
+  break;
 #define GPUM_HEAVY2(S, KIND, BX, BY)                                                   \
   if constexpr (S < D) {                                                               \
     _Pragma("unroll") for (int h = 0; h < H; ++h) {                                    \
@@ -240,6 +245,28 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G 
       _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_softplus(sv[0][h]);  \
     }                                                                                  \
     break;                                                                             \
+  case S * NKIND + K_ADD_C1: GPUM_UN1(S, gm2_add(gm2(pg.cst[a0]), s[S + 1][h]))       \
+  case S * NKIND + K_SUB_C1: GPUM_UN1(S, gm2_sub(gm2(pg.cst[a0]), s[S + 1][h]))       \
+  case S * NKIND + K_MUL_C1: GPUM_UN1(S, gm2_mul(gm2(pg.cst[a0]), s[S + 1][h]))       \
+  case S * NKIND + K_ADD_D1: GPUM_UN1(S, gm2_add(gm2(GPUM_XD(a0)), s[S + 1][h]))      \
+  case S * NKIND + K_SUB_D1: GPUM_UN1(S, gm2_sub(gm2(GPUM_XD(a0)), s[S + 1][h]))      \
+  case S * NKIND + K_MUL_D1: GPUM_UN1(S, gm2_mul(gm2(GPUM_XD(a0)), s[S + 1][h]))      \
+  case S * NKIND + K_ADD_P1:                                                           \
+  case S * NKIND + K_SUB_P1:                                                           \
+  case S * NKIND + K_MUL_P1:                                                           \
+    if constexpr (S + 1 < D) {                                                         \
+      float2 pv[H];                                                                    \
+      load_params2<G>(pc0 + (size_t)a0 * CG, pv);                                      \
+      const uint32_t kd = (w & kCaseMask) - S * NKIND;                                 \
+      if (kd == K_ADD_P1) {                                                            \
+        _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_add(pv[h], s[S + 1][h]); \
+      } else if (kd == K_SUB_P1) {                                                     \
+        _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_sub(pv[h], s[S + 1][h]); \
+      } else {                                                                         \
+        _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_mul(pv[h], s[S + 1][h]); \
+      }                                                                                \
+    }                                                                                  \
+    break;                                                                             \
   case S * NKIND + K_EXP_SV:                                                           \
     if constexpr (S < D && NS > 0) {                                                   \
       _Pragma("unroll") for (int h = 0; h < H; ++h) s[S][h] = gm2_exp(sv[0][h]);       \
@@ -303,6 +330,7 @@ __device__ __forceinline__ void interp_run(const EvalProg& pg, float2 (&s)[D][G 
 #undef GPUM_SLOTS_32
 #undef GPUM_SLOT
 #undef GPUM_UN
+#undef GPUM_UN1
 #undef GPUM_HEAVY2
 #undef GPUM_XD
 

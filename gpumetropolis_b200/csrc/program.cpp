@@ -179,6 +179,31 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
       softplus_kind[pc] = K_SOFTPLUS;
     }
   }
+  // A push that is the left operand of an ADD, SUB or MUL whose right operand
+  // is a subtree of two or more instructions: the push is deferred to the
+  // operation (defer_kind at the operation, the push's index in defer_src).
+  // Excluded: the softplus's parts, and acc + p*x, which stays one
+  // multiply-add.
+  std::vector<char> deferred(n, 0);
+  std::vector<int> defer_kind(n, 0);
+  std::vector<size_t> defer_src(n, 0);
+  for (size_t q = 2; q < n; ++q) {
+    const uint32_t b = op[q];
+    if (b != OP_ADD && b != OP_SUB && b != OP_MUL) continue;
+    const size_t r = q - 1;           // right operand root
+    const size_t pc = start[r] - 1;   // left operand root, when it is a push
+    if (start[r] == 0 || !is_push(op[pc]) || r - start[r] + 1 < 2 || omit[pc] || omit[q])
+      continue;
+    const bool fma = b == OP_ADD && q == pc + 4 && op[pc + 3] == OP_MUL &&
+                     ((op[pc + 1] == OP_PARAM && op[pc + 2] == OP_DATA) ||
+                      (op[pc + 1] == OP_DATA && op[pc + 2] == OP_PARAM));
+    if (fma) continue;
+    const int bi = b == OP_ADD ? 0 : (b == OP_SUB ? 1 : 2);
+    const int base = op[pc] == OP_CONST ? K_ADD_C1 : (op[pc] == OP_PARAM ? K_ADD_P1 : K_ADD_D1);
+    deferred[pc] = 1;
+    defer_kind[q] = base + bi;
+    defer_src[q] = pc;
+  }
   // save_end[pc] = k + 1 when the first copy of saved subtree k ends at pc;
   // load_at[pc] = k + 1 when a later copy of it starts at pc (skipped).
   std::vector<int> save_end(n, 0), load_at(n, 0);
@@ -244,8 +269,15 @@ int compile_program(const uint32_t* code, size_t n_code, const double* consts,
       after(pc);
       continue;
     }
-    if (omit[pc]) {  // the 1, EXP and ADD of a softplus
+    if (omit[pc] || deferred[pc]) {  // the 1, EXP and ADD of a softplus; a deferred push
       ++pc;
+      continue;
+    }
+    if (defer_kind[pc]) {
+      const size_t src = defer_src[pc];
+      emit((uint32_t)defer_kind[pc], before[src], arg[src], 0);
+      ++pc;
+      after(pc);
       continue;
     }
     if (softplus_kind[pc]) {

@@ -23,7 +23,10 @@
 // subtree of at least kMinSaved instructions that the program computes again
 // later (the logistic and Poisson likelihoods write their linear predictor
 // twice) is kept after its first evaluation (K_SAVEk) and every later copy
-// becomes one K_LOADk: the same FP32 value, computed once.  A last pass
+// becomes one K_LOADk: the same FP32 value, computed once.  A push whose
+// value waits on the stack while a subtree above it is evaluated, and then
+// meets it in an add, subtract or multiply, is not pushed: the operation
+// reads the operand directly (K_ADD_D1 and the like).  A last pass
 // folds micro-op pairs that always meet into one dispatch: a parameter push
 // that starts a K_DOT (K_DOTP), a K_SAVE0 of a K_DOT's result (a flag of the
 // K_DOT), and a K_LOAD0 whose value only feeds a softplus or an exponential
@@ -57,6 +60,9 @@ enum Kind : uint32_t {
                                                 //   the terms a0+1 .. a0+count as K_DOT
   K_SOFTPLUS_SV,                                // s[t] = log(1 + exp(saved[0]))
   K_EXP_SV,                                     // s[t] = exp(saved[0])
+  K_ADD_C1, K_SUB_C1, K_MUL_C1,                 // s[t] = const op s[t+1]
+  K_ADD_P1, K_SUB_P1, K_MUL_P1,                 // s[t] = param op s[t+1]
+  K_ADD_D1, K_SUB_D1, K_MUL_D1,                 // s[t] = data op s[t+1]
   NKIND
 };
 constexpr int kMaxSaves = 2;       // saved subtrees per program
