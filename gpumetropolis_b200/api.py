@@ -98,7 +98,7 @@ def _data_matrix(model: GpumModel, data):
 # adapted random-walk proposal in the two-stage phase (screening makes
 # rejections cheap, so longer steps pay: Sherlock, Thiery & Golightly 2021);
 # whiten: inputs whitened by the pairs' covariance.
-SURROGATE_DEFAULTS = {"hidden": 128, "batch": 4096, "steps": 1200, "lr": 3e-3,
+SURROGATE_DEFAULTS = {"hidden": 128, "batch": 4096, "steps": 800, "lr": 3e-3,
                       "max_pairs": 1 << 20, "min_pairs": 2048, "seed": 1,
                       "step_scale": 1.6, "whiten": True}
 
