@@ -64,6 +64,7 @@ SIGNATURES = {
                                           _sz]),
     "gpum_b200_session_set_engine": (C.c_int, [C.c_void_p, C.c_int, _errp, _sz]),
     "gpum_b200_session_engine": (C.c_int, [C.c_void_p]),
+    "gpum_b200_session_tensor_cores": (C.c_int, [C.c_void_p]),
     "gpum_b200_session_grad_batch": (C.c_int, [C.c_void_p, _f64p, _sz, _f64p, _errp, _sz]),
     "gpum_b200_loglik_batch_noalloc": (C.c_int, [_u32p, _sz, _f64p, _sz, C.c_uint32,
                                                  C.c_void_p, C.c_uint64, C.c_uint32,
@@ -557,6 +558,11 @@ class Session:
     @property
     def engine(self) -> int:
         return int(self._lib.gpum_b200_session_engine(self._h))
+
+    @property
+    def tensor_cores(self) -> bool:
+        """Whether sums and value-only steps run the tensor-core value kernel."""
+        return self._lib.gpum_b200_session_tensor_cores(self._h) == 1
 
     def grad_batch(self, points):
         pts = _f64(points)

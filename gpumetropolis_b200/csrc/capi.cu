@@ -192,6 +192,8 @@ struct KernelChoice {
   int W = 1;                 // values per chain (1, or 1 + np with the gradient)
   bool lanes = false;        // chain-lane body: G = 32 chains per warp group
   bool grad_interp = false;  // the interpreter engine's gradient (tape) kernel
+  bool tc = false;           // the compiled engine's tensor-core value kernel
+  int threads = kThreads;    // threads per CTA
 };
 
 struct Geometry {
@@ -247,6 +249,12 @@ struct gpum_b200_session {
   TmapDesc tmap_c;
   int T_c = 256;
   uint32_t ncols_c = 0;
+  // The compiled engine's tensor-core value path (cm.tc): the data packed
+  // as [hi | lo | tail] tiles once per session; off when a product column
+  // holds a non-finite value or GPUM_B200_TENSOR_CORES=0.
+  DBuf<float> tc_data;
+  DBuf<uint32_t> tc_flag;
+  bool tc_ok = false;
   DBuf<uint32_t> d_prior_code;
   DBuf<double> d_prior_consts;
   DBuf<uint32_t> d_err;
@@ -312,8 +320,41 @@ struct gpum_b200_session {
       return false;
     }
     if (cm.n_mat > 0 && ncols > 0 && n_obs > 0) materialize();
+    if (cm.tc && n_obs > 0 && tensor_cores_enabled()) pack_tc();
     cm_ready = true;
     return true;
+  }
+
+  static bool tensor_cores_enabled() {
+    const char* e = std::getenv("GPUM_B200_TENSOR_CORES");
+    return !(e && e[0] == '0');
+  }
+
+  // The tensor-core value kernel's operand B, once per session: every tile
+  // of tc_tn observations as [hi | lo] product columns in the MMA's
+  // core-matrix layout and the tail columns (gm_tc_pack).
+  void pack_tc() {
+    const long long tn = cm.tc_tn;
+    long long ntl = (long long)((n_obs + (uint64_t)tn - 1) / (uint64_t)tn);
+    const size_t stage = (size_t)(2 * cm.tc_kp + cm.tc_ntail) * (size_t)tn;
+    tc_data.ensure(stage * (size_t)ntl);
+    tc_flag.ensure(1);
+    GPUM_CK(cudaMemsetAsync(tc_flag.p, 0, sizeof(uint32_t), stream));
+    const float* cols = cm.n_mat > 0 ? data_c.p : data.p;
+    long long nobs = (long long)n_obs, lld = (long long)ld;
+    float* xt = tc_data.p;
+    uint32_t* flag = tc_flag.p;
+    void* args[] = {(void*)&cols, (void*)&nobs, (void*)&lld, (void*)&ntl, (void*)&xt,
+                    (void*)&flag};
+    GPUM_CK(cudaLaunchKernel((const void*)cm.k_tc_pack,
+                             dim3((unsigned)((ntl * tn + 255) / 256)), dim3(256), args, 0,
+                             stream));
+    ++launches;
+    uint32_t bad = 0;
+    GPUM_CK(cudaMemcpyAsync(&bad, tc_flag.p, sizeof bad, cudaMemcpyDeviceToHost, stream));
+    GPUM_CK(cudaStreamSynchronize(stream));
+    tc_ok = bad == 0;
+    if (!tc_ok) tc_data.release();
   }
 
   // Extra columns for the compiled model's data-only operations, computed
@@ -335,7 +376,9 @@ struct gpum_b200_session {
   }
   bool ext(const KernelChoice& k) const { return k.compiled && cm.n_mat > 0; }
 
-  KernelChoice choose(bool need_grad) {
+  // `pointwise`: per-observation output, which the tensor-core value kernel
+  // does not write.
+  KernelChoice choose(bool need_grad, bool pointwise = false) {
     KernelChoice k;
     // Gradients: the compiled engine's adjoint unless the interpreter engine
     // was chosen or NVRTC cannot build the model; then the interpreted tape.
@@ -365,6 +408,13 @@ struct gpum_b200_session {
       k.lanes = need_grad ? cm.lanes_grad : cm.lanes;
       k.G = k.lanes ? 32 : (need_grad ? cm.GG : cm.G);
       k.W = need_grad ? 1 + (int)np : 1;
+      if (!need_grad && !pointwise && tc_ok) {
+        k.tc = true;
+        k.fn = (const void*)cm.k_value_tc;
+        k.lanes = false;
+        k.G = kTcM;
+        k.threads = kTcThreads;
+      }
     } else {
       k.compiled = false;
       k.fn = interp_kernel(variant);
@@ -379,16 +429,17 @@ struct gpum_b200_session {
     g.G = k.G;
     const int groups = (n + g.G - 1) / g.G;
     g.WC = 1;
-    while (g.WC < kWarps && g.WC < groups) g.WC *= 2;
+    while (!k.tc && g.WC < kWarps && g.WC < groups) g.WC *= 2;
     g.CG = g.WC * g.G;
     g.NCB = (n + g.CG - 1) / g.CG;
     g.C_pad = g.NCB * g.CG;
-    const int Tk = ext(k) ? T_c : T;
+    const int Tk = k.tc ? cm.tc_tn : (ext(k) ? T_c : T);
     g.ntiles = (int)((n_obs + Tk - 1) / Tk);
-    g.smem = skel_smem_bytes(Tk, (int)(ext(k) ? ncols_c : ncols), (int)np, g.CG, g.G, k.W,
-                             k.lanes);
+    g.smem = k.tc ? tc_smem_bytes(cm.tc_kp, cm.tc_ntail, cm.tc_tn, cm.tc_stages)
+                  : skel_smem_bytes(Tk, (int)(ext(k) ? ncols_c : ncols), (int)np, g.CG, g.G,
+                                    k.W, k.lanes);
     int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, kThreads, g.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k.fn, k.threads, g.smem);
     if (occ < 1) occ = 1;
     const int slots = num_sms() * occ;
     int nob = std::max(1, (4 * slots) / g.NCB);
@@ -410,8 +461,8 @@ struct gpum_b200_session {
   }
 
   // Evaluation-argument block for `n` points (params in `params`).
-  void setup_eval(int n, bool need_grad) {
-    kc = choose(need_grad);
+  void setup_eval(int n, bool need_grad, bool pointwise = false) {
+    kc = choose(need_grad, pointwise);
     geo = geometry(n, kc);
     if (geo.smem + static_smem(kc.fn) > 48 * 1024)
       GPUM_CK(cudaFuncSetAttribute(kc.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -423,7 +474,7 @@ struct gpum_b200_session {
     E = EvalArgs{};
     E.n_obs = (int)n_obs;
     E.ncols = (int)(ext(kc) ? ncols_c : ncols);
-    E.T = ext(kc) ? T_c : T;
+    E.T = kc.tc ? cm.tc_tn : (ext(kc) ? T_c : T);
     E.ntiles = geo.ntiles;
     E.tiles_per_cta = geo.tiles_per_cta;
     E.CG = geo.CG;
@@ -472,7 +523,10 @@ struct gpum_b200_session {
 
   void launch_with(const Geometry& g, EvalArgs& e, int phase) {
     const dim3 grid(g.NCB, g.NOB);
-    if (kc.compiled) {
+    if (kc.tc) {
+      void* args[] = {(void*)&tc_data.p, (void*)&e, (void*)&A, (void*)&phase};
+      GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kc.threads), args, g.smem, stream));
+    } else if (kc.compiled) {
       void* args[] = {(void*)(ext(kc) ? &tmap_c : &tmap), (void*)&e, (void*)&A, (void*)&phase};
       GPUM_CK(cudaLaunchKernel(kc.fn, grid, dim3(kThreads), args, g.smem, stream));
     } else if (kc.grad_interp) {
@@ -852,7 +906,7 @@ void batch(gpum_b200_session* s, const double* pts, size_t n_points, double* out
     chunk = std::max<size_t>(1, std::min<size_t>(n_points, (size_t)(1ull << 27) / s->n_obs));
   for (size_t p0 = 0; p0 < n_points; p0 += chunk) {
     const int n = (int)std::min(chunk, n_points - p0);
-    s->setup_eval(n, kind == B_GRAD);
+    s->setup_eval(n, kind == B_GRAD, kind == B_POINTWISE);
     s->upload_points(pts + p0 * np, n);
     s->A = ChainArgs{};
     if (kind == B_POINTWISE) {
@@ -1003,7 +1057,7 @@ void run_da(gpum_b200_session* s, gpum_b200_mlp* mlp, const double* init, const 
   s->geo_da = g;
   {
     int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kc.fn, kThreads, g.smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kc.fn, s->kc.threads, g.smem);
     // one wave of resident CTAs: with few survivors each CTA then takes many
     // tiles, so the per-CTA set-up is paid once per SM slot
     s->geo_da.NCB = std::max(num_sms() * std::max(occ, 1), g.NCB);
@@ -1172,6 +1226,11 @@ int gpum_b200_session_engine(gpum_b200_session* s) {
   if (s->engine == GPUM_ENGINE_AUTO)
     return s->compiled_available() ? GPUM_ENGINE_COMPILED : GPUM_ENGINE_INTERP;
   return s->engine;
+}
+
+int gpum_b200_session_tensor_cores(gpum_b200_session* s) {
+  if (!s) return -1;
+  return gpum_b200_session_engine(s) == GPUM_ENGINE_COMPILED && s->tc_ok ? 1 : 0;
 }
 
 void gpum_b200_session_destroy(gpum_b200_session* s) {

@@ -160,6 +160,17 @@ std::string dlit(double v) {
 
 bool is_const2(const Graph& g, int i) { return g.n[i].op == O_C && g.n[i].c == 2.0; }
 
+// A constant divisor +-2^k whose reciprocal is a normal float: x / c and
+// x * (1 / c) are the same correctly rounded value, so the division becomes
+// a product.  Returns the reciprocal's literal, or "".
+std::string pow2_recip(const Graph& g, int b) {
+  if (b < 0 || g.n[b].op != O_C || g.n[b].c == 0.0 || !std::isfinite(g.n[b].c)) return "";
+  int e = 0;
+  const double m = std::frexp(g.n[b].c, &e);
+  if (std::fabs(m) != 0.5 || e - 1 < -125 || e - 1 > 125) return "";
+  return flit(1.0 / g.n[b].c);
+}
+
 // Emits the value of `i` from child names.
 std::string op_expr(const Graph& g, int i, const std::string& a, const std::string& b,
                     bool f32) {
@@ -168,7 +179,11 @@ std::string op_expr(const Graph& g, int i, const std::string& a, const std::stri
     case O_ADD: return "(" + a + " + " + b + ")";
     case O_SUB: return "(" + a + " - " + b + ")";
     case O_MUL: return "(" + a + " * " + b + ")";
-    case O_DIV: return "(" + a + " / " + b + ")";
+    case O_DIV: {
+      const std::string r = pow2_recip(g, g.n[i].b);
+      if (!r.empty()) return "(" + a + " * " + (f32 ? r : dlit(1.0 / g.n[g.n[i].b].c)) + ")";
+      return "(" + a + " / " + b + ")";
+    }
     case O_NEG: return "(-" + a + ")";
     case O_EXP: return std::string("exp") + sfx + "(" + a + ")";
     case O_LOG: return std::string("log") + sfx + "(" + a + ")";
@@ -186,7 +201,11 @@ std::string op_expr2(const Graph& g, int i, const std::string& a, const std::str
     case O_ADD: return "gm2_add(" + a + ", " + b + ")";
     case O_SUB: return "gm2_sub(" + a + ", " + b + ")";
     case O_MUL: return "gm2_mul(" + a + ", " + b + ")";
-    case O_DIV: return "gm2_div(" + a + ", " + b + ")";
+    case O_DIV: {
+      const std::string r = pow2_recip(g, g.n[i].b);
+      if (!r.empty()) return "gm2_mul(" + a + ", gm2(" + r + "))";
+      return "gm2_div(" + a + ", " + b + ")";
+    }
     case O_NEG: return "gm2_neg(" + a + ")";
     case O_EXP: return "gm2_exp(" + a + ")";
     case O_LOG: return "gm2_log(" + a + ")";
@@ -401,6 +420,117 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
     return "(" + a + (e.sign > 0 ? " + " : " - ") + lw + ")";
   };
 
+  // Linear predictor for the tensor cores: the per-observation node with the
+  // most data columns that is affine in the data with parameter-only
+  // coefficients, sum_c coef_c(theta) x_c + offset(theta).  Over a tile of
+  // observations and a block of chains it is a matrix product (chains x
+  // columns times columns x observations); the value kernel gm_iter_value_tc
+  // runs it on the tensor cores and evaluates the rest of the expression
+  // (the tail, gm_tc_tail2) with the node replaced by its product.
+  struct AffTerm {
+    double c;
+    int pn;  // c * value(pn); pn = -1: the constant c
+  };
+  struct Aff {
+    bool ok = false;
+    std::map<int, std::vector<AffTerm>> col;  // data column -> coefficient terms
+    std::vector<AffTerm> off;
+  };
+  std::vector<Aff> aff(N);
+  auto scaled = [](const std::vector<AffTerm>& v, double c, int pn) {
+    std::vector<AffTerm> o;
+    for (const AffTerm& t : v) {
+      if (pn >= 0 && t.pn >= 0) return std::vector<AffTerm>{{0.0, -2}};  // product of two
+      o.push_back({t.c * c, pn >= 0 ? pn : t.pn});
+    }
+    return o;
+  };
+  auto bad_terms = [](const std::vector<AffTerm>& v) {
+    for (const AffTerm& t : v)
+      if (t.pn == -2) return true;
+    return false;
+  };
+  for (int i = 0; i < N; ++i) {
+    if (!live[i]) continue;
+    const Node& x = g.n[i];
+    Aff& r = aff[i];
+    if (x.op == O_C) {
+      r.ok = true;
+      r.off.push_back({x.c, -1});
+    } else if ((x.dep & DEP_D) == 0) {  // parameter-only
+      r.ok = true;
+      r.off.push_back({1.0, i});
+    } else if (is_d(i)) {  // a data column (given or materialized)
+      const int c = col_of(i);
+      if (c >= 0) {
+        r.ok = true;
+        r.col[c].push_back({1.0, -1});
+      }
+    } else if ((x.op == O_ADD || x.op == O_SUB) && aff[x.a].ok && aff[x.b].ok) {
+      r = aff[x.a];
+      const double sg = x.op == O_ADD ? 1.0 : -1.0;
+      for (auto& kv : aff[x.b].col)
+        for (const AffTerm& t : kv.second) r.col[kv.first].push_back({sg * t.c, t.pn});
+      for (const AffTerm& t : aff[x.b].off) r.off.push_back({sg * t.c, t.pn});
+    } else if (x.op == O_NEG && aff[x.a].ok) {
+      r = aff[x.a];
+      for (auto& kv : r.col)
+        for (AffTerm& t : kv.second) t.c = -t.c;
+      for (AffTerm& t : r.off) t.c = -t.c;
+    } else if (x.op == O_MUL && aff[x.a].ok && aff[x.b].ok) {
+      // one side free of data: scale the other side by it
+      const bool a_scalar = (g.n[x.a].dep & DEP_D) == 0, b_scalar = (g.n[x.b].dep & DEP_D) == 0;
+      if (a_scalar == b_scalar) continue;
+      const int k = a_scalar ? x.a : x.b, o = a_scalar ? x.b : x.a;
+      const double kc = g.n[k].op == O_C ? g.n[k].c : 1.0;
+      const int kp = g.n[k].op == O_C ? -1 : k;
+      Aff t;
+      t.ok = true;
+      for (auto& kv : aff[o].col) t.col[kv.first] = scaled(kv.second, kc, kp);
+      t.off = scaled(aff[o].off, kc, kp);
+      bool bad = bad_terms(t.off);
+      for (auto& kv : t.col) bad = bad || bad_terms(kv.second);
+      if (!bad) r = t;
+    } else if (x.op == O_DIV && aff[x.a].ok && (g.n[x.a].dep & DEP_D) && g.n[x.b].op == O_C &&
+               g.n[x.b].c != 0.0 && std::isfinite(g.n[x.b].c)) {
+      // division by a constant: the coefficients scaled by its reciprocal
+      const double kc = 1.0 / g.n[x.b].c;
+      for (auto& kv : aff[x.a].col) r.col[kv.first] = scaled(kv.second, kc, -1);
+      r.off = scaled(aff[x.a].off, kc, -1);
+      r.ok = true;
+    }
+  }
+  int tc_root = -1;
+  for (int i = 0; i < N; ++i) {
+    if (!live[i] || !is_pd(i) || !aff[i].ok) continue;
+    if (tc_root < 0 || aff[i].col.size() >= aff[tc_root].col.size()) tc_root = i;
+  }
+  std::vector<char> in_tc(N, 0);  // nodes of the linear predictor's subtree
+  if (tc_root >= 0) {
+    in_tc[tc_root] = 1;
+    for (int i = tc_root; i >= 0; --i) {
+      if (!in_tc[i]) continue;
+      if (g.n[i].a >= 0) in_tc[g.n[i].a] = 1;
+      if (g.n[i].b >= 0) in_tc[g.n[i].b] = 1;
+    }
+    bool ok = aff[tc_root].col.size() >= 6;
+    // per-observation values inside the subtree must feed nothing outside it
+    for (int i = 0; i < N && ok; ++i) {
+      if (!live[i] || in_tc[i]) continue;
+      for (int c : {g.n[i].a, g.n[i].b})
+        if (c >= 0 && c != tc_root && in_tc[c] && is_pd(c)) ok = false;
+    }
+    if (!ok) tc_root = -1;
+  }
+  std::vector<int> tc_cols;  // column of each product column (-1: the ones column)
+  if (tc_root >= 0) {
+    for (auto& kv : aff[tc_root].col) tc_cols.push_back(kv.first);
+    bool has_off = false;
+    for (const AffTerm& t : aff[tc_root].off) has_off = has_off || t.pn >= 0 || t.c != 0.0;
+    if (has_off) tc_cols.push_back(-1);
+    if (tc_cols.size() > 96) tc_root = -1;  // the shared-memory operands' limit
+  }
+
   std::ostringstream s;
   s << "#define GM_NP " << n_params << "\n";
   s << "#define GM_NH " << std::max(1, out->n_hoist) << "\n";
@@ -612,6 +742,104 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
         s << "  const float2 " << name[i] << " = " << value2_expr(i, ref2) << ";\n";
     const std::string root2 = root < 0 ? std::string("gm2(0.0f)") : ref2(root);
     s << "  (void)d; (void)pp; (void)hh;\n  return " << root2 << ";\n}\n";
+
+    // The tensor-core value path.  A linear predictor that is itself a
+    // product folded into an FFMA2 of its consumer keeps the FP32 path.
+    if (tc_root >= 0 && fused[tc_root]) tc_root = -1;
+    if (tc_root >= 0) {
+      // gm_tc_tail2: the paired value with the linear predictor's pair `eta`;
+      // t[k] = the k-th data column the tail reads (gm_tc_tailvals).
+      std::vector<int> tslot(N, -1), tail_cols;
+      auto refT = [&](int i) -> std::string {
+        if (i == tc_root) return "eta";
+        const Node& x = g.n[i];
+        if (x.op == O_C) return "gm2(" + flit(x.c) + ")";
+        if (x.op == O_P) return "pp[" + std::to_string(x.arg) + "]";
+        if (hslot[i] >= 0) return "hh[" + std::to_string(hslot[i]) + "]";
+        if (dslot[i] >= 0) {
+          if (tslot[i] < 0) {
+            tslot[i] = (int)tail_cols.size();
+            tail_cols.push_back(col_of(i));
+          }
+          return "t[" + std::to_string(tslot[i]) + "]";
+        }
+        return name[i];
+      };
+      std::ostringstream body;
+      for (int i = 0; i < N; ++i)
+        if (value_node(i) && !in_tc[i])
+          body << "  const float2 " << name[i] << " = " << value2_expr(i, refT) << ";\n";
+      const std::string rootT = refT(root);
+      const int K = (int)tc_cols.size(), KP = (K + 7) / 8 * 8, NT = (int)tail_cols.size();
+      // Observations per tile and pipeline stages: the largest that fit
+      // shared memory (stages of [hi | lo | tail] x TN, the coefficient
+      // operand [hi | lo] x 128 chains, the reduction buffer).
+      int TN = 0, S = 0;
+      for (int tn : {256, 128, 64}) {
+        for (int st : {3, 2}) {
+          if (tc_smem_bytes(KP, NT, tn, st) <= 231424) {
+            TN = tn;
+            S = st;
+            break;
+          }
+        }
+        if (TN) break;
+      }
+      if (TN == 0) tc_root = -1;
+      if (tc_root >= 0) {
+        out->tc = true;
+        out->tc_k = K;
+        out->tc_kp = KP;
+        out->tc_ntail = NT;
+        out->tc_tn = TN;
+        out->tc_stages = S;
+        s << "#define GM_TC 1\n#define GM_TC_K " << K << "\n#define GM_TC_KP " << KP
+          << "\n#define GM_TC_NTAIL " << NT << "\n#define GM_TC_NT1 " << std::max(NT, 1)
+          << "\n#define GM_TC_TN " << TN << "\n#define GM_TC_STAGES " << S << "\n";
+        // gm_tc_colvals / gm_tc_tailvals: one observation's product columns
+        // and tail columns from the column-major data (x[c * ld]).
+        s << "__device__ __forceinline__ void gm_tc_colvals(const float* __restrict__ x, "
+             "long long ld, float* __restrict__ v) {\n";
+        for (int k = 0; k < K; ++k)
+          s << "  v[" << k << "] = "
+            << (tc_cols[k] < 0 ? std::string("1.0f")
+                               : "x[" + std::to_string(tc_cols[k]) + " * ld]")
+            << ";\n";
+        s << "  (void)x; (void)ld;\n}\n";
+        s << "__device__ __forceinline__ void gm_tc_tailvals(const float* __restrict__ x, "
+             "long long ld, float* __restrict__ t) {\n";
+        for (int k = 0; k < NT; ++k)
+          s << "  t[" << k << "] = x[" << tail_cols[k] << " * ld];\n";
+        s << "  (void)x; (void)ld; (void)t;\n}\n";
+        // gm_tc_coef: the coefficients of one chain (the ones column's is the
+        // offset), from its parameters.
+        s << "__device__ __forceinline__ void gm_tc_coef(const float* __restrict__ p, "
+             "float* __restrict__ a) {\n";
+        emit_hoist_body(s);
+        auto term_sum = [&](const std::vector<AffTerm>& ts) {
+          std::string e;
+          for (const AffTerm& t : ts) {
+            std::string v = t.pn < 0 ? flit(t.c)
+                            : t.c == 1.0 ? name[t.pn]
+                            : t.c == -1.0 ? "(-" + name[t.pn] + ")"
+                                          : "(" + flit(t.c) + " * " + name[t.pn] + ")";
+            e = e.empty() ? v : "(" + e + " + " + v + ")";
+          }
+          return e.empty() ? std::string("0.0f") : e;
+        };
+        for (int k = 0; k < K; ++k)
+          s << "  a[" << k << "] = "
+            << term_sum(tc_cols[k] < 0 ? aff[tc_root].off : aff[tc_root].col[tc_cols[k]])
+            << ";\n";
+        s << "  (void)p;\n}\n";
+        s << "__device__ __forceinline__ float2 gm_tc_tail2(float2 eta, "
+             "const float2* __restrict__ t, const float2* __restrict__ pp, "
+             "const float2* __restrict__ hh) {\n"
+          << body.str() << "  (void)eta; (void)t; (void)pp; (void)hh;\n  return " << rootT
+          << ";\n}\n";
+      }
+    }
+    if (tc_root < 0) s << "#define GM_TC 0\n";
   }
 
   // Value + gradient: forward, then adjoints in reverse order.

@@ -21,6 +21,12 @@ namespace gpum {
 
 constexpr int kWarps = 8;  // warps per CTA
 constexpr int kThreads = kWarps * 32;
+// The tensor-core value kernel (gm_iter_value_tc): 128 chains per CTA (the
+// MMA's M), eight epilogue warps (two per TMEM lane quarter) and a control
+// warp whose one thread issues the copies and the MMAs.
+constexpr int kTcM = 128;
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 1);
 constexpr int kMaxStackF64 = 32;
 
 enum Phase : int { PH_EVAL = 0, PH_INIT = 1, PH_STEP = 2, PH_POINTWISE = 3 };
@@ -457,6 +463,46 @@ __device__ inline void finalize_chain(const ChainArgs& A, int c, int cb, double 
   A.ctr[c] = rs.ctr;
 }
 
+// The last CTA of chain block cb to write its partials (an atomic ticket, no
+// spinning) finishes the iteration for the block's CG chains: the partials
+// summed in observation-block order, then accept/reject, record and
+// propose.  Every one of the CTA's nthreads threads calls it.
+template <int W, class Prior>
+__device__ __forceinline__ void finish_chain_block(const EvalArgs& E, const ChainArgs& A, int cb,
+                                                   int CG, int phase, uint32_t* s_ticket,
+                                                   int nthreads) {
+  const int tid = threadIdx.x, np = E.np;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) *s_ticket = atomicAdd(&E.tickets[cb], 1u);
+  __syncthreads();
+  const uint32_t nob = gridDim.y;
+  if (*s_ticket != nob - 1) return;
+  __threadfence();
+  for (int cl = tid; cl < CG; cl += nthreads) {
+    const int c = cb * CG + cl;
+    if (c >= A.n_chains) continue;
+    double ll = 0.0;
+    for (uint32_t o = 0; o < nob; ++o) ll += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W]);
+    if (A.mode == MODE_MALA) {
+      double* gsum = (phase == PH_INIT ? A.gx : A.gy) + (size_t)c * np;
+      const double b = A.beta ? A.beta[c] : 1.0;
+      for (int j = 0; j < np; ++j) {
+        double v = 0.0;
+        for (uint32_t o = 0; o < nob; ++o)
+          v += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W + 1 + j]);
+        gsum[j] = b * v;
+      }
+    }
+    finalize_chain<Prior>(A, c, cb, ll, phase, const_cast<float*>(E.params), E.C_pad);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    E.tickets[cb] = 0;
+    if (phase == PH_STEP) A.iter[cb] += 1;
+  }
+}
+
 // --------------------------------------------------------- kernel skeleton
 // Shared-memory carve-up (the host's smem_bytes() must agree):
 //   2 data stages [ncols][T] f32 | params [np][CG] f32 (rounded to 4; none
@@ -686,37 +732,7 @@ __device__ __forceinline__ void run_iteration(const TmapDesc* tmap, const EvalAr
     E.partials[((size_t)ob * E.C_pad + (size_t)cb * CG + cl) * W + w] = v;
   }
   if (phase == PH_EVAL) return;
-
-  // Last CTA of this chain block (ticket) finishes the iteration.
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) *s_ticket = atomicAdd(&E.tickets[cb], 1u);
-  __syncthreads();
-  const uint32_t nob = gridDim.y;
-  if (*s_ticket != nob - 1) return;
-  __threadfence();
-  for (int cl = tid; cl < CG; cl += kThreads) {
-    const int c = cb * CG + cl;
-    if (c >= A.n_chains) continue;
-    double ll = 0.0;
-    for (uint32_t o = 0; o < nob; ++o) ll += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W]);
-    if (A.mode == MODE_MALA) {
-      double* gsum = (phase == PH_INIT ? A.gx : A.gy) + (size_t)c * np;
-      const double b = A.beta ? A.beta[c] : 1.0;
-      for (int j = 0; j < np; ++j) {
-        double v = 0.0;
-        for (uint32_t o = 0; o < nob; ++o)
-          v += __ldcg(&E.partials[((size_t)o * E.C_pad + c) * W + 1 + j]);
-        gsum[j] = b * v;
-      }
-    }
-    finalize_chain<Prior>(A, c, cb, ll, phase, const_cast<float*>(E.params), E.C_pad);
-  }
-  __syncthreads();
-  if (tid == 0) {
-    E.tickets[cb] = 0;
-    if (phase == PH_STEP) A.iter[cb] += 1;
-  }
+  finish_chain_block<W, Prior>(E, A, cb, CG, phase, s_ticket, kThreads);
 }
 
 // Fixed-order sum of the partials of each point: out[p*W + w].

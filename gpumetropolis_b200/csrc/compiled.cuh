@@ -414,3 +414,358 @@ gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum
                                                                             phase,
                                                                         body);
 }
+
+#if GM_TC
+// ----------------------------------------------------------------------------
+// Tensor-core value kernel.  The model's linear predictor eta = sum_c
+// coef_c(theta) x_c (codegen: the largest per-observation node affine in the
+// data with parameter-only coefficients; an offset is the coefficient of a
+// ones column) is, for the 128 chains of a CTA and a tile of GM_TC_TN
+// observations, the product A (128 x K, coefficients) . B^T (TN x K, data).
+// It runs on the 5th-generation tensor cores in TF32 with both operands split
+// into a TF32 head and a TF32 rounding of the remainder, v = hi + lo:
+// a.x ~ a_hi.x_hi + a_hi.x_lo + a_lo.x_hi, the dropped a_lo.x_lo and the
+// truncation of lo below 2^-21 relative to |a x|, FP32 accumulation in tensor
+// memory.  The rest of the per-observation expression (gm_tc_tail2) runs on
+// the FP32 pipes with eta read from tensor memory.
+//
+// Roles (kTcThreads = 288):
+//   warps 0..7   epilogue: warp w reads TMEM lane quarter w % 4 (chains
+//                32 (w % 4) .. + 31, one chain per lane) and column half
+//                w / 4 of each tile, evaluates the tail and sums its terms
+//   warp 8       control, one thread: the copies (one bulk copy per tile of
+//                the packed data, below, into a GM_TC_STAGES-deep ring) and
+//                the MMAs (3 KP/8 per tile into one of two accumulators of TN
+//                TMEM columns); the warp allocates the tensor memory
+// Barriers: full[s] (copy landed), empty[s] (the epilogue is done with the
+// stage; the MMAs were done with it before the epilogue started), accf[a]
+// (accumulator a holds a tile), acce[a] (the epilogue has read it).  Every
+// wait is bounded; one that runs out sets DEV_ERR_TC_TIMEOUT and a CTA-wide
+// abort flag, the roles leave their loops, the control thread waits (bounded)
+// for its MMAs and copies, and the CTA frees its tensor memory and finishes
+// the chain block's bookkeeping.
+//
+// Packed data (gm_tc_pack, once per session): per tile of TN observations
+// [hi: KP/4 chunks][TN][4] | [lo: same] | [tail: NTAIL][TN] floats, i.e. the
+// canonical K-major, no-swizzle core-matrix layout of the MMA's B operand
+// (core matrix (k/4, o/8) at (k/4 * TN/8 + o/8) * 128 bytes), so one
+// contiguous copy fills a stage.
+namespace gpum {
+constexpr int kTcTN = GM_TC_TN;
+constexpr int kTcKP = GM_TC_KP;
+constexpr int kTcS = GM_TC_STAGES;
+constexpr uint32_t kTcStageFloats = (uint32_t)(2 * kTcKP + GM_TC_NTAIL) * kTcTN;
+constexpr uint32_t kTcAFloats = (uint32_t)2 * kTcKP * kTcM;
+constexpr uint32_t kTcTmemCols = 2 * kTcTN;
+constexpr int kTcParts = kTcEpiWarps / 4;  // epilogue warps per lane quarter
+constexpr int kTcColsPerWarp = kTcTN / kTcParts;
+static_assert(kTcKP % 8 == 0 && kTcTN % 64 == 0 && kTcTN <= 256 && kTcColsPerWarp % 32 == 0,
+              "tensor-core tile shape");
+}  // namespace gpum
+
+extern "C" __global__ void gm_tc_pack(const float* __restrict__ cols, long long n_obs,
+                                      long long ld, long long n_tiles, float* __restrict__ xt,
+                                      unsigned int* __restrict__ nonfinite) {
+  using namespace gpum;
+  const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= n_tiles * kTcTN) return;
+  const long long tile = o / kTcTN;
+  const int r = (int)(o % kTcTN);
+  float* base = xt + (size_t)tile * kTcStageFloats;
+  const bool valid = o < n_obs;
+  float v[GM_TC_K], t[GM_TC_NT1];
+#pragma unroll
+  for (int k = 0; k < GM_TC_K; ++k) v[k] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < GM_TC_NT1; ++k) t[k] = 0.0f;
+  if (valid) {
+    gm_tc_colvals(cols + o, ld, v);
+    gm_tc_tailvals(cols + o, ld, t);
+  }
+  bool bad = false;
+#pragma unroll
+  for (int kc = 0; kc < kTcKP / 4; ++kc) {
+    float hi[4], lo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int k = 4 * kc + e;
+      float x = 0.0f;
+      if (k < GM_TC_K) x = v[k];
+      hi[e] = tf32_rna(x);
+      lo[e] = isfinite(hi[e]) ? tf32_rna(x - hi[e]) : 0.0f;
+      bad = bad || !isfinite(x);
+    }
+    *reinterpret_cast<float4*>(base + ((size_t)kc * kTcTN + r) * 4) =
+        make_float4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<float4*>(base + (size_t)kTcKP * kTcTN + ((size_t)kc * kTcTN + r) * 4) =
+        make_float4(lo[0], lo[1], lo[2], lo[3]);
+  }
+#pragma unroll
+  for (int m = 0; m < GM_TC_NTAIL; ++m) base[(size_t)2 * kTcKP * kTcTN + m * kTcTN + r] = t[m];
+  // a non-finite product column would turn into inf * 0 = NaN in the split
+  // products: the host keeps such data on the FP32 kernel
+  if (bad) atomicOr(nonfinite, 1u);
+}
+
+// eta of observation `col` of the tile on the FP32 pipe from the operands'
+// hi + lo: for a chain with an infinite coefficient, whose inf * 0 products
+// in the split form would be NaN where the plain product is +-inf.
+__device__ __noinline__ float gm_tc_eta_fp32(const float* __restrict__ As,
+                                                const float* __restrict__ xs, int cl, int col) {
+  using namespace gpum;
+  float e = 0.0f;
+  for (int k = 0; k < kTcKP; ++k) {
+    const int ao = ((((k >> 2) * (kTcM / 8) + (cl >> 3)) << 5) + ((cl & 7) << 2) + (k & 3));
+    const int xo = ((((k >> 2) * (kTcTN / 8) + (col >> 3)) << 5) + ((col & 7) << 2) + (k & 3));
+    const float a = As[ao] + As[kTcKP * kTcM + ao];
+    const float x = xs[xo] + xs[kTcKP * kTcTN + xo];
+    if (a != 0.0f) e = fmaf(a, x, e);
+  }
+  return e;
+}
+
+extern "C" __global__ void __launch_bounds__(gpum::kTcThreads, 1)
+gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs A, int phase) {
+  using namespace gpum;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int cb = blockIdx.x, ob = blockIdx.y, tiles_per_cta = E.tiles_per_cta;
+  if (E.active) {  // delayed acceptance: geometry from the live count
+    const int live = (int)*E.active;
+    const int busy = (live + kTcM - 1) / kTcM;
+    const int nob = da_obs_blocks(live, kTcM, (int)(gridDim.x * gridDim.y), E.ntiles,
+                                  &tiles_per_cta);
+    const int id = (int)(blockIdx.y * gridDim.x + blockIdx.x);
+    if (busy == 0 || id >= busy * nob) return;
+    cb = id % busy;
+    ob = id / busy;
+  }
+  float* stg = reinterpret_cast<float*>(smem_raw);
+  float* As = stg + (size_t)kTcS * kTcStageFloats;
+  double* red = reinterpret_cast<double*>(As + kTcAFloats);  // [column parts][128]
+  uint32_t* inf_chain = reinterpret_cast<uint32_t*>(red + 4 * kTcM);  // [128]
+  uint64_t* full = reinterpret_cast<uint64_t*>(inf_chain + kTcM);
+  uint64_t* empty = full + kTcS;
+  uint64_t* accf = empty + kTcS;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  uint32_t* misc = reinterpret_cast<uint32_t*>(drain + 1);  // TMEM base, ticket, abort
+  volatile uint32_t* abort_flag = misc + 2;
+
+  const int t0 = ob * tiles_per_cta;
+  const int t1 = min(t0 + tiles_per_cta, E.ntiles);
+  const int nt = max(t1 - t0, 0);
+  const int chain0 = cb * kTcM;
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kTcEpiWarps);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&accf[a], 1);
+      mbar_init(&acce[a], kTcEpiWarps);
+    }
+    mbar_init(drain, 1);
+    misc[2] = 0;
+    mbar_fence_init();
+  }
+  if (warp == kTcEpiWarps) tmem_alloc(&misc[0], kTcTmemCols);
+  // The coefficient operand, one chain per thread: [hi | lo] in the
+  // canonical layout (core matrix (k/4, r/8) at (k/4 * 16 + r/8) * 128 bytes).
+  if (tid < kTcM) {
+    float p[GM_NP], a[GM_TC_K];
+#pragma unroll
+    for (int j = 0; j < GM_NP; ++j) p[j] = E.params[(size_t)j * E.C_pad + chain0 + tid];
+    gm_tc_coef(p, a);
+    uint32_t inf = 0;
+#pragma unroll
+    for (int kc = 0; kc < kTcKP / 4; ++kc) {
+      float hi[4], lo[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int k = 4 * kc + e;
+        float v = 0.0f;
+        if (k < GM_TC_K) v = a[k];
+        hi[e] = tf32_rna(v);
+        lo[e] = isfinite(hi[e]) ? tf32_rna(v - hi[e]) : 0.0f;
+        inf |= isinf(v) ? 1u : 0u;
+      }
+      const int off = ((kc * (kTcM / 8) + (tid >> 3)) << 5) + ((tid & 7) << 2);
+      *reinterpret_cast<float4*>(As + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<float4*>(As + kTcKP * kTcM + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
+    inf_chain[tid] = inf;
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = misc[0];
+  auto give_up = [&]() {
+    atomicOr(E.err, DEV_ERR_TC_TIMEOUT);
+    *abort_flag = 1u;
+  };
+
+  if (warp == kTcEpiWarps) {
+    // ---- control: copies and MMAs
+    if (lane == 0) {
+      constexpr uint32_t bytes = kTcStageFloats * 4;
+      constexpr uint32_t idesc = umma_idesc_tf32(kTcM, kTcTN);
+      constexpr uint32_t lbo_a = (kTcM / 8) * 128, lbo_b = (kTcTN / 8) * 128;
+      const uint32_t a_hi = smem_addr(As), a_lo = a_hi + (uint32_t)kTcKP * kTcM * 4;
+      auto load = [&](int k) {
+        const int s = k % kTcS;
+        mbar_expect_tx(&full[s], bytes);
+        bulk_load(stg + (size_t)s * kTcStageFloats, xt + (size_t)(t0 + k) * kTcStageFloats,
+                  bytes, &full[s]);
+      };
+      int issued = 0;
+      for (; issued < kTcS && issued < nt; ++issued) load(issued);
+      for (int k = 0; k < nt; ++k) {
+        if (*abort_flag) break;
+        const int s = k % kTcS, acc = k & 1;
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / kTcS) & 1))) {
+          give_up();
+          break;
+        }
+        if (k >= 2 && !mbar_wait_bounded(&acce[acc], (uint32_t)(((k >> 1) - 1) & 1))) {
+          give_up();
+          break;
+        }
+        tc_fence_after();
+        const uint32_t b_hi = smem_addr(stg + (size_t)s * kTcStageFloats);
+        const uint32_t b_lo = b_hi + (uint32_t)kTcKP * kTcTN * 4;
+        const uint32_t d = tmem + (uint32_t)(acc * kTcTN);
+        // the small products first: the accumulator rounds toward zero, so
+        // only the KP/8 head products are added onto a large partial sum
+#pragma unroll
+        for (int kk = 0; kk < kTcKP / 8; ++kk) {
+          const uint64_t ah = umma_smem_desc(a_hi + 2 * kk * lbo_a, lbo_a, 128);
+          const uint64_t al = umma_smem_desc(a_lo + 2 * kk * lbo_a, lbo_a, 128);
+          const uint64_t bh = umma_smem_desc(b_hi + 2 * kk * lbo_b, lbo_b, 128);
+          const uint64_t bl = umma_smem_desc(b_lo + 2 * kk * lbo_b, lbo_b, 128);
+          umma_tf32(d, ah, bl, idesc, kk > 0 ? 1u : 0u);
+          umma_tf32(d, al, bh, idesc, 1u);
+        }
+#pragma unroll
+        for (int kk = 0; kk < kTcKP / 8; ++kk)
+          umma_tf32(d, umma_smem_desc(a_hi + 2 * kk * lbo_a, lbo_a, 128),
+                    umma_smem_desc(b_hi + 2 * kk * lbo_b, lbo_b, 128), idesc, 1u);
+        umma_commit(&accf[acc]);
+        // refill the stage of tile k - 1 once its epilogue is done with it
+        if (k >= 1 && issued < nt && issued == k - 1 + kTcS) {
+          if (!mbar_wait_bounded(&empty[(k - 1) % kTcS], (uint32_t)(((k - 1) / kTcS) & 1))) {
+            give_up();
+            break;
+          }
+          load(issued++);
+        }
+      }
+      // every MMA has finished before the tensor memory is released, and no
+      // copy is still writing into shared memory
+      umma_commit(drain);
+      if (!mbar_wait_bounded(drain, 0u)) give_up();
+      for (int i = max(0, issued - kTcS); i < issued; ++i)
+        if (!mbar_wait_bounded(&full[i % kTcS], (uint32_t)((i / kTcS) & 1))) give_up();
+    }
+  } else {
+    // ---- epilogue
+    const int q = warp & 3, part = warp >> 2;
+    const int cl = q * 32 + lane;
+    const int c = chain0 + cl;
+    float2 pp[GM_NP], hh[GM_NH];
+    {
+      float p[GM_NP], h[GM_NH];
+#pragma unroll
+      for (int j = 0; j < GM_NP; ++j) p[j] = E.params[(size_t)j * E.C_pad + c];
+      gm_hoist(p, h);
+#pragma unroll
+      for (int j = 0; j < GM_NP; ++j) pp[j] = make_float2(p[j], p[j]);
+#pragma unroll
+      for (int j = 0; j < GM_NH; ++j) hh[j] = make_float2(h[j], h[j]);
+    }
+    const bool inf = inf_chain[cl] != 0;
+    const bool warp_inf = __any_sync(0xffffffffu, inf);
+    double sum = 0.0;
+    for (int k = 0; k < nt; ++k) {
+      if (*abort_flag) break;
+      const int s = k % kTcS, acc = k & 1;
+      // warp-uniform waits: the accumulator, and the stage's copy (already
+      // complete; waited on so its tail columns are visible to this thread)
+      bool ok = mbar_wait_bounded(&accf[acc], (uint32_t)((k >> 1) & 1)) &&
+                mbar_wait_bounded(&full[s], (uint32_t)((k / kTcS) & 1));
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
+        if (lane == 0) give_up();
+        break;
+      }
+      tc_fence_after();
+      const float* xs = stg + (size_t)s * kTcStageFloats;
+      const float* tail = xs + (size_t)2 * kTcKP * kTcTN;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
+                             (uint32_t)(acc * kTcTN + part * kTcColsPerWarp);
+      const long long obs0 = (long long)(t0 + k) * kTcTN + part * kTcColsPerWarp;
+      float2 tsum = make_float2(0.0f, 0.0f);
+#pragma unroll 1
+      for (int ch = 0; ch < kTcColsPerWarp / 32; ++ch) {
+        float v[32];
+        tmem_ld32(taddr + (uint32_t)(ch * 32), v);
+        const int col0 = part * kTcColsPerWarp + ch * 32;
+        if (warp_inf) {  // a chain of this warp has an infinite coefficient
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (inf) v[j] = gm_tc_eta_fp32(As, xs, cl, col0 + j);
+        }
+        float2 val[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float2 t[GM_TC_NT1];
+#pragma unroll
+          for (int m = 0; m < GM_TC_NTAIL; ++m)
+            t[m] = *reinterpret_cast<const float2*>(tail + m * kTcTN + col0 + 2 * j);
+          val[j] = gm_tc_tail2(make_float2(v[2 * j], v[2 * j + 1]), t, pp, hh);
+        }
+        const long long o0 = obs0 + ch * 32;
+        if (o0 + 32 > (long long)E.n_obs) {  // the ragged end of the last tile
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            if (o0 + 2 * j >= E.n_obs) val[j].x = 0.0f;
+            if (o0 + 2 * j + 1 >= E.n_obs) val[j].y = 0.0f;
+          }
+        }
+        // pairwise: the FP32 error of a chunk grows with log2 of its terms
+#pragma unroll
+        for (int w = 8; w > 0; w >>= 1) {
+#pragma unroll
+          for (int j = 0; j < w; ++j) val[j] = __fadd2_rn(val[j], val[j + w]);
+        }
+        tsum = __fadd2_rn(tsum, val[0]);
+      }
+      sum += (double)tsum.x + (double)tsum.y;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&acce[acc]);
+        mbar_arrive(&empty[s]);
+      }
+    }
+    red[part * kTcM + cl] = sum;
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kTcEpiWarps) tmem_dealloc(tmem, kTcTmemCols);
+  // The chain's value over this observation block: the column parts in
+  // order.
+  if (tid < kTcM) {
+    double v = red[tid];
+#pragma unroll
+    for (int pt = 1; pt < kTcParts; ++pt) v += red[pt * kTcM + tid];
+    E.partials[(size_t)ob * E.C_pad + chain0 + tid] = v;
+  }
+  if (phase == PH_EVAL) return;
+  finish_chain_block<1, JitPrior>(E, A, cb, kTcM, phase, &misc[1], kTcThreads);
+}
+#endif  // GM_TC

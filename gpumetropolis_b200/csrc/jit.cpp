@@ -265,6 +265,18 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
     cudaLibraryUnload(e.lib);
     return 1;
   }
+  if (gm.tc && (cudaLibraryGetKernel(&e.model.k_value_tc, e.lib, "gm_iter_value_tc") !=
+                    cudaSuccess ||
+                cudaLibraryGetKernel(&e.model.k_tc_pack, e.lib, "gm_tc_pack") != cudaSuccess)) {
+    *err = "compiled model is missing its tensor-core kernels";
+    cudaLibraryUnload(e.lib);
+    return 1;
+  }
+  e.model.tc = gm.tc;
+  e.model.tc_kp = gm.tc_kp;
+  e.model.tc_ntail = gm.tc_ntail;
+  e.model.tc_tn = gm.tc_tn;
+  e.model.tc_stages = gm.tc_stages;
   e.model.G = G;
   e.model.GG = GG;
   e.model.pair = pair;

@@ -24,6 +24,12 @@ struct CompiledModel {
   bool lanes_grad = false;          // gradient kernel: one chain per lane
   int np = 0;
   double compile_seconds = 0.0;
+  // Linear predictor on the tensor cores (GenModel::tc): the value kernel
+  // gm_iter_value_tc and the packing kernel gm_tc_pack, with their shapes.
+  bool tc = false;
+  cudaKernel_t k_value_tc = nullptr;
+  cudaKernel_t k_tc_pack = nullptr;
+  int tc_kp = 0, tc_ntail = 0, tc_tn = 0, tc_stages = 0;
 };
 
 // Chains per thread for the value and gradient kernels, and whether the

@@ -201,6 +201,19 @@ GPUM_API int gpum_b200_session_set_engine(gpum_b200_session* s, int engine, char
                                           size_t err_len);
 /* The engine plain evaluations use (GPUM_ENGINE_INTERP or _COMPILED). */
 GPUM_API int gpum_b200_session_engine(gpum_b200_session* s);
+/* 1 when the session's log-likelihood sums and value-only sampler steps
+ * (rwm, pt, de, cholesky; delayed acceptance's exact stage) run the
+ * compiled engine's tensor-core value kernel: the model's linear predictor
+ * (the largest per-observation subexpression that is affine in the data
+ * with parameter-only coefficients, at least 6 data columns) as a TF32
+ * tensor-core product with a three-term split, the rest of each term on the
+ * FP32 pipes.  0 otherwise: no such predictor, a non-finite value in one of
+ * its data columns, the interpreter engine, or GPUM_B200_TENSOR_CORES=0 in
+ * the environment at the session's first compiled evaluation.  Pointwise
+ * output and gradients keep the FP32 kernels.  No counterpart in the
+ * reference (src/rust/src/chain_kernel.rs:305-321 evaluates the bytecode
+ * per chain and observation). */
+GPUM_API int gpum_b200_session_tensor_cores(gpum_b200_session* s);
 
 /* loglik_batch / loglik_pointwise / grad_batch on a session. */
 GPUM_API int gpum_b200_session_loglik_batch(gpum_b200_session* s, const double* points, size_t n_points,
