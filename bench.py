@@ -16,8 +16,11 @@ accept/propose step).
 * ``e2e``: the same metric through the reference-facing C ABI
   (``gpum_b200_run``) with host buffers: data upload + layout conversion,
   K iterations, draws copied back, wall-clock.
-* ``roofline``: the iteration kernel against the FP32 pipe (the kernel is
-  FP32/issue-bound), plus the HBM view of the same launch.
+* ``roofline``: the iteration kernel against the pipe that bounds it.  With
+  the model's linear predictor on the tensor cores (gm_iter_value_tc) that is
+  the special-function (XU) pipe: two MUFU operations (ex2, rcp) per
+  chain-observation in the softplus; the tensor-core, FP32-equivalent and HBM
+  views of the same launch are sub-objects.
 * ``cpu_baseline``: the oracle port of the reference CPU backend (bytecode ->
   C -> gcc JIT, OpenMP over chains) on this host, a bounded sample.
 * ``delayed_acceptance``: the ESS/s half of the metric on the same workload --
@@ -62,8 +65,10 @@ sys.path.insert(0, ROOT)
 METRIC = ("ESS/s on 1 B200, surrogate-DA vs plain exact MH at <=1e-6 rel logp err; "
           "chain-obs/s")
 UNIT = "chain-obs/s"
-FLOP_PER_CHAIN_OBS = 34.0   # essential FP32 flops of the logistic term (FMA = 2)
-MUFU_PER_CHAIN_OBS = 2.0    # exp, log
+FLOP_PER_CHAIN_OBS = 34.0   # the logistic term's 17-term linear predictor (FMA = 2)
+MUFU_PER_CHAIN_OBS = 2.0    # ex2 and rcp of the softplus
+TC_COLS = 17                # product columns of the tensor-core kernel (16 + ones)
+PACKED_ROW_BYTES = (2 * 24 + 1) * 4  # hi | lo (17 columns padded to 24) | y, f32
 ROW_BYTES = 17 * 4          # one f32 observation row
 
 
@@ -385,10 +390,10 @@ def da_measure(w, C, n_warm, n_samp, seed=11):
         call.close()
 
 
-def _traffic_per_launch():
-    """dram read+write bytes of one iteration launch from the committed ncu
-    summary (profiles/gm_iter_value_logistic_n2e20_c1024.md, line `dram_bytes_per_launch: X`)."""
-    path = os.path.join(ROOT, "profiles", "gm_iter_value_logistic_n2e20_c1024.md")
+def _traffic_per_launch(profile):
+    """dram read+write bytes of one iteration launch from a committed ncu
+    summary under profiles/ (its line `dram_bytes_per_launch: X`)."""
+    path = os.path.join(ROOT, "profiles", profile)
     try:
         for line in open(path):
             cell = line.strip().strip("|").strip()
@@ -426,6 +431,7 @@ def run_b200(a):
     sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
                            m.n_params, w.data, m.n_cols, w.n_obs, engine=a.engine)
     engine = {0: "interpreter", 1: "compiled"}[sess.engine]
+    tensor_cores = sess.tensor_cores
     sess.prepare(init, sd, temps, Wm + K, R.replica_seed(1, rank), 0, rng=_native.RNG_PHILOX)
     sess.advance(Wm)
     sess.sync()
@@ -468,7 +474,7 @@ def run_b200(a):
     mhz = clocks["sm_mhz"] or 1965.0
     n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
     fp32_peak = n_sm * 128 * 2 * mhz * 1e6 / 1e12
-    achieved = C * N * FLOP_PER_CHAIN_OBS / (ms_step / 1e3) / 1e12
+    fp32_achieved = C * N * FLOP_PER_CHAIN_OBS / (ms_step / 1e3) / 1e12
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -476,24 +482,66 @@ def run_b200(a):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    traffic = _traffic_per_launch()
-    roofline = {
-        "bound": "fp32", "achieved": round(achieved, 3), "peak": round(fp32_peak, 3),
-        "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4), "traffic": traffic,
-        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
-                          "kernel on this workload from the committed ncu capture "
-                          "(profiles/gm_iter_value_logistic_n2e20_c1024.md), not measured by "
-                          "this run",
-        "peak_source": f"nominal {n_sm} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz "
-                       "(median SM clock sampled in the timed region; "
-                       "MEASURED_PEAKS.json has no FP32 figure)",
-        "work_per_launch": f"{C} chains x {N} obs x {FLOP_PER_CHAIN_OBS:.0f} flop "
-                           f"(+{MUFU_PER_CHAIN_OBS:.0f} MUFU)",
-        "hbm": {"achieved_gbs": round(N * ROW_BYTES / (ms_step / 1e3) / 1e9, 2),
-                "peak_gbs": hbm_peak, "peak_source": hbm_src,
-                "frac": round(N * ROW_BYTES / (ms_step / 1e3) / 1e9 / hbm_peak, 5),
-                "bytes_per_launch": N * ROW_BYTES},
-    }
+    secs = ms_step / 1e3
+    if tensor_cores:
+        # gm_iter_value_tc: the linear predictor on the tensor cores, the
+        # softplus tail on the FP32 and special-function pipes
+        mufu_peak = n_sm * 16 * mhz * 1e6 / 1e12
+        mufu = C * N * MUFU_PER_CHAIN_OBS / secs / 1e12
+        bf16 = float(peaks.get("bf16_tflops", 1590.0))
+        tf32_peak = bf16 / 2.0
+        tf32 = C * N * 3 * 2 * TC_COLS / secs / 1e12
+        packed = N * PACKED_ROW_BYTES
+        roofline = {
+            "bound": "xu", "kernel": "gm_iter_value_tc",
+            "achieved": round(mufu, 4), "peak": round(mufu_peak, 4),
+            "unit": "Tops/s (MUFU ex2 + rcp)", "frac": round(mufu / mufu_peak, 4),
+            "traffic": _traffic_per_launch("gm_iter_value_tc_logistic_n2e20_c1024.md"),
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                              "this kernel on this workload from the committed ncu capture "
+                              "(profiles/gm_iter_value_tc_logistic_n2e20_c1024.md), not "
+                              "measured by this run",
+            "peak_source": f"nominal {n_sm} SMs x 16 SFU lanes x {mhz:.0f} MHz (median SM "
+                           "clock sampled in the timed region; MEASURED_PEAKS.json has no "
+                           "SFU figure)",
+            "work_per_launch": f"{C} chains x {N} obs x {MUFU_PER_CHAIN_OBS:.0f} MUFU "
+                               f"(+ {3 * 2 * TC_COLS} TF32 flop on the tensor cores)",
+            "tensor": {"achieved_tflops": round(tf32, 2), "peak_tflops": round(tf32_peak, 1),
+                       "frac": round(tf32 / tf32_peak, 4),
+                       "work": f"3 split products x {TC_COLS} columns x 2 flop per "
+                               "chain-observation",
+                       "peak_source": "half the measured dense bf16 burst of "
+                                      "MEASURED_PEAKS.json (TF32 runs at half the bf16 rate)"},
+            "fp32_equiv": {"achieved_tflops": round(fp32_achieved, 3),
+                           "peak_tflops": round(fp32_peak, 3),
+                           "frac": round(fp32_achieved / fp32_peak, 4),
+                           "work": f"{FLOP_PER_CHAIN_OBS:.0f} flop per chain-observation (the "
+                                   "linear predictor), against the FP32 pipes it no longer "
+                                   "runs on"},
+            "hbm": {"achieved_gbs": round(packed / secs / 1e9, 2), "peak_gbs": hbm_peak,
+                    "peak_source": hbm_src, "frac": round(packed / secs / 1e9 / hbm_peak, 5),
+                    "bytes_per_launch": packed},
+        }
+    else:
+        roofline = {
+            "bound": "fp32", "kernel": "gm_iter_value",
+            "achieved": round(fp32_achieved, 3), "peak": round(fp32_peak, 3),
+            "unit": "TFLOP/s", "frac": round(fp32_achieved / fp32_peak, 4),
+            "traffic": _traffic_per_launch("gm_iter_value_logistic_n2e20_c1024.md"),
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                              "this kernel on this workload from the committed ncu capture "
+                              "(profiles/gm_iter_value_logistic_n2e20_c1024.md), not "
+                              "measured by this run",
+            "peak_source": f"nominal {n_sm} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz "
+                           "(median SM clock sampled in the timed region; "
+                           "MEASURED_PEAKS.json has no FP32 figure)",
+            "work_per_launch": f"{C} chains x {N} obs x {FLOP_PER_CHAIN_OBS:.0f} flop "
+                               f"(+{MUFU_PER_CHAIN_OBS:.0f} MUFU)",
+            "hbm": {"achieved_gbs": round(N * ROW_BYTES / secs / 1e9, 2),
+                    "peak_gbs": hbm_peak, "peak_source": hbm_src,
+                    "frac": round(N * ROW_BYTES / secs / 1e9 / hbm_peak, 5),
+                    "bytes_per_launch": N * ROW_BYTES},
+        }
 
     # The interpreter engine on the same workload (a few steps, same timing).
     interp = None
@@ -580,7 +628,7 @@ def run_b200(a):
                    "bytecode_instructions": m.loglik.n_instr,
                    "l2": "flushed (256 MiB write) before every timed step",
                    "rng": "philox", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-        "engine": engine, "interpreter_engine": interp,
+        "engine": engine, "tensor_cores": tensor_cores, "interpreter_engine": interp,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "delayed_acceptance": da, "logp_rel_err": logp_err,
         "logp_rel_err_note": "max over 32 chains of |sampler's log posterior of its final state "
@@ -650,7 +698,9 @@ CONFIG_WORK = {
     "mixture": {"flop": 20.0, "mufu": 5.0,
                 "what": "two Gaussian kernels, their weights and the log (RWM)"},
     "student_t": {"flop": 133.0, "mufu": 1.0,
-                  "what": "64-term linear predictor, scaled residual, log (DE)"},
+                  "what": "64-term linear predictor, scaled residual, log (DE); on the "
+                          "tensor-core kernel the 130 flop of the predictor run as TF32 MMAs, "
+                          "so fp32_frac is an FP32-equivalent rate and can exceed 1"},
     "student_t_mala": {"flop": 263.0, "mufu": 1.0,
                        "what": "forward 133 flop + adjoint of 65 parameters 130 flop (MALA)"},
 }
@@ -701,11 +751,16 @@ def configs_measure(configs, obs_shift=0, n_warm=2, n_timed=6, logp_points=16):
             mode, jitter, step = _native.MODE_DE, 0.01, 1e-4
             centre = np.concatenate([w.truth["beta"], [math.log(1.5)]])
             gamma = 2.38 / math.sqrt(2 * npar)
-            method = "de (chain-lane value body gm_iter_value)"
+            method = "de"
         init = centre + rng.normal(0.0, jitter, (C, npar))
         sd = np.full((C, npar), step)
         sess = _native.Session(m.loglik.code, m.loglik.consts, m.prior.code, m.prior.consts,
                                npar, w.data, m.n_cols, N)
+        tc = mode != _native.MODE_MALA and sess.tensor_cores
+        if mode != _native.MODE_MALA:
+            method += (" (tensor-core value kernel gm_iter_value_tc: the linear predictor as "
+                       "TF32 MMAs, the rest of the term on the FP32 pipes)" if tc
+                       else " (value kernel gm_iter_value)")
         try:
             if ladder:
                 sess.set_exchange(ladder, 10)
@@ -741,6 +796,7 @@ def configs_measure(configs, obs_shift=0, n_warm=2, n_timed=6, logp_points=16):
         out.append({
             "config": label, "n_chains": C, "n_obs": N, "n_params": npar, "method": method,
             "ms_per_iter": round(ms, 3), "chain_obs_per_s": rate,
+            "tensor_cores": tc,
             "fp32_frac": round(rate * wk["flop"] / fp32_peak, 4),
             "mufu_frac": round(rate * wk["mufu"] / mufu_peak, 4),
             "work_per_chain_obs": f"{wk['flop']:.0f} flop + {wk['mufu']:.0f} MUFU: {wk['what']}",

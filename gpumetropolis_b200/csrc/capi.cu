@@ -413,7 +413,7 @@ struct gpum_b200_session {
         k.fn = (const void*)cm.k_value_tc;
         k.lanes = false;
         k.G = kTcM;
-        k.threads = kTcThreads;
+        k.threads = cm.tc_threads;
       }
     } else {
       k.compiled = false;

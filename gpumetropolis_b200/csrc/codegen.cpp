@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -774,8 +775,16 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
       // Observations per tile and pipeline stages: the largest that fit
       // shared memory (stages of [hi | lo | tail] x TN, the coefficient
       // operand [hi | lo] x 128 chains, the reduction buffer).
+      // Epilogue warps: four per column part, each part a multiple of 16
+      // columns of the tile.
+      int EW = 16;
+      if (const char* e = std::getenv("GPUM_B200_TC_WARPS")) {
+        const int v = std::atoi(e);
+        if (v == 8 || v == 12 || v == 16) EW = v;
+      }
+      const int parts = EW / 4;
       int TN = 0, S = 0;
-      for (int tn : {256, 128, 64}) {
+      for (int tn = 256 / (16 * parts) * (16 * parts); tn >= 16 * parts && !TN; tn -= 16 * parts) {
         for (int st : {3, 2}) {
           if (tc_smem_bytes(KP, NT, tn, st) <= 231424) {
             TN = tn;
@@ -783,7 +792,6 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
             break;
           }
         }
-        if (TN) break;
       }
       if (TN == 0) tc_root = -1;
       if (tc_root >= 0) {
@@ -793,7 +801,9 @@ int generate_model(const uint32_t* code, size_t n_code, const double* consts,
         out->tc_ntail = NT;
         out->tc_tn = TN;
         out->tc_stages = S;
-        s << "#define GM_TC 1\n#define GM_TC_K " << K << "\n#define GM_TC_KP " << KP
+        out->tc_warps = EW;
+        s << "#define GM_TC 1\n#define GM_TC_EW " << EW << "\n#define GM_TC_K " << K
+          << "\n#define GM_TC_KP " << KP
           << "\n#define GM_TC_NTAIL " << NT << "\n#define GM_TC_NT1 " << std::max(NT, 1)
           << "\n#define GM_TC_TN " << TN << "\n#define GM_TC_STAGES " << S << "\n";
         // gm_tc_colvals / gm_tc_tailvals: one observation's product columns

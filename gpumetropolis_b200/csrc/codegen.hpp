@@ -31,17 +31,20 @@ struct GenModel {
   // Linear predictor on the tensor cores (gm_iter_value_tc): product
   // columns (data, materialized, and a ones column for the offset), padded
   // to a multiple of 8, tail data columns, observations per tile, stages.
+  // tc_warps: epilogue warps (8, 12 or 16; GPUM_B200_TC_WARPS, default 16),
+  // the kernel adds one control warp.
   bool tc = false;
-  int tc_k = 0, tc_kp = 0, tc_ntail = 0, tc_tn = 0, tc_stages = 0;
+  int tc_k = 0, tc_kp = 0, tc_ntail = 0, tc_tn = 0, tc_stages = 0, tc_warps = 8;
 };
 
 // Dynamic shared memory of the tensor-core value kernel: `stages` stages of
-// [hi | lo] product columns (kp, a multiple of 8) and nt tail columns for tn
-// observations, the coefficient operand [hi | lo] x 128 chains, the FP64
-// reduction buffer [4][128], per-chain flags [128] and the barriers.
+// [hi | lo] product columns (kp, a multiple of 8) for tn observations, four
+// slots of the nt tail columns, the coefficient operand [hi | lo] x 128
+// chains, the FP64 reduction buffer [4][128], per-chain flags [128] and the
+// barriers.
 inline size_t tc_smem_bytes(int kp, int nt, int tn, int stages) {
-  return (size_t)stages * (2 * kp + nt) * tn * 4 + (size_t)2 * kp * 128 * 4 + 4 * 128 * 8 +
-         128 * 4 + 512;
+  return (size_t)stages * 2 * kp * tn * 4 + (size_t)4 * nt * tn * 4 +
+         (size_t)2 * kp * 128 * 4 + 4 * 128 * 8 + 128 * 4 + 512;
 }
 
 // Builds the model functions for the log-likelihood program (f32 per

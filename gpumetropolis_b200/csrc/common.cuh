@@ -22,11 +22,9 @@ namespace gpum {
 constexpr int kWarps = 8;  // warps per CTA
 constexpr int kThreads = kWarps * 32;
 // The tensor-core value kernel (gm_iter_value_tc): 128 chains per CTA (the
-// MMA's M), eight epilogue warps (two per TMEM lane quarter) and a control
-// warp whose one thread issues the copies and the MMAs.
+// MMA's M); its epilogue warps (a multiple of four, GenModel::tc_warps) and
+// one control warp.
 constexpr int kTcM = 128;
-constexpr int kTcEpiWarps = 8;
-constexpr int kTcThreads = 32 * (kTcEpiWarps + 1);
 constexpr int kMaxStackF64 = 32;
 
 enum Phase : int { PH_EVAL = 0, PH_INIT = 1, PH_STEP = 2, PH_POINTWISE = 3 };

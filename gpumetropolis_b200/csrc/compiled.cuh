@@ -429,17 +429,20 @@ gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum
 // memory.  The rest of the per-observation expression (gm_tc_tail2) runs on
 // the FP32 pipes with eta read from tensor memory.
 //
-// Roles (kTcThreads = 288):
-//   warps 0..7   epilogue: warp w reads TMEM lane quarter w % 4 (chains
-//                32 (w % 4) .. + 31, one chain per lane) and column half
+// Roles (GM_TC_EW epilogue warps, a multiple of four, and a control warp):
+//   warps 0 .. EW-1  epilogue: warp w reads TMEM lane quarter w % 4 (chains
+//                32 (w % 4) .. + 31, one chain per lane) and column part
 //                w / 4 of each tile, evaluates the tail and sums its terms
-//   warp 8       control, one thread: the copies (one bulk copy per tile of
-//                the packed data, below, into a GM_TC_STAGES-deep ring) and
-//                the MMAs (3 KP/8 per tile into one of two accumulators of TN
-//                TMEM columns); the warp allocates the tensor memory
-// Barriers: full[s] (copy landed), empty[s] (the epilogue is done with the
-// stage; the MMAs were done with it before the epilogue started), accf[a]
-// (accumulator a holds a tile), acce[a] (the epilogue has read it).  Every
+//   warp EW      control, one thread: the copies (per tile of the packed
+//                data, below, one bulk copy of the product columns into a
+//                GM_TC_STAGES-deep operand ring and one of the tail columns
+//                into a ring of four slots) and the MMAs (3 KP/8 per tile
+//                into one of two accumulators of TN TMEM columns); the warp
+//                allocates the tensor memory
+// Barriers: bfull[s] / tfull[s] (copy landed), bempty[s] (the tile's MMAs
+// are done with the operand stage: a tcgen05.commit), tempty[s] (the
+// epilogue is done with the tail slot), accf[a] (accumulator a holds a tile),
+// acce[a] (the epilogue has read it).  Every
 // wait is bounded; one that runs out sets DEV_ERR_TC_TIMEOUT and a CTA-wide
 // abort flag, the roles leave their loops, the control thread waits (bounded)
 // for its MMAs and copies, and the CTA frees its tensor memory and finishes
@@ -451,15 +454,26 @@ gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum
 // (core matrix (k/4, o/8) at (k/4 * TN/8 + o/8) * 128 bytes), so one
 // contiguous copy fills a stage.
 namespace gpum {
+constexpr int kTcEpiWarps = GM_TC_EW;
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 1);
 constexpr int kTcTN = GM_TC_TN;
 constexpr int kTcKP = GM_TC_KP;
-constexpr int kTcS = GM_TC_STAGES;
-constexpr uint32_t kTcStageFloats = (uint32_t)(2 * kTcKP + GM_TC_NTAIL) * kTcTN;
+constexpr int kTcS = GM_TC_STAGES;  // operand stages (hi | lo product columns)
+constexpr int kTcST = 4;            // tail-column slots
+constexpr uint32_t kTcTileFloats = (uint32_t)(2 * kTcKP + GM_TC_NTAIL) * kTcTN;  // packed tile
+constexpr uint32_t kTcStageFloats = (uint32_t)2 * kTcKP * kTcTN;
+constexpr uint32_t kTcTailFloats = (uint32_t)GM_TC_NTAIL * kTcTN;
 constexpr uint32_t kTcAFloats = (uint32_t)2 * kTcKP * kTcM;
-constexpr uint32_t kTcTmemCols = 2 * kTcTN;
+// two accumulators, each at a power-of-two column offset (tcgen05.alloc
+// takes a power of two)
+constexpr uint32_t kTcAccCols = kTcTN <= 32 ? 32 : kTcTN <= 64 ? 64 : kTcTN <= 128 ? 128 : 256;
+constexpr uint32_t kTcTmemCols = 2 * kTcAccCols;
 constexpr int kTcParts = kTcEpiWarps / 4;  // epilogue warps per lane quarter
 constexpr int kTcColsPerWarp = kTcTN / kTcParts;
-static_assert(kTcKP % 8 == 0 && kTcTN % 64 == 0 && kTcTN <= 256 && kTcColsPerWarp % 32 == 0,
+// columns per TMEM load: 32 where the warp's share divides into them, else 16
+constexpr int kTcChunk = kTcColsPerWarp % 32 == 0 ? 32 : 16;
+static_assert(kTcKP % 8 == 0 && kTcTN % 16 == 0 && kTcTN <= 256 && kTcColsPerWarp % 16 == 0 &&
+                  kTcEpiWarps % 4 == 0 && kTcParts <= 4,  // the reduction buffer holds 4 parts
               "tensor-core tile shape");
 }  // namespace gpum
 
@@ -471,7 +485,7 @@ extern "C" __global__ void gm_tc_pack(const float* __restrict__ cols, long long 
   if (o >= n_tiles * kTcTN) return;
   const long long tile = o / kTcTN;
   const int r = (int)(o % kTcTN);
-  float* base = xt + (size_t)tile * kTcStageFloats;
+  float* base = xt + (size_t)tile * kTcTileFloats;
   const bool valid = o < n_obs;
   float v[GM_TC_K], t[GM_TC_NT1];
 #pragma unroll
@@ -508,8 +522,9 @@ extern "C" __global__ void gm_tc_pack(const float* __restrict__ cols, long long 
 }
 
 // eta of observation `col` of the tile on the FP32 pipe from the operands'
-// hi + lo: for a chain with an infinite coefficient, whose inf * 0 products
-// in the split form would be NaN where the plain product is +-inf.
+// hi + lo (the coefficients in shared memory, the tile's packed data in
+// global memory): for a chain with an infinite coefficient, whose inf * 0
+// products in the split form would be NaN where the plain product is +-inf.
 __device__ __noinline__ float gm_tc_eta_fp32(const float* __restrict__ As,
                                                 const float* __restrict__ xs, int cl, int col) {
   using namespace gpum;
@@ -541,12 +556,15 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
     ob = id / busy;
   }
   float* stg = reinterpret_cast<float*>(smem_raw);
-  float* As = stg + (size_t)kTcS * kTcStageFloats;
+  float* tls = stg + (size_t)kTcS * kTcStageFloats;            // tail slots
+  float* As = tls + (size_t)kTcST * kTcTailFloats;
   double* red = reinterpret_cast<double*>(As + kTcAFloats);  // [column parts][128]
   uint32_t* inf_chain = reinterpret_cast<uint32_t*>(red + 4 * kTcM);  // [128]
-  uint64_t* full = reinterpret_cast<uint64_t*>(inf_chain + kTcM);
-  uint64_t* empty = full + kTcS;
-  uint64_t* accf = empty + kTcS;
+  uint64_t* bfull = reinterpret_cast<uint64_t*>(inf_chain + kTcM);
+  uint64_t* bempty = bfull + kTcS;
+  uint64_t* tfull = bempty + kTcS;
+  uint64_t* tempty = tfull + kTcST;
+  uint64_t* accf = tempty + kTcST;
   uint64_t* acce = accf + 2;
   uint64_t* drain = acce + 2;
   uint32_t* misc = reinterpret_cast<uint32_t*>(drain + 1);  // TMEM base, ticket, abort
@@ -559,8 +577,12 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
 
   if (tid == 0) {
     for (int s = 0; s < kTcS; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kTcEpiWarps);
+      mbar_init(&bfull[s], 1);
+      mbar_init(&bempty[s], 1);
+    }
+    for (int s = 0; s < kTcST; ++s) {
+      mbar_init(&tfull[s], 1);
+      mbar_init(&tempty[s], kTcEpiWarps);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&accf[a], 1);
@@ -610,22 +632,30 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
   if (warp == kTcEpiWarps) {
     // ---- control: copies and MMAs
     if (lane == 0) {
-      constexpr uint32_t bytes = kTcStageFloats * 4;
       constexpr uint32_t idesc = umma_idesc_tf32(kTcM, kTcTN);
       constexpr uint32_t lbo_a = (kTcM / 8) * 128, lbo_b = (kTcTN / 8) * 128;
       const uint32_t a_hi = smem_addr(As), a_lo = a_hi + (uint32_t)kTcKP * kTcM * 4;
-      auto load = [&](int k) {
+      auto load_b = [&](int k) {
         const int s = k % kTcS;
-        mbar_expect_tx(&full[s], bytes);
-        bulk_load(stg + (size_t)s * kTcStageFloats, xt + (size_t)(t0 + k) * kTcStageFloats,
-                  bytes, &full[s]);
+        mbar_expect_tx(&bfull[s], kTcStageFloats * 4);
+        bulk_load(stg + (size_t)s * kTcStageFloats, xt + (size_t)(t0 + k) * kTcTileFloats,
+                  kTcStageFloats * 4, &bfull[s]);
       };
-      int issued = 0;
-      for (; issued < kTcS && issued < nt; ++issued) load(issued);
+      auto load_t = [&](int k) {
+        const int s = k % kTcST;
+        mbar_expect_tx(&tfull[s], kTcTailFloats * 4);
+        bulk_load(tls + (size_t)s * kTcTailFloats,
+                  xt + (size_t)(t0 + k) * kTcTileFloats + kTcStageFloats, kTcTailFloats * 4,
+                  &tfull[s]);
+      };
+      int nb = 0, ntl = 0;  // tiles whose operands / tail columns were issued
+      for (; nb < kTcS && nb < nt; ++nb) load_b(nb);
+      if (GM_TC_NTAIL > 0)
+        for (; ntl < kTcST && ntl < nt; ++ntl) load_t(ntl);
       for (int k = 0; k < nt; ++k) {
         if (*abort_flag) break;
         const int s = k % kTcS, acc = k & 1;
-        if (!mbar_wait_bounded(&full[s], (uint32_t)((k / kTcS) & 1))) {
+        if (!mbar_wait_bounded(&bfull[s], (uint32_t)((k / kTcS) & 1))) {
           give_up();
           break;
         }
@@ -636,7 +666,7 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
         tc_fence_after();
         const uint32_t b_hi = smem_addr(stg + (size_t)s * kTcStageFloats);
         const uint32_t b_lo = b_hi + (uint32_t)kTcKP * kTcTN * 4;
-        const uint32_t d = tmem + (uint32_t)(acc * kTcTN);
+        const uint32_t d = tmem + (uint32_t)acc * kTcAccCols;
         // the small products first: the accumulator rounds toward zero, so
         // only the KP/8 head products are added onto a large partial sum
 #pragma unroll
@@ -653,21 +683,35 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
           umma_tf32(d, umma_smem_desc(a_hi + 2 * kk * lbo_a, lbo_a, 128),
                     umma_smem_desc(b_hi + 2 * kk * lbo_b, lbo_b, 128), idesc, 1u);
         umma_commit(&accf[acc]);
-        // refill the stage of tile k - 1 once its epilogue is done with it
-        if (k >= 1 && issued < nt && issued == k - 1 + kTcS) {
-          if (!mbar_wait_bounded(&empty[(k - 1) % kTcS], (uint32_t)(((k - 1) / kTcS) & 1))) {
-            give_up();
-            break;
+        umma_commit(&bempty[s]);
+        if (k >= 1) {
+          // the operand stage of tile k - 1 is free once its MMAs are done
+          if (nb < nt) {
+            if (!mbar_wait_bounded(&bempty[(k - 1) % kTcS], (uint32_t)(((k - 1) / kTcS) & 1))) {
+              give_up();
+              break;
+            }
+            load_b(nb++);
           }
-          load(issued++);
+          // the tail slot of tile k - 1 once its epilogue is done (the next
+          // tile's MMAs wait for that epilogue anyway)
+          if (GM_TC_NTAIL > 0 && ntl < nt) {
+            if (!mbar_wait_bounded(&tempty[(k - 1) % kTcST], (uint32_t)(((k - 1) / kTcST) & 1))) {
+              give_up();
+              break;
+            }
+            load_t(ntl++);
+          }
         }
       }
       // every MMA has finished before the tensor memory is released, and no
       // copy is still writing into shared memory
       umma_commit(drain);
       if (!mbar_wait_bounded(drain, 0u)) give_up();
-      for (int i = max(0, issued - kTcS); i < issued; ++i)
-        if (!mbar_wait_bounded(&full[i % kTcS], (uint32_t)((i / kTcS) & 1))) give_up();
+      for (int i = max(0, nb - kTcS); i < nb; ++i)
+        if (!mbar_wait_bounded(&bfull[i % kTcS], (uint32_t)((i / kTcS) & 1))) give_up();
+      for (int i = max(0, ntl - kTcST); i < ntl; ++i)
+        if (!mbar_wait_bounded(&tfull[i % kTcST], (uint32_t)((i / kTcST) & 1))) give_up();
     }
   } else {
     // ---- epilogue
@@ -690,53 +734,56 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
     double sum = 0.0;
     for (int k = 0; k < nt; ++k) {
       if (*abort_flag) break;
-      const int s = k % kTcS, acc = k & 1;
-      // warp-uniform waits: the accumulator, and the stage's copy (already
-      // complete; waited on so its tail columns are visible to this thread)
+      const int st = k % kTcST, acc = k & 1;
+      // warp-uniform waits: the accumulator and the tile's tail columns
       bool ok = mbar_wait_bounded(&accf[acc], (uint32_t)((k >> 1) & 1)) &&
-                mbar_wait_bounded(&full[s], (uint32_t)((k / kTcS) & 1));
+                (GM_TC_NTAIL == 0 || mbar_wait_bounded(&tfull[st], (uint32_t)((k / kTcST) & 1)));
       ok = __all_sync(0xffffffffu, ok);
       if (!ok) {
         if (lane == 0) give_up();
         break;
       }
       tc_fence_after();
-      const float* xs = stg + (size_t)s * kTcStageFloats;
-      const float* tail = xs + (size_t)2 * kTcKP * kTcTN;
+      const float* xg = xt + (size_t)(t0 + k) * kTcTileFloats;  // the packed tile
+      const float* tail = tls + (size_t)st * kTcTailFloats;
       const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
-                             (uint32_t)(acc * kTcTN + part * kTcColsPerWarp);
+                             (uint32_t)acc * kTcAccCols + (uint32_t)(part * kTcColsPerWarp);
       const long long obs0 = (long long)(t0 + k) * kTcTN + part * kTcColsPerWarp;
       float2 tsum = make_float2(0.0f, 0.0f);
 #pragma unroll 1
-      for (int ch = 0; ch < kTcColsPerWarp / 32; ++ch) {
-        float v[32];
-        tmem_ld32(taddr + (uint32_t)(ch * 32), v);
-        const int col0 = part * kTcColsPerWarp + ch * 32;
+      for (int ch = 0; ch < kTcColsPerWarp / kTcChunk; ++ch) {
+        float v[kTcChunk];
+        tmem_ld(taddr + (uint32_t)(ch * kTcChunk), v);
+        const int col0 = part * kTcColsPerWarp + ch * kTcChunk;
         if (warp_inf) {  // a chain of this warp has an infinite coefficient
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (inf) v[j] = gm_tc_eta_fp32(As, xs, cl, col0 + j);
+          for (int j = 0; j < kTcChunk; ++j)
+            if (inf) v[j] = gm_tc_eta_fp32(As, xg, cl, col0 + j);
         }
-        float2 val[16];
+        float2 val[kTcChunk / 2];
+        float4 tq[GM_TC_NT1];  // the tail columns of two pairs (a 16-byte broadcast load)
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < kTcChunk / 2; ++j) {
           float2 t[GM_TC_NT1];
 #pragma unroll
-          for (int m = 0; m < GM_TC_NTAIL; ++m)
-            t[m] = *reinterpret_cast<const float2*>(tail + m * kTcTN + col0 + 2 * j);
+          for (int m = 0; m < GM_TC_NTAIL; ++m) {
+            if ((j & 1) == 0)
+              tq[m] = *reinterpret_cast<const float4*>(tail + m * kTcTN + col0 + 2 * j);
+            t[m] = (j & 1) ? make_float2(tq[m].z, tq[m].w) : make_float2(tq[m].x, tq[m].y);
+          }
           val[j] = gm_tc_tail2(make_float2(v[2 * j], v[2 * j + 1]), t, pp, hh);
         }
-        const long long o0 = obs0 + ch * 32;
-        if (o0 + 32 > (long long)E.n_obs) {  // the ragged end of the last tile
+        const long long o0 = obs0 + ch * kTcChunk;
+        if (o0 + kTcChunk > (long long)E.n_obs) {  // the ragged end of the last tile
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
+          for (int j = 0; j < kTcChunk / 2; ++j) {
             if (o0 + 2 * j >= E.n_obs) val[j].x = 0.0f;
             if (o0 + 2 * j + 1 >= E.n_obs) val[j].y = 0.0f;
           }
         }
         // pairwise: the FP32 error of a chunk grows with log2 of its terms
 #pragma unroll
-        for (int w = 8; w > 0; w >>= 1) {
+        for (int w = kTcChunk / 4; w > 0; w >>= 1) {
 #pragma unroll
           for (int j = 0; j < w; ++j) val[j] = __fadd2_rn(val[j], val[j + w]);
         }
@@ -747,7 +794,7 @@ gm_iter_value_tc(const float* __restrict__ xt, gpum::EvalArgs E, gpum::ChainArgs
       __syncwarp();
       if (lane == 0) {
         mbar_arrive(&acce[acc]);
-        mbar_arrive(&empty[s]);
+        if (GM_TC_NTAIL > 0) mbar_arrive(&tempty[st]);
       }
     }
     red[part * kTcM + cl] = sum;

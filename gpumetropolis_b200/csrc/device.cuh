@@ -217,6 +217,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[16]) { tmem_ld16(taddr, v); }
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[32]) { tmem_ld32(taddr, v); }
+
 // x rounded to the nearest tf32 value (ties away from zero), in an f32
 // container: the tensor core reads tf32 operands from the top 19 bits.
 __device__ __forceinline__ float tf32_rna(float x) {

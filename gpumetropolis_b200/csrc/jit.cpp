@@ -277,6 +277,7 @@ int jit_compile(const GenModel& gm, CompiledModel* out, std::string* err) {
   e.model.tc_ntail = gm.tc_ntail;
   e.model.tc_tn = gm.tc_tn;
   e.model.tc_stages = gm.tc_stages;
+  e.model.tc_threads = 32 * (gm.tc_warps + 1);
   e.model.G = G;
   e.model.GG = GG;
   e.model.pair = pair;

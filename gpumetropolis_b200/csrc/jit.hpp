@@ -29,7 +29,7 @@ struct CompiledModel {
   bool tc = false;
   cudaKernel_t k_value_tc = nullptr;
   cudaKernel_t k_tc_pack = nullptr;
-  int tc_kp = 0, tc_ntail = 0, tc_tn = 0, tc_stages = 0;
+  int tc_kp = 0, tc_ntail = 0, tc_tn = 0, tc_stages = 0, tc_threads = 0;
 };
 
 // Chains per thread for the value and gradient kernels, and whether the
