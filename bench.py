@@ -92,6 +92,10 @@ def _args():
     p.add_argument("--no-pt-da", action="store_true",
                    help="leave the mixture PT + delayed-acceptance leg out of the line")
     p.add_argument("--da-warmup", type=int, default=1000)
+    p.add_argument("--da-step-scale", type=float, default=None,
+                   help="two-stage proposal scale (default: the library's)")
+    p.add_argument("--da-train-steps", type=int, default=None,
+                   help="surrogate steps per learning-rate stage (default: the library's)")
     p.add_argument("--da-iters", type=int, default=5000,
                    help="sampling iterations of each delayed-acceptance leg (the logistic "
                         "configuration's 5,000)")
@@ -301,7 +305,7 @@ def logp_check(sess, w, n=32):
     return float(np.max(np.abs(cur[:n] - ref) / np.abs(ref)))
 
 
-def da_measure(w, C, n_warm, n_samp, seed=11):
+def da_measure(w, C, n_warm, n_samp, seed=11, step_scale=None, train_steps=None):
     """Exact MH vs surrogate delayed acceptance, ESS per second of sampling.
 
     Runs through the production driver (gpumetropolis_b200.api._Backend): the
@@ -313,6 +317,10 @@ def da_measure(w, C, n_warm, n_samp, seed=11):
     m = w.model
     npar = m.n_params
     cfg = dict(api.SURROGATE_DEFAULTS)
+    if step_scale:
+        cfg["step_scale"] = float(step_scale)
+    if train_steps:
+        cfg["steps"] = int(train_steps)
     call = api._Backend(m, w.data, w.n_obs, _native.RNG_PHILOX, cfg)
     try:
         call.record_at = n_warm // 2
@@ -602,7 +610,8 @@ def run_b200(a):
 
     da = None
     if rank == 0 and world == 1 and not a.no_da:
-        da = da_measure(w, C, a.da_warmup, a.da_iters)
+        da = da_measure(w, C, a.da_warmup, a.da_iters, step_scale=a.da_step_scale,
+                        train_steps=a.da_train_steps)
 
     configs = None
     if rank == 0 and world == 1 and not a.no_configs:
