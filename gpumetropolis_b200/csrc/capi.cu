@@ -320,7 +320,17 @@ struct gpum_b200_session {
       return false;
     }
     if (cm.n_mat > 0 && ncols > 0 && n_obs > 0) materialize();
-    if (cm.tc && n_obs > 0 && tensor_cores_enabled()) pack_tc();
+    if (cm.tc && n_obs > 0 && tensor_cores_enabled()) {
+      // Without room for the packed copy the session keeps the FP32 kernel.
+      try {
+        pack_tc();
+      } catch (const Failure& f) {
+        if (f.code != GPUM_ERR_NOMEM) throw;
+        cudaGetLastError();  // an allocation failure is not sticky
+        tc_data.release();
+        tc_ok = false;
+      }
+    }
     cm_ready = true;
     return true;
   }

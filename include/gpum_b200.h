@@ -208,8 +208,10 @@ GPUM_API int gpum_b200_session_engine(gpum_b200_session* s);
  * with parameter-only coefficients, at least 6 data columns) as a TF32
  * tensor-core product with a three-term split, the rest of each term on the
  * FP32 pipes.  0 otherwise: no such predictor, a non-finite value in one of
- * its data columns, the interpreter engine, or GPUM_B200_TENSOR_CORES=0 in
- * the environment at the session's first compiled evaluation.  Pointwise
+ * its data columns, no device memory for its packed copy of those columns
+ * (8 bytes per column per observation), the interpreter engine, or
+ * GPUM_B200_TENSOR_CORES=0 in the environment at the session's first
+ * compiled evaluation.  Pointwise
  * output and gradients keep the FP32 kernels.  No counterpart in the
  * reference (src/rust/src/chain_kernel.rs:305-321 evaluates the bytecode
  * per chain and observation). */
