@@ -631,8 +631,11 @@ def run_b200(a):
         "warmup": Wm, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "logistic regression: N=2^20 obs, 16 N(0,1) covariates + "
-                               "intercept, 17 params, 1024 chains, exact RWM, FP32 bytecode, "
-                               "f64 sums/totals/accept",
+                               "intercept, 17 params, 1024 chains, exact RWM, "
+                               + ("linear predictor as split-TF32 tensor-core products, the "
+                                  "rest of each term FP32" if tensor_cores
+                                  else "FP32 bytecode")
+                               + ", f64 sums/totals/accept",
                    "n_obs": N, "n_chains": C, "n_params": m.n_params,
                    "bytecode_instructions": m.loglik.n_instr,
                    "l2": "flushed (256 MiB write) before every timed step",

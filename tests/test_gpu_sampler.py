@@ -50,8 +50,9 @@ def _normals(seed, c, n, start=0):
 @pytest.mark.parametrize("name,n_obs,C,step", [("logistic", 4096, 512, 0.01),
                                                 ("student_t", 1031, 300, 0.006)])
 def test_single_step_decisions_match(gpu, name, n_obs, C, step):
-    # student_t (65 parameters) runs the chain-lane value body: 300 chains are
-    # two ragged blocks of 256 chains
+    # both models run the tensor-core value kernel (their linear predictors
+    # as TF32 products): 512 and 300 chains are 4 and 3 (ragged) blocks of
+    # 128 chains
     w = W.make(name, n_obs=n_obs)
     m = w.model
     seed = 11

@@ -142,20 +142,24 @@ def test_nonfinite_data_column_keeps_the_fp32_kernel(gpu):
         assert (np.abs(got[fin] - ref[fin]) / np.abs(ref[fin])).max() <= REL_SUM
 
 
-def test_sampler_steps_on_tensor_cores_follow_the_fp32_kernel(gpu):
-    # the same RWM run (triple32 stream) with and without the tensor-core
-    # kernel: identical accept decisions away from ties, log posteriors equal
-    # to 1e-6
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["rwm", "de", "cholesky"])
+def test_sampler_steps_on_tensor_cores_follow_the_fp32_kernel(gpu, mode):
+    # the same run (triple32 stream) with and without the tensor-core kernel:
+    # identical accept rates for nearly every chain (a decision inside the
+    # FP32 rounding of the data sum may differ), and then log posteriors
+    # equal to 1e-6
     w = W.make("logistic", n_obs=3001)
     m = w.model
-    C = 160
+    C, npar = 160, m.n_params
     init = _points(w, C, seed=6, scale=0.02)
-    sd = np.full((C, m.n_params), 0.01)
+    sd = np.full((C, npar), 0.01)
+    gamma = 2.38 / np.sqrt(2 * npar) if mode == 1 else 0.0
+    L = np.tile(np.eye(npar) * 0.01, (C, 1, 1)) if mode == 2 else None
     out = []
     for tc in (True, False):
         with _session(gpu, m, w.data, w.n_obs, tensor_cores=tc) as s:
             assert s.tensor_cores == tc
-            out.append(s.run(init, sd, np.ones(C), 60, 7, 0))
+            out.append(s.run(init, sd, np.ones(C), 60, 7, mode, gamma, 1e-4, proposal_l=L))
     (_, a1, l1), (_, a0, l0) = out
     same = a1 == a0
     assert same.mean() >= 0.95
