@@ -164,3 +164,36 @@ def test_sampler_steps_on_tensor_cores_follow_the_fp32_kernel(gpu, mode):
     same = a1 == a0
     assert same.mean() >= 0.95
     assert (np.abs(l1[same] - l0[same]) / np.abs(l0[same])).max() <= REL_SUM
+
+
+@pytest.mark.parametrize("formula,params,data,uses", [
+    # five data columns: below the predictor's minimum of six
+    ("~ -((y - (a + b1 * x1 + b2 * x2 + b3 * x3 + b4 * x4))^2) / 2",
+     ["a", "b1", "b2", "b3", "b4"], ["x1", "x2", "x3", "x4", "y"], False),
+    # a per-observation product inside the predictor is also read outside it
+    ("~ -((y - (b1 * x1 + b2 * x2 + b3 * x3 + b4 * x4 + b5 * x5 + b6 * x6))^2) / 2"
+     " - (b1 * x1)^2", ["b1", "b2", "b3", "b4", "b5", "b6"],
+     ["x1", "x2", "x3", "x4", "x5", "x6", "y"], False),
+    # no affine predictor at all
+    ("~ -((y - mu)^2) / (2 * exp(2 * ls)) - ls", ["mu", "ls"], ["y"], False),
+    # six columns: eligible
+    ("~ -((y - (b1 * x1 + b2 * x2 + b3 * x3 + b4 * x4 + b5 * x5))^2) / 2",
+     ["b1", "b2", "b3", "b4", "b5"], ["x1", "x2", "x3", "x4", "x5", "y"], True),
+])
+def test_which_models_run_on_tensor_cores(gpu, formula, params, data, uses):
+    # eligibility of the linear predictor, and the value either way against
+    # the oracle
+    m = gpum_model(formula, params, data)
+    rng = np.random.default_rng(9)
+    n = 1500
+    d = rng.normal(0, 1, (n, len(data)))
+    pts = rng.normal(0, 0.3, (9, len(params)))
+    ref = _oracle(m, d, n, pts)
+    with _session(gpu, m, d, n) as s:
+        assert s.tensor_cores == uses
+        got = s.loglik_batch(pts)
+        # pointwise output keeps the FP32 kernel in every case
+        pw = s.loglik_pointwise(pts[:2])
+    assert (np.abs(got - ref) / np.abs(ref)).max() <= REL_SUM
+    pref = O.loglik_pointwise(m.loglik.code, m.loglik.consts, m.n_params, d, m.n_cols, n, pts[:2])
+    np.testing.assert_allclose(pw, pref, rtol=2e-5, atol=2e-5)
