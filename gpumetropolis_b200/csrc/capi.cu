@@ -681,7 +681,10 @@ gpum_b200_session* create_session(const uint32_t* code, size_t n_code, const dou
     // padded to 4 floats so every TMA row stride is a multiple of 16 bytes.
     s->ld = (int64_t)((n_obs + 3) & ~3ull);
     s->data.ensure((size_t)s->ld * n_cols);
-    const int64_t rows_per_chunk = std::max<int64_t>(1, (int64_t)(32u << 20) / n_cols);
+    // f64 rows through a 16 MB staging buffer (2M values per chunk; the
+    // copy of a chunk follows the conversion of the previous one on the
+    // stream), so a session does not allocate a second full copy.
+    const int64_t rows_per_chunk = std::max<int64_t>(1, (int64_t)(2u << 20) / n_cols);
     DBuf<double> stage;
     stage.ensure((size_t)std::min<int64_t>(rows_per_chunk, (int64_t)n_obs) * n_cols);
     for (int64_t r0 = 0; r0 < (int64_t)n_obs; r0 += rows_per_chunk) {
