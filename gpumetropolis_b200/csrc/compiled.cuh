@@ -424,9 +424,9 @@ gm_iter_grad(const __grid_constant__ gpum::TmapDesc tmap, gpum::EvalArgs E, gpum
 // observations, the product A (128 x K, coefficients) . B^T (TN x K, data).
 // It runs on the 5th-generation tensor cores in TF32 with both operands split
 // into a TF32 head and a TF32 rounding of the remainder, v = hi + lo:
-// a.x ~ a_hi.x_hi + a_hi.x_lo + a_lo.x_hi, the dropped a_lo.x_lo and the
-// truncation of lo below 2^-21 relative to |a x|, FP32 accumulation in tensor
-// memory.  The rest of the per-observation expression (gm_tc_tail2) runs on
+// a.x ~ a_hi.x_hi + a_hi.x_lo + a_lo.x_hi, within 2^-20 of |a x| (2^-21 on
+// average: the dropped a_lo.x_lo and the rounding of the lo parts), FP32
+// accumulation in tensor memory.  The rest of the per-observation expression (gm_tc_tail2) runs on
 // the FP32 pipes with eta read from tensor memory.
 //
 // Roles (GM_TC_EW epilogue warps, a multiple of four, and a control warp):
