@@ -128,6 +128,11 @@ def _args():
     return p.parse_args()
 
 
+def _pow2(n):
+    """n as 2^k when it is a power of two (the configurations' sizes)."""
+    return f"2^{n.bit_length() - 1}" if n > 0 and n & (n - 1) == 0 else str(n)
+
+
 def _workload(n_obs):
     from gpumetropolis_b200 import workloads as W
     return W.make("logistic", n_obs=n_obs)
@@ -632,7 +637,7 @@ def run_b200(a):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": Wm, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "logistic regression: N=2^20 obs, 16 N(0,1) covariates + "
+        "config": {"workload": f"logistic regression: N={_pow2(N)} obs, 16 N(0,1) covariates + "
                                "intercept, 17 params, 1024 chains, exact RWM, "
                                + ("linear predictor as split-TF32 tensor-core products, the "
                                   "rest of each term FP32" if tensor_cores
@@ -692,7 +697,7 @@ def run_reference(a):
         "steps": K, "warmup": Wm, "ms_per_step": 1e3 * sum(times) / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "logistic regression: N=2^20 obs, 17 params; bounded chain "
+        "config": {"workload": f"logistic regression: N={_pow2(w.n_obs)} obs, 17 params; bounded chain "
                                "sample per step", "n_obs": w.n_obs,
                    "n_chains_per_step": C},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
